@@ -1,0 +1,313 @@
+"""Benchmark of the LS-SPH engine: particle-updates/s per RK step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Workload (one "step" = one full time step of the hot path: RK4 stages, ghosts, PST):
+Taylor-Green vortex, Re = 100, 128^2 fluid particles (+1,572 ghost particles), RK4 with
+particle shifting, CFL 0.1, FP64 -- the reference's problem 2 in its free-slip box with
+TG_A = TG_B = 2 (synthetic initial state generated by the setup code; no dataset).
+
+value  : interior particles x K / device time of the K timed steps (CUDA events on the
+         engine's stream; an L2 flush -- a 256 MB write -- separates consecutive steps).
+         With N > 1 each rank runs an independent replica; value is the sum over ranks
+         computed from the max over ranks of the device time (weak scaling).
+e2e    : the same metric through the C ABI with host buffers: every step uploads the
+         particle state from pinned host memory, steps, and downloads it again.
+reference arm: the CPU restatement of the reference (oracle/) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ls-sph-benchmarks_b200"))
+
+METRIC = "particle-updates/s per RK step"
+UNIT = "particle-updates/s"
+WORKLOAD = "taylor_green_re100_128x128_rk4_pst_fp64"
+
+
+def _params(lanes: int = 0):
+    import lssph
+    return lssph.taylor_green_params(num=128, re=100.0, coe_cfl=0.1, tg=2, lanes=lanes)
+
+
+def _config(p, extra=None):
+    cfg = {"workload": WORKLOAD, "problem": "taylor_green", "num_x": p.num_x, "num_y": p.num_y,
+           "num_int": None, "num_total": None, "rk": p.rk, "pst": True, "re": 1.0 / p.vis_ref,
+           "dt": p.dt, "precision": "fp64", "l2": "flushed between timed steps (256 MB write)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+_REASONS = ["gpu_idle", "applications_clocks_setting", "sw_power_cap", "hw_slowdown", "sync_boost",
+            "sw_thermal_slowdown", "hw_thermal_slowdown", "hw_power_brake_slowdown"]
+
+
+class ClockSampler:
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for line in self.lines:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 4:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+                bits = int(parts[3], 16) if parts[3].startswith("0x") else int(parts[3])
+            except ValueError:
+                continue
+            for i, name in enumerate(_REASONS):
+                if bits & (1 << i) and name != "gpu_idle":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _profile_traffic():
+    """DRAM bytes per k_stage launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "k_stage_taylor_green_128.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def _measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(min_seconds: float = 10.0, max_steps: int = 2000) -> dict:
+    """The oracle on all host cores for a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = O.set_threads(os.cpu_count() or 1)
+    p = _params()
+    orc = O.Oracle(p)
+    orc.run(2)                       # warm-up
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps:
+        orc.run(5)
+        steps += 5
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": orc.num_int * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} time steps of the same workload ({dt:.1f} s, oracle/ C++ restatement, "
+                      f"OpenMP over {cores} threads)", "num_int": orc.num_int}
+
+
+def run_reference(args) -> int:
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = O.set_threads(os.cpu_count() or 1)
+    p = _params()
+    orc = O.Oracle(p)
+    orc.run(args.warmup)
+    t0 = time.perf_counter()
+    orc.run(args.steps)
+    dt = time.perf_counter() - t0
+    value = orc.num_int * args.steps / dt
+    cfg = _config(p, {"num_int": orc.num_int, "num_total": orc.num_total, "parallelism": "cpu",
+                      "l2": "n/a (host CPU)"})
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} time steps after {args.warmup} warm-up steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_engine(args) -> int:
+    import numpy as np
+    import torch
+
+    import lssph
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    p = _params(lanes=args.lanes)
+    st, ni = lssph.setup_particles(p)
+    sim = lssph.Simulation(p, st, ni)
+    sim.ghost()
+    n_total = sim.num_total
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    # mean in-radius neighbour count P (the per-pair work unit of the roofline)
+    off, _ = sim.neighbors(0)
+    mean_p = float(off[-1]) / ni
+
+    sim.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    dev_ms, launches = 0.0, 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            sim.step(1)
+            ms, nl = sim.last_step_stats()
+            dev_ms += ms
+            launches += nl
+    torch.cuda.synchronize()
+    if dist:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+        dist.barrier()
+    value = ws * ni * args.steps / (dev_ms * 1e-3)
+
+    # ---- per-kernel device times (same launch sequence, un-graphed, events per launch) ----
+    prof_steps = max(5, min(50, args.steps))
+    prof = sim.step_profiled(prof_steps)
+    stage_ms, stage_n = prof["stage"]
+    stage_avg_s = stage_ms * 1e-3 / max(stage_n, 1)
+    flops_per_launch = ni * (101.0 * mean_p + 315.0)           # LSSPH_A q = 5, nb = 4
+    bytes_per_launch = ni * 300.0                               # per particle-stage, FP64 SoA
+    hbm_peak, peak_src = _measured_peaks()
+    achieved_gbs = bytes_per_launch / stage_avg_s / 1e9
+    traffic = _profile_traffic()
+    roofline = {"bound": "hbm", "kernel": "k_stage<NB=4,G=4>", "achieved": achieved_gbs, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "fp64": {"achieved_tflops": flops_per_launch / stage_avg_s / 1e12,
+                         "flops_per_launch": flops_per_launch, "mean_neighbours": mean_p},
+                "launch_avg_us": stage_avg_s * 1e6,
+                "kernel_share": {k: v[0] for k, v in prof.items()}}
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e_steps = max(5, min(200, args.steps))
+    pinned = {k: torch.empty(n_total, dtype=torch.float64, pin_memory=True).numpy()
+              for k in ("x", "y", "u", "v", "rho", "pre")}
+    host = sim.download()
+    for k in pinned:
+        pinned[k][:] = getattr(host, k)
+    hst = lssph.State(host.ptype, *(pinned[k] for k in ("x", "y", "u", "v", "rho", "pre")))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.upload(hst)
+        sim.step(1)
+        sim.download_into(hst)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    nbytes = 6 * n_total * 8
+    e2e = {"value": ws * ni * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+           "d2h_bytes_per_step": nbytes, "steps": e2e_steps,
+           "path": "lssph_upload + lssph_step(1) + lssph_download per step, wall clock"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    cfg = _config(p, {"num_int": ni, "num_total": n_total, "parallelism": f"replicas{ws}",
+                      "lanes": args.lanes or 4, "global_batch": ni * ws})
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_engine(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

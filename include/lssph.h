@@ -1,0 +1,204 @@
+/*
+ * lssph.h -- C ABI of the B200 LS-SPH engine.
+ *
+ * The engine replaces the time-step loop of the LS-SPH-Benchmarks Fortran solver
+ * (source/main.f90:119-166): RK2/RK4 stages, LS-SPH type-A right-hand sides, cell-list
+ * neighbour search, multi-layer ghost walls and the particle shifting technique all run
+ * as sm_100a kernels on device-resident state.  Host code (the Fortran iso_c_binding
+ * shim, the C++ driver, the Python ctypes wrapper) keeps the reference's config.h
+ * parameter surface and its results/ file layout.
+ *
+ * Conventions
+ *   - Every function returns an int status: 0 = OK, negative = LSSPH_E_*.  A message
+ *     for the last failure is available from lssph_last_error() / lssph_handle_error().
+ *   - Particle indices are 0-based (the Fortran shim adds 1).  Particle order is the
+ *     reference order: interior (fluid) particles 0..num_int-1 in lattice scan order,
+ *     then ghost wall particles num_int..num_total-1 (setup_closed_box_mod.f90:120-136).
+ *   - All arrays are caller-owned host buffers, SoA, float64 unless noted.
+ *   - A handle owns its device state and one CUDA stream.  A handle is not thread-safe;
+ *     distinct handles are independent.
+ */
+#ifndef LSSPH_H
+#define LSSPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSSPH_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define LSSPH_OK                 0
+#define LSSPH_E_BAD_PARAM      (-1)  /* check_param_mod.f90 would `error stop` */
+#define LSSPH_E_CUDA           (-2)  /* a CUDA runtime call failed */
+#define LSSPH_E_CELL_OVERFLOW  (-3)  /* a cell holds more than its slot capacity */
+#define LSSPH_E_OUT_OF_DOMAIN  (-4)  /* a particle left the cell grid */
+#define LSSPH_E_NONFINITE      (-5)  /* a NaN/Inf appeared in the state */
+#define LSSPH_E_SINGULAR       (-6)  /* a zero pivot in a moment-matrix solve */
+#define LSSPH_E_IO             (-7)  /* file I/O failed */
+#define LSSPH_E_CAPACITY       (-8)  /* an output buffer is too small / batch full */
+#define LSSPH_E_TIMEOUT        (-9)  /* a bounded device wait gave up */
+#define LSSPH_E_UNSUPPORTED    (-10) /* option combination not implemented */
+
+/* ---- engine options (no counterpart in the reference) ----------------------------- */
+#define LSSPH_PRECISION_FP64   0     /* plain FP64 path (reference arithmetic) */
+#define LSSPH_PRECISION_MIXED  1     /* FP32 pair sums, FP64 solve + refinement */
+
+/*
+ * lssph_params -- mirrors Param_type (source/core/global_types.f90:22-73) plus the
+ * compile-time macros of config.h that Param_type does not store (boundary codes, RK
+ * order).  User fields come from config.h; derived fields are filled by
+ * lssph_init_param() exactly as init_param_mod.f90:92-199 derives them.
+ */
+typedef struct lssph_params {
+    /* ---- user-defined (config.h) ---- */
+    int32_t target_problem;                                     /* TARGET_PROBLEM 1..4 */
+    int32_t u_bc_top, u_bc_bottom, u_bc_left, u_bc_right;       /* U_BOUNDARY_*  1..3  */
+    int32_t tem_bc_top, tem_bc_bottom, tem_bc_left, tem_bc_right; /* TEM_BOUNDARY_* 1..2 */
+    double  u_top;
+    double  tem_top, tem_bottom, tem_left, tem_right;
+    char    save_name[256];
+    char    read_name[256];
+    int32_t omp_threads;
+    int32_t rk;                                                 /* RK 2 or 4 */
+    double  len_x, len_y;
+    int32_t num_x, num_y;
+    int32_t start_step, end_step, write_step;
+    int32_t pad0_;
+    double  threshold, coe_CFL, coe_dif, zeta_RSST, xi_VIM;
+    double  rho_ref, vis_ref, K_ref, k_th_ref, cp_ref, alpha_ref;
+    double  gravity, pos_pert;
+    int32_t tg_a, tg_b;
+    double  coe_h, PST_c, coe_delta_sph;
+    int32_t kernel_type, sph_model, wall_model;
+    /* ---- derived (init_param_mod.f90:92-199) ---- */
+    int32_t total_step, num_WL;
+    int32_t pad1_;
+    double  dx, SP_mass, h, h_eff, W_ave, WL_thick;
+    double  delta_tem, tem_ave;
+    double  sound_speed, kinematic_vis, thermal_dif;
+    double  Re, Ra, Pr;
+    double  dt, dt_CFL, dt_vis, dt_th, dt_CFL_relax, dt_vis_relax;
+    /* ---- engine options (no reference counterpart) ---- */
+    int32_t  precision;   /* LSSPH_PRECISION_* */
+    int32_t  lanes;       /* lanes per particle in neighbour loops: 0 = auto,
+                             1 = reference summation order (bit-exact vs the oracle) */
+    uint64_t seed;        /* POS_PERT jitter seed (the reference seeds from the clock,
+                             impose_initial_conditions_mod.f90:43-51) */
+} lssph_params;
+
+typedef struct lssph_handle lssph_handle;
+
+/* ---- library ------------------------------------------------------------------------ */
+int         lssph_abi_version(void);
+/* sizeof(lssph_params) as compiled into the library (FFI layout check). */
+size_t      lssph_params_sizeof(void);
+/* Last error message of the calling thread (for calls that have no handle). */
+const char* lssph_last_error(void);
+const char* lssph_status_string(int status);
+
+/* ---- parameters (host only) ---------------------------------------------------------- */
+/* Reference defaults: the values of the shipped config.h. */
+int lssph_params_default(lssph_params* out);
+/* Parse a config.h (`#define NAME value` lines), then lssph_init_param + lssph_check_param.
+   Replaces init_param (init_param_mod.f90:24) + check_param (check_param_mod.f90:22). */
+int lssph_params_from_config(const char* config_h_path, lssph_params* out);
+/* Fill the derived fields of *p from its user fields (init_param_mod.f90:92-199). */
+int lssph_init_param(lssph_params* p);
+/* Validate user fields (check_param_mod.f90:22-284).  LSSPH_E_BAD_PARAM + message. */
+int lssph_check_param(const lssph_params* p);
+
+/* ---- particle setup (host only) ------------------------------------------------------ */
+/* Particle counts of the closed box: num_total = (num_x+2 num_WL)(num_y+2 num_WL). */
+int lssph_setup_counts(const lssph_params* p, int32_t* num_total, int32_t* num_int);
+/* setup_closed_box (setup_closed_box_mod.f90:23-237) + impose_* initial conditions
+   (impose_initial_conditions_mod.f90).  tem may be NULL unless target_problem == 4. */
+int lssph_setup_particles(const lssph_params* p, int32_t num_total, int32_t* ptype,
+                          double* x, double* y, double* u, double* v, double* rho,
+                          double* pre, double* tem);
+
+/* ---- simulation handle ---------------------------------------------------------------- */
+/* Copy host state to the device and build the cell list (init_cell + update_cell,
+   init_cell_mod.f90:23, update_cell_mod.f90:21) and the virtual markers
+   (init_virtual_markers_mod.f90:23).  Ghost values are taken from the input; call
+   lssph_ghost() for a fresh start (write_param_mod.f90:144 does it there).  tem may be
+   NULL unless target_problem == 4.  Indices follow the reference order. */
+int lssph_create(const lssph_params* p, int32_t num_total, int32_t num_int,
+                 const int32_t* ptype, const double* x, const double* y, const double* u,
+                 const double* v, const double* rho, const double* pre, const double* tem,
+                 lssph_handle** out);
+void        lssph_destroy(lssph_handle* h);
+const char* lssph_handle_error(const lssph_handle* h);
+int lssph_get_params(const lssph_handle* h, lssph_params* out);
+int lssph_counts(const lssph_handle* h, int32_t* num_total, int32_t* num_int,
+                 int32_t* num_ext, int32_t* num_cells);
+
+/* One reference operator each (same names as the Fortran subroutines). */
+int lssph_calculate_rhs(lssph_handle* h);            /* calculate_RHS_mod.f90:29 */
+int lssph_update_cell(lssph_handle* h);              /* update_cell_mod.f90:21   */
+int lssph_ghost(lssph_handle* h);                    /* ghost_mod.f90:43         */
+int lssph_rk2(lssph_handle* h);                      /* RK2_mod.f90:30           */
+int lssph_rk4(lssph_handle* h);                      /* RK4_mod.f90:30           */
+int lssph_pst(lssph_handle* h);                      /* PST_mod.f90:28           */
+int lssph_check_steady_state(lssph_handle* h, int32_t* is_steady); /* check_steady_state_mod.f90:23 */
+
+/* The body of the time loop (main.f90:119-149) for nsteps steps, device-resident and
+   graph-replayed: RK2/RK4, PST (problems 2-4), steady check (problem 1).  Stops early at
+   a steady state; *steady_step_out (may be NULL) receives the 1-based step count within
+   this call at which it was reached, or 0. */
+int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out);
+
+/* Host <-> device state (caller buffers of length num_total; tem may be NULL). */
+int lssph_upload(lssph_handle* h, const double* x, const double* y, const double* u,
+                 const double* v, const double* rho, const double* pre, const double* tem);
+int lssph_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u,
+                   double* v, double* rho, double* pre, double* tem);
+/* RHS arrays of the last calculate_RHS (length num_int; rhs_tem may be NULL). */
+int lssph_download_rhs(lssph_handle* h, double* rhs_u, double* rhs_v, double* rhs_rho,
+                       double* rhs_tem);
+/* Virtual markers (length num_ext): VM.dat content (write_param_mod.f90:147-159). */
+int lssph_download_vm(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u,
+                      double* v, double* pre, double* tem);
+
+/* In-radius neighbour sets (r^2 <= h_eff^2 among the 3x3 cells) as sorted CSR, for parity
+   checks.  which = 0: interior particles over all particles (LSSPH_A_mod.f90:102-125);
+   which = 1: virtual markers over fluid particles (interpolate_LSSPH_B_mod.f90:158-180).
+   offsets has n+1 entries; *nnz_out receives the total. */
+int lssph_neighbors_csr(lssph_handle* h, int32_t which, int32_t* offsets, int32_t* idx,
+                        int64_t cap, int64_t* nnz_out);
+
+/* results/ layout read by analysis/common/read_utils.py. */
+int lssph_write_data(lssph_handle* h, const char* results_root, int32_t step);   /* write_data_mod.f90:22 */
+int lssph_write_param(lssph_handle* h, const char* results_root, const char* config_h_path); /* write_param_mod.f90:27 */
+/* parameters.csv alone (write_param_mod.f90:58-128), host only. */
+int lssph_write_parameters(const lssph_params* p, int32_t num_total, int32_t num_int,
+                           const char* path);
+/* Restart reader (restart_mod.f90:22-53): fills caller buffers of length num_total. */
+int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32_t* ptype,
+                    double* x, double* y, double* u, double* v, double* rho, double* pre,
+                    double* tem);
+
+/* Device time of the kernels launched by the last lssph_step call, in milliseconds
+   (CUDA events on the handle's stream), and the number of kernel launches it made. */
+int lssph_last_step_stats(const lssph_handle* h, double* device_ms, int64_t* kernel_launches);
+
+/* Kernel kinds of a time step, for lssph_step_profiled. */
+#define LSSPH_KIND_STAGE     0   /* RHS + RK stage update + cell scatter */
+#define LSSPH_KIND_CELLSORT  1   /* cell list finish (update_cell) */
+#define LSSPH_KIND_GHOST     2   /* virtual-marker interpolation + extrapolation */
+#define LSSPH_KIND_PST       3   /* particle shifting */
+#define LSSPH_KIND_OTHER     4   /* epilogue / reductions */
+#define LSSPH_KIND_COUNT     5
+/* The same launch sequence as lssph_step, issued without graph capture and with a
+   CUDA event pair around every kernel: ms_by_kind[k] receives the summed device time of
+   kind k, launches_by_kind[k] its launch count (arrays of LSSPH_KIND_COUNT). */
+int lssph_step_profiled(lssph_handle* h, int32_t nsteps, double* ms_by_kind,
+                        int64_t* launches_by_kind);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSSPH_H */

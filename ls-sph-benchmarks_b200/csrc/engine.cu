@@ -1,0 +1,775 @@
+// engine.cu -- device-resident LS-SPH solve: memory layout, launch sequences, graph
+// replay of the time loop, and the handle half of the C ABI (lssph.h).
+//
+// HBM layout of one solve (all SoA, FP64 unless noted):
+//   state      2 buffers x {x, y, u, v, rho, pre, tem, vol} over num_total (ping-pong:
+//              a stage reads one buffer and writes the other, so neighbour gathers never
+//              see half-updated particles); vol = SP_mass / rho is kept beside rho
+//   work       x/y/u/v/rho/tem _old and _acc (RK4 accumulators), RHS arrays, f_previous,
+//              the problem-1 source term, int32 cell key, over num_int
+//   cell list  2 buffers x {cnt, num, fnum} over ncell + slots[ncell * cap] (int32)
+//   markers    virtual-marker positions, normals, keys and interpolated values
+// A time step of problems 2-4 is 15 kernels (4 x {stage, cellsort, ghost} + {pst,
+// cellsort, ghost}); problem 1 is 5 (2 x {stage, ghost} + epilogue).  Each step is
+// captured once in a CUDA graph and replayed.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "kernels.cuh"
+
+using namespace lssph;
+
+struct lssph_handle {
+    lssph_params p{};
+    int num_total = 0, num_int = 0, num_ext = 0;
+    int problem = 0;
+    bool has_tem = false, p1 = false, pst_on = false;
+    int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
+    int G = 4, Gg = 4;
+    CellGrid grid;
+    VirtualMarkers vm;
+    std::vector<int32_t> ptype;
+    Phys P{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<void*> allocs;
+    Fld F[2]{};
+    Lst L[2]{};
+    Work W{};
+    VMd V{};
+    int* gstart = nullptr;
+    int* glist = nullptr;
+    Scalars* sc = nullptr;
+    int sb = 0, lb = 0;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int graph_launches = 0;   // kernels per captured step
+    int step_flip = 0;        // parity change per step
+    int64_t launch_counter = 0;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    // per-launch event pairs while profiling (lssph_step_profiled)
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_events;
+    std::vector<int> prof_kinds;
+    size_t prof_next = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(lssph_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    set_last_error(msg);
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                      \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail((h), LSSPH_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int dalloc(lssph_handle* h, T** ptr, size_t n) {
+    *ptr = nullptr;
+    if (n == 0) n = 1;
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    h->allocs.push_back(p);
+    *ptr = static_cast<T*>(p);
+    return LSSPH_OK;
+}
+
+inline int blocks_for(long n, int per_block) { return (int)((n + per_block - 1) / per_block); }
+
+// Event pair around one launch while profiling; no-op otherwise (and during capture).
+struct ProfScope {
+    lssph_handle* h;
+    size_t slot = (size_t)-1;
+    ProfScope(lssph_handle* hh, int kind) : h(hh) {
+        if (!h->profiling) return;
+        if (h->prof_next + 2 > h->prof_events.size()) {
+            for (int k = 0; k < 64; ++k) {
+                cudaEvent_t e;
+                if (cudaEventCreate(&e) != cudaSuccess) return;
+                h->prof_events.push_back(e);
+            }
+        }
+        slot = h->prof_next;
+        h->prof_next += 2;
+        h->prof_kinds.push_back(kind);
+        cudaEventRecord(h->prof_events[slot], h->stream);
+    }
+    ~ProfScope() {
+        if (slot != (size_t)-1) cudaEventRecord(h->prof_events[slot + 1], h->stream);
+    }
+};
+
+// ---- kernel dispatch on the lane count ---------------------------------------------------
+template <int NB>
+void launch_stage(lssph_handle* h, const StageCfg& S) {
+    ProfScope prof(h, LSSPH_KIND_STAGE);
+    const Fld& cur = h->F[h->sb];
+    const Fld& nxt = h->F[h->sb ^ 1];
+    const Lst& Lc = h->L[h->lb];
+    const Lst& Ln = h->L[h->lb ^ 1];
+    const int G = h->G;
+    const int grid = blocks_for((long)h->num_int * G, 128);
+    switch (G) {
+        case 1: k_stage<NB, 1><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
+        case 2: k_stage<NB, 2><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
+        case 8: k_stage<NB, 8><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
+        default: k_stage<NB, 4><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
+    }
+    h->launch_counter++;
+}
+
+void launch_stage_any(lssph_handle* h, const StageCfg& S) {
+    if (h->nb_rhs == 1) launch_stage<1>(h, S);
+    else if (h->nb_rhs == 5) launch_stage<5>(h, S);
+    else launch_stage<4>(h, S);
+}
+
+template <int NB, int WQ>
+void launch_ghost_t(lssph_handle* h) {
+    ProfScope prof(h, LSSPH_KIND_GHOST);
+    const Fld& F = h->F[h->sb];
+    const Lst& L = h->L[h->lb];
+    const int G = h->Gg;
+    const int grid = blocks_for((long)h->num_ext * G, 128);
+    switch (G) {
+        case 1: k_ghost<NB, 1, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
+        case 2: k_ghost<NB, 2, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
+        case 8: k_ghost<NB, 8, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
+        default: k_ghost<NB, 4, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
+    }
+    h->launch_counter++;
+}
+
+template <int NB>
+void launch_ghost_nb(lssph_handle* h) {
+    if (h->wq == 1) launch_ghost_t<NB, 1>(h);
+    else if (h->wq == 6) launch_ghost_t<NB, 6>(h);
+    else launch_ghost_t<NB, 3>(h);
+}
+
+void launch_ghost(lssph_handle* h) {
+    if (h->nb_ghost == 1) launch_ghost_nb<1>(h);
+    else if (h->nb_ghost == 4) launch_ghost_nb<4>(h);
+    else launch_ghost_nb<3>(h);
+}
+
+template <int NB>
+void launch_pst_t(lssph_handle* h) {
+    ProfScope prof(h, LSSPH_KIND_PST);
+    const Fld& cur = h->F[h->sb];
+    const Fld& nxt = h->F[h->sb ^ 1];
+    const Lst& Lc = h->L[h->lb];
+    const Lst& Ln = h->L[h->lb ^ 1];
+    const int G = h->G;
+    const int grid = blocks_for((long)h->num_int * G, 128);
+    switch (G) {
+        case 1: k_pst<NB, 1><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
+        case 2: k_pst<NB, 2><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
+        case 8: k_pst<NB, 8><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
+        default: k_pst<NB, 4><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
+    }
+    h->launch_counter++;
+}
+
+void launch_cellsort(lssph_handle* h, int list, int reset_umax) {
+    ProfScope prof(h, LSSPH_KIND_CELLSORT);
+    k_cellsort<<<blocks_for(h->grid.ncell, 128), 128, 0, h->stream>>>(h->P, h->L[list], h->gstart, h->glist, h->sc,
+                                                                          reset_umax);
+    h->launch_counter++;
+}
+
+// ---- operator sequences (enqueue only) -----------------------------------------------------
+// One RK stage: RHS + update (+ scatter), cell list finish, ghost.
+void enq_stage(lssph_handle* h, int stage, bool fused_step) {
+    StageCfg S{};
+    S.mode = MODE_STAGE;
+    S.stage = stage;
+    const double dt = h->p.dt;
+    if (h->p.rk == 2) {
+        S.last = stage == 2;
+        S.dt2 = (stage == 1) ? dt / 2.0 : dt;
+    } else {
+        S.last = stage == 4;
+        if (stage == 1) { S.dt1 = dt / 6.0; S.dt2 = dt / 2.0; }
+        else if (stage == 2) { S.dt1 = dt / 3.0; S.dt2 = dt / 2.0; }
+        else if (stage == 3) { S.dt1 = dt / 3.0; S.dt2 = dt; }
+        else { S.dt1 = dt / 6.0; S.dt2 = 0.0; }
+    }
+    S.do_scatter = h->p1 ? 0 : 1;
+    S.do_umax = (fused_step && h->pst_on) ? 1 : 0;
+    S.do_steady = (fused_step && h->p1) ? 1 : 0;
+    S.write_rhs = 1;
+    launch_stage_any(h, S);
+    h->sb ^= 1;
+    if (!h->p1) {
+        launch_cellsort(h, h->lb ^ 1, 0);
+        h->lb ^= 1;
+    }
+    launch_ghost(h);
+}
+
+void enq_pst(lssph_handle* h) {
+    if (h->has_tem) launch_pst_t<4>(h);
+    else launch_pst_t<3>(h);
+    h->sb ^= 1;
+    launch_cellsort(h, h->lb ^ 1, 1);
+    h->lb ^= 1;
+    launch_ghost(h);
+}
+
+void enq_step(lssph_handle* h) {
+    const int ns = h->p.rk == 2 ? 2 : 4;
+    for (int s = 1; s <= ns; ++s) enq_stage(h, s, true);
+    if (h->pst_on) enq_pst(h);
+    if (h->p1) {
+        ProfScope prof(h, LSSPH_KIND_OTHER);
+        k_epilogue<<<1, 1, 0, h->stream>>>(h->P, h->sc);
+        h->launch_counter++;
+    }
+}
+
+int check_scalars(lssph_handle* h, Scalars* out) {
+    Scalars s{};
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaMemcpy(&s, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+    if (out) *out = s;
+    if (s.err & ERR_OUT_OF_DOMAIN) return fail(h, LSSPH_E_OUT_OF_DOMAIN, "a particle left the cell grid");
+    if (s.err & ERR_CELL_OVERFLOW) return fail(h, LSSPH_E_CELL_OVERFLOW, "a cell holds more particles than its slot capacity");
+    if (s.err & ERR_NONFINITE) return fail(h, LSSPH_E_NONFINITE, "a non-finite value appeared in the particle state");
+    return LSSPH_OK;
+}
+
+int sync_check(lssph_handle* h) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return check_scalars(h, nullptr);
+}
+
+// Build the cell list of the current positions into list buffer lb (fresh).
+int rebuild_cells(lssph_handle* h) {
+    for (int b = 0; b < 2; ++b) CUDA_TRY(h, cudaMemsetAsync(h->L[b].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
+    k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->gstart, h->W.key, h->sc);
+    launch_cellsort(h, h->lb, 0);
+    return LSSPH_OK;
+}
+
+int upload_fields(lssph_handle* h, const double* x, const double* y, const double* u, const double* v,
+                  const double* rho, const double* pre, const double* tem) {
+    const size_t bytes = sizeof(double) * (size_t)h->num_total;
+    for (int b = 0; b < 2; ++b) {
+        const Fld& F = h->F[b];
+        if (x) CUDA_TRY(h, cudaMemcpyAsync(F.x, x, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (y) CUDA_TRY(h, cudaMemcpyAsync(F.y, y, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (u) CUDA_TRY(h, cudaMemcpyAsync(F.u, u, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (v) CUDA_TRY(h, cudaMemcpyAsync(F.v, v, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (rho) CUDA_TRY(h, cudaMemcpyAsync(F.rho, rho, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (pre) CUDA_TRY(h, cudaMemcpyAsync(F.pre, pre, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (tem && h->has_tem) CUDA_TRY(h, cudaMemcpyAsync(F.tem, tem, bytes, cudaMemcpyHostToDevice, h->stream));
+        k_volume<<<blocks_for(h->num_total, 128), 128, 0, h->stream>>>(h->P, F);
+    }
+    return LSSPH_OK;
+}
+
+void free_handle(lssph_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& row : h->graph)
+        for (auto& g : row)
+            if (g) cudaGraphExecDestroy(g);
+    for (void* p : h->allocs) cudaFree(p);
+    for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int create_impl(const lssph_params* pin, int num_total, int num_int, const int32_t* ptype, const double* x,
+                const double* y, const double* u, const double* v, const double* rho, const double* pre,
+                const double* tem, lssph_handle** out) {
+    std::string msg;
+    if (!pin || !ptype || !x || !y || !u || !v || !rho || !pre || !out) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    *out = nullptr;
+    if (check_param(pin, &msg) != LSSPH_OK) return fail(nullptr, LSSPH_E_BAD_PARAM, msg);
+    if (pin->sph_model != 3)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED, "the GPU engine implements SPH_MODEL 3 (2nd-order LS-SPH)");
+    if (pin->precision != LSSPH_PRECISION_FP64)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED, "this entry point runs the FP64 path");
+    if (pin->target_problem == 4 && !tem) return fail(nullptr, LSSPH_E_BAD_PARAM, "tem required for problem 4");
+    if (num_int <= 0 || num_total <= num_int) return fail(nullptr, LSSPH_E_BAD_PARAM, "bad particle counts");
+    for (int i = 0; i < num_total; ++i) {
+        if ((i < num_int) != (ptype[i] == 0))
+            return fail(nullptr, LSSPH_E_BAD_PARAM, "ptype must be 0 for the first num_int particles and 1..8 after");
+    }
+    lssph_handle* h = new lssph_handle();
+    h->p = *pin;
+    init_param(&h->p);
+    h->num_total = num_total;
+    h->num_int = num_int;
+    h->num_ext = num_total - num_int;
+    h->problem = h->p.target_problem;
+    h->has_tem = h->problem == 4;
+    h->p1 = h->problem == 1;
+    h->pst_on = h->problem != 1;   // main.f90:132-134
+    h->nb_rhs = h->p1 ? 1 : (h->has_tem ? 5 : 4);
+    h->nb_ghost = h->p1 ? 1 : (h->has_tem ? 4 : 3);
+    h->wq = h->p.wall_model == 1 ? 1 : (h->p.wall_model == 3 ? 6 : 3);
+    h->G = h->p.lanes > 0 ? h->p.lanes : 4;
+    h->Gg = h->p.lanes > 0 ? h->p.lanes : 4;
+    h->ptype.assign(ptype, ptype + num_total);
+
+    int rc = build_virtual_markers(&h->p, num_total, num_int, ptype, x, y, &h->vm, &msg);
+    if (rc == LSSPH_OK) rc = build_cell_grid(&h->p, num_total, num_int, x, y, h->vm, &h->grid, &msg);
+    if (rc != LSSPH_OK) { free_handle(h); return fail(nullptr, rc, msg); }
+
+    // ---- constants ----
+    const lssph_params& p = h->p;
+    Phys& P = h->P;
+    P.problem = p.target_problem; P.kt = p.kernel_type; P.rk = p.rk; P.wall_model = p.wall_model;
+    P.u_bc_top = p.u_bc_top; P.u_bc_bottom = p.u_bc_bottom; P.u_bc_left = p.u_bc_left; P.u_bc_right = p.u_bc_right;
+    P.tem_bc_top = p.tem_bc_top; P.tem_bc_bottom = p.tem_bc_bottom; P.tem_bc_left = p.tem_bc_left;
+    P.tem_bc_right = p.tem_bc_right;
+    P.nx = h->grid.nx; P.ny = h->grid.ny; P.ncell = h->grid.ncell; P.cap = h->grid.cap;
+    P.num_total = num_total; P.num_int = num_int; P.num_ext = h->num_ext;
+    P.u_top = p.u_top; P.tem_top = p.tem_top; P.tem_bottom = p.tem_bottom; P.tem_left = p.tem_left;
+    P.tem_right = p.tem_right;
+    P.h = p.h;
+    P.ih1 = 1.0 / p.h;
+    P.ih2A = P.ih1 / p.h;          // inv_h(2) = inv_h(1)/h  (LSSPH_A_mod.f90:90-93)
+    P.ih2B = P.ih1 * P.ih1;        // inv_h2 = inv_h*inv_h  (interpolate_LSSPH_B_mod.f90:151-152)
+    P.h_eff_sq = p.h_eff * p.h_eff;
+    P.inv_h_eff = 1.0 / p.h_eff;
+    P.SP_mass = p.SP_mass;
+    P.W_ave = p.W_ave;
+    P.wnorm = kernel_norm(p.kernel_type, p.h);
+    P.dt = p.dt;
+    P.c_sq = p.sound_speed * p.sound_speed;
+    P.rho_ref = p.rho_ref;
+    P.vis_ref = p.vis_ref;
+    P.delta = ((p.coe_delta_sph * p.sound_speed) * p.h) * p.zeta_RSST;
+    P.zeta_sq = p.zeta_RSST * p.zeta_RSST;
+    P.xi_sq = p.xi_VIM * p.xi_VIM;
+    P.alpha_ref = p.alpha_ref;
+    P.gravity = p.gravity;
+    P.tem_ave = p.tem_ave;
+    P.thermal_dif = p.thermal_dif;
+    P.PST_c = p.PST_c;
+    P.threshold = p.threshold;
+    P.hydro_coef_top = ((p.rho_ref * p.alpha_ref) * (p.tem_top - p.tem_ave)) * p.gravity;
+    P.hydro_coef_bottom = ((p.rho_ref * p.alpha_ref) * (p.tem_bottom - p.tem_ave)) * p.gravity;
+
+    // ---- device memory ----
+    auto cu = [&](cudaError_t e) { return e == cudaSuccess ? LSSPH_OK : fail(nullptr, LSSPH_E_CUDA, cudaGetErrorString(e)); };
+    if ((rc = cu(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking))) != LSSPH_OK ||
+        (rc = cu(cudaEventCreate(&h->ev0))) != LSSPH_OK || (rc = cu(cudaEventCreate(&h->ev1))) != LSSPH_OK) {
+        free_handle(h);
+        return rc;
+    }
+    const size_t N = num_total, NI = num_int, NE = h->num_ext, NC = h->grid.ncell;
+    bool ok = true;
+    auto A = [&](auto** ptr, size_t n) { if (ok && dalloc(h, ptr, n) != LSSPH_OK) ok = false; };
+    for (int b = 0; b < 2; ++b) {
+        Fld& F = h->F[b];
+        A(&F.x, N); A(&F.y, N); A(&F.u, N); A(&F.v, N); A(&F.rho, N); A(&F.pre, N); A(&F.tem, N); A(&F.vol, N);
+        Lst& L = h->L[b];
+        A(&L.cnt, NC); A(&L.num, NC); A(&L.fnum, NC); A(&L.slots, NC * h->grid.cap);
+    }
+    Work& W = h->W;
+    A(&W.x_old, NI); A(&W.y_old, NI); A(&W.u_old, NI); A(&W.v_old, NI); A(&W.rho_old, NI); A(&W.tem_old, NI);
+    A(&W.x_acc, NI); A(&W.y_acc, NI); A(&W.u_acc, NI); A(&W.v_acc, NI); A(&W.rho_acc, NI); A(&W.tem_acc, NI);
+    A(&W.rhs_u, NI); A(&W.rhs_v, NI); A(&W.rhs_rho, NI); A(&W.rhs_tem, NI);
+    A(&W.f_prev, NI); A(&W.src, NI); A(&W.key, NI);
+    VMd& V = h->V;
+    A(&V.x, NE); A(&V.y, NE); A(&V.nx, NE); A(&V.ny, NE); A(&V.u, NE); A(&V.v, NE); A(&V.pre, NE); A(&V.tem, NE);
+    A(&V.K, NE); A(&V.ptype, NE); A(&V.key, NE); A(&V.mode, NE);
+    A(&h->gstart, NC + 1); A(&h->glist, NE);
+    A(&h->sc, 1);
+    if (!ok) { const std::string m = h->err; free_handle(h); return fail(nullptr, LSSPH_E_CUDA, m); }
+
+    // ---- host-side constant arrays ----
+    std::vector<double> src(NI, 0.0), K(NE, 0.0), zeros(std::max(NI, NE), 0.0), ones(NI, 1.0);
+    std::vector<int32_t> mode(NE, XM_NEG);
+    if (h->p1) {
+        for (size_t i = 0; i < NI; ++i)   // LSSPH_A_mod.f90:247-248 (positions never move in problem 1)
+            src[i] = ((2.0 * (kPi * kPi)) * std::sin(kPi * (x[i] - p.WL_thick))) * std::cos(kPi * (y[i] - p.WL_thick));
+        for (size_t me = 0; me < NE; ++me) {   // extrapolate_diff_test_mod.f90:40-103
+            const int t = h->vm.ptype[me];
+            const double vx = h->vm.x[me], vy = h->vm.y[me], xg = x[num_int + me];
+            if (t == 1) {
+                if (p.u_bc_bottom == 1) mode[me] = XM_COPY;
+                else { mode[me] = XM_K_MINUS; K[me] = 2.0 * std::sin(kPi * (vx - p.WL_thick)); }
+            } else if (t == 2) {
+                if (p.u_bc_top == 1) mode[me] = XM_COPY;
+                else { mode[me] = XM_K_MINUS; K[me] = 2.0 * (-std::sin(kPi * (vx - p.WL_thick))); }
+            } else if (t == 3) {
+                if (p.u_bc_left == 1) { mode[me] = XM_PLUS_K; K[me] = (kPi * std::cos(kPi * (vy - p.WL_thick))) * (xg - vx); }
+                else mode[me] = XM_NEG;
+            } else if (t == 4) {
+                if (p.u_bc_right == 1) { mode[me] = XM_PLUS_K; K[me] = ((-kPi) * std::cos(kPi * (vy - p.WL_thick))) * (xg - vx); }
+                else mode[me] = XM_NEG;
+            } else {
+                mode[me] = XM_NEG;
+            }
+        }
+    }
+    auto H2D = [&](void* dst, const void* srcp, size_t bytes) {
+        if (ok && bytes && cudaMemcpyAsync(dst, srcp, bytes, cudaMemcpyHostToDevice, h->stream) != cudaSuccess) ok = false;
+    };
+    H2D(W.src, src.data(), sizeof(double) * NI);
+    H2D(W.f_prev, ones.data(), sizeof(double) * NI);   // setup_closed_box_mod.f90:160-163
+    H2D(V.x, h->vm.x.data(), sizeof(double) * NE);
+    H2D(V.y, h->vm.y.data(), sizeof(double) * NE);
+    H2D(V.nx, h->vm.nx.data(), sizeof(double) * NE);
+    H2D(V.ny, h->vm.ny.data(), sizeof(double) * NE);
+    H2D(V.ptype, h->vm.ptype.data(), sizeof(int32_t) * NE);
+    H2D(V.key, h->grid.vm_key.data(), sizeof(int32_t) * NE);
+    H2D(V.K, K.data(), sizeof(double) * NE);
+    H2D(V.mode, mode.data(), sizeof(int32_t) * NE);
+    H2D(V.u, zeros.data(), sizeof(double) * NE);
+    H2D(V.v, zeros.data(), sizeof(double) * NE);
+    H2D(V.pre, zeros.data(), sizeof(double) * NE);
+    H2D(V.tem, zeros.data(), sizeof(double) * NE);
+    H2D(h->gstart, h->grid.gstart.data(), sizeof(int32_t) * (NC + 1));
+    H2D(h->glist, h->grid.glist.data(), sizeof(int32_t) * NE);
+    if (ok && cudaMemsetAsync(h->sc, 0, sizeof(Scalars), h->stream) != cudaSuccess) ok = false;
+    if (ok && cudaMemsetAsync(W.key, 0, sizeof(int32_t) * NI, h->stream) != cudaSuccess) ok = false;
+    for (int b = 0; b < 2 && ok; ++b) {
+        if (cudaMemsetAsync(h->F[b].tem, 0, sizeof(double) * N, h->stream) != cudaSuccess) ok = false;
+        if (cudaMemsetAsync(h->L[b].slots, 0xff, sizeof(int) * NC * h->grid.cap, h->stream) != cudaSuccess) ok = false;
+        if (cudaMemsetAsync(h->L[b].num, 0, sizeof(int) * NC, h->stream) != cudaSuccess) ok = false;
+        if (cudaMemsetAsync(h->L[b].fnum, 0, sizeof(int) * NC, h->stream) != cudaSuccess) ok = false;
+    }
+    if (!ok) { free_handle(h); return fail(nullptr, LSSPH_E_CUDA, "device initialisation failed"); }
+    if ((rc = upload_fields(h, x, y, u, v, rho, pre, tem)) != LSSPH_OK ||
+        (rc = rebuild_cells(h)) != LSSPH_OK || (rc = sync_check(h)) != LSSPH_OK) {
+        const std::string m = h->err;
+        free_handle(h);
+        return fail(nullptr, rc, m);
+    }
+    *out = h;
+    return LSSPH_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+// C ABI (handle half)
+// =====================================================================================
+extern "C" {
+
+int lssph_create(const lssph_params* p, int32_t num_total, int32_t num_int, const int32_t* ptype,
+                 const double* x, const double* y, const double* u, const double* v, const double* rho,
+                 const double* pre, const double* tem, lssph_handle** out) {
+    return create_impl(p, num_total, num_int, ptype, x, y, u, v, rho, pre, tem, out);
+}
+
+void lssph_destroy(lssph_handle* h) { free_handle(h); }
+
+const char* lssph_handle_error(const lssph_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int lssph_get_params(const lssph_handle* h, lssph_params* out) {
+    if (!h || !out) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    *out = h->p;
+    return LSSPH_OK;
+}
+
+int lssph_counts(const lssph_handle* h, int32_t* num_total, int32_t* num_int, int32_t* num_ext, int32_t* num_cells) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (num_total) *num_total = h->num_total;
+    if (num_int) *num_int = h->num_int;
+    if (num_ext) *num_ext = h->num_ext;
+    if (num_cells) *num_cells = h->grid.ncell;
+    return LSSPH_OK;
+}
+
+int lssph_calculate_rhs(lssph_handle* h) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    StageCfg S{};
+    S.mode = MODE_RHS_ONLY;
+    S.stage = 1;
+    S.write_rhs = 1;
+    launch_stage_any(h, S);
+    return sync_check(h);
+}
+
+int lssph_update_cell(lssph_handle* h) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb ^ 1], h->gstart,
+                                                                     h->W.key, h->sc);
+    launch_cellsort(h, h->lb ^ 1, 0);
+    h->lb ^= 1;
+    return sync_check(h);
+}
+
+int lssph_ghost(lssph_handle* h) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    launch_ghost(h);
+    return sync_check(h);
+}
+
+int lssph_rk2(lssph_handle* h) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (h->p.rk != 2) return fail(h, LSSPH_E_BAD_PARAM, "handle was configured with RK = 4");
+    for (int s = 1; s <= 2; ++s) enq_stage(h, s, false);
+    return sync_check(h);
+}
+
+int lssph_rk4(lssph_handle* h) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (h->p.rk != 4) return fail(h, LSSPH_E_BAD_PARAM, "handle was configured with RK = 2");
+    for (int s = 1; s <= 4; ++s) enq_stage(h, s, false);
+    return sync_check(h);
+}
+
+int lssph_pst(lssph_handle* h) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    CUDA_TRY(h, cudaMemsetAsync(&h->sc->umax2, 0, sizeof(unsigned long long), h->stream));
+    k_umax<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->sc);
+    enq_pst(h);
+    return sync_check(h);
+}
+
+int lssph_check_steady_state(lssph_handle* h, int32_t* is_steady) {
+    if (!h || !is_steady) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    CUDA_TRY(h, cudaMemsetAsync(&h->sc->dfmax, 0, sizeof(unsigned long long), h->stream));
+    k_steady_max<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->W, h->sc);
+    Scalars s{};
+    int rc = check_scalars(h, &s);
+    if (rc != LSSPH_OK) return rc;
+    double df;
+    std::memcpy(&df, &s.dfmax, sizeof(df));
+    *is_steady = (df < h->p.threshold) ? 1 : 0;
+    if (!*is_steady) k_copy_fprev<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->W);
+    CUDA_TRY(h, cudaMemsetAsync(&h->sc->dfmax, 0, sizeof(unsigned long long), h->stream));
+    return sync_check(h);
+}
+
+int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (steady_step_out) *steady_step_out = 0;
+    if (nsteps <= 0) return LSSPH_OK;
+    Scalars s0{};
+    int rc = check_scalars(h, &s0);
+    if (rc != LSSPH_OK) return rc;
+    if (s0.steady) return LSSPH_OK;   // the reference leaves the time loop at a steady state
+    const int64_t launches0 = h->launch_counter;
+    CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+    for (int st = 0; st < nsteps; ++st) {
+        cudaGraphExec_t& ge = h->graph[h->sb][h->lb];
+        if (!ge) {
+            const int sb0 = h->sb, lb0 = h->lb;
+            const int64_t c0 = h->launch_counter;
+            CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            enq_step(h);
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
+            const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+            h->graph_launches = (int)(h->launch_counter - c0);
+            h->launch_counter = c0;
+            h->step_flip = ((h->sb ^ sb0) << 1) | (h->lb ^ lb0);
+            h->sb = sb0;
+            h->lb = lb0;
+        }
+        CUDA_TRY(h, cudaGraphLaunch(ge, h->stream));
+        h->launch_counter += h->graph_launches;
+        h->sb ^= (h->step_flip >> 1) & 1;
+        h->lb ^= h->step_flip & 1;
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+    Scalars s1{};
+    rc = check_scalars(h, &s1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_ms = ms;
+    h->last_launches = h->launch_counter - launches0;
+    if (rc != LSSPH_OK) return rc;
+    if (s1.steady && steady_step_out) *steady_step_out = s1.steady_step - s0.step_count;
+    return LSSPH_OK;
+}
+
+int lssph_upload(lssph_handle* h, const double* x, const double* y, const double* u, const double* v,
+                 const double* rho, const double* pre, const double* tem) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    int rc = upload_fields(h, x, y, u, v, rho, pre, tem);
+    if (rc != LSSPH_OK) return rc;
+    if (!h->p1 && (x || y)) {
+        if ((rc = rebuild_cells(h)) != LSSPH_OK) return rc;
+    }
+    return sync_check(h);
+}
+
+int lssph_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u, double* v, double* rho,
+                   double* pre, double* tem) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    const size_t bytes = sizeof(double) * (size_t)h->num_total;
+    const Fld& F = h->F[h->sb];
+    if (x) CUDA_TRY(h, cudaMemcpyAsync(x, F.x, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (y) CUDA_TRY(h, cudaMemcpyAsync(y, F.y, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (u) CUDA_TRY(h, cudaMemcpyAsync(u, F.u, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (v) CUDA_TRY(h, cudaMemcpyAsync(v, F.v, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, F.rho, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (pre) CUDA_TRY(h, cudaMemcpyAsync(pre, F.pre, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (tem) {
+        if (h->has_tem) CUDA_TRY(h, cudaMemcpyAsync(tem, F.tem, bytes, cudaMemcpyDeviceToHost, h->stream));
+        else std::memset(tem, 0, bytes);
+    }
+    if (ptype) std::memcpy(ptype, h->ptype.data(), sizeof(int32_t) * h->num_total);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LSSPH_OK;
+}
+
+int lssph_download_rhs(lssph_handle* h, double* ru, double* rv, double* rr, double* rt) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    const size_t bytes = sizeof(double) * (size_t)h->num_int;
+    if (ru) CUDA_TRY(h, cudaMemcpyAsync(ru, h->W.rhs_u, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (rv) CUDA_TRY(h, cudaMemcpyAsync(rv, h->W.rhs_v, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (rr) CUDA_TRY(h, cudaMemcpyAsync(rr, h->W.rhs_rho, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (rt) CUDA_TRY(h, cudaMemcpyAsync(rt, h->W.rhs_tem, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LSSPH_OK;
+}
+
+int lssph_download_vm(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u, double* v, double* pre,
+                      double* tem) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    const size_t ne = h->num_ext, bytes = sizeof(double) * ne;
+    if (ptype) std::memcpy(ptype, h->vm.ptype.data(), sizeof(int32_t) * ne);
+    if (x) std::memcpy(x, h->vm.x.data(), bytes);
+    if (y) std::memcpy(y, h->vm.y.data(), bytes);
+    if (u) CUDA_TRY(h, cudaMemcpyAsync(u, h->V.u, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (v) CUDA_TRY(h, cudaMemcpyAsync(v, h->V.v, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (pre) CUDA_TRY(h, cudaMemcpyAsync(pre, h->V.pre, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (tem) CUDA_TRY(h, cudaMemcpyAsync(tem, h->V.tem, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return LSSPH_OK;
+}
+
+int lssph_neighbors_csr(lssph_handle* h, int32_t which, int32_t* offsets, int32_t* idx, int64_t cap, int64_t* nnz_out) {
+    if (!h || !offsets) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    const int n = which == 0 ? h->num_int : h->num_ext;
+    const int stride = 9 * h->grid.cap;
+    int *d_out = nullptr, *d_cnt = nullptr;
+    CUDA_TRY(h, cudaMallocAsync((void**)&d_out, sizeof(int) * (size_t)n * stride, h->stream));
+    CUDA_TRY(h, cudaMallocAsync((void**)&d_cnt, sizeof(int) * (size_t)n, h->stream));
+    k_neighbors<<<blocks_for(n, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->W.key, h->V, which,
+                                                           stride, d_out, d_cnt);
+    std::vector<int> out((size_t)n * stride), cnt(n);
+    CUDA_TRY(h, cudaMemcpyAsync(out.data(), d_out, sizeof(int) * out.size(), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaFreeAsync(d_out, h->stream));
+    CUDA_TRY(h, cudaFreeAsync(d_cnt, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    int64_t nnz = 0;
+    for (int i = 0; i < n; ++i) {
+        offsets[i] = (int32_t)nnz;
+        const int c = std::min(cnt[i], stride);
+        std::sort(out.begin() + (size_t)i * stride, out.begin() + (size_t)i * stride + c);
+        if (idx) {
+            if (nnz + c > cap) return fail(h, LSSPH_E_CAPACITY, "neighbour index buffer too small");
+            std::memcpy(idx + nnz, out.data() + (size_t)i * stride, sizeof(int32_t) * c);
+        }
+        nnz += c;
+    }
+    offsets[n] = (int32_t)nnz;
+    if (nnz_out) *nnz_out = nnz;
+    return LSSPH_OK;
+}
+
+int lssph_write_data(lssph_handle* h, const char* results_root, int32_t step) {
+    if (!h || !results_root) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    const size_t n = h->num_total;
+    std::vector<int32_t> pt(n);
+    std::vector<double> x(n), y(n), u(n), v(n), rho(n), pre(n), tem(n);
+    int rc = lssph_download(h, pt.data(), x.data(), y.data(), u.data(), v.data(), rho.data(), pre.data(), tem.data());
+    if (rc != LSSPH_OK) return rc;
+    const std::string dir = std::string(results_root) + "/" + h->p.save_name + "/data";
+    if (make_dirs(dir) != LSSPH_OK) return fail(h, LSSPH_E_IO, "cannot create " + dir);
+    std::string msg;
+    rc = write_data_file(dir + "/" + std::to_string(step) + ".dat", (int)n, h->has_tem, pt.data(), x.data(), y.data(),
+                         u.data(), v.data(), rho.data(), pre.data(), tem.data(), &msg);
+    return rc == LSSPH_OK ? rc : fail(h, rc, msg);
+}
+
+int lssph_write_param(lssph_handle* h, const char* results_root, const char* config_h_path) {
+    if (!h || !results_root) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    const std::string base = std::string(results_root) + "/" + h->p.save_name;
+    const std::string cfg = base + "/config", dat = base + "/data";
+    if (make_dirs(cfg) != LSSPH_OK || make_dirs(dat) != LSSPH_OK) return fail(h, LSSPH_E_IO, "cannot create " + base);
+    if (config_h_path && config_h_path[0] && copy_file(config_h_path, cfg + "/config.h") != LSSPH_OK)
+        return fail(h, LSSPH_E_IO, std::string("cannot copy ") + config_h_path);
+    std::string msg;
+    int rc = write_parameters_csv(cfg + "/parameters.csv", &h->p, h->num_total, h->num_int, h->num_ext, &msg);
+    if (rc != LSSPH_OK) return fail(h, rc, msg);
+    // cell_idx.dat: 1-based cell ids after init_cell + update_cell (write_param_mod.f90:133-136)
+    std::vector<int32_t> key(h->num_int), cell(h->num_total);
+    CUDA_TRY(h, cudaMemcpy(key.data(), h->W.key, sizeof(int32_t) * h->num_int, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < h->num_int; ++i) cell[i] = key[i] + 1;
+    for (int me = 0; me < h->num_ext; ++me) cell[h->num_int + me] = h->grid.ghost_key[me] + 1;
+    FILE* f = std::fopen((dat + "/cell_idx.dat").c_str(), "wb");
+    if (!f) return fail(h, LSSPH_E_IO, "cannot open cell_idx.dat");
+    const bool ok1 = std::fwrite(cell.data(), sizeof(int32_t), cell.size(), f) == cell.size();
+    std::fclose(f);
+    if (!ok1) return fail(h, LSSPH_E_IO, "short write to cell_idx.dat");
+    // ghost() then VM.dat (write_param_mod.f90:141-159)
+    if ((rc = lssph_ghost(h)) != LSSPH_OK) return rc;
+    const size_t ne = h->num_ext;
+    std::vector<int32_t> pt(ne);
+    std::vector<double> vx(ne), vy(ne), vu(ne), vv(ne), vp(ne), vt(ne);
+    if ((rc = lssph_download_vm(h, pt.data(), vx.data(), vy.data(), vu.data(), vv.data(), vp.data(), vt.data())) != LSSPH_OK)
+        return rc;
+    f = std::fopen((dat + "/VM.dat").c_str(), "wb");
+    if (!f) return fail(h, LSSPH_E_IO, "cannot open VM.dat");
+    bool ok = std::fwrite(pt.data(), sizeof(int32_t), ne, f) == ne;
+    for (const auto* a : {&vx, &vy, &vu, &vv, &vp}) ok = ok && std::fwrite(a->data(), sizeof(double), ne, f) == ne;
+    if (h->has_tem) ok = ok && std::fwrite(vt.data(), sizeof(double), ne, f) == ne;
+    std::fclose(f);
+    if (!ok) return fail(h, LSSPH_E_IO, "short write to VM.dat");
+    return LSSPH_OK;
+}
+
+int lssph_step_profiled(lssph_handle* h, int32_t nsteps, double* ms_by_kind, int64_t* launches_by_kind) {
+    if (!h || !ms_by_kind || !launches_by_kind) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    for (int k = 0; k < LSSPH_KIND_COUNT; ++k) { ms_by_kind[k] = 0.0; launches_by_kind[k] = 0; }
+    int rc = check_scalars(h, nullptr);
+    if (rc != LSSPH_OK) return rc;
+    h->profiling = true;
+    h->prof_next = 0;
+    h->prof_kinds.clear();
+    for (int st = 0; st < nsteps; ++st) enq_step(h);
+    h->profiling = false;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (size_t k = 0; k < h->prof_kinds.size(); ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->prof_events[2 * k], h->prof_events[2 * k + 1]);
+        ms_by_kind[h->prof_kinds[k]] += ms;
+        launches_by_kind[h->prof_kinds[k]] += 1;
+    }
+    return check_scalars(h, nullptr);
+}
+
+int lssph_last_step_stats(const lssph_handle* h, double* device_ms, int64_t* kernel_launches) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (device_ms) *device_ms = h->last_ms;
+    if (kernel_launches) *kernel_launches = h->last_launches;
+    return LSSPH_OK;
+}
+
+}  // extern "C"

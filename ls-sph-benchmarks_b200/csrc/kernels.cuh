@@ -1,0 +1,918 @@
+// kernels.cuh -- device code of the FP64 LS-SPH path (sm_100a).
+//
+// Every kernel here replaces one OpenMP region of the reference solver:
+//   k_stage      calculate_RHS (LSSPH_A_mod.f90:26-271) fused with the RK2/RK4 stage
+//                update + EOS (RK2_mod.f90:87-108, RK4_mod.f90:109-159) and with the
+//                scatter half of update_cell (update_cell_mod.f90:40-70)
+//   k_cellsort   the rest of update_cell: per-cell list in reference order (interior
+//                particles by ascending index, then the static ghost list, :75-93)
+//   k_ghost      ghost (ghost_mod.f90:55-74): LS type-B / CSPH interpolation at each
+//                virtual marker + extrapolation to its ghost particle
+//   k_pst        shift_interpolate (shift_interpolate_mod.f90:23-300) fused with the
+//                PST copy-back + EOS (PST_mod.f90:85-99) and the cell scatter
+//
+// Arithmetic follows the oracle's sequence: the file is compiled with -fmad=false so
+// no multiply-add is fused implicitly, and fma() appears only at the accumulation sites
+// and in the LU.  With one lane per particle the neighbour loop visits candidates in
+// the reference list order and the results are bit-identical to the oracle; with G>1
+// lanes each lane sums a strided share of the list and a butterfly shuffle combines the
+// partial sums (identical on every lane, so the G lanes agree bit for bit).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lssph {
+
+// ---- error bits (device scalars) -----------------------------------------------------
+enum : int {
+    ERR_CELL_OVERFLOW = 1,
+    ERR_OUT_OF_DOMAIN = 2,
+    ERR_NONFINITE = 4,
+};
+enum : int { WARN_SINGULAR = 1 };
+
+struct Scalars {
+    unsigned long long umax2;   // max(u^2+v^2) bits (non-negative doubles order as uint64)
+    unsigned long long dfmax;   // max |f_previous - u| bits (problem 1)
+    int err;                    // ERR_* bits; any set bit halts later kernels
+    int warn;                   // WARN_* bits
+    int steady;                 // 1 once the steady state is reached (problem 1)
+    int step_count;             // steps completed (problem 1 epilogue)
+    int steady_step;            // step_count value at which steady was reached
+    int pad;
+};
+
+// Constants of one solve (a subset of lssph_params plus precomputed factors).
+struct Phys {
+    int problem, kt, rk, wall_model;
+    int u_bc_top, u_bc_bottom, u_bc_left, u_bc_right;
+    int tem_bc_top, tem_bc_bottom, tem_bc_left, tem_bc_right;
+    int nx, ny, ncell, cap;
+    int num_total, num_int, num_ext, pad;
+    double u_top, tem_top, tem_bottom, tem_left, tem_right;
+    double h, ih1, ih2A, ih2B, h_eff_sq, inv_h_eff, SP_mass, W_ave, wnorm, dt;
+    double c_sq, rho_ref, vis_ref, delta, zeta_sq, xi_sq, alpha_ref, gravity, tem_ave;
+    double thermal_dif, PST_c, threshold, hydro_coef_top, hydro_coef_bottom;
+};
+
+struct Fld {   // SoA particle state over num_total
+    double *x, *y, *u, *v, *rho, *pre, *tem, *vol;
+};
+struct Lst {   // fixed-capacity cell list: slots[c*cap + k]
+    int *cnt, *num, *fnum, *slots;
+};
+struct Work {  // per-interior-particle arrays
+    double *x_old, *y_old, *u_old, *v_old, *rho_old, *tem_old;
+    double *x_acc, *y_acc, *u_acc, *v_acc, *rho_acc, *tem_acc;
+    double *rhs_u, *rhs_v, *rhs_rho, *rhs_tem;
+    double *f_prev, *src;
+    int* key;
+};
+struct VMd {   // virtual markers over num_ext
+    double *x, *y, *nx, *ny, *u, *v, *pre, *tem, *K;
+    int *ptype, *key, *mode;
+};
+
+enum : int { MODE_STAGE = 0, MODE_RHS_ONLY = 1 };
+struct StageCfg {
+    int mode;        // MODE_*
+    int stage;       // 1-based RK stage
+    int last;        // last stage of the step
+    int do_scatter;  // rebuild the cell list of the new positions
+    int do_umax;     // reduce max(u^2+v^2) of the new state for PST
+    int do_steady;   // problem-1 steady-state reduction + f_previous copy
+    int write_rhs;   // keep RHS arrays
+    int pad;
+    double dt1, dt2; // RK4: accumulator / intermediate factors; RK2: dt2 = dt_eff
+};
+
+// P1 ghost extrapolation modes (extrapolate_diff_test_mod.f90:40-103), K precomputed.
+enum : int { XM_COPY = 0, XM_K_MINUS = 1, XM_PLUS_K = 2, XM_NEG = 3 };
+
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ bool halted(const Scalars* sc) {
+    return (*(volatile const int*)&sc->err) != 0 || (*(volatile const int*)&sc->steady) != 0;
+}
+
+// cal_W / cal_dW (kernel_functions_mod.f90:26-146); nrm = kernel_norm(kt, h).
+__device__ __forceinline__ double dev_W(int kt, double r, double h, double nrm) {
+    const double q = r / h;
+    double W = 0.0;
+    if (kt == 3) {
+        if (0.0 <= q && q <= 2.0) {
+            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2;
+            W = t4 * (1.0 + 2.0 * q);
+        }
+    } else if (kt == 1) {
+        const double a = 2.0 - q, b = 1.0 - q, a3 = (a * a) * a, b3 = (b * b) * b;
+        if (0.0 <= q && q <= 1.0) W = a3 - 4.0 * b3;
+        else if (1.0 < q && q <= 2.0) W = a3;
+    } else if (kt == 2) {
+        const double a = 3.0 - q, b = 2.0 - q, c = 1.0 - q;
+        const double a2 = a * a, b2 = b * b, c2 = c * c;
+        const double a5 = (a2 * a2) * a, b5 = (b2 * b2) * b, c5 = (c2 * c2) * c;
+        if (0.0 <= q && q <= 1.0) W = (a5 - 6.0 * b5) + 15.0 * c5;
+        else if (1.0 < q && q <= 2.0) W = a5 - 6.0 * b5;
+        else if (2.0 < q && q <= 3.0) W = a5;
+    } else if (kt == 4) {
+        if (0.0 <= q && q <= 2.0) {
+            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t6 = t4 * t2;
+            W = t6 * ((1.0 + 3.0 * q) + (35.0 * (q * q)) / 12.0);
+        }
+    } else {
+        if (0.0 <= q && q <= 2.0) {
+            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t8 = t4 * t4;
+            const double q2 = q * q, q3 = q2 * q;
+            W = t8 * (((1.0 + 4.0 * q) + (25.0 * q2) / 4.0) + 4.0 * q3);
+        }
+    }
+    return nrm * W;
+}
+
+__device__ __forceinline__ double dev_dW(int kt, double r, double h, double nrm) {
+    const double q = r / h;
+    double dW = 0.0;
+    if (kt == 3) {
+        if (0.0 <= q && q <= 2.0) {
+            const double t = 1.0 - 0.5 * q, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+            dW = -(2.0 * t3) * (1.0 + 2.0 * q) + 2.0 * t4;
+        }
+        return (nrm * dW) / h;
+    } else if (kt == 1) {
+        const double a = 2.0 - q, b = 1.0 - q;
+        if (0.0 <= q && q <= 1.0) dW = a * a - 4.0 * (b * b);
+        else if (1.0 < q && q <= 2.0) dW = a * a;
+        return (nrm * dW) * (-3.0 / h);
+    } else if (kt == 2) {
+        const double a = 3.0 - q, b = 2.0 - q, c = 1.0 - q;
+        const double a2 = a * a, b2 = b * b, c2 = c * c;
+        const double a4 = a2 * a2, b4 = b2 * b2, c4 = c2 * c2;
+        if (0.0 <= q && q <= 1.0) dW = (a4 - 6.0 * b4) + 15.0 * c4;
+        else if (1.0 < q && q <= 2.0) dW = a4 - 6.0 * b4;
+        else if (2.0 < q && q <= 3.0) dW = a4;
+        return (nrm * dW) * (-5.0 / h);
+    } else if (kt == 4) {
+        if (0.0 <= q && q <= 2.0) {
+            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t5 = t4 * t, t6 = t4 * t2;
+            dW = -(3.0 * t5) * ((1.0 + 3.0 * q) + (35.0 * (q * q)) / 12.0) + t6 * (3.0 + (35.0 * q) / 6.0);
+        }
+        return (nrm * dW) / h;
+    } else {
+        if (0.0 <= q && q <= 2.0) {
+            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t7 = t6 * t, t8 = t4 * t4;
+            const double q2 = q * q, q3 = q2 * q;
+            dW = -(4.0 * t7) * (((1.0 + 4.0 * q) + (25.0 * q2) / 4.0) + 4.0 * q3) +
+                 t8 * ((4.0 + (25.0 * q) / 2.0) + 12.0 * q2);
+        }
+        return (nrm * dW) / h;
+    }
+}
+
+// Index of (row j, col i), j <= i, in a column-packed upper triangle.
+__host__ __device__ constexpr int UT(int j, int i) { return i * (i + 1) / 2 + j; }
+
+// Gaussian elimination with partial pivoting + substitutions, the DGESV restatement of
+// the oracle (first max |a| pivot, reciprocal column scaling, right-looking update).
+// A[row][col] is overwritten by LU; B[c][row] by the solution.  Returns false on a zero
+// pivot.
+template <int Q, int NB>
+__device__ __forceinline__ bool lu_solve(double (&A)[Q][Q], double (&B)[NB][Q]) {
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        int p = k;
+        double amax = fabs(A[k][k]);
+#pragma unroll
+        for (int i = k + 1; i < Q; ++i) {
+            const double a = fabs(A[i][k]);
+            if (a > amax) { amax = a; p = i; }
+        }
+#pragma unroll
+        for (int r = k + 1; r < Q; ++r) {
+            const bool s = (p == r);
+#pragma unroll
+            for (int c = 0; c < Q; ++c) {
+                const double t0 = A[k][c], t1 = A[r][c];
+                A[k][c] = s ? t1 : t0;
+                A[r][c] = s ? t0 : t1;
+            }
+#pragma unroll
+            for (int m = 0; m < NB; ++m) {
+                const double t0 = B[m][k], t1 = B[m][r];
+                B[m][k] = s ? t1 : t0;
+                B[m][r] = s ? t0 : t1;
+            }
+        }
+        const double piv = A[k][k];
+        if (piv != 0.0) {
+            const double rp = 1.0 / piv;
+#pragma unroll
+            for (int i = k + 1; i < Q; ++i) A[i][k] = A[i][k] * rp;
+        } else {
+            ok = false;
+        }
+#pragma unroll
+        for (int j = k + 1; j < Q; ++j)
+#pragma unroll
+            for (int i = k + 1; i < Q; ++i) A[i][j] = fma(-A[i][k], A[k][j], A[i][j]);
+    }
+#pragma unroll
+    for (int m = 0; m < NB; ++m) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k)
+#pragma unroll
+            for (int i = k + 1; i < Q; ++i) B[m][i] = fma(-B[m][k], A[i][k], B[m][i]);
+#pragma unroll
+        for (int k = Q - 1; k >= 0; --k) {
+            B[m][k] = B[m][k] / A[k][k];
+#pragma unroll
+            for (int i = 0; i < k; ++i) B[m][i] = fma(-B[m][k], A[i][k], B[m][i]);
+        }
+    }
+    return ok;
+}
+
+// Butterfly sum over aligned groups of G lanes; every lane of the group ends with the
+// same bits (IEEE addition is commutative).
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int off = G / 2; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+template <int G>
+__device__ __forceinline__ int group_sum_i(int v) {
+#pragma unroll
+    for (int off = G / 2; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// Visit the candidates of cell `key` (3x3 cells in reference order, list order within a
+// cell).  Lane `lane` of a G-lane group takes every G-th candidate of the concatenated
+// list.  FLUID_ONLY restricts each cell to its interior-particle prefix.
+template <int G, bool FLUID_ONLY, class F>
+__device__ __forceinline__ void for_candidates(const Phys& P, const Lst& L, int key, int lane, F&& f) {
+    const int cx = key % P.nx, cy = key / P.nx;
+    int base = 0;
+#pragma unroll 1
+    for (int dy = -1; dy <= 1; ++dy) {
+        const int yy = cy + dy;
+        if (yy < 0 || yy >= P.ny) continue;
+#pragma unroll 1
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int xx = cx + dx;
+            if (xx < 0 || xx >= P.nx) continue;
+            const int c = xx + yy * P.nx;
+            const int n = FLUID_ONLY ? __ldg(L.fnum + c) : __ldg(L.num + c);
+            const int* S = L.slots + (size_t)c * P.cap;
+            int t = (G == 1) ? 0 : ((lane - base) & (G - 1));
+#pragma unroll 1
+            for (; t < n; t += G) f(__ldg(S + t));
+            base += n;
+        }
+    }
+}
+
+// Cell key of an interior particle, update_cell_mod.f90:53-55 (multiplication form).
+__device__ __forceinline__ int cell_key_mul(const Phys& P, double x, double y, Scalars* sc) {
+    const double cxd = ceil(x * P.inv_h_eff), cyd = ceil(y * P.inv_h_eff);
+    if (!(cxd >= 1.0 && cxd <= (double)P.nx && cyd >= 1.0 && cyd <= (double)P.ny)) {
+        atomicOr(&sc->err, ERR_OUT_OF_DOMAIN);
+        return -1;
+    }
+    return ((int)cxd - 1) + ((int)cyd - 1) * P.nx;
+}
+
+__device__ __forceinline__ void scatter_to_cell(const Phys& P, const Lst& Ln, const int* gstart, int key,
+                                                int i, Scalars* sc) {
+    if (key < 0) return;
+    const int pos = atomicAdd(Ln.cnt + key, 1);
+    const int lim = P.cap - (gstart[key + 1] - gstart[key]);
+    if (pos < lim) Ln.slots[(size_t)key * P.cap + pos] = i;
+    else atomicOr(&sc->err, ERR_CELL_OVERFLOW);
+}
+
+__device__ __forceinline__ void warp_max_atomic(unsigned long long* dst, double v) {
+    // v >= 0 (or NaN); non-negative doubles order like their uint64 bit patterns
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+}
+
+// =======================================================================================
+// k_stage: LS-SPH type-A RHS (q = 5, SPH_MODEL 3) + RK stage update + cell scatter.
+// NB = number of b-vector columns: 1 (problem 1: u only), 4 (u,v,rho,p), 5 (+T).
+// =======================================================================================
+// Lane-0 tail of k_stage: solve, RHS, stage update, scatter.  Returns this particle's
+// value for the U_max / steady-state max reductions.
+template <int NB>
+__device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, const Lst& Ln,
+                                               const int* __restrict__ gstart, const Work& W, const StageCfg& S,
+                                               Scalars* sc, int i, double my_x, double my_y, double my_u,
+                                               double my_v, double my_rho, double my_tem, const double (&Mu)[15],
+                                               double (&B)[NB][5], int cnt) {
+    constexpr int Q = 5;
+    double d[NB][Q];
+    if (cnt >= Q) {
+        double A[Q][Q];
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+#pragma unroll
+            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
+        if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            d[c][0] = B[c][0] * P.ih1;
+            d[c][1] = B[c][1] * P.ih1;
+            d[c][2] = B[c][2] * P.ih2A;
+            d[c][3] = B[c][3] * P.ih2A;
+            d[c][4] = B[c][4] * P.ih2A;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) d[c][k] = 0.0;
+    }
+
+    // ---- RHS (LSSPH_A_mod.f90:246-269) ----
+    double Ru, Rv = 0.0, Rr = 0.0, Rt = 0.0;
+    if constexpr (NB == 1) {
+        Ru = (d[0][2] + d[0][3]) + W.src[i];
+    } else {
+        const double* du = d[0];
+        const double* dv = d[1];
+        const double* drho = d[2];
+        const double* dpre = d[3];
+        Rr = -(my_rho * (du[0] + dv[1])) + P.delta * (drho[2] + drho[3]);
+        Ru = -(dpre[0] / my_rho) + (P.vis_ref / my_rho) * (du[2] + du[3]);
+        Rv = -(dpre[1] / my_rho) + (P.vis_ref / my_rho) * (dv[2] + dv[3]);
+        Rr = Rr / P.zeta_sq;
+        if constexpr (NB == 5) {
+            const double* dtem = d[4];
+            Rv = Rv + ((P.alpha_ref * (my_tem - P.tem_ave)) * P.gravity);
+            Ru = Ru / P.xi_sq;
+            Rv = Rv / P.xi_sq;
+            Rt = P.thermal_dif * (dtem[2] + dtem[3]);
+        }
+    }
+    if (S.write_rhs) {
+        W.rhs_u[i] = Ru;
+        if constexpr (NB >= 4) { W.rhs_v[i] = Rv; W.rhs_rho[i] = Rr; }
+        if constexpr (NB == 5) W.rhs_tem[i] = Rt;
+    }
+    if (S.mode == MODE_RHS_ONLY) return 0.0;
+
+    // ---- stage update (RK2_mod.f90:87-108 / RK4_mod.f90:109-159) ----
+    constexpr bool p1 = (NB == 1);   // problem 1 updates u only and keeps positions
+    double xo = 0, yo = 0, uo, vo = 0, ro = 0, to = 0;
+    if (S.stage == 1) {
+        xo = my_x; yo = my_y; uo = my_u; vo = my_v; ro = my_rho; to = my_tem;
+        W.u_old[i] = uo;
+        if constexpr (!p1) { W.x_old[i] = xo; W.y_old[i] = yo; W.v_old[i] = vo; W.rho_old[i] = ro; }
+        if constexpr (NB == 5) W.tem_old[i] = to;
+    } else {
+        uo = W.u_old[i];
+        if constexpr (!p1) { xo = W.x_old[i]; yo = W.y_old[i]; vo = W.v_old[i]; ro = W.rho_old[i]; }
+        if constexpr (NB == 5) to = W.tem_old[i];
+    }
+    double xn = my_x, yn = my_y, un, vn = my_v, rn = my_rho, tn = my_tem;
+    if (P.rk == 2) {
+        const double dt = S.dt2;
+        if constexpr (!p1) {
+            xn = xo + my_u * dt;
+            yn = yo + my_v * dt;
+            vn = vo + Rv * dt;
+            rn = ro + Rr * dt;
+        }
+        un = uo + Ru * dt;
+        if constexpr (NB == 5) tn = to + Rt * dt;
+    } else {
+        double ua, va = 0, xa = 0, ya = 0, ra = 0, ta = 0;
+        if (S.stage == 1) {
+            ua = my_u; va = my_v; xa = my_x; ya = my_y; ra = my_rho; ta = my_tem;
+        } else {
+            ua = W.u_acc[i];
+            if constexpr (!p1) { va = W.v_acc[i]; xa = W.x_acc[i]; ya = W.y_acc[i]; ra = W.rho_acc[i]; }
+            if constexpr (NB == 5) ta = W.tem_acc[i];
+        }
+        ua = ua + Ru * S.dt1;
+        if constexpr (!p1) {
+            va = va + Rv * S.dt1;
+            xa = xa + my_u * S.dt1;
+            ya = ya + my_v * S.dt1;
+            ra = ra + Rr * S.dt1;
+        }
+        if constexpr (NB == 5) ta = ta + Rt * S.dt1;
+        if (!S.last) {
+            W.u_acc[i] = ua;
+            if constexpr (!p1) { W.v_acc[i] = va; W.x_acc[i] = xa; W.y_acc[i] = ya; W.rho_acc[i] = ra; }
+            if constexpr (NB == 5) W.tem_acc[i] = ta;
+            if constexpr (!p1) {
+                xn = xo + my_u * S.dt2;
+                yn = yo + my_v * S.dt2;
+                vn = vo + Rv * S.dt2;
+                rn = ro + Rr * S.dt2;
+            }
+            un = uo + Ru * S.dt2;
+            if constexpr (NB == 5) tn = to + Rt * S.dt2;
+        } else {
+            un = ua;
+            if constexpr (!p1) { vn = va; xn = xa; yn = ya; rn = ra; }
+            if constexpr (NB == 5) tn = ta;
+        }
+    }
+    nxt.u[i] = un;
+    bool finite = isfinite(un);
+    if constexpr (!p1) {
+        nxt.x[i] = xn; nxt.y[i] = yn; nxt.v[i] = vn; nxt.rho[i] = rn;
+        nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
+        nxt.vol[i] = P.SP_mass / rn;
+        finite = finite && isfinite(xn) && isfinite(yn) && isfinite(vn) && isfinite(rn);
+    }
+    if constexpr (NB == 5) { nxt.tem[i] = tn; finite = finite && isfinite(tn); }
+    if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
+
+    if (S.do_scatter) {
+        const int nk = cell_key_mul(P, xn, yn, sc);
+        if (nk >= 0) W.key[i] = nk;
+        scatter_to_cell(P, Ln, gstart, nk, i, sc);
+    }
+    double red = 0.0;
+    if (S.last && S.do_umax) red = un * un + vn * vn;
+    if (S.last && S.do_steady) {
+        red = fabs(W.f_prev[i] - un);
+        W.f_prev[i] = un;
+    }
+    return red;
+}
+
+template <int NB, int G>
+__global__ void __launch_bounds__(128) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+                                               const Lst Ln, const int* __restrict__ gstart, const Work W,
+                                               const StageCfg S, Scalars* sc) {
+    if (halted(sc)) return;
+    constexpr int Q = 5;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / G;
+    const int lane = gt & (G - 1);
+    const bool active = i < P.num_int;
+
+    double my_x = 0, my_y = 0, my_u = 0, my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
+    int key = 0;
+    if (active) {
+        my_x = cur.x[i]; my_y = cur.y[i]; my_u = cur.u[i];
+        if constexpr (NB >= 4) { my_v = cur.v[i]; my_rho = cur.rho[i]; my_pre = cur.pre[i]; }
+        if constexpr (NB == 5) my_tem = cur.tem[i];
+        key = W.key[i];
+    }
+    double Mu[15];
+    double B[NB][Q];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+#pragma unroll
+        for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+    int cnt = 0;
+
+    if (active) {
+        for_candidates<G, false>(P, Lc, key, lane, [&](int j) {
+            if (j == i) return;
+            const double xji = __ldg(cur.x + j) - my_x;
+            const double yji = __ldg(cur.y + j) - my_y;
+            const double r2 = xji * xji + yji * yji;
+            if (r2 > P.h_eff_sq) return;
+            const double r = sqrt(r2);
+            const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
+            ++cnt;
+            const double VW = __ldg(cur.vol + j) * Wv;
+            double a[Q];
+            a[0] = xji * P.ih1;
+            a[1] = yji * P.ih1;
+            a[2] = (0.5 * (xji * xji)) * P.ih2A;
+            a[3] = (0.5 * (yji * yji)) * P.ih2A;
+            a[4] = (xji * yji) * P.ih2A;
+            double df[NB];
+            df[0] = __ldg(cur.u + j) - my_u;
+            if constexpr (NB >= 4) {
+                df[1] = __ldg(cur.v + j) - my_v;
+                df[2] = __ldg(cur.rho + j) - my_rho;
+                df[3] = __ldg(cur.pre + j) - my_pre;
+            }
+            if constexpr (NB == 5) df[4] = __ldg(cur.tem + j) - my_tem;
+#pragma unroll
+            for (int ii = 0; ii < Q; ++ii) {
+                const double VWa = VW * a[ii];
+#pragma unroll
+                for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, df[c], B[c][ii]);
+#pragma unroll
+                for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
+            }
+        });
+    }
+    if constexpr (G > 1) {
+#pragma unroll
+        for (int k = 0; k < 15; ++k) Mu[k] = group_sum<G>(Mu[k]);
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) B[c][k] = group_sum<G>(B[c][k]);
+        cnt = group_sum_i<G>(cnt);
+    }
+    double red = 0.0;   // this lane's contribution to the U_max / steady reductions
+    if (active && lane == 0)
+        red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem, Mu, B, cnt);
+    if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
+        warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
+}
+
+// =======================================================================================
+// k_ghost: interpolation at the virtual markers + extrapolation to the ghost particles.
+// WQ = 3 / 6: LS type B (interpolate_LSSPH_B_mod.f90, WALL_MODEL 2 / 3); WQ = 1: CSPH
+// (interpolate_CSPH_mod.f90, WALL_MODEL 1).  NB = 1 (problem 1: u), 3 (u,v,p), 4 (+T).
+// =======================================================================================
+template <int NB, int G, int WQ>
+__global__ void __launch_bounds__(128) k_ghost(const Phys P, const Fld F, const Lst L, const VMd V, Scalars* sc) {
+    if (halted(sc)) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int me = gt / G;
+    const int lane = gt & (G - 1);
+    const bool active = me < P.num_ext;
+    constexpr int Q = (WQ == 1) ? 1 : WQ;
+    constexpr int NU = Q * (Q + 1) / 2;
+    double my_x = 0, my_y = 0;
+    int key = 0;
+    if (active) { my_x = V.x[me]; my_y = V.y[me]; key = V.key[me]; }
+    double Mu[NU];
+    double B[NB][Q];
+    double sw = 0.0;
+#pragma unroll
+    for (int k = 0; k < NU; ++k) Mu[k] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+#pragma unroll
+        for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+    int cnt = 0;
+    if (active) {
+        for_candidates<G, true>(P, L, key, lane, [&](int j) {
+            if constexpr (WQ == 1) {
+                const double xij = my_x - __ldg(F.x + j), yij = my_y - __ldg(F.y + j);
+                const double r2 = xij * xij + yij * yij;
+                if (r2 > P.h_eff_sq) return;
+                const double Wv = dev_W(P.kt, sqrt(r2), P.h, P.wnorm);
+                ++cnt;
+                const double VW = __ldg(F.vol + j) * Wv;
+                sw = sw + VW;
+                B[0][0] = fma(VW, __ldg(F.u + j), B[0][0]);
+                if constexpr (NB >= 3) {
+                    B[1][0] = fma(VW, __ldg(F.v + j), B[1][0]);
+                    B[2][0] = fma(VW, __ldg(F.pre + j), B[2][0]);
+                }
+                if constexpr (NB == 4) B[3][0] = fma(VW, __ldg(F.tem + j), B[3][0]);
+            } else {
+                const double xji = __ldg(F.x + j) - my_x, yji = __ldg(F.y + j) - my_y;
+                const double r2 = xji * xji + yji * yji;
+                if (r2 > P.h_eff_sq) return;
+                const double Wv = dev_W(P.kt, sqrt(r2), P.h, P.wnorm);
+                ++cnt;
+                const double VW = __ldg(F.vol + j) * Wv;
+                double a[Q];
+                a[0] = 1.0;
+                a[1] = xji * P.ih1;
+                a[2] = yji * P.ih1;
+                if constexpr (Q == 6) {
+                    a[3] = ((xji * xji) * 0.5) * P.ih2B;
+                    a[4] = (xji * yji) * P.ih2B;
+                    a[5] = ((yji * yji) * 0.5) * P.ih2B;
+                }
+                double f[NB];
+                f[0] = __ldg(F.u + j);
+                if constexpr (NB >= 3) { f[1] = __ldg(F.v + j); f[2] = __ldg(F.pre + j); }
+                if constexpr (NB == 4) f[3] = __ldg(F.tem + j);
+#pragma unroll
+                for (int ii = 0; ii < Q; ++ii) {
+                    const double VWa = VW * a[ii];
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, f[c], B[c][ii]);
+#pragma unroll
+                    for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
+                }
+            }
+        });
+    }
+    if constexpr (G > 1) {
+#pragma unroll
+        for (int k = 0; k < NU; ++k) Mu[k] = group_sum<G>(Mu[k]);
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) B[c][k] = group_sum<G>(B[c][k]);
+        sw = group_sum<G>(sw);
+        cnt = group_sum_i<G>(cnt);
+    }
+    if (!active || lane != 0) return;
+
+    double val[4] = {0.0, 0.0, 0.0, 0.0};
+    if constexpr (WQ == 1) {
+        if (cnt > 0 && sw > 1.0e-12) {
+#pragma unroll
+            for (int c = 0; c < NB; ++c) val[c] = B[c][0] / sw;
+        }
+    } else {
+        if (cnt >= Q) {
+            double A[Q][Q];
+#pragma unroll
+            for (int r = 0; r < Q; ++r)
+#pragma unroll
+                for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
+            if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) val[c] = B[c][0];
+        }
+    }
+    const int you = P.num_int + me;
+    if constexpr (NB == 1) {   // extrapolate_diff_test_mod.f90:40-103
+        const double vu = val[0];
+        const int md = V.mode[me];
+        const double K = V.K[me];
+        double ug;
+        if (md == XM_COPY) ug = vu;
+        else if (md == XM_K_MINUS) ug = K - vu;
+        else if (md == XM_PLUS_K) ug = vu + K;
+        else ug = -vu;
+        V.u[me] = vu;
+        F.u[you] = ug;
+    } else {                   // extrapolate_VM_to_WL_mod.f90:40-271
+        const double vu = val[0], vv = val[1], vp = val[2], vt = val[3];
+        V.u[me] = vu; V.v[me] = vv; V.pre[me] = vp;
+        if constexpr (NB == 4) V.tem[me] = vt;
+        const double nx = V.nx[me], ny = V.ny[me];
+        const int t = V.ptype[me];
+        int ubc = 2, tbc = 0;
+        double Tw = 0.0, hydro = 0.0;
+        bool hyd = false;
+        if (t == 1) { ubc = P.u_bc_bottom; tbc = P.tem_bc_bottom; Tw = P.tem_bottom; hyd = true; hydro = P.hydro_coef_bottom; }
+        else if (t == 2) { ubc = P.u_bc_top; tbc = P.tem_bc_top; Tw = P.tem_top; hyd = true; hydro = P.hydro_coef_top; }
+        else if (t == 3) { ubc = P.u_bc_left; tbc = P.tem_bc_left; Tw = P.tem_left; }
+        else if (t == 4) { ubc = P.u_bc_right; tbc = P.tem_bc_right; Tw = P.tem_right; }
+        else if (t == 5 || t == 6) { ubc = 2; tbc = P.tem_bc_bottom; Tw = P.tem_bottom; hyd = true; hydro = P.hydro_coef_bottom; }
+        else { ubc = (P.u_bc_top == 3) ? 3 : 2; tbc = P.tem_bc_top; Tw = P.tem_top; hyd = true; hydro = P.hydro_coef_top; }
+        double ug, vg;
+        if (ubc == 1) {
+            const double u_n = vu * nx + vv * ny;
+            ug = vu - (2.0 * u_n) * nx;
+            vg = vv - (2.0 * u_n) * ny;
+        } else if (ubc == 3) {
+            ug = 2.0 * P.u_top - vu;
+            vg = -vv;
+        } else {
+            ug = -vu;
+            vg = -vv;
+        }
+        double pg = vp;
+        if constexpr (NB == 4) {
+            if (hyd && tbc == 1) pg = vp + hydro * (F.y[you] - my_y);
+        }
+        F.u[you] = ug; F.v[you] = vg; F.pre[you] = pg;
+        if constexpr (NB == 4) F.tem[you] = (tbc == 1) ? 2.0 * Tw - vt : vt;
+    }
+}
+
+// =======================================================================================
+// k_pst: particle shifting (q = 5) + copy-back + EOS + cell scatter.
+// NB = 3 (u,v,rho) or 4 (+T).  umax2 holds max(u^2+v^2) of the state being shifted.
+// =======================================================================================
+template <int NB, int G>
+__global__ void __launch_bounds__(128) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+                                             const Lst Ln, const int* __restrict__ gstart, const Work W,
+                                             Scalars* sc) {
+    if (halted(sc)) return;
+    constexpr int Q = 5;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / G;
+    const int lane = gt & (G - 1);
+    const bool active = i < P.num_int;
+    const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
+    const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
+
+    double my_x = 0, my_y = 0, my_u = 0, my_v = 0, my_rho = 0, my_tem = 0;
+    int key = 0;
+    if (active) {
+        my_x = cur.x[i]; my_y = cur.y[i]; my_u = cur.u[i]; my_v = cur.v[i]; my_rho = cur.rho[i];
+        if constexpr (NB == 4) my_tem = cur.tem[i];
+        key = W.key[i];
+    }
+    double Mu[15];
+    double B[NB][Q];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+#pragma unroll
+        for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+    double sx = 0.0, sy = 0.0;
+    int cnt = 0;
+    if (active) {
+        for_candidates<G, false>(P, Lc, key, lane, [&](int j) {
+            if (j == i) return;
+            const double xji = __ldg(cur.x + j) - my_x;
+            const double yji = __ldg(cur.y + j) - my_y;
+            const double r2 = xji * xji + yji * yji;
+            if (r2 > P.h_eff_sq) return;
+            const double r = sqrt(r2);
+            const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
+            const double dWdr = dev_dW(P.kt, r, P.h, P.wnorm);
+            ++cnt;
+            const double Vj = __ldg(cur.vol + j);
+            const double VW = Vj * Wv;
+            const double gx = ((dWdr * (-xji)) / r) * Vj;
+            const double gy = ((dWdr * (-yji)) / r) * Vj;
+            const double t = Wv / P.W_ave, t2 = t * t, t4 = t2 * t2;
+            const double fac = 1.0 + 0.2 * t4;
+            sx = fma(fac, gx, sx);
+            sy = fma(fac, gy, sy);
+            double a[Q];
+            a[0] = xji * P.ih1;
+            a[1] = yji * P.ih1;
+            a[2] = (0.5 * (xji * xji)) * P.ih2A;
+            a[3] = (0.5 * (yji * yji)) * P.ih2A;
+            a[4] = (xji * yji) * P.ih2A;
+            double df[NB];
+            df[0] = __ldg(cur.u + j) - my_u;
+            df[1] = __ldg(cur.v + j) - my_v;
+            df[2] = __ldg(cur.rho + j) - my_rho;
+            if constexpr (NB == 4) df[3] = __ldg(cur.tem + j) - my_tem;
+#pragma unroll
+            for (int ii = 0; ii < Q; ++ii) {
+                const double VWa = VW * a[ii];
+#pragma unroll
+                for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, df[c], B[c][ii]);
+#pragma unroll
+                for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
+            }
+        });
+    }
+    if constexpr (G > 1) {
+#pragma unroll
+        for (int k = 0; k < 15; ++k) Mu[k] = group_sum<G>(Mu[k]);
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) B[c][k] = group_sum<G>(B[c][k]);
+        sx = group_sum<G>(sx);
+        sy = group_sum<G>(sy);
+        cnt = group_sum_i<G>(cnt);
+    }
+    if (!active || lane != 0) return;
+
+    // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
+    double dx = -coe * sx, dy = -coe * sy;
+    const double rr = sqrt(dx * dx + dy * dy);
+    if (rr > 0.2 * P.h) {
+        dx = ((0.2 * P.h) * dx) / rr;
+        dy = ((0.2 * P.h) * dy) / rr;
+    }
+    const double xn = my_x + dx, yn = my_y + dy;
+    if (cnt >= Q) {
+        double A[Q][Q];
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+#pragma unroll
+            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
+        if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+    } else {
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+    }
+    double a[Q];
+    a[0] = dx * P.ih1;
+    a[1] = dy * P.ih1;
+    a[2] = (0.5 * (dx * dx)) * P.ih2A;
+    a[3] = (0.5 * (dy * dy)) * P.ih2A;
+    a[4] = (dx * dy) * P.ih2A;
+    double acc[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) s = fma(a[k], B[c][k], s);
+        acc[c] = s;
+    }
+    const double un = my_u + acc[0], vn = my_v + acc[1], rn = my_rho + acc[2];
+    nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
+    nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
+    nxt.vol[i] = P.SP_mass / rn;
+    bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
+    if constexpr (NB == 4) { const double tn = my_tem + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
+    if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
+    const int nk = cell_key_mul(P, xn, yn, sc);
+    if (nk >= 0) W.key[i] = nk;
+    scatter_to_cell(P, Ln, gstart, nk, i, sc);
+}
+
+// =======================================================================================
+// Cell-list kernels
+// =======================================================================================
+// Scatter the interior particles of the current positions (standalone update_cell).
+__global__ void k_scatter(const Phys P, const Fld F, const Lst Ln, const int* __restrict__ gstart, int* key,
+                          Scalars* sc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.num_int) return;
+    const int k = cell_key_mul(P, F.x[i], F.y[i], sc);
+    if (k >= 0) key[i] = k;
+    scatter_to_cell(P, Ln, gstart, k, i, sc);
+}
+
+// Finish a cell list: interior slots sorted by particle index, then the cell's ghosts.
+// Clears the scatter counter so the buffer can be scattered into again.
+__global__ void k_cellsort(const Phys P, const Lst L, const int* __restrict__ gstart, const int* __restrict__ glist,
+                           Scalars* sc, int reset_umax) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (reset_umax && c == 0) sc->umax2 = 0ull;
+    if (c >= P.ncell) return;
+    int nf = L.cnt[c];
+    L.cnt[c] = 0;
+    const int g0 = gstart[c], ng = gstart[c + 1] - g0;
+    const int lim = P.cap - ng;
+    if (nf > lim) nf = lim;
+    int* S = L.slots + (size_t)c * P.cap;
+    int buf[64];
+    for (int k = 0; k < nf; ++k) {
+        const int v = S[k];
+        int t = k;
+        while (t > 0 && buf[t - 1] > v) { buf[t] = buf[t - 1]; --t; }
+        buf[t] = v;
+    }
+    for (int k = 0; k < nf; ++k) S[k] = buf[k];
+    for (int k = 0; k < ng; ++k) S[nf + k] = glist[g0 + k];
+    L.num[c] = nf + ng;
+    L.fnum[c] = nf;
+}
+
+// =======================================================================================
+// Small kernels
+// =======================================================================================
+__global__ void k_umax(const Phys P, const Fld F, Scalars* sc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < P.num_int) v = F.u[i] * F.u[i] + F.v[i] * F.v[i];
+    warp_max_atomic(&sc->umax2, v);
+}
+
+__global__ void k_steady_max(const Phys P, const Fld F, const Work W, Scalars* sc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < P.num_int) v = fabs(W.f_prev[i] - F.u[i]);
+    warp_max_atomic(&sc->dfmax, v);
+}
+
+__global__ void k_copy_fprev(const Phys P, const Fld F, const Work W) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P.num_int) W.f_prev[i] = F.u[i];
+}
+
+// Problem 1 epilogue of a step (main.f90:139-149 with check_steady_state_mod.f90:39-65):
+// the stage kernel already reduced max|f_previous - u|.
+__global__ void k_epilogue(const Phys P, Scalars* sc) {
+    if (sc->err != 0 || sc->steady != 0) return;
+    sc->step_count += 1;
+    const double df = __longlong_as_double((long long)sc->dfmax);
+    if (df < P.threshold) {
+        sc->steady = 1;
+        sc->steady_step = sc->step_count;
+    }
+    sc->dfmax = 0ull;
+}
+
+__global__ void k_volume(const Phys P, const Fld F) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P.num_total) F.vol[i] = P.SP_mass / F.rho[i];
+}
+
+// In-radius neighbour lists for parity checks (unsorted, fixed stride per particle).
+__global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const int* key, const VMd V, int which,
+                            int stride, int* out, int* count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = which == 0 ? P.num_int : P.num_ext;
+    if (i >= n) return;
+    const double mx = which == 0 ? F.x[i] : V.x[i];
+    const double my = which == 0 ? F.y[i] : V.y[i];
+    const int k = which == 0 ? key[i] : V.key[i];
+    int c = 0;
+    auto f = [&](int j) {
+        if (which == 0 && j == i) return;
+        const double xj = F.x[j] - mx, yj = F.y[j] - my;
+        if (xj * xj + yj * yj > P.h_eff_sq) return;
+        if (c < stride) out[(size_t)i * stride + c] = j;
+        ++c;
+    };
+    if (which == 0) for_candidates<1, false>(P, L, k, 0, f);
+    else for_candidates<1, true>(P, L, k, 0, f);
+    count[i] = c;
+}
+
+}  // namespace lssph

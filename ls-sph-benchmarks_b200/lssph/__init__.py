@@ -1,0 +1,13 @@
+"""lssph -- Python host of the B200 LS-SPH engine (ctypes over include/lssph.h)."""
+from ._abi import (LIB_PATH, PRECISION_FP64, PRECISION_MIXED, LssphError, Params, exported_names,
+                   load)
+from .params import (boussinesq_params, cavity_params, check_param, default_params, diffusion_params,
+                     from_config, init_param, make_params, taylor_green_params, write_config_h)
+from .simulation import Simulation, State, read_data, setup_particles
+
+__all__ = [
+    "LIB_PATH", "PRECISION_FP64", "PRECISION_MIXED", "LssphError", "Params", "exported_names", "load",
+    "boussinesq_params", "cavity_params", "check_param", "default_params", "diffusion_params",
+    "from_config", "init_param", "make_params", "taylor_green_params", "write_config_h",
+    "Simulation", "State", "read_data", "setup_particles",
+]
