@@ -7,11 +7,14 @@
 //              see half-updated particles); vol = SP_mass / rho is kept beside rho
 //   work       x/y/u/v/rho/tem _old and _acc (RK4 accumulators), RHS arrays, f_previous,
 //              the problem-1 source term, int32 cell key, over num_int
-//   cell list  2 buffers x {cnt, num, fnum} over ncell + slots[ncell * cap] (int32)
-//   markers    virtual-marker positions, normals, keys and interpolated values
-// A time step of problems 2-4 is 15 kernels (4 x {stage, cellsort, ghost} + {pst,
-// cellsort, ghost}); problem 1 is 5 (2 x {stage, ghost} + epilogue).  Each step is
-// captured once in a CUDA graph and replayed.
+//   cell list  2 buffers x {cnt over ncell, slots[ncell * cap]} (int32), interior
+//              particles in scatter order; static ghost lists per cell (CSR)
+//   markers    virtual-marker positions, normals, keys and interpolated values, plus
+//              the static list of cell tiles that hold markers
+// Kernels work on tiles of 2 x 2 cells staged in shared memory.  A time step of
+// problems 2-4 is 10 kernels (4 x {stage, ghost} + {pst, ghost}); problem 1 is 5
+// (2 x {stage, ghost} + epilogue).  Each step is captured once in a CUDA graph and
+// replayed.
 
 #include <cuda_runtime.h>
 
@@ -47,6 +50,11 @@ struct lssph_handle {
     VMd V{};
     int* gstart = nullptr;
     int* glist = nullptr;
+    int ntx = 0, nty = 0, ntiles = 0;   // cell tiles
+    int nvt = 0;                        // tiles holding virtual markers
+    int *vt_tile = nullptr, *vt_start = nullptr, *vt_vm = nullptr;
+    size_t smem_bytes = 0;
+    bool preparing = false;             // launch helpers only set kernel attributes
     Scalars* sc = nullptr;
     int sb = 0, lb = 0;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -115,6 +123,13 @@ struct ProfScope {
     }
 };
 
+// Dynamic shared memory above 48 KB needs an opt-in per kernel; set once per
+// instantiation while the handle is prepared (never during graph capture).
+template <class K>
+void smem_optin(K kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8));
+}
+
 // ---- kernel dispatch on the lane count ---------------------------------------------------
 template <int NB>
 void launch_stage(lssph_handle* h, const StageCfg& S) {
@@ -124,13 +139,19 @@ void launch_stage(lssph_handle* h, const StageCfg& S) {
     const Lst& Lc = h->L[h->lb];
     const Lst& Ln = h->L[h->lb ^ 1];
     const int G = h->G;
-    const int grid = blocks_for((long)h->num_int * G, 128);
+    const int grid = h->ntiles;
+    const size_t sm = h->smem_bytes;
+#define LSSPH_STAGE(GG)                                                                                 \
+    if (h->preparing) { smem_optin(k_stage<NB, GG>); return; }                                         \
+    k_stage<NB, GG><<<grid, PPB * GG, sm, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, S, \
+                                                  h->sc, h->ntx)
     switch (G) {
-        case 1: k_stage<NB, 1><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
-        case 2: k_stage<NB, 2><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
-        case 8: k_stage<NB, 8><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
-        default: k_stage<NB, 4><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, S, h->sc); break;
+        case 1: LSSPH_STAGE(1); break;
+        case 2: LSSPH_STAGE(2); break;
+        case 8: LSSPH_STAGE(8); break;
+        default: LSSPH_STAGE(4); break;
     }
+#undef LSSPH_STAGE
     h->launch_counter++;
 }
 
@@ -140,33 +161,41 @@ void launch_stage_any(lssph_handle* h, const StageCfg& S) {
     else launch_stage<4>(h, S);
 }
 
+// zero_list >= 0: clear that list's scatter counters (the list the preceding stage read).
 template <int NB, int WQ>
-void launch_ghost_t(lssph_handle* h) {
+void launch_ghost_t(lssph_handle* h, int zero_list, int reset_umax) {
     ProfScope prof(h, LSSPH_KIND_GHOST);
     const Fld& F = h->F[h->sb];
     const Lst& L = h->L[h->lb];
     const int G = h->Gg;
-    const int grid = blocks_for((long)h->num_ext * G, 128);
+    const VMTiles VT{h->vt_tile, h->vt_start, h->vt_vm};
+    int* zc = zero_list >= 0 ? h->L[zero_list].cnt : nullptr;
+    const size_t sm = h->smem_bytes;
+#define LSSPH_GHOST(GG)                                                                                    \
+    if (h->preparing) { smem_optin(k_ghost<NB, GG, WQ>); return; }                                        \
+    k_ghost<NB, GG, WQ><<<h->nvt, PPB * GG, sm, h->stream>>>(h->P, F, L, h->gstart, h->glist, h->V, VT, h->ntx, zc, \
+                                                          reset_umax, h->sc)
     switch (G) {
-        case 1: k_ghost<NB, 1, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
-        case 2: k_ghost<NB, 2, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
-        case 8: k_ghost<NB, 8, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
-        default: k_ghost<NB, 4, WQ><<<grid, 128, 0, h->stream>>>(h->P, F, L, h->V, h->sc); break;
+        case 1: LSSPH_GHOST(1); break;
+        case 2: LSSPH_GHOST(2); break;
+        case 8: LSSPH_GHOST(8); break;
+        default: LSSPH_GHOST(4); break;
     }
+#undef LSSPH_GHOST
     h->launch_counter++;
 }
 
 template <int NB>
-void launch_ghost_nb(lssph_handle* h) {
-    if (h->wq == 1) launch_ghost_t<NB, 1>(h);
-    else if (h->wq == 6) launch_ghost_t<NB, 6>(h);
-    else launch_ghost_t<NB, 3>(h);
+void launch_ghost_nb(lssph_handle* h, int zero_list, int reset_umax) {
+    if (h->wq == 1) launch_ghost_t<NB, 1>(h, zero_list, reset_umax);
+    else if (h->wq == 6) launch_ghost_t<NB, 6>(h, zero_list, reset_umax);
+    else launch_ghost_t<NB, 3>(h, zero_list, reset_umax);
 }
 
-void launch_ghost(lssph_handle* h) {
-    if (h->nb_ghost == 1) launch_ghost_nb<1>(h);
-    else if (h->nb_ghost == 4) launch_ghost_nb<4>(h);
-    else launch_ghost_nb<3>(h);
+void launch_ghost(lssph_handle* h, int zero_list = -1, int reset_umax = 0) {
+    if (h->nb_ghost == 1) launch_ghost_nb<1>(h, zero_list, reset_umax);
+    else if (h->nb_ghost == 4) launch_ghost_nb<4>(h, zero_list, reset_umax);
+    else launch_ghost_nb<3>(h, zero_list, reset_umax);
 }
 
 template <int NB>
@@ -177,20 +206,18 @@ void launch_pst_t(lssph_handle* h) {
     const Lst& Lc = h->L[h->lb];
     const Lst& Ln = h->L[h->lb ^ 1];
     const int G = h->G;
-    const int grid = blocks_for((long)h->num_int * G, 128);
+    const size_t sm = h->smem_bytes;
+#define LSSPH_PST(GG)                                                                                       \
+    if (h->preparing) { smem_optin(k_pst<NB, GG>); return; }                                               \
+    k_pst<NB, GG><<<h->ntiles, PPB * GG, sm, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, h->sc, \
+                                                      h->ntx)
     switch (G) {
-        case 1: k_pst<NB, 1><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
-        case 2: k_pst<NB, 2><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
-        case 8: k_pst<NB, 8><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
-        default: k_pst<NB, 4><<<grid, 128, 0, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->W, h->sc); break;
+        case 1: LSSPH_PST(1); break;
+        case 2: LSSPH_PST(2); break;
+        case 8: LSSPH_PST(8); break;
+        default: LSSPH_PST(4); break;
     }
-    h->launch_counter++;
-}
-
-void launch_cellsort(lssph_handle* h, int list, int reset_umax) {
-    ProfScope prof(h, LSSPH_KIND_CELLSORT);
-    k_cellsort<<<blocks_for(h->grid.ncell, 128), 128, 0, h->stream>>>(h->P, h->L[list], h->gstart, h->glist, h->sc,
-                                                                          reset_umax);
+#undef LSSPH_PST
     h->launch_counter++;
 }
 
@@ -218,19 +245,30 @@ void enq_stage(lssph_handle* h, int stage, bool fused_step) {
     launch_stage_any(h, S);
     h->sb ^= 1;
     if (!h->p1) {
-        launch_cellsort(h, h->lb ^ 1, 0);
         h->lb ^= 1;
+        launch_ghost(h, h->lb ^ 1, 0);   // also clears the list the stage just consumed
+    } else {
+        launch_ghost(h);
     }
-    launch_ghost(h);
 }
 
 void enq_pst(lssph_handle* h) {
     if (h->has_tem) launch_pst_t<4>(h);
     else launch_pst_t<3>(h);
     h->sb ^= 1;
-    launch_cellsort(h, h->lb ^ 1, 1);
     h->lb ^= 1;
+    launch_ghost(h, h->lb ^ 1, 1);
+}
+
+// Set the shared-memory opt-in of every kernel instantiation this handle launches.
+void prepare_kernels(lssph_handle* h) {
+    h->preparing = true;
+    StageCfg S{};
+    launch_stage_any(h, S);
     launch_ghost(h);
+    if (h->has_tem) launch_pst_t<4>(h);
+    else launch_pst_t<3>(h);
+    h->preparing = false;
 }
 
 void enq_step(lssph_handle* h) {
@@ -249,9 +287,10 @@ int check_scalars(lssph_handle* h, Scalars* out) {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     CUDA_TRY(h, cudaMemcpy(&s, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost));
     if (out) *out = s;
+    // a NaN position also leaves the grid: report the root cause first
+    if (s.err & ERR_NONFINITE) return fail(h, LSSPH_E_NONFINITE, "a non-finite value appeared in the particle state");
     if (s.err & ERR_OUT_OF_DOMAIN) return fail(h, LSSPH_E_OUT_OF_DOMAIN, "a particle left the cell grid");
     if (s.err & ERR_CELL_OVERFLOW) return fail(h, LSSPH_E_CELL_OVERFLOW, "a cell holds more particles than its slot capacity");
-    if (s.err & ERR_NONFINITE) return fail(h, LSSPH_E_NONFINITE, "a non-finite value appeared in the particle state");
     return LSSPH_OK;
 }
 
@@ -265,7 +304,6 @@ int sync_check(lssph_handle* h) {
 int rebuild_cells(lssph_handle* h) {
     for (int b = 0; b < 2; ++b) CUDA_TRY(h, cudaMemsetAsync(h->L[b].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
     k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->gstart, h->W.key, h->sc);
-    launch_cellsort(h, h->lb, 0);
     return LSSPH_OK;
 }
 
@@ -388,7 +426,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         Fld& F = h->F[b];
         A(&F.x, N); A(&F.y, N); A(&F.u, N); A(&F.v, N); A(&F.rho, N); A(&F.pre, N); A(&F.tem, N); A(&F.vol, N);
         Lst& L = h->L[b];
-        A(&L.cnt, NC); A(&L.num, NC); A(&L.fnum, NC); A(&L.slots, NC * h->grid.cap);
+        A(&L.cnt, NC); A(&L.slots, NC * h->grid.cap);
     }
     Work& W = h->W;
     A(&W.x_old, NI); A(&W.y_old, NI); A(&W.u_old, NI); A(&W.v_old, NI); A(&W.rho_old, NI); A(&W.tem_old, NI);
@@ -400,6 +438,31 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     A(&V.K, NE); A(&V.ptype, NE); A(&V.key, NE); A(&V.mode, NE);
     A(&h->gstart, NC + 1); A(&h->glist, NE);
     A(&h->sc, 1);
+    // cell tiles and the tiles that hold virtual markers (grouped, ascending marker id)
+    h->ntx = (h->grid.nx + TX - 1) / TX;
+    h->nty = (h->grid.ny + TY - 1) / TY;
+    h->ntiles = h->ntx * h->nty;
+    h->smem_bytes = std::max(tile_smem_bytes(h->grid.cap, h->G), tile_smem_bytes(h->grid.cap, h->Gg));
+    std::vector<int32_t> vt_tile, vt_start, vt_vm(NE);
+    {
+        std::vector<std::vector<int32_t>> by_tile(h->ntiles);
+        for (size_t me = 0; me < NE; ++me) {
+            const int key = h->grid.vm_key[me];
+            const int cx = key % h->grid.nx, cy = key / h->grid.nx;
+            by_tile[(cx / TX) + (cy / TY) * h->ntx].push_back((int32_t)me);
+        }
+        size_t k = 0;
+        vt_start.push_back(0);
+        for (int t = 0; t < h->ntiles; ++t) {   // chunks of at most one pass per CTA
+            for (size_t b = 0; b < by_tile[t].size(); b += PPB) {
+                vt_tile.push_back(t);
+                for (size_t e = b; e < std::min(by_tile[t].size(), b + PPB); ++e) vt_vm[k++] = by_tile[t][e];
+                vt_start.push_back((int32_t)k);
+            }
+        }
+        h->nvt = (int)vt_tile.size();
+    }
+    A(&h->vt_tile, std::max(h->nvt, 1)); A(&h->vt_start, h->nvt + 1); A(&h->vt_vm, NE);
     if (!ok) { const std::string m = h->err; free_handle(h); return fail(nullptr, LSSPH_E_CUDA, m); }
 
     // ---- host-side constant arrays ----
@@ -447,15 +510,17 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     H2D(V.tem, zeros.data(), sizeof(double) * NE);
     H2D(h->gstart, h->grid.gstart.data(), sizeof(int32_t) * (NC + 1));
     H2D(h->glist, h->grid.glist.data(), sizeof(int32_t) * NE);
+    H2D(h->vt_tile, vt_tile.data(), sizeof(int32_t) * vt_tile.size());
+    H2D(h->vt_start, vt_start.data(), sizeof(int32_t) * vt_start.size());
+    H2D(h->vt_vm, vt_vm.data(), sizeof(int32_t) * NE);
     if (ok && cudaMemsetAsync(h->sc, 0, sizeof(Scalars), h->stream) != cudaSuccess) ok = false;
     if (ok && cudaMemsetAsync(W.key, 0, sizeof(int32_t) * NI, h->stream) != cudaSuccess) ok = false;
     for (int b = 0; b < 2 && ok; ++b) {
         if (cudaMemsetAsync(h->F[b].tem, 0, sizeof(double) * N, h->stream) != cudaSuccess) ok = false;
         if (cudaMemsetAsync(h->L[b].slots, 0xff, sizeof(int) * NC * h->grid.cap, h->stream) != cudaSuccess) ok = false;
-        if (cudaMemsetAsync(h->L[b].num, 0, sizeof(int) * NC, h->stream) != cudaSuccess) ok = false;
-        if (cudaMemsetAsync(h->L[b].fnum, 0, sizeof(int) * NC, h->stream) != cudaSuccess) ok = false;
     }
     if (!ok) { free_handle(h); return fail(nullptr, LSSPH_E_CUDA, "device initialisation failed"); }
+    prepare_kernels(h);
     if ((rc = upload_fields(h, x, y, u, v, rho, pre, tem)) != LSSPH_OK ||
         (rc = rebuild_cells(h)) != LSSPH_OK || (rc = sync_check(h)) != LSSPH_OK) {
         const std::string m = h->err;
@@ -510,10 +575,11 @@ int lssph_calculate_rhs(lssph_handle* h) {
 
 int lssph_update_cell(lssph_handle* h) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    CUDA_TRY(h, cudaMemsetAsync(h->L[h->lb ^ 1].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
     k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb ^ 1], h->gstart,
                                                                      h->W.key, h->sc);
-    launch_cellsort(h, h->lb ^ 1, 0);
     h->lb ^= 1;
+    CUDA_TRY(h, cudaMemsetAsync(h->L[h->lb ^ 1].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
     return sync_check(h);
 }
 
@@ -669,8 +735,8 @@ int lssph_neighbors_csr(lssph_handle* h, int32_t which, int32_t* offsets, int32_
     int *d_out = nullptr, *d_cnt = nullptr;
     CUDA_TRY(h, cudaMallocAsync((void**)&d_out, sizeof(int) * (size_t)n * stride, h->stream));
     CUDA_TRY(h, cudaMallocAsync((void**)&d_cnt, sizeof(int) * (size_t)n, h->stream));
-    k_neighbors<<<blocks_for(n, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->W.key, h->V, which,
-                                                           stride, d_out, d_cnt);
+    k_neighbors<<<blocks_for(n, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->gstart, h->glist,
+                                                           h->W.key, h->V, which, stride, d_out, d_cnt);
     std::vector<int> out((size_t)n * stride), cnt(n);
     CUDA_TRY(h, cudaMemcpyAsync(out.data(), d_out, sizeof(int) * out.size(), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost, h->stream));

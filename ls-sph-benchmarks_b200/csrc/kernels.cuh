@@ -4,12 +4,18 @@
 //   k_stage      calculate_RHS (LSSPH_A_mod.f90:26-271) fused with the RK2/RK4 stage
 //                update + EOS (RK2_mod.f90:87-108, RK4_mod.f90:109-159) and with the
 //                scatter half of update_cell (update_cell_mod.f90:40-70)
-//   k_cellsort   the rest of update_cell: per-cell list in reference order (interior
-//                particles by ascending index, then the static ghost list, :75-93)
 //   k_ghost      ghost (ghost_mod.f90:55-74): LS type-B / CSPH interpolation at each
 //                virtual marker + extrapolation to its ghost particle
 //   k_pst        shift_interpolate (shift_interpolate_mod.f90:23-300) fused with the
 //                PST copy-back + EOS (PST_mod.f90:85-99) and the cell scatter
+// The cell lists are left in scatter (atomic) order; every consumer rebuilds the
+// reference order of update_cell (interior particles by ascending index, then the static
+// ghost list, update_cell_mod.f90:49-93) while staging a tile in shared memory.
+//
+// Work decomposition: one CTA per tile of TX x TY cells.  The CTA stages the particles of
+// the (TX+2) x (TY+2) halo cells into shared memory with independent loads (all in
+// flight at once), then each particle of the tile's own cells runs its neighbour loop
+// out of shared memory: the 3x3 candidate cells of any own particle lie in the halo.
 //
 // Arithmetic follows the oracle's sequence: the file is compiled with -fmad=false so
 // no multiply-add is fused implicitly, and fma() appears only at the accumulation sites
@@ -59,8 +65,8 @@ struct Phys {
 struct Fld {   // SoA particle state over num_total
     double *x, *y, *u, *v, *rho, *pre, *tem, *vol;
 };
-struct Lst {   // fixed-capacity cell list: slots[c*cap + k]
-    int *cnt, *num, *fnum, *slots;
+struct Lst {   // interior particles per cell, scatter order: slots[c*cap + k], k < cnt[c]
+    int *cnt, *slots;
 };
 struct Work {  // per-interior-particle arrays
     double *x_old, *y_old, *u_old, *v_old, *rho_old, *tem_old;
@@ -174,10 +180,12 @@ __host__ __device__ constexpr int UT(int j, int i) { return i * (i + 1) / 2 + j;
 
 // Gaussian elimination with partial pivoting + substitutions, the DGESV restatement of
 // the oracle (first max |a| pivot, reciprocal column scaling, right-looking update).
-// A[row][col] is overwritten by LU; B[c][row] by the solution.  Returns false on a zero
-// pivot.
+// lu_factor overwrites A[row][col] by its LU factors and applies the row interchanges to
+// the NB right-hand sides in B[c][row]; lu_subst then solves one column in place.
+// Returns false on a zero pivot.  Row interchanges are rare for LS moment matrices, so
+// the swap code runs only when the pivot row differs from the diagonal one.
 template <int Q, int NB>
-__device__ __forceinline__ bool lu_solve(double (&A)[Q][Q], double (&B)[NB][Q]) {
+__device__ __forceinline__ bool lu_factor(double (&A)[Q][Q], double (&B)[NB][Q]) {
     bool ok = true;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
@@ -188,20 +196,22 @@ __device__ __forceinline__ bool lu_solve(double (&A)[Q][Q], double (&B)[NB][Q]) 
             const double a = fabs(A[i][k]);
             if (a > amax) { amax = a; p = i; }
         }
+        if (p != k) {   // selects, not indexing by p: A and B stay in registers
 #pragma unroll
-        for (int r = k + 1; r < Q; ++r) {
-            const bool s = (p == r);
+            for (int r = k + 1; r < Q; ++r) {
+                const bool sw = (p == r);
 #pragma unroll
-            for (int c = 0; c < Q; ++c) {
-                const double t0 = A[k][c], t1 = A[r][c];
-                A[k][c] = s ? t1 : t0;
-                A[r][c] = s ? t0 : t1;
-            }
+                for (int c = 0; c < Q; ++c) {
+                    const double t0 = A[k][c], t1 = A[r][c];
+                    A[k][c] = sw ? t1 : t0;
+                    A[r][c] = sw ? t0 : t1;
+                }
 #pragma unroll
-            for (int m = 0; m < NB; ++m) {
-                const double t0 = B[m][k], t1 = B[m][r];
-                B[m][k] = s ? t1 : t0;
-                B[m][r] = s ? t0 : t1;
+                for (int m = 0; m < NB; ++m) {
+                    const double t0 = B[m][k], t1 = B[m][r];
+                    B[m][k] = sw ? t1 : t0;
+                    B[m][r] = sw ? t0 : t1;
+                }
             }
         }
         const double piv = A[k][k];
@@ -217,20 +227,64 @@ __device__ __forceinline__ bool lu_solve(double (&A)[Q][Q], double (&B)[NB][Q]) 
 #pragma unroll
             for (int i = k + 1; i < Q; ++i) A[i][j] = fma(-A[i][k], A[k][j], A[i][j]);
     }
+    return ok;
+}
+
+template <int Q>
+__device__ __forceinline__ void lu_subst(const double (&A)[Q][Q], double (&b)[Q]) {
 #pragma unroll
-    for (int m = 0; m < NB; ++m) {
+    for (int k = 0; k < Q; ++k)
 #pragma unroll
-        for (int k = 0; k < Q; ++k)
+        for (int i = k + 1; i < Q; ++i) b[i] = fma(-b[k], A[i][k], b[i]);
 #pragma unroll
-            for (int i = k + 1; i < Q; ++i) B[m][i] = fma(-B[m][k], A[i][k], B[m][i]);
+    for (int k = Q - 1; k >= 0; --k) {
+        b[k] = b[k] / A[k][k];
 #pragma unroll
-        for (int k = Q - 1; k >= 0; --k) {
-            B[m][k] = B[m][k] / A[k][k];
+        for (int i = 0; i < k; ++i) b[i] = fma(-b[k], A[i][k], b[i]);
+    }
+}
+
+template <int Q, int NB>
+__device__ __forceinline__ bool lu_solve(double (&A)[Q][Q], double (&B)[NB][Q]) {
+    const bool ok = lu_factor<Q, NB>(A, B);
 #pragma unroll
-            for (int i = 0; i < k; ++i) B[m][i] = fma(-B[m][k], A[i][k], B[m][i]);
+    for (int m = 0; m < NB; ++m) lu_subst<Q>(A, B[m]);
+    return ok;
+}
+
+// Solve the NB columns spread over the G lanes of a group: every lane factorises (the
+// same instructions on the same data), lane l substitutes columns l, l+G, ...; on return
+// X[r] holds column lane + r*G of this lane.  Pass xfer = true to gather afterwards with
+// column_value().
+template <int Q, int NB, int G>
+__device__ __forceinline__ bool group_solve(double (&A)[Q][Q], double (&B)[NB][Q], int lane,
+                                            double (&X)[(NB + G - 1) / G][Q]) {
+    const bool ok = lu_factor<Q, NB>(A, B);
+#pragma unroll
+    for (int r = 0; r < (NB + G - 1) / G; ++r) {
+        const int col = lane + r * G;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            double v = B[0][k];
+#pragma unroll
+            for (int c = 1; c < NB; ++c) v = (col == c) ? B[c][k] : v;
+            X[r][k] = v;
         }
+        lu_subst<Q>(A, X[r]);
     }
     return ok;
+}
+
+// Entry k of solved column c, fetched from the lane of the group that solved it.  Every
+// lane of the warp must call this (the shuffle is warp-wide).
+template <int Q, int NB, int G>
+__device__ __forceinline__ double column_value(const double (&X)[(NB + G - 1) / G][Q], int c, int k) {
+    if constexpr (G == 1) {
+        return X[c][k];
+    } else {
+        const int src = (threadIdx.x & 31 & ~(G - 1)) + (c % G);
+        return __shfl_sync(0xffffffffu, X[c / G][k], src);
+    }
 }
 
 // Butterfly sum over aligned groups of G lanes; every lane of the group ends with the
@@ -248,28 +302,25 @@ __device__ __forceinline__ int group_sum_i(int v) {
     return v;
 }
 
-// Visit the candidates of cell `key` (3x3 cells in reference order, list order within a
-// cell).  Lane `lane` of a G-lane group takes every G-th candidate of the concatenated
-// list.  FLUID_ONLY restricts each cell to its interior-particle prefix.
-template <int G, bool FLUID_ONLY, class F>
-__device__ __forceinline__ void for_candidates(const Phys& P, const Lst& L, int key, int lane, F&& f) {
+// Visit the candidates of cell `key` (3x3 cells in reference order; within a cell the
+// interior particles in list order, then the cell's ghosts).  Used by the parity-only
+// neighbour listing, which sorts its output.
+template <bool FLUID_ONLY, class F>
+__device__ __forceinline__ void for_candidates(const Phys& P, const Lst& L, const int* gstart, const int* glist,
+                                               int key, F&& f) {
     const int cx = key % P.nx, cy = key / P.nx;
-    int base = 0;
-#pragma unroll 1
     for (int dy = -1; dy <= 1; ++dy) {
         const int yy = cy + dy;
         if (yy < 0 || yy >= P.ny) continue;
-#pragma unroll 1
         for (int dx = -1; dx <= 1; ++dx) {
             const int xx = cx + dx;
             if (xx < 0 || xx >= P.nx) continue;
             const int c = xx + yy * P.nx;
-            const int n = FLUID_ONLY ? __ldg(L.fnum + c) : __ldg(L.num + c);
-            const int* S = L.slots + (size_t)c * P.cap;
-            int t = (G == 1) ? 0 : ((lane - base) & (G - 1));
-#pragma unroll 1
-            for (; t < n; t += G) f(__ldg(S + t));
-            base += n;
+            const int ng = gstart[c + 1] - gstart[c];
+            const int nf = min(L.cnt[c], P.cap - ng);
+            for (int t = 0; t < nf; ++t) f(L.slots[(size_t)c * P.cap + t]);
+            if (!FLUID_ONLY)
+                for (int t = 0; t < ng; ++t) f(glist[gstart[c] + t]);
         }
     }
 }
@@ -301,60 +352,227 @@ __device__ __forceinline__ void warp_max_atomic(unsigned long long* dst, double 
 }
 
 // =======================================================================================
+// Tile staging in shared memory
+// =======================================================================================
+constexpr int TX = 2, TY = 2;               // own cells of a tile
+constexpr int HX = TX + 2, HY = TY + 2;     // halo cells
+constexpr int HC = HX * HY;                 // 16 halo cells
+constexpr int OC = TX * TY;                 // 4 own cells
+constexpr int PPB = 32;                     // particles per pass: a CTA has PPB * G threads
+static_assert(HC <= 32 && OC <= 32, "tile scans run in one warp");
+
+struct TileHdr {
+    int cnt[HC];        // staged particles per halo cell (interior + ghosts)
+    int nf[HC];         // interior prefix of each halo cell
+    int off[HC + 1];    // smem offset of each halo cell
+    int own_off[OC + 1];
+};
+
+// Dynamic shared memory: SoA fields of up to HC*cap staged particles, their global
+// indices, and the own-particle list.
+struct SmemView {
+    double *x, *y, *u, *v, *rho, *pre, *vol, *tem;
+    int *idx, *own_k, *own_hc;
+    int* nbr;   // in-radius lists, entry e of thread t at nbr[e * blockDim.x + t]
+};
+
+// Per-thread in-radius list length: a lane tests at most ceil(9 cap / G) candidates.
+__host__ __device__ inline int nbr_list_len(int cap, int G) { return (9 * cap + G - 1) / G; }
+
+__host__ __device__ inline size_t tile_smem_bytes(int cap, int G) {
+    const size_t maxp = (size_t)HC * cap, maxo = (size_t)OC * cap;
+    const size_t lists = (size_t)PPB * G * nbr_list_len(cap, G);
+    return maxp * (8 * sizeof(double) + sizeof(int)) + 2 * maxo * sizeof(int) + lists * sizeof(int);
+}
+
+__device__ __forceinline__ SmemView smem_view(void* raw, int cap) {
+    SmemView S;
+    const int maxp = HC * cap, maxo = OC * cap;
+    double* d = static_cast<double*>(raw);
+    S.x = d; S.y = d + maxp; S.u = d + 2 * maxp; S.v = d + 3 * maxp; S.rho = d + 4 * maxp;
+    S.pre = d + 5 * maxp; S.vol = d + 6 * maxp; S.tem = d + 7 * maxp;
+    int* q = reinterpret_cast<int*>(d + 8 * maxp);
+    S.idx = q; S.own_k = q + maxp; S.own_hc = q + maxp + maxo;
+    S.nbr = q + maxp + 2 * maxo;
+    return S;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += t;
+    }
+    return v;
+}
+
+// Stage the halo of the tile whose halo cell (0,0) is global cell (cx0, cy0): counts,
+// reference-order index lists (interior particles ascending, then the ghost list) and
+// the SoA fields of every staged particle.  Own particles are the interior particles of
+// the TX x TY own cells.  All global loads of a phase are independent of each other.
+template <bool FLUID_ONLY, bool WITH_TEM>
+__device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Lst& L, const int* __restrict__ gstart,
+                                           const int* __restrict__ glist, int cx0, int cy0, TileHdr& T,
+                                           const SmemView& S) {
+    const int tid = threadIdx.x;
+    int c = -1, g0 = 0;
+    if (tid < HC) {
+        const int cx = cx0 + tid % HX, cy = cy0 + tid / HX;
+        int nf = 0, ng = 0;
+        if (cx >= 0 && cx < P.nx && cy >= 0 && cy < P.ny) {
+            c = cx + cy * P.nx;
+            g0 = __ldg(gstart + c);
+            const int gc = __ldg(gstart + c + 1) - g0;
+            nf = min(__ldg(L.cnt + c), P.cap - gc);
+            ng = FLUID_ONLY ? 0 : gc;
+        }
+        T.nf[tid] = nf;
+        T.cnt[tid] = nf + ng;
+    }
+    __syncthreads();
+    if (tid < 32) {
+        const int v = tid < HC ? T.cnt[tid] : 0;
+        const int incl = warp_incl_scan(v);
+        if (tid < HC) T.off[tid + 1] = incl;
+        if (tid == 0) T.off[0] = 0;
+        int w = 0;
+        if (tid < OC) w = T.nf[(1 + tid % TX) + (1 + tid / TX) * HX];
+        const int inclw = warp_incl_scan(w);
+        if (tid < OC) T.own_off[tid + 1] = inclw;
+        if (tid == 0) T.own_off[0] = 0;
+    }
+    __syncthreads();
+    if (tid < HC && c >= 0) {
+        const int nf = T.nf[tid], ng = T.cnt[tid] - nf, base = T.off[tid];
+        const int* src = L.slots + (size_t)c * P.cap;
+        for (int k = 0; k < nf; ++k) S.idx[base + k] = __ldg(src + k);                // independent loads
+        for (int g = 0; g < ng; ++g) S.idx[base + nf + g] = __ldg(glist + g0 + g);
+        for (int k = 1; k < nf; ++k) {                                                  // then sort in smem
+            const int v = S.idx[base + k];
+            int t = k;
+            while (t > 0 && S.idx[base + t - 1] > v) { S.idx[base + t] = S.idx[base + t - 1]; --t; }
+            S.idx[base + t] = v;
+        }
+        const int hx = tid % HX, hy = tid / HX;
+        if (hx >= 1 && hx <= TX && hy >= 1 && hy <= TY) {
+            const int o = (hx - 1) + (hy - 1) * TX;
+            const int ob = T.own_off[o];
+            for (int k = 0; k < nf; ++k) { S.own_k[ob + k] = base + k; S.own_hc[ob + k] = tid; }
+        }
+    }
+    __syncthreads();
+    const int n = T.off[HC];
+    for (int k = tid; k < n; k += blockDim.x) {
+        const int j = S.idx[k];
+        S.x[k] = __ldg(F.x + j);
+        S.y[k] = __ldg(F.y + j);
+        S.u[k] = __ldg(F.u + j);
+        S.v[k] = __ldg(F.v + j);
+        S.rho[k] = __ldg(F.rho + j);
+        S.pre[k] = __ldg(F.pre + j);
+        S.vol[k] = __ldg(F.vol + j);
+        if (WITH_TEM) S.tem[k] = __ldg(F.tem + j);
+    }
+    __syncthreads();
+}
+
+// Visit the staged candidates of an own particle in halo cell hc: 3x3 cells in reference
+// order; lane `lane` of a G-lane group takes every G-th candidate of the concatenation.
+template <int G, class Fn>
+__device__ __forceinline__ void for_tile_candidates(const TileHdr& T, int hc, int lane, Fn&& f) {
+    int base = 0;
+#pragma unroll 1
+    for (int dy = -1; dy <= 1; ++dy) {
+#pragma unroll 1
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int h = hc + dx + dy * HX;
+            const int n = T.cnt[h], o = T.off[h];
+            int t = (G == 1) ? 0 : ((lane - base) & (G - 1));
+            for (; t < n; t += G) f(o + t);
+            base += n;
+        }
+    }
+}
+
+// Two-phase neighbour loop.  Phase A: the cutoff test r^2 <= h_eff^2 over this lane's
+// candidates (same arithmetic as the reference, LSSPH_A_mod.f90:121-124), appending the
+// hits in visiting order to this thread's list.  Phase B: the pair body over the list
+// only, so a warp no longer runs the full pair body for candidates that most of its
+// lanes reject.  skip = the particle's own staged position (me == you), or -1.
+template <int G, class Fn>
+__device__ __forceinline__ int for_tile_neighbours(const TileHdr& T, const SmemView& S, int hc, int lane, int skip,
+                                                   double mx, double my, double h_eff_sq, Fn&& f) {
+    int n = 0;
+    int* list = S.nbr + threadIdx.x;
+    const int stride = blockDim.x;
+    for_tile_candidates<G>(T, hc, lane, [&](int k) {
+        const double xji = S.x[k] - mx;
+        const double yji = S.y[k] - my;
+        if (k != skip && !(xji * xji + yji * yji > h_eff_sq)) { list[n * stride] = k; ++n; }
+    });
+#pragma unroll 1
+    for (int t = 0; t < n; ++t) f(list[t * stride]);
+    return n;
+}
+
+// Accumulate the LS type-A moment matrix (upper triangle) and b vectors of one pair
+// (LSSPH_A_mod.f90:136-190), df[c] = f_j - f_i.
+template <int NB>
+__device__ __forceinline__ void accumulate_A(double (&Mu)[15], double (&B)[NB][5], double VW, const double (&a)[5],
+                                             const double (&df)[NB]) {
+#pragma unroll
+    for (int ii = 0; ii < 5; ++ii) {
+        const double VWa = VW * a[ii];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, df[c], B[c][ii]);
+#pragma unroll
+        for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
+    }
+}
+
+__device__ __forceinline__ void basis_A(const Phys& P, double x, double y, double (&a)[5]) {
+    a[0] = x * P.ih1;
+    a[1] = y * P.ih1;
+    a[2] = (0.5 * (x * x)) * P.ih2A;
+    a[3] = (0.5 * (y * y)) * P.ih2A;
+    a[4] = (x * y) * P.ih2A;
+}
+
+template <int G, int N>
+__device__ __forceinline__ void group_reduce(double (&v)[N]) {
+    if constexpr (G > 1) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) v[k] = group_sum<G>(v[k]);
+    }
+}
+
+// =======================================================================================
 // k_stage: LS-SPH type-A RHS (q = 5, SPH_MODEL 3) + RK stage update + cell scatter.
 // NB = number of b-vector columns: 1 (problem 1: u only), 4 (u,v,rho,p), 5 (+T).
 // =======================================================================================
-// Lane-0 tail of k_stage: solve, RHS, stage update, scatter.  Returns this particle's
-// value for the U_max / steady-state max reductions.
+// Lane-0 tail of k_stage: RHS, stage update, scatter.  d[c][k] are the derivatives of
+// field c.  Returns this particle's value for the U_max / steady-state max reductions.
 template <int NB>
 __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, const Lst& Ln,
                                                const int* __restrict__ gstart, const Work& W, const StageCfg& S,
                                                Scalars* sc, int i, double my_x, double my_y, double my_u,
-                                               double my_v, double my_rho, double my_tem, const double (&Mu)[15],
-                                               double (&B)[NB][5], int cnt) {
-    constexpr int Q = 5;
-    double d[NB][Q];
-    if (cnt >= Q) {
-        double A[Q][Q];
-#pragma unroll
-        for (int r = 0; r < Q; ++r)
-#pragma unroll
-            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
-        if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            d[c][0] = B[c][0] * P.ih1;
-            d[c][1] = B[c][1] * P.ih1;
-            d[c][2] = B[c][2] * P.ih2A;
-            d[c][3] = B[c][3] * P.ih2A;
-            d[c][4] = B[c][4] * P.ih2A;
-        }
-    } else {
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-#pragma unroll
-            for (int k = 0; k < Q; ++k) d[c][k] = 0.0;
-    }
-
+                                               double my_v, double my_rho, double my_tem, const double (&d)[NB][5]) {
     // ---- RHS (LSSPH_A_mod.f90:246-269) ----
     double Ru, Rv = 0.0, Rr = 0.0, Rt = 0.0;
     if constexpr (NB == 1) {
         Ru = (d[0][2] + d[0][3]) + W.src[i];
     } else {
-        const double* du = d[0];
-        const double* dv = d[1];
-        const double* drho = d[2];
-        const double* dpre = d[3];
-        Rr = -(my_rho * (du[0] + dv[1])) + P.delta * (drho[2] + drho[3]);
-        Ru = -(dpre[0] / my_rho) + (P.vis_ref / my_rho) * (du[2] + du[3]);
-        Rv = -(dpre[1] / my_rho) + (P.vis_ref / my_rho) * (dv[2] + dv[3]);
+        // d[0] = u, d[1] = v, d[2] = rho, d[3] = p (, d[4] = T); entries x, y, xx, yy, xy
+        Rr = -(my_rho * (d[0][0] + d[1][1])) + P.delta * (d[2][2] + d[2][3]);
+        Ru = -(d[3][0] / my_rho) + (P.vis_ref / my_rho) * (d[0][2] + d[0][3]);
+        Rv = -(d[3][1] / my_rho) + (P.vis_ref / my_rho) * (d[1][2] + d[1][3]);
         Rr = Rr / P.zeta_sq;
         if constexpr (NB == 5) {
-            const double* dtem = d[4];
             Rv = Rv + ((P.alpha_ref * (my_tem - P.tem_ave)) * P.gravity);
             Ru = Ru / P.xi_sq;
             Rv = Rv / P.xi_sq;
-            Rt = P.thermal_dif * (dtem[2] + dtem[3]);
+            Rt = P.thermal_dif * (d[NB - 1][2] + d[NB - 1][3]);
         }
     }
     if (S.write_rhs) {
@@ -449,102 +667,132 @@ __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, co
 }
 
 template <int NB, int G>
-__global__ void __launch_bounds__(128) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
-                                               const Lst Ln, const int* __restrict__ gstart, const Work W,
-                                               const StageCfg S, Scalars* sc) {
+__global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+                                                   const Lst Ln, const int* __restrict__ gstart,
+                                                   const int* __restrict__ glist, const Work W, const StageCfg S,
+                                                   Scalars* sc, int ntx) {
     if (halted(sc)) return;
     constexpr int Q = 5;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gt / G;
-    const int lane = gt & (G - 1);
-    const bool active = i < P.num_int;
-
-    double my_x = 0, my_y = 0, my_u = 0, my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
-    int key = 0;
-    if (active) {
-        my_x = cur.x[i]; my_y = cur.y[i]; my_u = cur.u[i];
-        if constexpr (NB >= 4) { my_v = cur.v[i]; my_rho = cur.rho[i]; my_pre = cur.pre[i]; }
-        if constexpr (NB == 5) my_tem = cur.tem[i];
-        key = W.key[i];
-    }
-    double Mu[15];
-    double B[NB][Q];
+    constexpr int NR = (NB + G - 1) / G;
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemView SM = smem_view(smem_raw, P.cap);
+    const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+    stage_halo<false, NB == 5>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    const int n_own = T.own_off[OC];
+    const int lane = threadIdx.x & (G - 1);
+    for (int ob = 0; ob < n_own; ob += PPB) {
+        const int o = ob + (int)threadIdx.x / G;
+        const bool active = o < n_own;
+        int ki = 0, hc = 0;
+        if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+        const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
+        double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
+        if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
+        if constexpr (NB == 5) my_tem = SM.tem[ki];
+        double Mu[15];
+        double B[NB][Q];
 #pragma unroll
-    for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
-#pragma unroll
-    for (int c = 0; c < NB; ++c)
-#pragma unroll
-        for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
-    int cnt = 0;
-
-    if (active) {
-        for_candidates<G, false>(P, Lc, key, lane, [&](int j) {
-            if (j == i) return;
-            const double xji = __ldg(cur.x + j) - my_x;
-            const double yji = __ldg(cur.y + j) - my_y;
-            const double r2 = xji * xji + yji * yji;
-            if (r2 > P.h_eff_sq) return;
-            const double r = sqrt(r2);
-            const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
-            ++cnt;
-            const double VW = __ldg(cur.vol + j) * Wv;
-            double a[Q];
-            a[0] = xji * P.ih1;
-            a[1] = yji * P.ih1;
-            a[2] = (0.5 * (xji * xji)) * P.ih2A;
-            a[3] = (0.5 * (yji * yji)) * P.ih2A;
-            a[4] = (xji * yji) * P.ih2A;
-            double df[NB];
-            df[0] = __ldg(cur.u + j) - my_u;
-            if constexpr (NB >= 4) {
-                df[1] = __ldg(cur.v + j) - my_v;
-                df[2] = __ldg(cur.rho + j) - my_rho;
-                df[3] = __ldg(cur.pre + j) - my_pre;
-            }
-            if constexpr (NB == 5) df[4] = __ldg(cur.tem + j) - my_tem;
-#pragma unroll
-            for (int ii = 0; ii < Q; ++ii) {
-                const double VWa = VW * a[ii];
-#pragma unroll
-                for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, df[c], B[c][ii]);
-#pragma unroll
-                for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
-            }
-        });
-    }
-    if constexpr (G > 1) {
-#pragma unroll
-        for (int k = 0; k < 15; ++k) Mu[k] = group_sum<G>(Mu[k]);
+        for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
 #pragma unroll
         for (int c = 0; c < NB; ++c)
 #pragma unroll
-            for (int k = 0; k < Q; ++k) B[c][k] = group_sum<G>(B[c][k]);
-        cnt = group_sum_i<G>(cnt);
+            for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+        int cnt = 0;
+        if (active) {
+            cnt = for_tile_neighbours<G>(T, SM, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+                const double xji = SM.x[k] - my_x;
+                const double yji = SM.y[k] - my_y;
+                const double r = sqrt(xji * xji + yji * yji);
+                const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
+                const double VW = SM.vol[k] * Wv;
+                double a[Q];
+                basis_A(P, xji, yji, a);
+                double df[NB];
+                df[0] = SM.u[k] - my_u;
+                if constexpr (NB >= 4) {
+                    df[1] = SM.v[k] - my_v;
+                    df[2] = SM.rho[k] - my_rho;
+                    df[3] = SM.pre[k] - my_pre;
+                }
+                if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
+                accumulate_A<NB>(Mu, B, VW, a, df);
+            });
+        }
+        group_reduce<G>(Mu);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
+        if constexpr (G > 1) cnt = group_sum_i<G>(cnt);
+
+        // ---- solve (DGESV, LSSPH_A_mod.f90:208-241): columns spread over the lanes ----
+        double X[NR][Q];
+        double A[Q][Q];
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+#pragma unroll
+            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
+        if (!group_solve<Q, NB, G>(A, B, lane, X) && active && cnt >= Q && lane == 0) atomicOr(&sc->warn, WARN_SINGULAR);
+        double d[NB][Q];
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                const double bv = column_value<Q, NB, G>(X, c, k);
+                d[c][k] = (cnt >= Q) ? bv * (k < 2 ? P.ih1 : P.ih2A) : 0.0;
+            }
+        double red = 0.0;
+        if (active && lane == 0)
+            red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, SM.idx[ki], my_x, my_y, my_u, my_v, my_rho, my_tem, d);
+        if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
+            warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
     }
-    double red = 0.0;   // this lane's contribution to the U_max / steady reductions
-    if (active && lane == 0)
-        red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem, Mu, B, cnt);
-    if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
-        warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
 }
 
 // =======================================================================================
 // k_ghost: interpolation at the virtual markers + extrapolation to the ghost particles.
 // WQ = 3 / 6: LS type B (interpolate_LSSPH_B_mod.f90, WALL_MODEL 2 / 3); WQ = 1: CSPH
 // (interpolate_CSPH_mod.f90, WALL_MODEL 1).  NB = 1 (problem 1: u), 3 (u,v,p), 4 (+T).
+// One CTA per chunk of at most PPB markers of one tile; also clears the scatter counters
+// of the cell list the preceding stage consumed (zero_cnt) and, after PST, the U_max slot.
 // =======================================================================================
+struct VMTiles {
+    const int* tile;    // [n] tile id of each chunk
+    const int* start;   // [n+1] chunk ranges into vm
+    const int* vm;      // virtual-marker ids grouped by tile, ascending
+};
+
 template <int NB, int G, int WQ>
-__global__ void __launch_bounds__(128) k_ghost(const Phys P, const Fld F, const Lst L, const VMd V, Scalars* sc) {
+__global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, const Lst L,
+                                                   const int* __restrict__ gstart, const int* __restrict__ glist,
+                                                   const VMd V, const VMTiles VT, int ntx, int* zero_cnt,
+                                                   int reset_umax, Scalars* sc) {
+    if (zero_cnt) {
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < P.ncell; c += gridDim.x * blockDim.x) zero_cnt[c] = 0;
+    }
+    if (reset_umax && blockIdx.x == 0 && threadIdx.x == 0) sc->umax2 = 0ull;
     if (halted(sc)) return;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int me = gt / G;
-    const int lane = gt & (G - 1);
-    const bool active = me < P.num_ext;
     constexpr int Q = (WQ == 1) ? 1 : WQ;
     constexpr int NU = Q * (Q + 1) / 2;
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemView SM = smem_view(smem_raw, P.cap);
+    const int tile = VT.tile[blockIdx.x];
+    const int tx = tile % ntx, ty = tile / ntx;
+    const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
+    stage_halo<true, NB == 4>(P, F, L, gstart, glist, cx0, cy0, T, SM);
+    const int v0 = VT.start[blockIdx.x], nvm = VT.start[blockIdx.x + 1] - v0;
+    const int lane = threadIdx.x & (G - 1);
+    const int o = (int)threadIdx.x / G;
+    const bool active = o < nvm;
+    int me = 0, hc = 0;
     double my_x = 0, my_y = 0;
-    int key = 0;
-    if (active) { my_x = V.x[me]; my_y = V.y[me]; key = V.key[me]; }
+    if (active) {
+        me = VT.vm[v0 + o];
+        my_x = V.x[me];
+        my_y = V.y[me];
+        const int key = V.key[me];
+        hc = (key % P.nx - cx0) + (key / P.nx - cy0) * HX;
+    }
     double Mu[NU];
     double B[NB][Q];
     double sw = 0.0;
@@ -555,60 +803,59 @@ __global__ void __launch_bounds__(128) k_ghost(const Phys P, const Fld F, const 
 #pragma unroll
         for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
     int cnt = 0;
-    if (active) {
-        for_candidates<G, true>(P, L, key, lane, [&](int j) {
+    if (active && WQ != 1) {
+        cnt = for_tile_neighbours<G>(T, SM, hc, lane, -1, my_x, my_y, P.h_eff_sq, [&](int k) {
+            const double xji = SM.x[k] - my_x, yji = SM.y[k] - my_y;
+            const double Wv = dev_W(P.kt, sqrt(xji * xji + yji * yji), P.h, P.wnorm);
+            const double VW = SM.vol[k] * Wv;
+            double a[Q];
+            a[0] = 1.0;
+            if constexpr (Q >= 3) {
+                a[1 % Q] = xji * P.ih1;
+                a[2 % Q] = yji * P.ih1;
+            }
+            if constexpr (Q == 6) {
+                a[3] = ((xji * xji) * 0.5) * P.ih2B;
+                a[4] = (xji * yji) * P.ih2B;
+                a[5] = ((yji * yji) * 0.5) * P.ih2B;
+            }
+            double f[NB];
+            f[0] = SM.u[k];
+            if constexpr (NB >= 3) { f[1] = SM.v[k]; f[2] = SM.pre[k]; }
+            if constexpr (NB == 4) f[3] = SM.tem[k];
+#pragma unroll
+            for (int ii = 0; ii < Q; ++ii) {
+                const double VWa = VW * a[ii];
+#pragma unroll
+                for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, f[c], B[c][ii]);
+#pragma unroll
+                for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
+            }
+        });
+    }
+    if (active && WQ == 1) {
+        for_tile_candidates<G>(T, hc, lane, [&](int k) {
             if constexpr (WQ == 1) {
-                const double xij = my_x - __ldg(F.x + j), yij = my_y - __ldg(F.y + j);
+                const double xij = my_x - SM.x[k], yij = my_y - SM.y[k];
                 const double r2 = xij * xij + yij * yij;
                 if (r2 > P.h_eff_sq) return;
                 const double Wv = dev_W(P.kt, sqrt(r2), P.h, P.wnorm);
                 ++cnt;
-                const double VW = __ldg(F.vol + j) * Wv;
+                const double VW = SM.vol[k] * Wv;
                 sw = sw + VW;
-                B[0][0] = fma(VW, __ldg(F.u + j), B[0][0]);
+                B[0][0] = fma(VW, SM.u[k], B[0][0]);
                 if constexpr (NB >= 3) {
-                    B[1][0] = fma(VW, __ldg(F.v + j), B[1][0]);
-                    B[2][0] = fma(VW, __ldg(F.pre + j), B[2][0]);
+                    B[1][0] = fma(VW, SM.v[k], B[1][0]);
+                    B[2][0] = fma(VW, SM.pre[k], B[2][0]);
                 }
-                if constexpr (NB == 4) B[3][0] = fma(VW, __ldg(F.tem + j), B[3][0]);
-            } else {
-                const double xji = __ldg(F.x + j) - my_x, yji = __ldg(F.y + j) - my_y;
-                const double r2 = xji * xji + yji * yji;
-                if (r2 > P.h_eff_sq) return;
-                const double Wv = dev_W(P.kt, sqrt(r2), P.h, P.wnorm);
-                ++cnt;
-                const double VW = __ldg(F.vol + j) * Wv;
-                double a[Q];
-                a[0] = 1.0;
-                a[1] = xji * P.ih1;
-                a[2] = yji * P.ih1;
-                if constexpr (Q == 6) {
-                    a[3] = ((xji * xji) * 0.5) * P.ih2B;
-                    a[4] = (xji * yji) * P.ih2B;
-                    a[5] = ((yji * yji) * 0.5) * P.ih2B;
-                }
-                double f[NB];
-                f[0] = __ldg(F.u + j);
-                if constexpr (NB >= 3) { f[1] = __ldg(F.v + j); f[2] = __ldg(F.pre + j); }
-                if constexpr (NB == 4) f[3] = __ldg(F.tem + j);
-#pragma unroll
-                for (int ii = 0; ii < Q; ++ii) {
-                    const double VWa = VW * a[ii];
-#pragma unroll
-                    for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, f[c], B[c][ii]);
-#pragma unroll
-                    for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
-                }
+                if constexpr (NB == 4) B[3][0] = fma(VW, SM.tem[k], B[3][0]);
             }
         });
     }
+    group_reduce<G>(Mu);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
     if constexpr (G > 1) {
-#pragma unroll
-        for (int k = 0; k < NU; ++k) Mu[k] = group_sum<G>(Mu[k]);
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-#pragma unroll
-            for (int k = 0; k < Q; ++k) B[c][k] = group_sum<G>(B[c][k]);
         sw = group_sum<G>(sw);
         cnt = group_sum_i<G>(cnt);
     }
@@ -685,137 +932,119 @@ __global__ void __launch_bounds__(128) k_ghost(const Phys P, const Fld F, const 
 // NB = 3 (u,v,rho) or 4 (+T).  umax2 holds max(u^2+v^2) of the state being shifted.
 // =======================================================================================
 template <int NB, int G>
-__global__ void __launch_bounds__(128) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
-                                             const Lst Ln, const int* __restrict__ gstart, const Work W,
-                                             Scalars* sc) {
+__global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+                                                 const Lst Ln, const int* __restrict__ gstart,
+                                                 const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
     if (halted(sc)) return;
     constexpr int Q = 5;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gt / G;
-    const int lane = gt & (G - 1);
-    const bool active = i < P.num_int;
+    constexpr int NR = (NB + G - 1) / G;
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemView SM = smem_view(smem_raw, P.cap);
+    const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+    stage_halo<false, NB == 4>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    const int n_own = T.own_off[OC];
     const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
     const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
-
-    double my_x = 0, my_y = 0, my_u = 0, my_v = 0, my_rho = 0, my_tem = 0;
-    int key = 0;
-    if (active) {
-        my_x = cur.x[i]; my_y = cur.y[i]; my_u = cur.u[i]; my_v = cur.v[i]; my_rho = cur.rho[i];
-        if constexpr (NB == 4) my_tem = cur.tem[i];
-        key = W.key[i];
-    }
-    double Mu[15];
-    double B[NB][Q];
+    const int lane = threadIdx.x & (G - 1);
+    for (int ob = 0; ob < n_own; ob += PPB) {
+        const int o = ob + (int)threadIdx.x / G;
+        const bool active = o < n_own;
+        int ki = 0, hc = 0;
+        if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+        const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
+        double my_tem = 0.0;
+        if constexpr (NB == 4) my_tem = SM.tem[ki];
+        double Mu[15];
+        double B[NB][Q];
 #pragma unroll
-    for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
-#pragma unroll
-    for (int c = 0; c < NB; ++c)
-#pragma unroll
-        for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
-    double sx = 0.0, sy = 0.0;
-    int cnt = 0;
-    if (active) {
-        for_candidates<G, false>(P, Lc, key, lane, [&](int j) {
-            if (j == i) return;
-            const double xji = __ldg(cur.x + j) - my_x;
-            const double yji = __ldg(cur.y + j) - my_y;
-            const double r2 = xji * xji + yji * yji;
-            if (r2 > P.h_eff_sq) return;
-            const double r = sqrt(r2);
-            const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
-            const double dWdr = dev_dW(P.kt, r, P.h, P.wnorm);
-            ++cnt;
-            const double Vj = __ldg(cur.vol + j);
-            const double VW = Vj * Wv;
-            const double gx = ((dWdr * (-xji)) / r) * Vj;
-            const double gy = ((dWdr * (-yji)) / r) * Vj;
-            const double t = Wv / P.W_ave, t2 = t * t, t4 = t2 * t2;
-            const double fac = 1.0 + 0.2 * t4;
-            sx = fma(fac, gx, sx);
-            sy = fma(fac, gy, sy);
-            double a[Q];
-            a[0] = xji * P.ih1;
-            a[1] = yji * P.ih1;
-            a[2] = (0.5 * (xji * xji)) * P.ih2A;
-            a[3] = (0.5 * (yji * yji)) * P.ih2A;
-            a[4] = (xji * yji) * P.ih2A;
-            double df[NB];
-            df[0] = __ldg(cur.u + j) - my_u;
-            df[1] = __ldg(cur.v + j) - my_v;
-            df[2] = __ldg(cur.rho + j) - my_rho;
-            if constexpr (NB == 4) df[3] = __ldg(cur.tem + j) - my_tem;
-#pragma unroll
-            for (int ii = 0; ii < Q; ++ii) {
-                const double VWa = VW * a[ii];
-#pragma unroll
-                for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, df[c], B[c][ii]);
-#pragma unroll
-                for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
-            }
-        });
-    }
-    if constexpr (G > 1) {
-#pragma unroll
-        for (int k = 0; k < 15; ++k) Mu[k] = group_sum<G>(Mu[k]);
+        for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
 #pragma unroll
         for (int c = 0; c < NB; ++c)
 #pragma unroll
-            for (int k = 0; k < Q; ++k) B[c][k] = group_sum<G>(B[c][k]);
-        sx = group_sum<G>(sx);
-        sy = group_sum<G>(sy);
-        cnt = group_sum_i<G>(cnt);
-    }
-    if (!active || lane != 0) return;
+            for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+        double sxy[2] = {0.0, 0.0};
+        int cnt = 0;
+        if (active) {
+            cnt = for_tile_neighbours<G>(T, SM, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+                const double xji = SM.x[k] - my_x;
+                const double yji = SM.y[k] - my_y;
+                const double r = sqrt(xji * xji + yji * yji);
+                const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
+                const double dWdr = dev_dW(P.kt, r, P.h, P.wnorm);
+                const double Vj = SM.vol[k];
+                const double VW = Vj * Wv;
+                const double gx = ((dWdr * (-xji)) / r) * Vj;
+                const double gy = ((dWdr * (-yji)) / r) * Vj;
+                const double t = Wv / P.W_ave, t2 = t * t, t4 = t2 * t2;
+                const double fac = 1.0 + 0.2 * t4;
+                sxy[0] = fma(fac, gx, sxy[0]);
+                sxy[1] = fma(fac, gy, sxy[1]);
+                double a[Q];
+                basis_A(P, xji, yji, a);
+                double df[NB];
+                df[0] = SM.u[k] - my_u;
+                df[1] = SM.v[k] - my_v;
+                df[2] = SM.rho[k] - my_rho;
+                if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
+                accumulate_A<NB>(Mu, B, VW, a, df);
+            });
+        }
+        group_reduce<G>(Mu);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
+        group_reduce<G>(sxy);
+        if constexpr (G > 1) cnt = group_sum_i<G>(cnt);
 
-    // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
-    double dx = -coe * sx, dy = -coe * sy;
-    const double rr = sqrt(dx * dx + dy * dy);
-    if (rr > 0.2 * P.h) {
-        dx = ((0.2 * P.h) * dx) / rr;
-        dy = ((0.2 * P.h) * dy) / rr;
-    }
-    const double xn = my_x + dx, yn = my_y + dy;
-    if (cnt >= Q) {
+        // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
+        double dx = -coe * sxy[0], dy = -coe * sxy[1];
+        const double rr = sqrt(dx * dx + dy * dy);
+        if (rr > 0.2 * P.h) {
+            dx = ((0.2 * P.h) * dx) / rr;
+            dy = ((0.2 * P.h) * dy) / rr;
+        }
+        double X[NR][Q];
         double A[Q][Q];
 #pragma unroll
         for (int r = 0; r < Q; ++r)
 #pragma unroll
             for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
-        if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
-    } else {
+        if (!group_solve<Q, NB, G>(A, B, lane, X) && active && cnt >= Q && lane == 0) atomicOr(&sc->warn, WARN_SINGULAR);
+        // interpolation a(dr) . d for the columns this lane solved (shift_interpolate_mod.f90:255-298)
+        double a[Q];
+        basis_A(P, dx, dy, a);
+        double accr[NR];
 #pragma unroll
-        for (int c = 0; c < NB; ++c)
+        for (int r = 0; r < NR; ++r) {
+            double s = 0.0;
 #pragma unroll
-            for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+            for (int k = 0; k < Q; ++k) s = fma(a[k], (cnt >= Q) ? X[r][k] : 0.0, s);
+            accr[r] = s;
+        }
+        double acc[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            if constexpr (G == 1) acc[c] = accr[c];
+            else acc[c] = __shfl_sync(0xffffffffu, accr[c / G], (threadIdx.x & 31 & ~(G - 1)) + (c % G));
+        }
+        if (!active || lane != 0) continue;
+        const int i = SM.idx[ki];
+        const double xn = my_x + dx, yn = my_y + dy;
+        const double un = my_u + acc[0], vn = my_v + acc[1], rn = my_rho + acc[2];
+        nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
+        nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
+        nxt.vol[i] = P.SP_mass / rn;
+        bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
+        if constexpr (NB == 4) { const double tn = my_tem + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
+        if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
+        const int nk = cell_key_mul(P, xn, yn, sc);
+        if (nk >= 0) W.key[i] = nk;
+        scatter_to_cell(P, Ln, gstart, nk, i, sc);
     }
-    double a[Q];
-    a[0] = dx * P.ih1;
-    a[1] = dy * P.ih1;
-    a[2] = (0.5 * (dx * dx)) * P.ih2A;
-    a[3] = (0.5 * (dy * dy)) * P.ih2A;
-    a[4] = (dx * dy) * P.ih2A;
-    double acc[NB];
-#pragma unroll
-    for (int c = 0; c < NB; ++c) {
-        double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < Q; ++k) s = fma(a[k], B[c][k], s);
-        acc[c] = s;
-    }
-    const double un = my_u + acc[0], vn = my_v + acc[1], rn = my_rho + acc[2];
-    nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
-    nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
-    nxt.vol[i] = P.SP_mass / rn;
-    bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
-    if constexpr (NB == 4) { const double tn = my_tem + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
-    if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
-    const int nk = cell_key_mul(P, xn, yn, sc);
-    if (nk >= 0) W.key[i] = nk;
-    scatter_to_cell(P, Ln, gstart, nk, i, sc);
 }
 
 // =======================================================================================
-// Cell-list kernels
+// Small kernels
 // =======================================================================================
 // Scatter the interior particles of the current positions (standalone update_cell).
 __global__ void k_scatter(const Phys P, const Fld F, const Lst Ln, const int* __restrict__ gstart, int* key,
@@ -827,35 +1056,6 @@ __global__ void k_scatter(const Phys P, const Fld F, const Lst Ln, const int* __
     scatter_to_cell(P, Ln, gstart, k, i, sc);
 }
 
-// Finish a cell list: interior slots sorted by particle index, then the cell's ghosts.
-// Clears the scatter counter so the buffer can be scattered into again.
-__global__ void k_cellsort(const Phys P, const Lst L, const int* __restrict__ gstart, const int* __restrict__ glist,
-                           Scalars* sc, int reset_umax) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (reset_umax && c == 0) sc->umax2 = 0ull;
-    if (c >= P.ncell) return;
-    int nf = L.cnt[c];
-    L.cnt[c] = 0;
-    const int g0 = gstart[c], ng = gstart[c + 1] - g0;
-    const int lim = P.cap - ng;
-    if (nf > lim) nf = lim;
-    int* S = L.slots + (size_t)c * P.cap;
-    int buf[64];
-    for (int k = 0; k < nf; ++k) {
-        const int v = S[k];
-        int t = k;
-        while (t > 0 && buf[t - 1] > v) { buf[t] = buf[t - 1]; --t; }
-        buf[t] = v;
-    }
-    for (int k = 0; k < nf; ++k) S[k] = buf[k];
-    for (int k = 0; k < ng; ++k) S[nf + k] = glist[g0 + k];
-    L.num[c] = nf + ng;
-    L.fnum[c] = nf;
-}
-
-// =======================================================================================
-// Small kernels
-// =======================================================================================
 __global__ void k_umax(const Phys P, const Fld F, Scalars* sc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
@@ -894,8 +1094,9 @@ __global__ void k_volume(const Phys P, const Fld F) {
 }
 
 // In-radius neighbour lists for parity checks (unsorted, fixed stride per particle).
-__global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const int* key, const VMd V, int which,
-                            int stride, int* out, int* count) {
+__global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const int* __restrict__ gstart,
+                            const int* __restrict__ glist, const int* key, const VMd V, int which, int stride,
+                            int* out, int* count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = which == 0 ? P.num_int : P.num_ext;
     if (i >= n) return;
@@ -910,8 +1111,8 @@ __global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const int* k
         if (c < stride) out[(size_t)i * stride + c] = j;
         ++c;
     };
-    if (which == 0) for_candidates<1, false>(P, L, k, 0, f);
-    else for_candidates<1, true>(P, L, k, 0, f);
+    if (which == 0) for_candidates<false>(P, L, gstart, glist, k, f);
+    else for_candidates<true>(P, L, gstart, glist, k, f);
     count[i] = c;
 }
 
