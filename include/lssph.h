@@ -198,6 +198,31 @@ int lssph_last_step_stats(const lssph_handle* h, double* device_ms, int64_t* ker
 int lssph_step_profiled(lssph_handle* h, int32_t nsteps, double* ms_by_kind,
                         int64_t* launches_by_kind);
 
+/* ---- allocation-free RHS (no counterpart in the reference) ---------------------------- */
+/* One calculate_RHS pass (LS-SPH type A, problems 2-4, FP64) over a particle state that
+   already lives in caller-owned device memory, writing the RHS arrays to caller-owned
+   device memory, for callers that cannot allocate GPU memory at the point of the call
+   (their memory is already committed to their own pool, or the call sits in a loop where
+   a driver allocation is not acceptable).  It calls no cudaMalloc/cudaFree: its working
+   set is one statically sized device array that every GPU loading this library reserves
+   until the process exits.  Limits: num_total <= LSSPH_NOALLOC_MAX_PARTICLES, cell grid
+   <= LSSPH_NOALLOC_MAX_CELLS cells, at most LSSPH_NOALLOC_CELL_CAP particles per cell;
+   larger inputs return LSSPH_E_CAPACITY before any GPU work.  The first call on a device
+   sets that device up (looks up the array's device address), so make that first call
+   before any stream capture.  The call runs on `stream` (NULL = default stream) and
+   returns when that work is done.  All calls share the one array: calls that overlap on
+   the GPU (other threads or streams) race and give wrong results.  Inputs x..pre (and tem
+   for problem 4) have num_total entries in the reference particle order; rhs_* have
+   num_int entries (rhs_tem only for problem 4). */
+#define LSSPH_NOALLOC_MAX_PARTICLES 262144
+#define LSSPH_NOALLOC_MAX_CELLS     32768
+#define LSSPH_NOALLOC_CELL_CAP      32
+int lssph_rhs_noalloc(const lssph_params* p, int32_t num_total, int32_t num_int,
+                      const double* x, const double* y, const double* u, const double* v,
+                      const double* rho, const double* pre, const double* tem,
+                      double* rhs_u, double* rhs_v, double* rhs_rho, double* rhs_tem,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "liblssph.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 
-SOURCES = ["host.cpp", "engine.cu"]
+SOURCES = ["host.cpp", "engine.cu", "noalloc.cu"]
 HEADERS = ["engine.h", "kernels.cuh"]
 
 NVCC_FLAGS = [

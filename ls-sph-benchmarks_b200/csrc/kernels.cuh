@@ -1044,10 +1044,10 @@ __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, co
 }
 
 // =======================================================================================
-// Small kernels
+// Small kernels (static: this header is compiled into more than one translation unit)
 // =======================================================================================
 // Scatter the interior particles of the current positions (standalone update_cell).
-__global__ void k_scatter(const Phys P, const Fld F, const Lst Ln, const int* __restrict__ gstart, int* key,
+static __global__ void k_scatter(const Phys P, const Fld F, const Lst Ln, const int* __restrict__ gstart, int* key,
                           Scalars* sc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.num_int) return;
@@ -1056,28 +1056,28 @@ __global__ void k_scatter(const Phys P, const Fld F, const Lst Ln, const int* __
     scatter_to_cell(P, Ln, gstart, k, i, sc);
 }
 
-__global__ void k_umax(const Phys P, const Fld F, Scalars* sc) {
+static __global__ void k_umax(const Phys P, const Fld F, Scalars* sc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
     if (i < P.num_int) v = F.u[i] * F.u[i] + F.v[i] * F.v[i];
     warp_max_atomic(&sc->umax2, v);
 }
 
-__global__ void k_steady_max(const Phys P, const Fld F, const Work W, Scalars* sc) {
+static __global__ void k_steady_max(const Phys P, const Fld F, const Work W, Scalars* sc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
     if (i < P.num_int) v = fabs(W.f_prev[i] - F.u[i]);
     warp_max_atomic(&sc->dfmax, v);
 }
 
-__global__ void k_copy_fprev(const Phys P, const Fld F, const Work W) {
+static __global__ void k_copy_fprev(const Phys P, const Fld F, const Work W) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < P.num_int) W.f_prev[i] = F.u[i];
 }
 
 // Problem 1 epilogue of a step (main.f90:139-149 with check_steady_state_mod.f90:39-65):
 // the stage kernel already reduced max|f_previous - u|.
-__global__ void k_epilogue(const Phys P, Scalars* sc) {
+static __global__ void k_epilogue(const Phys P, Scalars* sc) {
     if (sc->err != 0 || sc->steady != 0) return;
     sc->step_count += 1;
     const double df = __longlong_as_double((long long)sc->dfmax);
@@ -1088,13 +1088,13 @@ __global__ void k_epilogue(const Phys P, Scalars* sc) {
     sc->dfmax = 0ull;
 }
 
-__global__ void k_volume(const Phys P, const Fld F) {
+static __global__ void k_volume(const Phys P, const Fld F) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < P.num_total) F.vol[i] = P.SP_mass / F.rho[i];
 }
 
 // In-radius neighbour lists for parity checks (unsorted, fixed stride per particle).
-__global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const int* __restrict__ gstart,
+static __global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const int* __restrict__ gstart,
                             const int* __restrict__ glist, const int* key, const VMd V, int which, int stride,
                             int* out, int* count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -158,6 +158,10 @@ _PROTOS = {
     "lssph_read_data": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _i, _d, _d, _d, _d, _d, _d, _d]),
     "lssph_last_step_stats": (C.c_int, [_H, _P(C.c_double), _P(C.c_int64)]),
     "lssph_step_profiled": (C.c_int, [_H, C.c_int32, _d, _P(C.c_int64)]),
+    # device pointers (caller-owned device memory), stream handle
+    "lssph_rhs_noalloc": (C.c_int, [_P(Params), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
