@@ -252,41 +252,6 @@ __device__ __forceinline__ bool lu_solve(double (&A)[Q][Q], double (&B)[NB][Q]) 
     return ok;
 }
 
-// Solve the NB columns spread over the G lanes of a group: every lane factorises (the
-// same instructions on the same data), lane l substitutes columns l, l+G, ...; on return
-// X[r] holds column lane + r*G of this lane.  Pass xfer = true to gather afterwards with
-// column_value().
-template <int Q, int NB, int G>
-__device__ __forceinline__ bool group_solve(double (&A)[Q][Q], double (&B)[NB][Q], int lane,
-                                            double (&X)[(NB + G - 1) / G][Q]) {
-    const bool ok = lu_factor<Q, NB>(A, B);
-#pragma unroll
-    for (int r = 0; r < (NB + G - 1) / G; ++r) {
-        const int col = lane + r * G;
-#pragma unroll
-        for (int k = 0; k < Q; ++k) {
-            double v = B[0][k];
-#pragma unroll
-            for (int c = 1; c < NB; ++c) v = (col == c) ? B[c][k] : v;
-            X[r][k] = v;
-        }
-        lu_subst<Q>(A, X[r]);
-    }
-    return ok;
-}
-
-// Entry k of solved column c, fetched from the lane of the group that solved it.  Every
-// lane of the warp must call this (the shuffle is warp-wide).
-template <int Q, int NB, int G>
-__device__ __forceinline__ double column_value(const double (&X)[(NB + G - 1) / G][Q], int c, int k) {
-    if constexpr (G == 1) {
-        return X[c][k];
-    } else {
-        const int src = (threadIdx.x & 31 & ~(G - 1)) + (c % G);
-        return __shfl_sync(0xffffffffu, X[c / G][k], src);
-    }
-}
-
 // Butterfly sum over aligned groups of G lanes; every lane of the group ends with the
 // same bits (IEEE addition is commutative).
 template <int G>
@@ -358,7 +323,10 @@ constexpr int TX = 2, TY = 2;               // own cells of a tile
 constexpr int HX = TX + 2, HY = TY + 2;     // halo cells
 constexpr int HC = HX * HY;                 // 16 halo cells
 constexpr int OC = TX * TY;                 // 4 own cells
-constexpr int PPB = 32;                     // particles per pass: a CTA has PPB * G threads
+#ifndef LSSPH_PPB
+#define LSSPH_PPB 32
+#endif
+constexpr int PPB = LSSPH_PPB;              // particles per pass: a CTA has PPB * G threads
 static_assert(HC <= 32 && OC <= 32, "tile scans run in one warp");
 
 struct TileHdr {
@@ -371,6 +339,7 @@ struct TileHdr {
 // Dynamic shared memory: SoA fields of up to HC*cap staged particles, their global
 // indices, and the own-particle list.
 struct SmemView {
+    double* sums;   // [PPB][SUMS]
     double *x, *y, *u, *v, *rho, *pre, *vol, *tem;
     int *idx, *own_k, *own_hc;
     int* nbr;   // in-radius lists, entry e of thread t at nbr[e * blockDim.x + t]
@@ -379,16 +348,22 @@ struct SmemView {
 // Per-thread in-radius list length: a lane tests at most ceil(9 cap / G) candidates.
 __host__ __device__ inline int nbr_list_len(int cap, int G) { return (9 * cap + G - 1) / G; }
 
+// Reduced sums handed from the pair phase to the solve phase, per particle of a pass.
+constexpr int SUMS = 48;   // 15 moment entries + up to 5 x 5 b entries + shift (2) + count
+
 __host__ __device__ inline size_t tile_smem_bytes(int cap, int G) {
     const size_t maxp = (size_t)HC * cap, maxo = (size_t)OC * cap;
     const size_t lists = (size_t)PPB * G * nbr_list_len(cap, G);
-    return maxp * (8 * sizeof(double) + sizeof(int)) + 2 * maxo * sizeof(int) + lists * sizeof(int);
+    return (size_t)PPB * SUMS * sizeof(double) + maxp * (8 * sizeof(double) + sizeof(int)) +
+           2 * maxo * sizeof(int) + lists * sizeof(int);
 }
 
 __device__ __forceinline__ SmemView smem_view(void* raw, int cap) {
     SmemView S;
     const int maxp = HC * cap, maxo = OC * cap;
     double* d = static_cast<double*>(raw);
+    S.sums = d;
+    d += PPB * SUMS;
     S.x = d; S.y = d + maxp; S.u = d + 2 * maxp; S.v = d + 3 * maxp; S.rho = d + 4 * maxp;
     S.pre = d + 5 * maxp; S.vol = d + 6 * maxp; S.tem = d + 7 * maxp;
     int* q = reinterpret_cast<int*>(d + 8 * maxp);
@@ -497,23 +472,53 @@ __device__ __forceinline__ void for_tile_candidates(const TileHdr& T, int hc, in
 
 // Two-phase neighbour loop.  Phase A: the cutoff test r^2 <= h_eff^2 over this lane's
 // candidates (same arithmetic as the reference, LSSPH_A_mod.f90:121-124), appending the
-// hits in visiting order to this thread's list.  Phase B: the pair body over the list
-// only, so a warp no longer runs the full pair body for candidates that most of its
-// lanes reject.  skip = the particle's own staged position (me == you), or -1.
+// hits in visiting order to this thread's list.  Phase B: the pair body over the hits
+// only, so a warp no longer runs the full pair body for candidates most lanes reject.
+// With G > 1 the G lanes of a particle split its combined hit list round-robin, so every
+// lane gets ceil(hits / G) pairs.  Every lane of the warp must call this (shuffles);
+// inactive lanes pass active = false.  skip = own staged position (me == you), or -1.
 template <int G, class Fn>
-__device__ __forceinline__ int for_tile_neighbours(const TileHdr& T, const SmemView& S, int hc, int lane, int skip,
-                                                   double mx, double my, double h_eff_sq, Fn&& f) {
-    int n = 0;
-    int* list = S.nbr + threadIdx.x;
+__device__ __forceinline__ int tile_pairs(const TileHdr& T, const SmemView& S, bool active, int hc, int lane,
+                                          int skip, double mx, double my, double h_eff_sq, Fn&& f) {
+    int nl = 0;
     const int stride = blockDim.x;
-    for_tile_candidates<G>(T, hc, lane, [&](int k) {
-        const double xji = S.x[k] - mx;
-        const double yji = S.y[k] - my;
-        if (k != skip && !(xji * xji + yji * yji > h_eff_sq)) { list[n * stride] = k; ++n; }
-    });
+    int* list = S.nbr + threadIdx.x;
+    if (active) {
+        for_tile_candidates<G>(T, hc, lane, [&](int k) {
+            const double xji = S.x[k] - mx;
+            const double yji = S.y[k] - my;
+            if (k != skip && !(xji * xji + yji * yji > h_eff_sq)) { list[nl * stride] = k; ++nl; }
+        });
+    }
+    if constexpr (G == 1) {
 #pragma unroll 1
-    for (int t = 0; t < n; ++t) f(list[t * stride]);
-    return n;
+        for (int t = 0; t < nl; ++t) f(list[t * stride]);
+        return nl;
+    } else {
+        int incl = nl;
+#pragma unroll
+        for (int off = 1; off < G; off <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, off, G);
+            if (lane >= off) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, G - 1, G);
+        int bases[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) bases[q] = __shfl_sync(0xffffffffu, incl - nl, q, G);
+        const int lane0 = (int)threadIdx.x - lane;
+#pragma unroll 1
+        for (int pidx = lane; pidx < total; pidx += G) {
+            int o = 0, bo = bases[0];
+#pragma unroll
+            for (int q = 1; q < G; ++q) {   // owner lane of hit pidx (selects keep bases in registers)
+                const bool ge = pidx >= bases[q];
+                o = ge ? q : o;
+                bo = ge ? bases[q] : bo;
+            }
+            f(S.nbr[(pidx - bo) * stride + lane0 + o]);
+        }
+        return total;
+    }
 }
 
 // Accumulate the LS type-A moment matrix (upper triangle) and b vectors of one pair
@@ -673,7 +678,7 @@ __global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, 
                                                    Scalars* sc, int ntx) {
     if (halted(sc)) return;
     constexpr int Q = 5;
-    constexpr int NR = (NB + G - 1) / G;
+    static_assert(15 + 5 * NB + 1 <= SUMS, "reduced sums overflow");
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
     const SmemView SM = smem_view(smem_raw, P.cap);
@@ -682,25 +687,26 @@ __global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, 
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
     for (int ob = 0; ob < n_own; ob += PPB) {
-        const int o = ob + (int)threadIdx.x / G;
-        const bool active = o < n_own;
-        int ki = 0, hc = 0;
-        if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
-        const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
-        double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
-        if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
-        if constexpr (NB == 5) my_tem = SM.tem[ki];
-        double Mu[15];
-        double B[NB][Q];
+        // ---- pair phase: G lanes per particle ----
+        {
+            const int slot = (int)threadIdx.x / G;
+            const int o = ob + slot;
+            const bool active = o < n_own;
+            int ki = 0, hc = 0;
+            if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+            const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
+            double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
+            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
+            if constexpr (NB == 5) my_tem = SM.tem[ki];
+            double Mu[15];
+            double B[NB][Q];
 #pragma unroll
-        for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
+            for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
 #pragma unroll
-        for (int c = 0; c < NB; ++c)
+            for (int c = 0; c < NB; ++c)
 #pragma unroll
-            for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
-        int cnt = 0;
-        if (active) {
-            cnt = for_tile_neighbours<G>(T, SM, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+                for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+            const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
                 const double xji = SM.x[k] - my_x;
                 const double yji = SM.y[k] - my_y;
                 const double r = sqrt(xji * xji + yji * yji);
@@ -718,33 +724,60 @@ __global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, 
                 if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
                 accumulate_A<NB>(Mu, B, VW, a, df);
             });
-        }
-        group_reduce<G>(Mu);
+            group_reduce<G>(Mu);
 #pragma unroll
-        for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
-        if constexpr (G > 1) cnt = group_sum_i<G>(cnt);
-
-        // ---- solve (DGESV, LSSPH_A_mod.f90:208-241): columns spread over the lanes ----
-        double X[NR][Q];
-        double A[Q][Q];
+            for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
+            if (active && lane == 0) {
+                double* sm = SM.sums + slot * SUMS;
 #pragma unroll
-        for (int r = 0; r < Q; ++r)
+                for (int k = 0; k < 15; ++k) sm[k] = Mu[k];
 #pragma unroll
-            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
-        if (!group_solve<Q, NB, G>(A, B, lane, X) && active && cnt >= Q && lane == 0) atomicOr(&sc->warn, WARN_SINGULAR);
-        double d[NB][Q];
+                for (int c = 0; c < NB; ++c)
 #pragma unroll
-        for (int c = 0; c < NB; ++c)
-#pragma unroll
-            for (int k = 0; k < Q; ++k) {
-                const double bv = column_value<Q, NB, G>(X, c, k);
-                d[c][k] = (cnt >= Q) ? bv * (k < 2 ? P.ih1 : P.ih2A) : 0.0;
+                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = B[c][k];
+                sm[SUMS - 1] = (double)cnt;
             }
+        }
+        __syncthreads();
+        // ---- solve phase: one thread per particle (DGESV, LSSPH_A_mod.f90:203-241) ----
         double red = 0.0;
-        if (active && lane == 0)
-            red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, SM.idx[ki], my_x, my_y, my_u, my_v, my_rho, my_tem, d);
+        const int o = ob + (int)threadIdx.x;
+        if ((int)threadIdx.x < PPB && o < n_own) {
+            const double* sm = SM.sums + threadIdx.x * SUMS;
+            const int ki = SM.own_k[o];
+            const int cnt = (int)sm[SUMS - 1];
+            double A[Q][Q];
+            double B[NB][Q];
+#pragma unroll
+            for (int r = 0; r < Q; ++r)
+#pragma unroll
+                for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+#pragma unroll
+                for (int k = 0; k < Q; ++k) B[c][k] = sm[15 + 5 * c + k];
+            double d[NB][Q];
+            if (cnt >= Q) {
+                if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) d[c][k] = B[c][k] * (k < 2 ? P.ih1 : P.ih2A);
+            } else {
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) d[c][k] = 0.0;
+            }
+            double my_v = 0, my_rho = 0, my_tem = 0;
+            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
+            if constexpr (NB == 5) my_tem = SM.tem[ki];
+            red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, SM.idx[ki], SM.x[ki], SM.y[ki], SM.u[ki], my_v,
+                                   my_rho, my_tem, d);
+        }
         if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
             warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
+        __syncthreads();
     }
 }
 
@@ -803,8 +836,8 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
 #pragma unroll
         for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
     int cnt = 0;
-    if (active && WQ != 1) {
-        cnt = for_tile_neighbours<G>(T, SM, hc, lane, -1, my_x, my_y, P.h_eff_sq, [&](int k) {
+    if (WQ != 1) {
+        cnt = tile_pairs<G>(T, SM, active, hc, lane, -1, my_x, my_y, P.h_eff_sq, [&](int k) {
             const double xji = SM.x[k] - my_x, yji = SM.y[k] - my_y;
             const double Wv = dev_W(P.kt, sqrt(xji * xji + yji * yji), P.h, P.wnorm);
             const double VW = SM.vol[k] * Wv;
@@ -857,7 +890,7 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
     for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
     if constexpr (G > 1) {
         sw = group_sum<G>(sw);
-        cnt = group_sum_i<G>(cnt);
+        if (WQ == 1) cnt = group_sum_i<G>(cnt);   // tile_pairs already returns the group total
     }
     if (!active || lane != 0) return;
 
@@ -937,7 +970,7 @@ __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, co
                                                  const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
     if (halted(sc)) return;
     constexpr int Q = 5;
-    constexpr int NR = (NB + G - 1) / G;
+    static_assert(15 + 5 * NB + 3 <= SUMS, "reduced sums overflow");
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
     const SmemView SM = smem_view(smem_raw, P.cap);
@@ -948,25 +981,25 @@ __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, co
     const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
     const int lane = threadIdx.x & (G - 1);
     for (int ob = 0; ob < n_own; ob += PPB) {
-        const int o = ob + (int)threadIdx.x / G;
-        const bool active = o < n_own;
-        int ki = 0, hc = 0;
-        if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
-        const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
-        double my_tem = 0.0;
-        if constexpr (NB == 4) my_tem = SM.tem[ki];
-        double Mu[15];
-        double B[NB][Q];
+        {
+            const int slot = (int)threadIdx.x / G;
+            const int o = ob + slot;
+            const bool active = o < n_own;
+            int ki = 0, hc = 0;
+            if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+            const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
+            double my_tem = 0.0;
+            if constexpr (NB == 4) my_tem = SM.tem[ki];
+            double Mu[15];
+            double B[NB][Q];
 #pragma unroll
-        for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
+            for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
 #pragma unroll
-        for (int c = 0; c < NB; ++c)
+            for (int c = 0; c < NB; ++c)
 #pragma unroll
-            for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
-        double sxy[2] = {0.0, 0.0};
-        int cnt = 0;
-        if (active) {
-            cnt = for_tile_neighbours<G>(T, SM, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+                for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+            double sxy[2] = {0.0, 0.0};
+            const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
                 const double xji = SM.x[k] - my_x;
                 const double yji = SM.y[k] - my_y;
                 const double r = sqrt(xji * xji + yji * yji);
@@ -989,57 +1022,80 @@ __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, co
                 if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
                 accumulate_A<NB>(Mu, B, VW, a, df);
             });
+            group_reduce<G>(Mu);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
+            group_reduce<G>(sxy);
+            if (active && lane == 0) {
+                double* sm = SM.sums + slot * SUMS;
+#pragma unroll
+                for (int k = 0; k < 15; ++k) sm[k] = Mu[k];
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = B[c][k];
+                sm[SUMS - 3] = sxy[0];
+                sm[SUMS - 2] = sxy[1];
+                sm[SUMS - 1] = (double)cnt;
+            }
         }
-        group_reduce<G>(Mu);
+        __syncthreads();
+        const int o = ob + (int)threadIdx.x;
+        if ((int)threadIdx.x < PPB && o < n_own) {
+            const double* sm = SM.sums + threadIdx.x * SUMS;
+            const int ki = SM.own_k[o];
+            const int cnt = (int)sm[SUMS - 1];
+            // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
+            double dx = -coe * sm[SUMS - 3], dy = -coe * sm[SUMS - 2];
+            const double rr = sqrt(dx * dx + dy * dy);
+            if (rr > 0.2 * P.h) {
+                dx = ((0.2 * P.h) * dx) / rr;
+                dy = ((0.2 * P.h) * dy) / rr;
+            }
+            double A[Q][Q];
+            double B[NB][Q];
 #pragma unroll
-        for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
-        group_reduce<G>(sxy);
-        if constexpr (G > 1) cnt = group_sum_i<G>(cnt);
-
-        // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
-        double dx = -coe * sxy[0], dy = -coe * sxy[1];
-        const double rr = sqrt(dx * dx + dy * dy);
-        if (rr > 0.2 * P.h) {
-            dx = ((0.2 * P.h) * dx) / rr;
-            dy = ((0.2 * P.h) * dy) / rr;
+            for (int r = 0; r < Q; ++r)
+#pragma unroll
+                for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+#pragma unroll
+                for (int k = 0; k < Q; ++k) B[c][k] = sm[15 + 5 * c + k];
+            if (cnt >= Q) {
+                if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+            } else {
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+            }
+            // interpolation a(dr) . d (shift_interpolate_mod.f90:255-298)
+            double a[Q];
+            basis_A(P, dx, dy, a);
+            double acc[NB];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                double sacc = 0.0;
+#pragma unroll
+                for (int k = 0; k < Q; ++k) sacc = fma(a[k], B[c][k], sacc);
+                acc[c] = sacc;
+            }
+            const int i = SM.idx[ki];
+            const double my_x = SM.x[ki], my_y = SM.y[ki];
+            const double xn = my_x + dx, yn = my_y + dy;
+            const double un = SM.u[ki] + acc[0], vn = SM.v[ki] + acc[1], rn = SM.rho[ki] + acc[2];
+            nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
+            nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
+            nxt.vol[i] = P.SP_mass / rn;
+            bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
+            if constexpr (NB == 4) { const double tn = SM.tem[ki] + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
+            if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
+            const int nk = cell_key_mul(P, xn, yn, sc);
+            if (nk >= 0) W.key[i] = nk;
+            scatter_to_cell(P, Ln, gstart, nk, i, sc);
         }
-        double X[NR][Q];
-        double A[Q][Q];
-#pragma unroll
-        for (int r = 0; r < Q; ++r)
-#pragma unroll
-            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? Mu[UT(r, c)] : Mu[UT(c, r)];
-        if (!group_solve<Q, NB, G>(A, B, lane, X) && active && cnt >= Q && lane == 0) atomicOr(&sc->warn, WARN_SINGULAR);
-        // interpolation a(dr) . d for the columns this lane solved (shift_interpolate_mod.f90:255-298)
-        double a[Q];
-        basis_A(P, dx, dy, a);
-        double accr[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            double s = 0.0;
-#pragma unroll
-            for (int k = 0; k < Q; ++k) s = fma(a[k], (cnt >= Q) ? X[r][k] : 0.0, s);
-            accr[r] = s;
-        }
-        double acc[NB];
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            if constexpr (G == 1) acc[c] = accr[c];
-            else acc[c] = __shfl_sync(0xffffffffu, accr[c / G], (threadIdx.x & 31 & ~(G - 1)) + (c % G));
-        }
-        if (!active || lane != 0) continue;
-        const int i = SM.idx[ki];
-        const double xn = my_x + dx, yn = my_y + dy;
-        const double un = my_u + acc[0], vn = my_v + acc[1], rn = my_rho + acc[2];
-        nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
-        nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
-        nxt.vol[i] = P.SP_mass / rn;
-        bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
-        if constexpr (NB == 4) { const double tn = my_tem + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
-        if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
-        const int nk = cell_key_mul(P, xn, yn, sc);
-        if (nk >= 0) W.key[i] = nk;
-        scatter_to_cell(P, Ln, gstart, nk, i, sc);
+        __syncthreads();
     }
 }
 

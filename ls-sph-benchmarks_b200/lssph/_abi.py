@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_PKG), "lib", "liblssph.so")
+# LSSPH_LIB selects another build of the engine (e.g. a tuning variant)
+LIB_PATH = os.environ.get("LSSPH_LIB") or os.path.join(os.path.dirname(_PKG), "lib", "liblssph.so")
 
 OK = 0
 E_BAD_PARAM = -1
