@@ -411,6 +411,11 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     P.threshold = p.threshold;
     P.hydro_coef_top = ((p.rho_ref * p.alpha_ref) * (p.tem_top - p.tem_ave)) * p.gravity;
     P.hydro_coef_bottom = ((p.rho_ref * p.alpha_ref) * (p.tem_bottom - p.tem_ave)) * p.gravity;
+    P.iWave = 1.0 / p.W_ave;
+    P.izeta2 = 1.0 / (p.zeta_RSST * p.zeta_RSST);
+    P.ixi2 = 1.0 / (p.xi_VIM * p.xi_VIM);
+    P.m3h = -3.0 / p.h;
+    P.m5h = -5.0 / p.h;
 
     // ---- device memory ----
     auto cu = [&](cudaError_t e) { return e == cudaSuccess ? LSSPH_OK : fail(nullptr, LSSPH_E_CUDA, cudaGetErrorString(e)); };

@@ -54,7 +54,7 @@ double kernel_norm(int kt, double h) {
 
 // cal_W (kernel_functions_mod.f90:26-81); used for W_ave = W(dx, h).
 double kernel_W_host(int kt, double r, double h) {
-    const double q = r / h;
+    const double q = r * (1.0 / h);   // a division by the loop-invariant h as a reciprocal multiply
     double W = 0.0;
     if (kt == 1) {
         const double a = 2.0 - q, b = 1.0 - q, a3 = p2(a) * a, b3 = p2(b) * b;

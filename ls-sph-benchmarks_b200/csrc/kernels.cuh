@@ -60,6 +60,8 @@ struct Phys {
     double h, ih1, ih2A, ih2B, h_eff_sq, inv_h_eff, SP_mass, W_ave, wnorm, dt;
     double c_sq, rho_ref, vis_ref, delta, zeta_sq, xi_sq, alpha_ref, gravity, tem_ave;
     double thermal_dif, PST_c, threshold, hydro_coef_top, hydro_coef_bottom;
+    // reciprocals of loop-invariant divisors (1/W_ave, 1/zeta^2, 1/xi^2, -3/h, -5/h)
+    double iWave, izeta2, ixi2, m3h, m5h;
 };
 
 struct Fld {   // SoA particle state over num_total
@@ -101,9 +103,9 @@ __device__ __forceinline__ bool halted(const Scalars* sc) {
     return (*(volatile const int*)&sc->err) != 0 || (*(volatile const int*)&sc->steady) != 0;
 }
 
-// cal_W / cal_dW (kernel_functions_mod.f90:26-146); nrm = kernel_norm(kt, h).
-__device__ __forceinline__ double dev_W(int kt, double r, double h, double nrm) {
-    const double q = r / h;
+// cal_W / cal_dW (kernel_functions_mod.f90:26-146); nrm = kernel_norm(kt, h), ih = 1/h.
+__device__ __forceinline__ double dev_W(int kt, double r, double ih, double nrm) {
+    const double q = r * ih;
     double W = 0.0;
     if (kt == 3) {
         if (0.0 <= q && q <= 2.0) {
@@ -136,20 +138,20 @@ __device__ __forceinline__ double dev_W(int kt, double r, double h, double nrm) 
     return nrm * W;
 }
 
-__device__ __forceinline__ double dev_dW(int kt, double r, double h, double nrm) {
-    const double q = r / h;
+__device__ __forceinline__ double dev_dW(int kt, double r, double ih, double m3h, double m5h, double nrm) {
+    const double q = r * ih;
     double dW = 0.0;
     if (kt == 3) {
         if (0.0 <= q && q <= 2.0) {
             const double t = 1.0 - 0.5 * q, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
             dW = -(2.0 * t3) * (1.0 + 2.0 * q) + 2.0 * t4;
         }
-        return (nrm * dW) / h;
+        return (nrm * dW) * ih;
     } else if (kt == 1) {
         const double a = 2.0 - q, b = 1.0 - q;
         if (0.0 <= q && q <= 1.0) dW = a * a - 4.0 * (b * b);
         else if (1.0 < q && q <= 2.0) dW = a * a;
-        return (nrm * dW) * (-3.0 / h);
+        return (nrm * dW) * m3h;
     } else if (kt == 2) {
         const double a = 3.0 - q, b = 2.0 - q, c = 1.0 - q;
         const double a2 = a * a, b2 = b * b, c2 = c * c;
@@ -157,13 +159,13 @@ __device__ __forceinline__ double dev_dW(int kt, double r, double h, double nrm)
         if (0.0 <= q && q <= 1.0) dW = (a4 - 6.0 * b4) + 15.0 * c4;
         else if (1.0 < q && q <= 2.0) dW = a4 - 6.0 * b4;
         else if (2.0 < q && q <= 3.0) dW = a4;
-        return (nrm * dW) * (-5.0 / h);
+        return (nrm * dW) * m5h;
     } else if (kt == 4) {
         if (0.0 <= q && q <= 2.0) {
             const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t5 = t4 * t, t6 = t4 * t2;
             dW = -(3.0 * t5) * ((1.0 + 3.0 * q) + (35.0 * (q * q)) / 12.0) + t6 * (3.0 + (35.0 * q) / 6.0);
         }
-        return (nrm * dW) / h;
+        return (nrm * dW) * ih;
     } else {
         if (0.0 <= q && q <= 2.0) {
             const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t7 = t6 * t, t8 = t4 * t4;
@@ -171,7 +173,7 @@ __device__ __forceinline__ double dev_dW(int kt, double r, double h, double nrm)
             dW = -(4.0 * t7) * (((1.0 + 4.0 * q) + (25.0 * q2) / 4.0) + 4.0 * q3) +
                  t8 * ((4.0 + (25.0 * q) / 2.0) + 12.0 * q2);
         }
-        return (nrm * dW) / h;
+        return (nrm * dW) * ih;
     }
 }
 
@@ -185,7 +187,7 @@ __host__ __device__ constexpr int UT(int j, int i) { return i * (i + 1) / 2 + j;
 // Returns false on a zero pivot.  Row interchanges are rare for LS moment matrices, so
 // the swap code runs only when the pivot row differs from the diagonal one.
 template <int Q, int NB>
-__device__ __forceinline__ bool lu_factor(double (&A)[Q][Q], double (&B)[NB][Q]) {
+__device__ __forceinline__ bool lu_factor(double (&A)[Q][Q], double (&B)[NB][Q], double (&rpiv)[Q]) {
     bool ok = true;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
@@ -222,6 +224,7 @@ __device__ __forceinline__ bool lu_factor(double (&A)[Q][Q], double (&B)[NB][Q])
         } else {
             ok = false;
         }
+        rpiv[k] = 1.0 / piv;
 #pragma unroll
         for (int j = k + 1; j < Q; ++j)
 #pragma unroll
@@ -231,14 +234,14 @@ __device__ __forceinline__ bool lu_factor(double (&A)[Q][Q], double (&B)[NB][Q])
 }
 
 template <int Q>
-__device__ __forceinline__ void lu_subst(const double (&A)[Q][Q], double (&b)[Q]) {
+__device__ __forceinline__ void lu_subst(const double (&A)[Q][Q], const double (&rpiv)[Q], double (&b)[Q]) {
 #pragma unroll
     for (int k = 0; k < Q; ++k)
 #pragma unroll
         for (int i = k + 1; i < Q; ++i) b[i] = fma(-b[k], A[i][k], b[i]);
 #pragma unroll
     for (int k = Q - 1; k >= 0; --k) {
-        b[k] = b[k] / A[k][k];
+        b[k] = b[k] * rpiv[k];
 #pragma unroll
         for (int i = 0; i < k; ++i) b[i] = fma(-b[k], A[i][k], b[i]);
     }
@@ -246,9 +249,10 @@ __device__ __forceinline__ void lu_subst(const double (&A)[Q][Q], double (&b)[Q]
 
 template <int Q, int NB>
 __device__ __forceinline__ bool lu_solve(double (&A)[Q][Q], double (&B)[NB][Q]) {
-    const bool ok = lu_factor<Q, NB>(A, B);
+    double rpiv[Q];
+    const bool ok = lu_factor<Q, NB>(A, B, rpiv);
 #pragma unroll
-    for (int m = 0; m < NB; ++m) lu_subst<Q>(A, B[m]);
+    for (int m = 0; m < NB; ++m) lu_subst<Q>(A, rpiv, B[m]);
     return ok;
 }
 
@@ -464,6 +468,7 @@ __device__ __forceinline__ void for_tile_candidates(const TileHdr& T, int hc, in
             const int h = hc + dx + dy * HX;
             const int n = T.cnt[h], o = T.off[h];
             int t = (G == 1) ? 0 : ((lane - base) & (G - 1));
+#pragma unroll 4
             for (; t < n; t += G) f(o + t);
             base += n;
         }
@@ -491,8 +496,8 @@ __device__ __forceinline__ int tile_pairs(const TileHdr& T, const SmemView& S, b
         });
     }
     if constexpr (G == 1) {
-#pragma unroll 1
-        for (int t = 0; t < nl; ++t) f(list[t * stride]);
+#pragma unroll 2
+        for (int t = 0; t < nl; ++t) f(list[t * stride]);   // two pair bodies in flight
         return nl;
     } else {
         int incl = nl;
@@ -506,7 +511,7 @@ __device__ __forceinline__ int tile_pairs(const TileHdr& T, const SmemView& S, b
 #pragma unroll
         for (int q = 0; q < G; ++q) bases[q] = __shfl_sync(0xffffffffu, incl - nl, q, G);
         const int lane0 = (int)threadIdx.x - lane;
-#pragma unroll 1
+#pragma unroll 2
         for (int pidx = lane; pidx < total; pidx += G) {
             int o = 0, bo = bases[0];
 #pragma unroll
@@ -569,14 +574,15 @@ __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, co
         Ru = (d[0][2] + d[0][3]) + W.src[i];
     } else {
         // d[0] = u, d[1] = v, d[2] = rho, d[3] = p (, d[4] = T); entries x, y, xx, yy, xy
+        const double irho = 1.0 / my_rho;
         Rr = -(my_rho * (d[0][0] + d[1][1])) + P.delta * (d[2][2] + d[2][3]);
-        Ru = -(d[3][0] / my_rho) + (P.vis_ref / my_rho) * (d[0][2] + d[0][3]);
-        Rv = -(d[3][1] / my_rho) + (P.vis_ref / my_rho) * (d[1][2] + d[1][3]);
-        Rr = Rr / P.zeta_sq;
+        Ru = -(d[3][0] * irho) + (P.vis_ref * irho) * (d[0][2] + d[0][3]);
+        Rv = -(d[3][1] * irho) + (P.vis_ref * irho) * (d[1][2] + d[1][3]);
+        Rr = Rr * P.izeta2;
         if constexpr (NB == 5) {
             Rv = Rv + ((P.alpha_ref * (my_tem - P.tem_ave)) * P.gravity);
-            Ru = Ru / P.xi_sq;
-            Rv = Rv / P.xi_sq;
+            Ru = Ru * P.ixi2;
+            Rv = Rv * P.ixi2;
             Rt = P.thermal_dif * (d[NB - 1][2] + d[NB - 1][3]);
         }
     }
@@ -676,7 +682,7 @@ __global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, 
                                                    const Lst Ln, const int* __restrict__ gstart,
                                                    const int* __restrict__ glist, const Work W, const StageCfg S,
                                                    Scalars* sc, int ntx) {
-    if (halted(sc)) return;
+    const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
     static_assert(15 + 5 * NB + 1 <= SUMS, "reduced sums overflow");
     __shared__ TileHdr T;
@@ -684,6 +690,7 @@ __global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, 
     const SmemView SM = smem_view(smem_raw, P.cap);
     const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
     stage_halo<false, NB == 5>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    if (stop) return;
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
     for (int ob = 0; ob < n_own; ob += PPB) {
@@ -710,7 +717,7 @@ __global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, 
                 const double xji = SM.x[k] - my_x;
                 const double yji = SM.y[k] - my_y;
                 const double r = sqrt(xji * xji + yji * yji);
-                const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
+                const double Wv = dev_W(P.kt, r, P.ih1, P.wnorm);
                 const double VW = SM.vol[k] * Wv;
                 double a[Q];
                 basis_A(P, xji, yji, a);
@@ -803,7 +810,7 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
         for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < P.ncell; c += gridDim.x * blockDim.x) zero_cnt[c] = 0;
     }
     if (reset_umax && blockIdx.x == 0 && threadIdx.x == 0) sc->umax2 = 0ull;
-    if (halted(sc)) return;
+    const bool stop = halted(sc);   // consumed after staging
     constexpr int Q = (WQ == 1) ? 1 : WQ;
     constexpr int NU = Q * (Q + 1) / 2;
     __shared__ TileHdr T;
@@ -813,6 +820,7 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
     const int tx = tile % ntx, ty = tile / ntx;
     const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
     stage_halo<true, NB == 4>(P, F, L, gstart, glist, cx0, cy0, T, SM);
+    if (stop) return;
     const int v0 = VT.start[blockIdx.x], nvm = VT.start[blockIdx.x + 1] - v0;
     const int lane = threadIdx.x & (G - 1);
     const int o = (int)threadIdx.x / G;
@@ -839,7 +847,7 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
     if (WQ != 1) {
         cnt = tile_pairs<G>(T, SM, active, hc, lane, -1, my_x, my_y, P.h_eff_sq, [&](int k) {
             const double xji = SM.x[k] - my_x, yji = SM.y[k] - my_y;
-            const double Wv = dev_W(P.kt, sqrt(xji * xji + yji * yji), P.h, P.wnorm);
+            const double Wv = dev_W(P.kt, sqrt(xji * xji + yji * yji), P.ih1, P.wnorm);
             const double VW = SM.vol[k] * Wv;
             double a[Q];
             a[0] = 1.0;
@@ -872,7 +880,7 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
                 const double xij = my_x - SM.x[k], yij = my_y - SM.y[k];
                 const double r2 = xij * xij + yij * yij;
                 if (r2 > P.h_eff_sq) return;
-                const double Wv = dev_W(P.kt, sqrt(r2), P.h, P.wnorm);
+                const double Wv = dev_W(P.kt, sqrt(r2), P.ih1, P.wnorm);
                 ++cnt;
                 const double VW = SM.vol[k] * Wv;
                 sw = sw + VW;
@@ -968,7 +976,7 @@ template <int NB, int G>
 __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
                                                  const Lst Ln, const int* __restrict__ gstart,
                                                  const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
-    if (halted(sc)) return;
+    const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
     static_assert(15 + 5 * NB + 3 <= SUMS, "reduced sums overflow");
     __shared__ TileHdr T;
@@ -976,6 +984,7 @@ __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, co
     const SmemView SM = smem_view(smem_raw, P.cap);
     const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
     stage_halo<false, NB == 4>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    if (stop) return;
     const int n_own = T.own_off[OC];
     const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
     const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
@@ -1003,13 +1012,14 @@ __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, co
                 const double xji = SM.x[k] - my_x;
                 const double yji = SM.y[k] - my_y;
                 const double r = sqrt(xji * xji + yji * yji);
-                const double Wv = dev_W(P.kt, r, P.h, P.wnorm);
-                const double dWdr = dev_dW(P.kt, r, P.h, P.wnorm);
+                const double Wv = dev_W(P.kt, r, P.ih1, P.wnorm);
+                const double dWdr = dev_dW(P.kt, r, P.ih1, P.m3h, P.m5h, P.wnorm);
                 const double Vj = SM.vol[k];
                 const double VW = Vj * Wv;
-                const double gx = ((dWdr * (-xji)) / r) * Vj;
-                const double gy = ((dWdr * (-yji)) / r) * Vj;
-                const double t = Wv / P.W_ave, t2 = t * t, t4 = t2 * t2;
+                const double rinv = 1.0 / r;
+                const double gx = ((dWdr * (-xji)) * rinv) * Vj;
+                const double gy = ((dWdr * (-yji)) * rinv) * Vj;
+                const double t = Wv * P.iWave, t2 = t * t, t4 = t2 * t2;
                 const double fac = 1.0 + 0.2 * t4;
                 sxy[0] = fma(fac, gx, sxy[0]);
                 sxy[1] = fma(fac, gy, sxy[1]);

@@ -192,6 +192,8 @@ extern "C" int lssph_rhs_noalloc(const lssph_params* pin, int32_t num_total, int
     P.delta = ((p.coe_delta_sph * p.sound_speed) * p.h) * p.zeta_RSST;
     P.zeta_sq = p.zeta_RSST * p.zeta_RSST; P.xi_sq = p.xi_VIM * p.xi_VIM;
     P.alpha_ref = p.alpha_ref; P.gravity = p.gravity; P.tem_ave = p.tem_ave; P.thermal_dif = p.thermal_dif;
+    P.iWave = 1.0 / p.W_ave; P.izeta2 = 1.0 / (p.zeta_RSST * p.zeta_RSST); P.ixi2 = 1.0 / (p.xi_VIM * p.xi_VIM);
+    P.m3h = -3.0 / p.h; P.m5h = -5.0 / p.h;
 
     Fld F{};
     F.x = const_cast<double*>(x); F.y = const_cast<double*>(y); F.u = const_cast<double*>(u);

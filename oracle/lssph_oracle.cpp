@@ -15,6 +15,12 @@
 //     b vectors, shift vector, dot products) and in the LU update/substitutions;
 //   * Fortran integer powers x**n are evaluated as products p2=x*x, p3=p2*x, p4=p2*p2,
 //     p5=p4*x, p6=p4*p2, p7=p6*x, p8=p4*p4;
+//   * a division by a quantity that is invariant over a loop (h, W_ave, rho_i, zeta^2,
+//     xi^2, a pivot, r in the two shift components) is a multiplication by its
+//     reciprocal, as an optimising Fortran compiler under a fast floating-point model
+//     (ifx's default fp-model fast=1, the reference Makefile's first option) may emit it;
+//     gfortran -O2 keeps true divisions, so the reference's own bits differ between its
+//     two documented builds at this level;
 //   * LAPACK DGESV (LSSPH_A_mod.f90:211, shift_interpolate_mod.f90:241,
 //     interpolate_LSSPH_B_mod.f90:158) is restated as Gaussian elimination with partial
 //     pivoting (first max |a| pivot, reciprocal scaling of the column, right-looking
@@ -63,7 +69,7 @@ double kernel_norm(int kt, double h) {
 
 // kernel_functions_mod.f90:26-81
 double cal_W(int kt, double r, double h) {
-    const double q = r / h;
+    const double q = r * (1.0 / h);
     double W = 0.0;
     if (kt == 1) {
         const double a = 2.0 - q, b = 1.0 - q;
@@ -99,7 +105,8 @@ double cal_W(int kt, double r, double h) {
 
 // kernel_functions_mod.f90:87-146
 double cal_dW(int kt, double r, double h) {
-    const double q = r / h;
+    const double ih = 1.0 / h;
+    const double q = r * ih;
     double dW = 0.0;
     const double nrm = kernel_norm(kt, h);
     if (kt == 1) {
@@ -135,7 +142,7 @@ double cal_dW(int kt, double r, double h) {
                  + t8 * ((4.0 + (25.0 * q) / 2.0) + 12.0 * q2);
         }
     }
-    return (nrm * dW) / h;
+    return (nrm * dW) * ih;
 }
 
 // ---------------------------------------------------------------------------------
@@ -145,6 +152,7 @@ double cal_dW(int kt, double r, double h) {
 // ---------------------------------------------------------------------------------
 int gepp_solve(int n, int nrhs, double* A, double* B) {
     int info = 0;
+    double rpiv[32];   // reciprocal pivots, reused by the back substitution
     for (int k = 0; k < n; ++k) {
         int p = k;
         double amax = std::fabs(A[k + k * n]);
@@ -162,6 +170,7 @@ int gepp_solve(int n, int nrhs, double* A, double* B) {
         } else if (info == 0) {
             info = k + 1;
         }
+        rpiv[k] = 1.0 / A[k + k * n];
         for (int j = k + 1; j < n; ++j)
             for (int i = k + 1; i < n; ++i)
                 A[i + j * n] = std::fma(-A[i + k * n], A[k + j * n], A[i + j * n]);
@@ -171,7 +180,7 @@ int gepp_solve(int n, int nrhs, double* A, double* B) {
         for (int k = 0; k < n; ++k)
             for (int i = k + 1; i < n; ++i) b[i] = std::fma(-b[k], A[i + k * n], b[i]);
         for (int k = n - 1; k >= 0; --k) {
-            b[k] = b[k] / A[k + k * n];
+            b[k] = b[k] * rpiv[k];
             for (int i = 0; i < k; ++i) b[i] = std::fma(-b[k], A[i + k * n], b[i]);
         }
     }
@@ -573,14 +582,16 @@ void LSSPH_A(orc_state* s, int me) {
                                              std::cos(PI * (my_y - p.WL_thick));
     } else {
         const double delta = ((p.coe_delta_sph * p.sound_speed) * h) * p.zeta_RSST;
+        const double irho = 1.0 / my_rho;
         double Rr = -(my_rho * (du[0] + dv[1])) + delta * (drho[2] + drho[3]);
-        double Ru = -(dpre[0] / my_rho) + (p.vis_ref / my_rho) * (du[2] + du[3]);
-        double Rv = -(dpre[1] / my_rho) + (p.vis_ref / my_rho) * (dv[2] + dv[3]);
-        Rr = Rr / (p.zeta_RSST * p.zeta_RSST);
+        double Ru = -(dpre[0] * irho) + (p.vis_ref * irho) * (du[2] + du[3]);
+        double Rv = -(dpre[1] * irho) + (p.vis_ref * irho) * (dv[2] + dv[3]);
+        Rr = Rr * (1.0 / (p.zeta_RSST * p.zeta_RSST));
         if (p.target_problem == 4) {
+            const double ixi2 = 1.0 / (p.xi_VIM * p.xi_VIM);
             Rv = Rv + ((p.alpha_ref * (my_tem - p.tem_ave)) * p.gravity);
-            Ru = Ru / (p.xi_VIM * p.xi_VIM);
-            Rv = Rv / (p.xi_VIM * p.xi_VIM);
+            Ru = Ru * ixi2;
+            Rv = Rv * ixi2;
             s->RHS_tem[me] = p.thermal_dif * (dtem[2] + dtem[3]);
         }
         s->RHS_rho[me] = Rr; s->RHS_u[me] = Ru; s->RHS_v[me] = Rv;
@@ -949,9 +960,10 @@ void shift_interpolate(orc_state* s, int me, double coe_PST) {
         ++num_neighbors;
         const double V_j = SP_mass / s->rho[you];
         const double VW = V_j * W;
-        const double gx = ((dW_dr * (-x_ji)) / r) * V_j;
-        const double gy = ((dW_dr * (-y_ji)) / r) * V_j;
-        const double t = W / W_ave, t2 = t * t, t4 = t2 * t2;
+        const double rinv = 1.0 / r;
+        const double gx = ((dW_dr * (-x_ji)) * rinv) * V_j;
+        const double gy = ((dW_dr * (-y_ji)) * rinv) * V_j;
+        const double t = W * (1.0 / W_ave), t2 = t * t, t4 = t2 * t2;
         const double fac = 1.0 + 0.2 * t4;
         dx = std::fma(fac, gx, dx);
         dy = std::fma(fac, gy, dy);
