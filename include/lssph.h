@@ -91,6 +91,7 @@ typedef struct lssph_params {
 } lssph_params;
 
 typedef struct lssph_handle lssph_handle;
+typedef struct lssph_batch lssph_batch;
 
 /* ---- library ------------------------------------------------------------------------ */
 int         lssph_abi_version(void);
@@ -197,6 +198,30 @@ int lssph_last_step_stats(const lssph_handle* h, double* device_ms, int64_t* ker
    kind k, launches_by_kind[k] its launch count (arrays of LSSPH_KIND_COUNT). */
 int lssph_step_profiled(lssph_handle* h, int32_t nsteps, double* ms_by_kind,
                         int64_t* launches_by_kind);
+
+/* ---- batched time loop (no counterpart in the reference) ------------------------------ */
+/* A batch advances many independent solves (handles) together: each kernel of a time
+   step is launched once for all members of the same kind (same RHS width, RK order, wall
+   model and lane count), members of different kinds run concurrently, and the whole step
+   is one CUDA graph.  Every member computes exactly what lssph_step computes for it
+   alone (bit-identical results), each stops at its own steady state or error, and
+   members may join or leave between calls.  A handle belongs to at most one batch; it
+   stays usable on its own between batch calls (its own lssph_step, uploads, downloads,
+   files), and destroying it removes it from its batch.  Members are numbered in the
+   order they were added; removal shifts later members down by one. */
+int  lssph_batch_create(lssph_batch** out);
+void lssph_batch_destroy(lssph_batch* b);
+const char* lssph_batch_error(const lssph_batch* b);
+int  lssph_batch_add(lssph_batch* b, lssph_handle* h);      /* LSSPH_E_BAD_PARAM if h is in a batch */
+int  lssph_batch_remove(lssph_batch* b, lssph_handle* h);
+int  lssph_batch_size(const lssph_batch* b);
+/* nsteps time steps of every member.  status[i] (may be NULL) receives member i's status
+   (LSSPH_OK or the code lssph_step would return), steady[i] (may be NULL) the 1-based step
+   within this call at which member i reached a steady state, or 0.  Returns LSSPH_OK, or
+   the first member error, or LSSPH_E_CUDA for a failure of the batch itself. */
+int  lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady);
+/* Device time and kernel launches of the last lssph_batch_step (all members). */
+int  lssph_batch_last_step_stats(const lssph_batch* b, double* device_ms, int64_t* kernel_launches);
 
 /* ---- allocation-free RHS (no counterpart in the reference) ---------------------------- */
 /* One calculate_RHS pass (LS-SPH type A, problems 2-4, FP64) over a particle state that

@@ -16,15 +16,15 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "liblssph.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 
-SOURCES = ["host.cpp", "engine.cu", "noalloc.cu"]
-HEADERS = ["engine.h", "kernels.cuh"]
+SOURCES = ["host.cpp", "engine.cu", "batch.cu", "noalloc.cu"]
+HEADERS = ["engine.h", "handle.h", "kernels.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
     "-Xcompiler", "-fPIC,-O2,-Wall",
-    "-shared",
 ]
+OBJ_DIR = os.path.join(LIB_DIR, "_obj")
 
 
 def _nvcc() -> str:
@@ -44,14 +44,23 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
+    """Compile each source to an object in parallel, then link the shared library."""
     if not force and not _stale():
         return LIB
-    os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [_nvcc(), *NVCC_FLAGS]
-    if verbose_ptxas:
-        cmd += ["-Xptxas", "-v"]
-    cmd += ["-I", INCLUDE, *[os.path.join(CSRC, f) for f in SOURCES], "-o", LIB + ".tmp"]
-    subprocess.run(cmd, check=True)
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    base = [_nvcc(), *NVCC_FLAGS] + (["-Xptxas", "-v"] if verbose_ptxas else []) + ["-I", INCLUDE]
+
+    def compile_one(src: str) -> str:
+        obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+        subprocess.run([*base, "-c", os.path.join(CSRC, src), "-o", obj], check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
+    subprocess.run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs,
+                    "-o", LIB + ".tmp"], check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,0 +1,462 @@
+// batch.cu -- many independent solves advanced by one CUDA graph per time step.
+//
+// Members are grouped by kind (RHS width, ghost quadrature, RK order, lanes).  A group's
+// phase kernel is launched once over the concatenated tiles (or marker chunks) of all
+// its members; each CTA finds its solve through a (solve, tile) map and reads that
+// solve's descriptor (constants + buffer pointers + buffer parities).  Groups run on
+// their own streams, forked from and joined back into the batch stream inside the
+// captured step, so small solves of one kind overlap large solves of another.
+//
+// Parities.  A solo step flips the state/list parities of problems 2-4 once per stage
+// plus once for PST (an odd count for RK2 and RK4) and leaves problem 1's unchanged
+// (an even number of state flips, no list flips).  So after k batch steps every member
+// of a group sits at (descriptor parity) xor (flip_g & k & 1), and two graphs (k even,
+// k odd) cover every step.  Descriptors are rewritten whenever the membership changes
+// or a member was advanced on its own between batch calls.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <vector>
+
+#include "handle.h"
+
+using namespace lssph;
+
+namespace {
+
+struct BatchGroup {
+    int nb = 4, nbg = 3, wq = 3, rk = 4, G = 4;
+    bool p1 = false, pst_on = true;
+    int flip = 1;                  // both parities flip once per step (problems 2-4)
+    std::vector<int> members;      // indices into lssph_batch::members
+    SolveDesc* D = nullptr;        // device, one descriptor per member
+    int2* tiles = nullptr;         // (solve, tile) per CTA of stage / PST launches
+    int2* chunks = nullptr;        // (solve, chunk) per CTA of ghost launches
+    int ntiles = 0, nchunks = 0;
+    size_t smem = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t join = nullptr;
+};
+
+}  // namespace
+
+struct lssph_batch {
+    std::vector<lssph_handle*> members;
+    std::vector<int> base_sb, base_lb;   // member parities the descriptors were written with
+    std::vector<int> flip;               // per member: its group's per-step flip
+    std::vector<BatchGroup> groups;
+    bool dirty = true;
+    int t = 0;                           // steps since the descriptors were written, mod 2
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_launches = 0;
+    SolveDesc* all_desc = nullptr;       // device, every member in member order (scalar gather)
+    Scalars* d_sc = nullptr;             // device gather buffer
+    Scalars* h_sc = nullptr;             // pinned host copy
+    size_t sc_cap = 0;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    std::string err;
+};
+
+namespace {
+
+int bfail(lssph_batch* b, int code, const std::string& msg) {
+    if (b) b->err = msg;
+    set_last_error(msg);
+    return code;
+}
+
+#define BATCH_TRY(b, call)                                                                       \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return bfail((b), LSSPH_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class F>
+void dispatch_lanes(int G, F&& f) {
+    switch (G) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        default: f(std::integral_constant<int, 4>{}); break;
+    }
+}
+
+template <class K>
+void optin(K kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8));
+}
+
+// Launch (or, with prep, only opt in the shared memory of) one batched phase kernel.
+void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
+    dispatch_lanes(g.G, [&](auto GG) {
+        constexpr int G = decltype(GG)::value;
+        auto run = [&](auto kern) {
+            if (prep) { optin(kern); return; }
+            kern<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, S, ps, pl);
+            ++*count;
+        };
+        if (g.nb == 1) run(kb_stage<1, G>);
+        else if (g.nb == 5) run(kb_stage<5, G>);
+        else run(kb_stage<4, G>);
+    });
+}
+
+void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset_umax, bool prep, int* count) {
+    dispatch_lanes(g.G, [&](auto GG) {
+        constexpr int G = decltype(GG)::value;
+        auto run = [&](auto kern) {
+            if (prep) { optin(kern); return; }
+            kern<<<g.nchunks, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.chunks}, ps, pl, zero_other, reset_umax);
+            ++*count;
+        };
+        auto by_wq = [&](auto NBc) {
+            constexpr int NB = decltype(NBc)::value;
+            if (g.wq == 1) run(kb_ghost<NB, G, 1>);
+            else if (g.wq == 6) run(kb_ghost<NB, G, 6>);
+            else run(kb_ghost<NB, G, 3>);
+        };
+        if (g.nbg == 1) by_wq(std::integral_constant<int, 1>{});
+        else if (g.nbg == 4) by_wq(std::integral_constant<int, 4>{});
+        else by_wq(std::integral_constant<int, 3>{});
+    });
+}
+
+void launch_pst(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
+    dispatch_lanes(g.G, [&](auto GG) {
+        constexpr int G = decltype(GG)::value;
+        auto run = [&](auto kern) {
+            if (prep) { optin(kern); return; }
+            kern<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, ps, pl);
+            ++*count;
+        };
+        if (g.nb == 5) run(kb_pst<4, G>);
+        else run(kb_pst<3, G>);
+    });
+}
+
+// One time step of one group, starting at relative parity (ps, pl); the same sequence
+// as a solo step (enq_step in engine.cu).
+void enq_group_step(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
+    const int ns = g.rk == 2 ? 2 : 4;
+    for (int s = 1; s <= ns; ++s) {
+        StageCfg S{};
+        S.mode = MODE_STAGE;
+        S.stage = s;
+        S.last = (s == ns) ? 1 : 0;
+        S.do_scatter = g.p1 ? 0 : 1;
+        S.do_umax = g.pst_on ? 1 : 0;
+        S.do_steady = g.p1 ? 1 : 0;
+        S.write_rhs = 1;
+        launch_stage(g, S, ps, pl, prep, count);
+        ps ^= 1;
+        if (!g.p1) {
+            pl ^= 1;
+            launch_ghost(g, ps, pl, 1, 0, prep, count);
+        } else {
+            launch_ghost(g, ps, pl, 0, 0, prep, count);
+        }
+    }
+    if (g.pst_on) {
+        launch_pst(g, ps, pl, prep, count);
+        ps ^= 1;
+        pl ^= 1;
+        launch_ghost(g, ps, pl, 1, 1, prep, count);
+    }
+    if (g.p1 && !prep) {
+        kb_epilogue<<<(int)((g.members.size() + 127) / 128), 128, 0, g.stream>>>(g.D, (int)g.members.size());
+        ++*count;
+    }
+}
+
+SolveDesc make_desc(const lssph_handle* h) {
+    SolveDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.P = h->P;
+    d.F[0] = h->F[0];
+    d.F[1] = h->F[1];
+    d.L[0] = h->L[0];
+    d.L[1] = h->L[1];
+    d.W = h->W;
+    d.V = h->V;
+    d.VT = VMTiles{h->vt_tile, h->vt_start, h->vt_vm};
+    d.gstart = h->gstart;
+    d.glist = h->glist;
+    d.sc = h->sc;
+    d.ntx = h->ntx;
+    d.sb = h->sb;
+    d.lb = h->lb;
+    d.nchunk = h->nvt;
+    const double dt = h->p.dt;   // the step sizes enq_stage (engine.cu) hands each stage
+    if (h->p.rk == 2) {
+        d.dt2[0] = dt / 2.0;
+        d.dt2[1] = dt;
+    } else {
+        d.dt1[0] = dt / 6.0; d.dt2[0] = dt / 2.0;
+        d.dt1[1] = dt / 3.0; d.dt2[1] = dt / 2.0;
+        d.dt1[2] = dt / 3.0; d.dt2[2] = dt;
+        d.dt1[3] = dt / 6.0; d.dt2[3] = 0.0;
+    }
+    return d;
+}
+
+void release_groups(lssph_batch* b) {
+    for (auto& g : b->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto& g : b->groups) {
+        cudaFree(g.D);
+        cudaFree(g.tiles);
+        cudaFree(g.chunks);
+        if (g.join) cudaEventDestroy(g.join);
+        if (g.stream) cudaStreamDestroy(g.stream);
+    }
+    b->groups.clear();
+    cudaFree(b->all_desc);
+    b->all_desc = nullptr;
+}
+
+template <class T>
+int upload(lssph_batch* b, T** dst, const std::vector<T>& src) {
+    *dst = nullptr;
+    BATCH_TRY(b, cudaMalloc(dst, sizeof(T) * std::max<size_t>(src.size(), 1)));
+    if (!src.empty()) BATCH_TRY(b, cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, b->stream));
+    return LSSPH_OK;
+}
+
+// Regroup the members and rewrite descriptors and CTA maps from their current parities.
+int rebuild(lssph_batch* b) {
+    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    release_groups(b);
+    const size_t n = b->members.size();
+    b->base_sb.assign(n, 0);
+    b->base_lb.assign(n, 0);
+    b->flip.assign(n, 0);
+    std::map<std::tuple<int, int, int, int>, int> index;
+    for (size_t i = 0; i < n; ++i) {
+        const lssph_handle* h = b->members[i];
+        const auto key = std::make_tuple(h->nb_rhs, h->wq, h->p.rk, h->G);
+        auto it = index.find(key);
+        if (it == index.end()) {
+            BatchGroup g;
+            g.nb = h->nb_rhs;
+            g.nbg = h->nb_ghost;
+            g.wq = h->wq;
+            g.rk = h->p.rk;
+            g.G = h->G;
+            g.p1 = h->p1;
+            g.pst_on = h->pst_on;
+            g.flip = h->p1 ? 0 : 1;
+            it = index.emplace(key, (int)b->groups.size()).first;
+            b->groups.push_back(g);
+        }
+        b->groups[it->second].members.push_back((int)i);
+        b->base_sb[i] = b->members[i]->sb;
+        b->base_lb[i] = b->members[i]->lb;
+        b->flip[i] = b->groups[it->second].flip;
+    }
+    std::vector<SolveDesc> all;
+    for (auto& g : b->groups) {
+        std::vector<SolveDesc> desc;
+        std::vector<int2> tiles, chunks;
+        for (size_t s = 0; s < g.members.size(); ++s) {
+            const lssph_handle* h = b->members[g.members[s]];
+            desc.push_back(make_desc(h));
+            for (int t = 0; t < h->ntiles; ++t) tiles.push_back(make_int2((int)s, t));
+            for (int c = 0; c < h->nvt; ++c) chunks.push_back(make_int2((int)s, c));
+            g.smem = std::max(g.smem, h->smem_bytes);
+        }
+        g.ntiles = (int)tiles.size();
+        g.nchunks = (int)chunks.size();
+        int rc;
+        if ((rc = upload(b, &g.D, desc)) != LSSPH_OK || (rc = upload(b, &g.tiles, tiles)) != LSSPH_OK ||
+            (rc = upload(b, &g.chunks, chunks)) != LSSPH_OK)
+            return rc;
+        BATCH_TRY(b, cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+        BATCH_TRY(b, cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
+        int unused = 0;
+        enq_group_step(g, 0, 0, true, &unused);   // shared-memory opt-in of every kernel used
+    }
+    for (size_t i = 0; i < n; ++i) all.push_back(make_desc(b->members[i]));
+    int rc = upload(b, &b->all_desc, all);
+    if (rc != LSSPH_OK) return rc;
+    if (b->sc_cap < n) {
+        cudaFree(b->d_sc);
+        cudaFreeHost(b->h_sc);
+        b->d_sc = nullptr;
+        b->h_sc = nullptr;
+        b->sc_cap = 0;
+        BATCH_TRY(b, cudaMalloc(&b->d_sc, sizeof(Scalars) * n));
+        BATCH_TRY(b, cudaMallocHost(&b->h_sc, sizeof(Scalars) * n));
+        b->sc_cap = n;
+    }
+    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    b->t = 0;
+    b->dirty = false;
+    return LSSPH_OK;
+}
+
+// Every member's scalars, read back in one copy (the batch stream is idle afterwards).
+int gather_scalars(lssph_batch* b) {
+    const int n = (int)b->members.size();
+    kb_gather_scalars<<<(n + 127) / 128, 128, 0, b->stream>>>(b->all_desc, n, b->d_sc);
+    BATCH_TRY(b, cudaGetLastError());
+    BATCH_TRY(b, cudaMemcpyAsync(b->h_sc, b->d_sc, sizeof(Scalars) * n, cudaMemcpyDeviceToHost, b->stream));
+    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    return LSSPH_OK;
+}
+
+int capture(lssph_batch* b, int t, cudaGraphExec_t* out) {
+    BATCH_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(b->fork, b->stream);
+    int count = 0;
+    for (auto& g : b->groups) {
+        cudaStreamWaitEvent(g.stream, b->fork, 0);
+        const int par = g.flip & t;
+        enq_group_step(g, par, par, false, &count);
+        cudaEventRecord(g.join, g.stream);
+        cudaStreamWaitEvent(b->stream, g.join, 0);
+    }
+    cudaGraph_t graph = nullptr;
+    BATCH_TRY(b, cudaStreamEndCapture(b->stream, &graph));
+    const cudaError_t e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return bfail(b, LSSPH_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    b->graph_launches = count;
+    return LSSPH_OK;
+}
+
+int member_status(const Scalars& s) {
+    if (s.err & ERR_NONFINITE) return LSSPH_E_NONFINITE;
+    if (s.err & ERR_OUT_OF_DOMAIN) return LSSPH_E_OUT_OF_DOMAIN;
+    if (s.err & ERR_CELL_OVERFLOW) return LSSPH_E_CELL_OVERFLOW;
+    return LSSPH_OK;
+}
+
+}  // namespace
+
+namespace lssph {
+void batch_forget(lssph_batch* b, lssph_handle* h) { lssph_batch_remove(b, h); }
+}  // namespace lssph
+
+extern "C" {
+
+int lssph_batch_create(lssph_batch** out) {
+    if (!out) return bfail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    *out = nullptr;
+    lssph_batch* b = new lssph_batch();
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
+        lssph_batch_destroy(b);
+        return bfail(nullptr, LSSPH_E_CUDA, "stream/event creation failed");
+    }
+    *out = b;
+    return LSSPH_OK;
+}
+
+void lssph_batch_destroy(lssph_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (lssph_handle* h : b->members) h->batch = nullptr;
+    release_groups(b);
+    cudaFree(b->d_sc);
+    cudaFreeHost(b->h_sc);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char* lssph_batch_error(const lssph_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int lssph_batch_add(lssph_batch* b, lssph_handle* h) {
+    if (!b || !h) return bfail(b, LSSPH_E_BAD_PARAM, "null argument");
+    if (h->batch) return bfail(b, LSSPH_E_BAD_PARAM, "the handle is already a member of a batch");
+    b->members.push_back(h);
+    h->batch = b;
+    b->dirty = true;
+    return LSSPH_OK;
+}
+
+int lssph_batch_remove(lssph_batch* b, lssph_handle* h) {
+    if (!b || !h) return bfail(b, LSSPH_E_BAD_PARAM, "null argument");
+    auto it = std::find(b->members.begin(), b->members.end(), h);
+    if (it == b->members.end()) return bfail(b, LSSPH_E_BAD_PARAM, "the handle is not a member of this batch");
+    cudaStreamSynchronize(b->stream);
+    b->members.erase(it);
+    h->batch = nullptr;
+    b->dirty = true;
+    return LSSPH_OK;
+}
+
+int lssph_batch_size(const lssph_batch* b) { return b ? (int)b->members.size() : 0; }
+
+int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady) {
+    if (!b) return bfail(nullptr, LSSPH_E_BAD_PARAM, "null batch");
+    const size_t n = b->members.size();
+    for (size_t i = 0; i < n; ++i) {
+        if (status) status[i] = LSSPH_OK;
+        if (steady) steady[i] = 0;
+    }
+    b->last_ms = 0.0;
+    b->last_launches = 0;
+    if (nsteps <= 0 || n == 0) return LSSPH_OK;
+    // a member stepped on its own since the last batch call: rewrite the descriptors
+    for (size_t i = 0; i < n && !b->dirty; ++i) {
+        const int par = b->flip[i] & b->t;
+        if (b->members[i]->sb != (b->base_sb[i] ^ par) || b->members[i]->lb != (b->base_lb[i] ^ par)) b->dirty = true;
+    }
+    int rc;
+    if (b->dirty && (rc = rebuild(b)) != LSSPH_OK) return rc;
+    if ((rc = gather_scalars(b)) != LSSPH_OK) return rc;
+    std::vector<Scalars> s0(b->h_sc, b->h_sc + n);
+    BATCH_TRY(b, cudaEventRecord(b->ev0, b->stream));
+    for (int st = 0; st < nsteps; ++st) {
+        cudaGraphExec_t& ge = b->graph[b->t];
+        if (!ge && (rc = capture(b, b->t, &ge)) != LSSPH_OK) return rc;
+        BATCH_TRY(b, cudaGraphLaunch(ge, b->stream));
+        b->t ^= 1;
+        for (size_t i = 0; i < n; ++i) {   // members follow the batch's parity
+            b->members[i]->sb ^= b->flip[i];
+            b->members[i]->lb ^= b->flip[i];
+        }
+    }
+    BATCH_TRY(b, cudaEventRecord(b->ev1, b->stream));
+    if ((rc = gather_scalars(b)) != LSSPH_OK) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->last_ms = ms;
+    b->last_launches = (int64_t)nsteps * b->graph_launches;
+    int first = LSSPH_OK;
+    for (size_t i = 0; i < n; ++i) {
+        const Scalars& s1 = b->h_sc[i];
+        const int st = member_status(s1);
+        if (status) status[i] = st;
+        if (st != LSSPH_OK) {
+            b->members[i]->err = lssph_status_string(st);
+            if (first == LSSPH_OK) first = st;
+        }
+        if (steady && s1.steady && !s0[i].steady) steady[i] = s1.steady_step - s0[i].step_count;
+    }
+    if (first != LSSPH_OK) return bfail(b, first, "a batch member stopped with an error (see the status array)");
+    return LSSPH_OK;
+}
+
+int lssph_batch_last_step_stats(const lssph_batch* b, double* device_ms, int64_t* kernel_launches) {
+    if (!b) return bfail(nullptr, LSSPH_E_BAD_PARAM, "null batch");
+    if (device_ms) *device_ms = b->last_ms;
+    if (kernel_launches) *kernel_launches = b->last_launches;
+    return LSSPH_OK;
+}
+
+}  // extern "C"

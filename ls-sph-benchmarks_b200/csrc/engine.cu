@@ -26,50 +26,10 @@
 #include <vector>
 
 #include "engine.h"
-#include "kernels.cuh"
+#include "handle.h"
 
 using namespace lssph;
 
-struct lssph_handle {
-    lssph_params p{};
-    int num_total = 0, num_int = 0, num_ext = 0;
-    int problem = 0;
-    bool has_tem = false, p1 = false, pst_on = false;
-    int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
-    int G = 4, Gg = 4;
-    CellGrid grid;
-    VirtualMarkers vm;
-    std::vector<int32_t> ptype;
-    Phys P{};
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<void*> allocs;
-    Fld F[2]{};
-    Lst L[2]{};
-    Work W{};
-    VMd V{};
-    int* gstart = nullptr;
-    int* glist = nullptr;
-    int ntx = 0, nty = 0, ntiles = 0;   // cell tiles
-    int nvt = 0;                        // tiles holding virtual markers
-    int *vt_tile = nullptr, *vt_start = nullptr, *vt_vm = nullptr;
-    size_t smem_bytes = 0;
-    bool preparing = false;             // launch helpers only set kernel attributes
-    Scalars* sc = nullptr;
-    int sb = 0, lb = 0;
-    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    int graph_launches = 0;   // kernels per captured step
-    int step_flip = 0;        // parity change per step
-    int64_t launch_counter = 0;
-    double last_ms = 0.0;
-    int64_t last_launches = 0;
-    // per-launch event pairs while profiling (lssph_step_profiled)
-    bool profiling = false;
-    std::vector<cudaEvent_t> prof_events;
-    std::vector<int> prof_kinds;
-    size_t prof_next = 0;
-    std::string err;
-};
 
 namespace {
 
@@ -326,6 +286,7 @@ int upload_fields(lssph_handle* h, const double* x, const double* y, const doubl
 
 void free_handle(lssph_handle* h) {
     if (!h) return;
+    if (h->batch) batch_forget(h->batch, h);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& row : h->graph)
         for (auto& g : row)

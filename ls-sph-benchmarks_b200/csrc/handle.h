@@ -1,0 +1,59 @@
+// handle.h -- the device state of one solve (lssph_handle), shared by the single-solve
+// entry points (engine.cu) and the batched time loop (batch.cu).  Internal header.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "kernels.cuh"
+
+struct lssph_handle {
+
+    lssph_params p{};
+    int num_total = 0, num_int = 0, num_ext = 0;
+    int problem = 0;
+    bool has_tem = false, p1 = false, pst_on = false;
+    int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
+    int G = 4, Gg = 4;
+    lssph::CellGrid grid;
+    lssph::VirtualMarkers vm;
+    std::vector<int32_t> ptype;
+    lssph::Phys P{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<void*> allocs;
+    lssph::Fld F[2]{};
+    lssph::Lst L[2]{};
+    lssph::Work W{};
+    lssph::VMd V{};
+    int* gstart = nullptr;
+    int* glist = nullptr;
+    int ntx = 0, nty = 0, ntiles = 0;   // cell tiles
+    int nvt = 0;                        // tiles holding virtual markers
+    int *vt_tile = nullptr, *vt_start = nullptr, *vt_vm = nullptr;
+    size_t smem_bytes = 0;
+    bool preparing = false;             // launch helpers only set kernel attributes
+    lssph::Scalars* sc = nullptr;
+    int sb = 0, lb = 0;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int graph_launches = 0;   // kernels per captured step
+    int step_flip = 0;        // parity change per step
+    int64_t launch_counter = 0;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    // per-launch event pairs while profiling (lssph_step_profiled)
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_events;
+    std::vector<int> prof_kinds;
+    size_t prof_next = 0;
+    lssph_batch* batch = nullptr;   // the batch this solve is a member of, if any
+    std::string err;
+};
+
+namespace lssph {
+// Drop a handle that is being destroyed from the batch that holds it (batch.cu).
+void batch_forget(lssph_batch* b, lssph_handle* h);
+}  // namespace lssph

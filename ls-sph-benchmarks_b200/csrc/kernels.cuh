@@ -677,18 +677,18 @@ __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, co
     return red;
 }
 
+// One tile of one solve (the CTA's work in both the single-solve and the batched kernel).
 template <int NB, int G>
-__global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
-                                                   const Lst Ln, const int* __restrict__ gstart,
-                                                   const int* __restrict__ glist, const Work W, const StageCfg S,
-                                                   Scalars* sc, int ntx) {
+__device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
+                                           const int* __restrict__ gstart, const int* __restrict__ glist,
+                                           const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
     const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
     static_assert(15 + 5 * NB + 1 <= SUMS, "reduced sums overflow");
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
     const SmemView SM = smem_view(smem_raw, P.cap);
-    const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+    const int tx = tile % ntx, ty = tile / ntx;
     stage_halo<false, NB == 5>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
     if (stop) return;
     const int n_own = T.own_off[OC];
@@ -788,6 +788,14 @@ __global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, 
     }
 }
 
+template <int NB, int G>
+__global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+                                                   const Lst Ln, const int* __restrict__ gstart,
+                                                   const int* __restrict__ glist, const Work W, const StageCfg S,
+                                                   Scalars* sc, int ntx) {
+    stage_body<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, blockIdx.x);
+}
+
 // =======================================================================================
 // k_ghost: interpolation at the virtual markers + extrapolation to the ghost particles.
 // WQ = 3 / 6: LS type B (interpolate_LSSPH_B_mod.f90, WALL_MODEL 2 / 3); WQ = 1: CSPH
@@ -801,27 +809,27 @@ struct VMTiles {
     const int* vm;      // virtual-marker ids grouped by tile, ascending
 };
 
+// One chunk (<= PPB markers of one tile) of one solve; nchunk = chunks of this solve.
 template <int NB, int G, int WQ>
-__global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, const Lst L,
-                                                   const int* __restrict__ gstart, const int* __restrict__ glist,
-                                                   const VMd V, const VMTiles VT, int ntx, int* zero_cnt,
-                                                   int reset_umax, Scalars* sc) {
+__device__ __forceinline__ void ghost_body(const Phys& P, const Fld& F, const Lst& L, const int* __restrict__ gstart,
+                                           const int* __restrict__ glist, const VMd& V, const VMTiles& VT, int ntx,
+                                           int* zero_cnt, int reset_umax, Scalars* sc, int chunk, int nchunk) {
     if (zero_cnt) {
-        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < P.ncell; c += gridDim.x * blockDim.x) zero_cnt[c] = 0;
+        for (int c = chunk * blockDim.x + threadIdx.x; c < P.ncell; c += nchunk * blockDim.x) zero_cnt[c] = 0;
     }
-    if (reset_umax && blockIdx.x == 0 && threadIdx.x == 0) sc->umax2 = 0ull;
+    if (reset_umax && chunk == 0 && threadIdx.x == 0) sc->umax2 = 0ull;
     const bool stop = halted(sc);   // consumed after staging
     constexpr int Q = (WQ == 1) ? 1 : WQ;
     constexpr int NU = Q * (Q + 1) / 2;
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
     const SmemView SM = smem_view(smem_raw, P.cap);
-    const int tile = VT.tile[blockIdx.x];
+    const int tile = VT.tile[chunk];
     const int tx = tile % ntx, ty = tile / ntx;
     const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
     stage_halo<true, NB == 4>(P, F, L, gstart, glist, cx0, cy0, T, SM);
     if (stop) return;
-    const int v0 = VT.start[blockIdx.x], nvm = VT.start[blockIdx.x + 1] - v0;
+    const int v0 = VT.start[chunk], nvm = VT.start[chunk + 1] - v0;
     const int lane = threadIdx.x & (G - 1);
     const int o = (int)threadIdx.x / G;
     const bool active = o < nvm;
@@ -968,21 +976,29 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
     }
 }
 
+template <int NB, int G, int WQ>
+__global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, const Lst L,
+                                                   const int* __restrict__ gstart, const int* __restrict__ glist,
+                                                   const VMd V, const VMTiles VT, int ntx, int* zero_cnt,
+                                                   int reset_umax, Scalars* sc) {
+    ghost_body<NB, G, WQ>(P, F, L, gstart, glist, V, VT, ntx, zero_cnt, reset_umax, sc, blockIdx.x, gridDim.x);
+}
+
 // =======================================================================================
 // k_pst: particle shifting (q = 5) + copy-back + EOS + cell scatter.
 // NB = 3 (u,v,rho) or 4 (+T).  umax2 holds max(u^2+v^2) of the state being shifted.
 // =======================================================================================
 template <int NB, int G>
-__global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
-                                                 const Lst Ln, const int* __restrict__ gstart,
-                                                 const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
+__device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
+                                         const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
+                                         Scalars* sc, int ntx, int tile) {
     const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
     static_assert(15 + 5 * NB + 3 <= SUMS, "reduced sums overflow");
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
     const SmemView SM = smem_view(smem_raw, P.cap);
-    const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+    const int tx = tile % ntx, ty = tile / ntx;
     stage_halo<false, NB == 4>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
     if (stop) return;
     const int n_own = T.own_off[OC];
@@ -1109,6 +1125,80 @@ __global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, co
     }
 }
 
+template <int NB, int G>
+__global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+                                                 const Lst Ln, const int* __restrict__ gstart,
+                                                 const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
+    pst_body<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, blockIdx.x);
+}
+
+// =======================================================================================
+// Batched kernels: one launch runs a phase for every solve of a batch.  Each CTA reads
+// its (solve, tile-or-chunk) from a map built on the host and that solve's descriptor;
+// buffer parities are the solve's base parity xor the launch's parity, so solves that
+// joined the batch at different times keep their own ping-pong state.
+// =======================================================================================
+struct SolveDesc {
+    Phys P;
+    Fld F[2];
+    Lst L[2];
+    Work W;
+    VMd V;
+    VMTiles VT;
+    const int* gstart;
+    const int* glist;
+    Scalars* sc;
+    double dt1[4], dt2[4];     // per-stage RK step sizes (StageCfg.dt1/dt2 of a solo step)
+    int ntx, sb, lb, nchunk;   // sb/lb: buffer parity of the solve when the descriptor was written
+    int pad_;
+};
+
+struct BatchMap {
+    const int2* cta;     // (solve, tile-or-chunk) per CTA
+};
+
+// Copy the CTA's solve descriptor to shared memory (one global round trip for all of it).
+__device__ __forceinline__ const SolveDesc& load_desc(const SolveDesc* D, int s, SolveDesc& sd) {
+    static_assert(sizeof(SolveDesc) % 8 == 0, "descriptor is copied in 8-byte words");
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(D + s);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+    for (int k = threadIdx.x; k < (int)(sizeof(SolveDesc) / 8); k += blockDim.x) dst[k] = src[k];
+    __syncthreads();
+    return sd;
+}
+
+template <int NB, int G>
+__global__ void __launch_bounds__(PPB * G) kb_stage(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
+                                                    int ps, int pl) {
+    __shared__ SolveDesc sd;
+    const int2 m = M.cta[blockIdx.x];
+    const SolveDesc& d = load_desc(D, m.x, sd);
+    const int sb = d.sb ^ ps, lb = d.lb ^ pl;
+    S.dt1 = d.dt1[S.stage - 1];
+    S.dt2 = d.dt2[S.stage - 1];
+    stage_body<NB, G>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, S, d.sc, d.ntx, m.y);
+}
+
+template <int NB, int G, int WQ>
+__global__ void __launch_bounds__(PPB * G) kb_ghost(const SolveDesc* __restrict__ D, const BatchMap M, int ps, int pl,
+                                                    int zero_other, int reset_umax) {
+    __shared__ SolveDesc sd;
+    const int2 m = M.cta[blockIdx.x];
+    const SolveDesc& d = load_desc(D, m.x, sd);
+    const int sb = d.sb ^ ps, lb = d.lb ^ pl;
+    ghost_body<NB, G, WQ>(d.P, d.F[sb], d.L[lb], d.gstart, d.glist, d.V, d.VT, d.ntx,
+                          zero_other ? d.L[lb ^ 1].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
+}
+
+template <int NB, int G>
+__global__ void __launch_bounds__(PPB * G) kb_pst(const SolveDesc* __restrict__ D, const BatchMap M, int ps, int pl) {
+    __shared__ SolveDesc sd;
+    const int2 m = M.cta[blockIdx.x];
+    const SolveDesc& d = load_desc(D, m.x, sd);
+    const int sb = d.sb ^ ps, lb = d.lb ^ pl;
+    pst_body<NB, G>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, d.sc, d.ntx, m.y);
+}
+
 // =======================================================================================
 // Small kernels (static: this header is compiled into more than one translation unit)
 // =======================================================================================
@@ -1143,15 +1233,29 @@ static __global__ void k_copy_fprev(const Phys P, const Fld F, const Work W) {
 
 // Problem 1 epilogue of a step (main.f90:139-149 with check_steady_state_mod.f90:39-65):
 // the stage kernel already reduced max|f_previous - u|.
-static __global__ void k_epilogue(const Phys P, Scalars* sc) {
+__device__ __forceinline__ void epilogue_body(double threshold, Scalars* sc) {
     if (sc->err != 0 || sc->steady != 0) return;
     sc->step_count += 1;
     const double df = __longlong_as_double((long long)sc->dfmax);
-    if (df < P.threshold) {
+    if (df < threshold) {
         sc->steady = 1;
         sc->steady_step = sc->step_count;
     }
     sc->dfmax = 0ull;
+}
+
+static __global__ void k_epilogue(const Phys P, Scalars* sc) { epilogue_body(P.threshold, sc); }
+
+// Problem-1 epilogue for every solve of a batch (one thread per solve).
+static __global__ void kb_epilogue(const SolveDesc* __restrict__ D, int nsolve) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nsolve) epilogue_body(D[s].P.threshold, D[s].sc);
+}
+
+// Copy every batch member's scalars into one array (one read-back per batch call).
+static __global__ void kb_gather_scalars(const SolveDesc* __restrict__ D, int nsolve, Scalars* out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nsolve) out[s] = *D[s].sc;
 }
 
 static __global__ void k_volume(const Phys P, const Fld F) {

@@ -4,10 +4,11 @@ from ._abi import (LIB_PATH, PRECISION_FP64, PRECISION_MIXED, LssphError, Params
 from .params import (boussinesq_params, cavity_params, check_param, default_params, diffusion_params,
                      from_config, init_param, make_params, taylor_green_params, write_config_h)
 from .simulation import Simulation, State, read_data, setup_particles
+from .batch import Batch
 
 __all__ = [
     "LIB_PATH", "PRECISION_FP64", "PRECISION_MIXED", "LssphError", "Params", "exported_names", "load",
     "boussinesq_params", "cavity_params", "check_param", "default_params", "diffusion_params",
     "from_config", "init_param", "make_params", "taylor_green_params", "write_config_h",
-    "Simulation", "State", "read_data", "setup_particles",
+    "Simulation", "State", "read_data", "setup_particles", "Batch",
 ]

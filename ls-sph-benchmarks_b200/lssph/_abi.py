@@ -159,6 +159,14 @@ _PROTOS = {
     "lssph_read_data": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _i, _d, _d, _d, _d, _d, _d, _d]),
     "lssph_last_step_stats": (C.c_int, [_H, _P(C.c_double), _P(C.c_int64)]),
     "lssph_step_profiled": (C.c_int, [_H, C.c_int32, _d, _P(C.c_int64)]),
+    "lssph_batch_create": (C.c_int, [_P(C.c_void_p)]),
+    "lssph_batch_destroy": (None, [_H]),
+    "lssph_batch_error": (C.c_char_p, [_H]),
+    "lssph_batch_add": (C.c_int, [_H, _H]),
+    "lssph_batch_remove": (C.c_int, [_H, _H]),
+    "lssph_batch_size": (C.c_int, [_H]),
+    "lssph_batch_step": (C.c_int, [_H, C.c_int32, _i, _i]),
+    "lssph_batch_last_step_stats": (C.c_int, [_H, _P(C.c_double), _P(C.c_int64)]),
     # device pointers (caller-owned device memory), stream handle
     "lssph_rhs_noalloc": (C.c_int, [_P(Params), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
