@@ -56,53 +56,101 @@ _REASONS = ["gpu_idle", "applications_clocks_setting", "sw_power_cap", "hw_slowd
 
 
 class ClockSampler:
+    """SM clock, max clock and clock-event reasons sampled every 10 ms while the timed
+    region runs.  Reads NVML (the library nvidia-smi reports from); falls back to
+    `nvidia-smi -lms 200` when the NVML binding is missing."""
+
     def __init__(self, device_index: int):
         self.dev = device_index
-        self.proc = None
-        self.lines = []
+        self.rows = []            # (sm_mhz, max_mhz, reasons_bits)
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+        self._h = None
+        self._proc = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _sample(self):
+        nv, h = self._nvml, self._h
+        try:
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except AttributeError:
+            reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                          float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)), int(reasons)))
+
+    def _loop(self):
+        while not self._stop.wait(0.01):
+            try:
+                self._sample()
+            except Exception:
+                return
+
+    def _smi_loop(self):
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            try:
+                bits = int(parts[2], 16) if parts[2].startswith("0x") else int(parts[2])
+                self.rows.append((float(parts[0]), float(parts[1]), bits))
+            except (ValueError, IndexError):
+                continue
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.dev),
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            threading.Thread(target=self._read, daemon=True).start()
-        except OSError:
-            self.proc = None
+            self._h = self._nvml_handle()
+            self._sample()
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+        except Exception:
+            self._nvml = None
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+                     "--format=csv,noheader,nounits", "-lms", "200"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._thread = threading.Thread(target=self._smi_loop, daemon=True)
+            except OSError:
+                self._thread = None
+        if self._thread:
+            self._thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self._nvml is not None:
+            if self._thread:
+                self._thread.join(timeout=1)
             try:
-                self.proc.wait(timeout=5)
+                self._sample()
+            except Exception:
+                pass
+        elif self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        for line in self.lines:
-            parts = [s.strip() for s in line.split(",")]
-            if len(parts) < 4:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-                bits = int(parts[3], 16) if parts[3].startswith("0x") else int(parts[3])
-            except ValueError:
-                continue
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        reasons = set()
+        for _, _, bits in self.rows:
             for i, name in enumerate(_REASONS):
                 if bits & (1 << i) and name != "gpu_idle":
                     reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.rows[-1][1],
+                "reasons": sorted(reasons), "samples": len(self.rows),
+                "source": "nvml" if self._nvml is not None else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------------------
@@ -241,7 +289,8 @@ def run_engine(args) -> int:
     hbm_peak, peak_src = _measured_peaks()
     achieved_gbs = bytes_per_launch / stage_avg_s / 1e9
     traffic = _profile_traffic()
-    roofline = {"bound": "hbm", "kernel": "k_stage<NB=4,G=4>", "achieved": achieved_gbs, "peak": hbm_peak,
+    tune = sim.tuning()
+    roofline = {"bound": "hbm", "kernel": f"k_stage<NB=4,G={tune['lanes']},{tune['register_budget']} registers>", "achieved": achieved_gbs, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
                 "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_launch": bytes_per_launch,
@@ -284,7 +333,8 @@ def run_engine(args) -> int:
     if rank != 0:
         return 0
     cfg = _config(p, {"num_int": ni, "num_total": n_total, "parallelism": f"replicas{ws}",
-                      "lanes": args.lanes or 4, "global_batch": ni * ws})
+                      "lanes": tune["lanes"], "register_budget": tune["register_budget"],
+                      "global_batch": ni * ws})
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,

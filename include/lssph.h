@@ -182,6 +182,13 @@ int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32
                     double* x, double* y, double* u, double* v, double* rho, double* pre,
                     double* tem);
 
+/* Kernel configuration the handle runs (no counterpart in the reference): lanes per
+   particle, and whether the stage/PST kernels use the tight register budget (1) or the
+   loose one (0), with the RHS-pass time of each measured when the handle was created.
+   The budget is picked by that measurement; it never changes a result. */
+int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
+                     double* rhs_us_tight);
+
 /* Device time of the kernels launched by the last lssph_step call, in milliseconds
    (CUDA events on the handle's stream), and the number of kernel launches it made. */
 int lssph_last_step_stats(const lssph_handle* h, double* device_ms, int64_t* kernel_launches);

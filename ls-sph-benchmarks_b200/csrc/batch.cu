@@ -39,6 +39,7 @@ struct BatchGroup {
     int2* tiles = nullptr;         // (solve, tile) per CTA of stage / PST launches
     int2* chunks = nullptr;        // (solve, chunk) per CTA of ghost launches
     int ntiles = 0, nchunks = 0;
+    bool tight = false;            // register budget of the stage / PST kernels
     size_t smem = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t join = nullptr;
@@ -68,6 +69,10 @@ struct lssph_batch {
 
 namespace {
 
+// Tiles per launch above which a group uses the tight register budget even when none of
+// its members chose it alone (about two waves at the loose budget's 3 CTAs per SM).
+constexpr size_t kTightTiles = 2 * 148 * 3;
+
 int bfail(lssph_batch* b, int code, const std::string& msg) {
     if (b) b->err = msg;
     set_last_error(msg);
@@ -93,21 +98,21 @@ void dispatch_lanes(int G, F&& f) {
 
 template <class K>
 void optin(K kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8));
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8, true));
 }
 
 // Launch (or, with prep, only opt in the shared memory of) one batched phase kernel.
 void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
     dispatch_lanes(g.G, [&](auto GG) {
         constexpr int G = decltype(GG)::value;
-        auto run = [&](auto kern) {
-            if (prep) { optin(kern); return; }
-            kern<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, S, ps, pl);
+        auto run = [&](auto loose, auto tight) {
+            if (prep) { optin(loose); optin(tight); return; }
+            (g.tight ? tight : loose)<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, S, ps, pl);
             ++*count;
         };
-        if (g.nb == 1) run(kb_stage<1, G>);
-        else if (g.nb == 5) run(kb_stage<5, G>);
-        else run(kb_stage<4, G>);
+        if (g.nb == 1) run(kb_stage<1, G, false>, kb_stage<1, G, true>);
+        else if (g.nb == 5) run(kb_stage<5, G, false>, kb_stage<5, G, true>);
+        else run(kb_stage<4, G, false>, kb_stage<4, G, true>);
     });
 }
 
@@ -134,13 +139,13 @@ void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset
 void launch_pst(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
     dispatch_lanes(g.G, [&](auto GG) {
         constexpr int G = decltype(GG)::value;
-        auto run = [&](auto kern) {
-            if (prep) { optin(kern); return; }
-            kern<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, ps, pl);
+        auto run = [&](auto loose, auto tight) {
+            if (prep) { optin(loose); optin(tight); return; }
+            (g.tight ? tight : loose)<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, ps, pl);
             ++*count;
         };
-        if (g.nb == 5) run(kb_pst<4, G>);
-        else run(kb_pst<3, G>);
+        if (g.nb == 5) run(kb_pst<4, G, false>, kb_pst<4, G, true>);
+        else run(kb_pst<3, G, false>, kb_pst<3, G, true>);
     });
 }
 
@@ -273,7 +278,11 @@ int rebuild(lssph_batch* b) {
             for (int t = 0; t < h->ntiles; ++t) tiles.push_back(make_int2((int)s, t));
             for (int c = 0; c < h->nvt; ++c) chunks.push_back(make_int2((int)s, c));
             g.smem = std::max(g.smem, h->smem_bytes);
+            g.tight = g.tight || h->tight;
         }
+        // the tight budget wins once a launch has more tiles than fit at the loose one
+        // (3 CTAs per SM); a member that chose it alone keeps it in the group
+        g.tight = g.tight || tiles.size() > kTightTiles;
         g.ntiles = (int)tiles.size();
         g.nchunks = (int)chunks.size();
         int rc;

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -87,7 +88,7 @@ struct ProfScope {
 // instantiation while the handle is prepared (never during graph capture).
 template <class K>
 void smem_optin(K kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8));
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8, true));
 }
 
 // ---- kernel dispatch on the lane count ---------------------------------------------------
@@ -102,9 +103,9 @@ void launch_stage(lssph_handle* h, const StageCfg& S) {
     const int grid = h->ntiles;
     const size_t sm = h->smem_bytes;
 #define LSSPH_STAGE(GG)                                                                                 \
-    if (h->preparing) { smem_optin(k_stage<NB, GG>); return; }                                         \
-    k_stage<NB, GG><<<grid, PPB * GG, sm, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, S, \
-                                                  h->sc, h->ntx)
+    if (h->preparing) { smem_optin(k_stage<NB, GG, false>); smem_optin(k_stage<NB, GG, true>); return; }   \
+    (h->tight ? k_stage<NB, GG, true> : k_stage<NB, GG, false>)<<<grid, PPB * GG, sm, h->stream>>>(         \
+        h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, S, h->sc, h->ntx)
     switch (G) {
         case 1: LSSPH_STAGE(1); break;
         case 2: LSSPH_STAGE(2); break;
@@ -168,9 +169,9 @@ void launch_pst_t(lssph_handle* h) {
     const int G = h->G;
     const size_t sm = h->smem_bytes;
 #define LSSPH_PST(GG)                                                                                       \
-    if (h->preparing) { smem_optin(k_pst<NB, GG>); return; }                                               \
-    k_pst<NB, GG><<<h->ntiles, PPB * GG, sm, h->stream>>>(h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, h->sc, \
-                                                      h->ntx)
+    if (h->preparing) { smem_optin(k_pst<NB, GG, false>); smem_optin(k_pst<NB, GG, true>); return; }           \
+    (h->tight ? k_pst<NB, GG, true> : k_pst<NB, GG, false>)<<<h->ntiles, PPB * GG, sm, h->stream>>>(             \
+        h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, h->sc, h->ntx)
     switch (G) {
         case 1: LSSPH_PST(1); break;
         case 2: LSSPH_PST(2); break;
@@ -240,6 +241,38 @@ void enq_step(lssph_handle* h) {
         k_epilogue<<<1, 1, 0, h->stream>>>(h->P, h->sc);
         h->launch_counter++;
     }
+}
+
+int sync_check(lssph_handle* h);
+
+// Pick the register budget of the stage and PST kernels: time the RHS pass of the
+// current state (writes only the RHS arrays) with each budget, keep the faster.  Both
+// budgets give bit-identical results, so the choice never changes an answer.
+int autotune(lssph_handle* h) {
+    StageCfg S{};
+    S.mode = MODE_RHS_ONLY;
+    S.stage = 1;
+    S.write_rhs = 1;
+    const int64_t c0 = h->launch_counter;
+    const char* force = std::getenv("LSSPH_REGISTER_BUDGET");   // "loose" / "tight": skip the timing
+    if (force && (std::strcmp(force, "loose") == 0 || std::strcmp(force, "tight") == 0)) {
+        h->tight = std::strcmp(force, "tight") == 0;
+        return LSSPH_OK;
+    }
+    for (int t = 0; t < 2; ++t) {
+        h->tight = t == 1;
+        launch_stage_any(h, S);   // warm-up (instruction cache, L2)
+        CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+        for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
+        CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+        CUDA_TRY(h, cudaEventSynchronize(h->ev1));
+        float ms = 0.f;
+        CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        h->tune_us[t] = 1e3 * ms / 3.0;
+    }
+    h->tight = h->tune_us[1] < h->tune_us[0];
+    h->launch_counter = c0;
+    return sync_check(h);
 }
 
 int check_scalars(lssph_handle* h, Scalars* out) {
@@ -408,7 +441,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->ntx = (h->grid.nx + TX - 1) / TX;
     h->nty = (h->grid.ny + TY - 1) / TY;
     h->ntiles = h->ntx * h->nty;
-    h->smem_bytes = std::max(tile_smem_bytes(h->grid.cap, h->G), tile_smem_bytes(h->grid.cap, h->Gg));
+    h->smem_bytes = std::max(tile_smem_bytes(h->grid.cap, h->G, h->has_tem), tile_smem_bytes(h->grid.cap, h->Gg, h->has_tem));
     std::vector<int32_t> vt_tile, vt_start, vt_vm(NE);
     {
         std::vector<std::vector<int32_t>> by_tile(h->ntiles);
@@ -488,7 +521,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (!ok) { free_handle(h); return fail(nullptr, LSSPH_E_CUDA, "device initialisation failed"); }
     prepare_kernels(h);
     if ((rc = upload_fields(h, x, y, u, v, rho, pre, tem)) != LSSPH_OK ||
-        (rc = rebuild_cells(h)) != LSSPH_OK || (rc = sync_check(h)) != LSSPH_OK) {
+        (rc = rebuild_cells(h)) != LSSPH_OK || (rc = sync_check(h)) != LSSPH_OK ||
+        (rc = autotune(h)) != LSSPH_OK) {
         const std::string m = h->err;
         free_handle(h);
         return fail(nullptr, rc, m);
@@ -795,6 +829,16 @@ int lssph_step_profiled(lssph_handle* h, int32_t nsteps, double* ms_by_kind, int
         launches_by_kind[h->prof_kinds[k]] += 1;
     }
     return check_scalars(h, nullptr);
+}
+
+int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
+                     double* rhs_us_tight) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (lanes) *lanes = h->G;
+    if (tight) *tight = h->tight ? 1 : 0;
+    if (rhs_us_loose) *rhs_us_loose = h->tune_us[0];
+    if (rhs_us_tight) *rhs_us_tight = h->tune_us[1];
+    return LSSPH_OK;
 }
 
 int lssph_last_step_stats(const lssph_handle* h, double* device_ms, int64_t* kernel_launches) {

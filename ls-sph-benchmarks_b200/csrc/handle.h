@@ -18,6 +18,8 @@ struct lssph_handle {
     bool has_tem = false, p1 = false, pst_on = false;
     int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
     int G = 4, Gg = 4;
+    bool tight = false;                 // register budget of stage/PST kernels (autotuned)
+    double tune_us[2] = {0.0, 0.0};     // RHS pass time with the loose / tight budget
     lssph::CellGrid grid;
     lssph::VirtualMarkers vm;
     std::vector<int32_t> ptype;

@@ -331,6 +331,13 @@ constexpr int OC = TX * TY;                 // 4 own cells
 #define LSSPH_PPB 32
 #endif
 constexpr int PPB = LSSPH_PPB;              // particles per pass: a CTA has PPB * G threads
+// Register budgets of the stage and PST kernels.  Loose: the compiler's choice (about 148
+// registers per thread, 3 CTAs of 128 threads per SM).  Tight: at most 128 registers, so
+// that 512 threads fit per SM, for a few spilled values.  Both compute identical results;
+// which is faster depends on how many tiles a launch has, and each handle times both.
+__host__ __device__ constexpr int tile_min_blocks(int G, bool tight) {
+    return (tight && PPB * G <= 512) ? 512 / (PPB * G) : 1;
+}
 static_assert(HC <= 32 && OC <= 32, "tile scans run in one warp");
 
 struct TileHdr {
@@ -343,7 +350,7 @@ struct TileHdr {
 // Dynamic shared memory: SoA fields of up to HC*cap staged particles, their global
 // indices, and the own-particle list.
 struct SmemView {
-    double* sums;   // [PPB][SUMS]
+    double* sums;   // [PPB][row stride]
     double *x, *y, *u, *v, *rho, *pre, *vol, *tem;
     int *idx, *own_k, *own_hc;
     int* nbr;   // in-radius lists, entry e of thread t at nbr[e * blockDim.x + t]
@@ -352,25 +359,30 @@ struct SmemView {
 // Per-thread in-radius list length: a lane tests at most ceil(9 cap / G) candidates.
 __host__ __device__ inline int nbr_list_len(int cap, int G) { return (9 * cap + G - 1) / G; }
 
-// Reduced sums handed from the pair phase to the solve phase, per particle of a pass.
-constexpr int SUMS = 48;   // 15 moment entries + up to 5 x 5 b entries + shift (2) + count
+// Reduced sums handed from the pair phase to the solve phase, one row per particle of a
+// pass: 15 moment entries + 5 x NB b entries + (PST) shift (2) + count.  The row stride is
+// odd so that a warp reading one row per thread spreads over all shared-memory banks.
+__host__ __device__ constexpr int sums_stride(int n) { return n | 1; }
+constexpr int SUMS_MAX = sums_stride(15 + 5 * 5 + 1);
 
-__host__ __device__ inline size_t tile_smem_bytes(int cap, int G) {
+// Dynamic shared memory of one tile CTA; temperature is staged only when `tem` is set.
+__host__ __device__ inline size_t tile_smem_bytes(int cap, int G, bool tem) {
     const size_t maxp = (size_t)HC * cap, maxo = (size_t)OC * cap;
     const size_t lists = (size_t)PPB * G * nbr_list_len(cap, G);
-    return (size_t)PPB * SUMS * sizeof(double) + maxp * (8 * sizeof(double) + sizeof(int)) +
+    return (size_t)PPB * SUMS_MAX * sizeof(double) + maxp * ((tem ? 8 : 7) * sizeof(double) + sizeof(int)) +
            2 * maxo * sizeof(int) + lists * sizeof(int);
 }
 
+template <bool TEM>
 __device__ __forceinline__ SmemView smem_view(void* raw, int cap) {
     SmemView S;
     const int maxp = HC * cap, maxo = OC * cap;
     double* d = static_cast<double*>(raw);
     S.sums = d;
-    d += PPB * SUMS;
+    d += PPB * SUMS_MAX;
     S.x = d; S.y = d + maxp; S.u = d + 2 * maxp; S.v = d + 3 * maxp; S.rho = d + 4 * maxp;
-    S.pre = d + 5 * maxp; S.vol = d + 6 * maxp; S.tem = d + 7 * maxp;
-    int* q = reinterpret_cast<int*>(d + 8 * maxp);
+    S.pre = d + 5 * maxp; S.vol = d + 6 * maxp; S.tem = TEM ? d + 7 * maxp : nullptr;
+    int* q = reinterpret_cast<int*>(d + (TEM ? 8 : 7) * maxp);
     S.idx = q; S.own_k = q + maxp; S.own_hc = q + maxp + maxo;
     S.nbr = q + maxp + 2 * maxo;
     return S;
@@ -684,10 +696,11 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
                                            const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
     const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
-    static_assert(15 + 5 * NB + 1 <= SUMS, "reduced sums overflow");
+    constexpr int SR = sums_stride(15 + 5 * NB + 1);
+    static_assert(SR <= SUMS_MAX, "reduced sums overflow");
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
-    const SmemView SM = smem_view(smem_raw, P.cap);
+    const SmemView SM = smem_view<NB == 5>(smem_raw, P.cap);
     const int tx = tile % ntx, ty = tile / ntx;
     stage_halo<false, NB == 5>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
     if (stop) return;
@@ -735,14 +748,14 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
 #pragma unroll
             for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
             if (active && lane == 0) {
-                double* sm = SM.sums + slot * SUMS;
+                double* sm = SM.sums + slot * SR;
 #pragma unroll
                 for (int k = 0; k < 15; ++k) sm[k] = Mu[k];
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
                     for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = B[c][k];
-                sm[SUMS - 1] = (double)cnt;
+                sm[SR - 1] = (double)cnt;
             }
         }
         __syncthreads();
@@ -750,9 +763,9 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
         double red = 0.0;
         const int o = ob + (int)threadIdx.x;
         if ((int)threadIdx.x < PPB && o < n_own) {
-            const double* sm = SM.sums + threadIdx.x * SUMS;
+            const double* sm = SM.sums + threadIdx.x * SR;
             const int ki = SM.own_k[o];
-            const int cnt = (int)sm[SUMS - 1];
+            const int cnt = (int)sm[SR - 1];
             double A[Q][Q];
             double B[NB][Q];
 #pragma unroll
@@ -788,8 +801,8 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
     }
 }
 
-template <int NB, int G>
-__global__ void __launch_bounds__(PPB * G) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+template <int NB, int G, bool TIGHT = false>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
                                                    const Lst Ln, const int* __restrict__ gstart,
                                                    const int* __restrict__ glist, const Work W, const StageCfg S,
                                                    Scalars* sc, int ntx) {
@@ -823,7 +836,7 @@ __device__ __forceinline__ void ghost_body(const Phys& P, const Fld& F, const Ls
     constexpr int NU = Q * (Q + 1) / 2;
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
-    const SmemView SM = smem_view(smem_raw, P.cap);
+    const SmemView SM = smem_view<NB == 4>(smem_raw, P.cap);
     const int tile = VT.tile[chunk];
     const int tx = tile % ntx, ty = tile / ntx;
     const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
@@ -994,10 +1007,11 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
                                          Scalars* sc, int ntx, int tile) {
     const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
-    static_assert(15 + 5 * NB + 3 <= SUMS, "reduced sums overflow");
+    constexpr int SR = sums_stride(15 + 5 * NB + 3);
+    static_assert(SR <= SUMS_MAX, "reduced sums overflow");
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
-    const SmemView SM = smem_view(smem_raw, P.cap);
+    const SmemView SM = smem_view<NB == 4>(smem_raw, P.cap);
     const int tx = tile % ntx, ty = tile / ntx;
     stage_halo<false, NB == 4>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
     if (stop) return;
@@ -1053,26 +1067,26 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
             for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
             group_reduce<G>(sxy);
             if (active && lane == 0) {
-                double* sm = SM.sums + slot * SUMS;
+                double* sm = SM.sums + slot * SR;
 #pragma unroll
                 for (int k = 0; k < 15; ++k) sm[k] = Mu[k];
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
                     for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = B[c][k];
-                sm[SUMS - 3] = sxy[0];
-                sm[SUMS - 2] = sxy[1];
-                sm[SUMS - 1] = (double)cnt;
+                sm[SR - 3] = sxy[0];
+                sm[SR - 2] = sxy[1];
+                sm[SR - 1] = (double)cnt;
             }
         }
         __syncthreads();
         const int o = ob + (int)threadIdx.x;
         if ((int)threadIdx.x < PPB && o < n_own) {
-            const double* sm = SM.sums + threadIdx.x * SUMS;
+            const double* sm = SM.sums + threadIdx.x * SR;
             const int ki = SM.own_k[o];
-            const int cnt = (int)sm[SUMS - 1];
+            const int cnt = (int)sm[SR - 1];
             // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
-            double dx = -coe * sm[SUMS - 3], dy = -coe * sm[SUMS - 2];
+            double dx = -coe * sm[SR - 3], dy = -coe * sm[SR - 2];
             const double rr = sqrt(dx * dx + dy * dy);
             if (rr > 0.2 * P.h) {
                 dx = ((0.2 * P.h) * dx) / rr;
@@ -1125,8 +1139,8 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
     }
 }
 
-template <int NB, int G>
-__global__ void __launch_bounds__(PPB * G) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
+template <int NB, int G, bool TIGHT = false>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
                                                  const Lst Ln, const int* __restrict__ gstart,
                                                  const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
     pst_body<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, blockIdx.x);
@@ -1167,8 +1181,8 @@ __device__ __forceinline__ const SolveDesc& load_desc(const SolveDesc* D, int s,
     return sd;
 }
 
-template <int NB, int G>
-__global__ void __launch_bounds__(PPB * G) kb_stage(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
+template <int NB, int G, bool TIGHT = false>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_stage(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
                                                     int ps, int pl) {
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
@@ -1190,8 +1204,8 @@ __global__ void __launch_bounds__(PPB * G) kb_ghost(const SolveDesc* __restrict_
                           zero_other ? d.L[lb ^ 1].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
 }
 
-template <int NB, int G>
-__global__ void __launch_bounds__(PPB * G) kb_pst(const SolveDesc* __restrict__ D, const BatchMap M, int ps, int pl) {
+template <int NB, int G, bool TIGHT = false>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(const SolveDesc* __restrict__ D, const BatchMap M, int ps, int pl) {
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);

@@ -136,7 +136,7 @@ int scratch_base(int dev, unsigned char** out, std::string* msg) {
         const cudaError_t e = cudaGetSymbolAddress(&ptr, g_rhs_scratch);
         if (e != cudaSuccess) { *msg = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return LSSPH_E_CUDA; }
         // the same opt-in value the simulation handles use for these kernels
-        const int bytes = (int)tile_smem_bytes(64, 8);
+        const int bytes = (int)tile_smem_bytes(64, 8, true);
         for (cudaError_t a : {cudaFuncSetAttribute(k_stage<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
                               cudaFuncSetAttribute(k_stage<5, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)}) {
             if (a != cudaSuccess) { *msg = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(a); return LSSPH_E_CUDA; }
@@ -227,7 +227,7 @@ extern "C" int lssph_rhs_noalloc(const lssph_params* pin, int32_t num_total, int
     S.stage = 1;
     S.write_rhs = 1;
     const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY;
-    const size_t sm = tile_smem_bytes(kCap, 4);
+    const size_t sm = tile_smem_bytes(kCap, 4, p.target_problem == 4);
     if (p.target_problem == 4)
         k_stage<5, 4><<<ntx * nty, PPB * 4, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx);
     else

@@ -158,6 +158,7 @@ _PROTOS = {
     "lssph_write_parameters": (C.c_int, [_P(Params), C.c_int32, C.c_int32, C.c_char_p]),
     "lssph_read_data": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _i, _d, _d, _d, _d, _d, _d, _d]),
     "lssph_last_step_stats": (C.c_int, [_H, _P(C.c_double), _P(C.c_int64)]),
+    "lssph_get_tuning": (C.c_int, [_H, _i, _i, _P(C.c_double), _P(C.c_double)]),
     "lssph_step_profiled": (C.c_int, [_H, C.c_int32, _d, _P(C.c_int64)]),
     "lssph_batch_create": (C.c_int, [_P(C.c_void_p)]),
     "lssph_batch_destroy": (None, [_H]),

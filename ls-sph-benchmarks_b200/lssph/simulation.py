@@ -213,6 +213,14 @@ class Simulation:
         self._chk(self._lib.lssph_step_profiled(self._h, int(nsteps), ms, nl))
         return {k: (ms[i], nl[i]) for i, k in enumerate(_abi.KIND_NAMES)}
 
+    def tuning(self) -> dict:
+        """Kernel configuration picked for this solve (lanes, register budget, timings)."""
+        lanes, tight = C.c_int32(), C.c_int32()
+        lo, ti = C.c_double(), C.c_double()
+        self._chk(self._lib.lssph_get_tuning(self._h, C.byref(lanes), C.byref(tight), C.byref(lo), C.byref(ti)))
+        return {"lanes": lanes.value, "register_budget": "tight" if tight.value else "loose",
+                "rhs_us_loose": lo.value, "rhs_us_tight": ti.value}
+
     def last_step_stats(self) -> tuple[float, int]:
         ms = C.c_double()
         nl = C.c_int64()

@@ -202,3 +202,24 @@ def test_snapshot_files(tmp_path):
     ga, gb = r.download(), sim.download()
     for k in FIELDS:
         assert np.allclose(getattr(ga, k), getattr(gb, k), rtol=1e-12, atol=1e-14), k
+
+
+@pytest.mark.parametrize("case", ["taylor_green", "boussinesq"])
+def test_register_budgets_are_bit_identical(case, monkeypatch):
+    # the autotuner's two kernel variants differ only in register allocation
+    p = CASES[case]()
+    out = {}
+    for budget in ("loose", "tight"):
+        monkeypatch.setenv("LSSPH_REGISTER_BUDGET", budget)
+        st, ni = _perturbed(p, 0.1, 4)
+        sim = lssph.Simulation(p, st, ni)
+        assert sim.tuning()["register_budget"] == budget
+        sim.ghost()
+        sim.step(4)
+        out[budget] = sim.download()
+    for k in FIELDS:
+        assert np.array_equal(getattr(out["loose"], k), getattr(out["tight"], k)), k
+    monkeypatch.delenv("LSSPH_REGISTER_BUDGET")
+    t = lssph.Simulation(p, *_perturbed(p, 0.1, 4)).tuning()
+    assert t["rhs_us_loose"] > 0 and t["rhs_us_tight"] > 0
+    assert t["register_budget"] == ("tight" if t["rhs_us_tight"] < t["rhs_us_loose"] else "loose")
