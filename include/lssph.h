@@ -152,6 +152,23 @@ int lssph_check_steady_state(lssph_handle* h, int32_t* is_steady); /* check_stea
    this call at which it was reached, or 0. */
 int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out);
 
+/* Device memory (no counterpart in the reference), for admission control: the bytes a
+   handle holds, and the bytes lssph_create would allocate for a fresh start with *p
+   (host-only; both count requested bytes, before the allocator's rounding). */
+int lssph_device_bytes(const lssph_handle* h, int64_t* bytes);
+/* Free and total memory of the current device (cudaMemGetInfo). */
+int lssph_mem_info(int64_t* free_bytes, int64_t* total_bytes);
+int lssph_estimate_device_bytes(const lssph_params* p, int64_t* bytes);
+
+/* Step budget (no counterpart in the reference): after nsteps more time steps the handle
+   stops advancing, as it does at a steady state; later lssph_step / lssph_batch_step calls
+   leave it where it stopped.  The stop takes effect exactly at the step boundary, also
+   inside a batch.  nsteps = 0 removes the budget (and resumes a handle stopped by one). */
+int lssph_set_step_budget(lssph_handle* h, int32_t nsteps);
+/* Time steps completed since creation; *stopped = 0 running, 1 steady state, 2 step budget
+   used up. */
+int lssph_get_progress(lssph_handle* h, int32_t* steps_done, int32_t* stopped);
+
 /* Host <-> device state (caller buffers of length num_total; tem may be NULL). */
 int lssph_upload(lssph_handle* h, const double* x, const double* y, const double* u,
                  const double* v, const double* rho, const double* pre, const double* tem);
@@ -224,9 +241,12 @@ int  lssph_batch_remove(lssph_batch* b, lssph_handle* h);
 int  lssph_batch_size(const lssph_batch* b);
 /* nsteps time steps of every member.  status[i] (may be NULL) receives member i's status
    (LSSPH_OK or the code lssph_step would return), steady[i] (may be NULL) the 1-based step
-   within this call at which member i reached a steady state, or 0.  Returns LSSPH_OK, or
-   the first member error, or LSSPH_E_CUDA for a failure of the batch itself. */
-int  lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady);
+   within this call at which member i reached a steady state, or 0, and steps_taken[i]
+   (may be NULL) the steps member i actually advanced (fewer than nsteps once it stopped:
+   steady state, step budget or error).  Returns LSSPH_OK, or the first member error, or
+   LSSPH_E_CUDA for a failure of the batch itself. */
+int  lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady,
+                      int32_t* steps_taken);
 /* Device time and kernel launches of the last lssph_batch_step (all members). */
 int  lssph_batch_last_step_stats(const lssph_batch* b, double* device_ms, int64_t* kernel_launches);
 

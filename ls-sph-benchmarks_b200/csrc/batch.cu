@@ -32,7 +32,7 @@ namespace {
 
 struct BatchGroup {
     int nb = 4, nbg = 3, wq = 3, rk = 4, G = 4;
-    bool p1 = false, pst_on = true;
+    bool p1 = false, pst_on = true, mixed = false;
     int flip = 1;                  // both parities flip once per step (problems 2-4)
     std::vector<int> members;      // indices into lssph_batch::members
     SolveDesc* D = nullptr;        // device, one descriptor per member
@@ -102,17 +102,25 @@ void optin(K kernel) {
 }
 
 // Launch (or, with prep, only opt in the shared memory of) one batched phase kernel.
+// Precision x lanes: the mixed-precision kernels exist for 4 lanes only.
+template <class F>
+void dispatch_kind(const BatchGroup& g, F&& f) {
+    if (g.mixed) f(std::integral_constant<int, 4>{}, std::true_type{});
+    else dispatch_lanes(g.G, [&](auto GG) { f(GG, std::false_type{}); });
+}
+
 void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
-    dispatch_lanes(g.G, [&](auto GG) {
+    dispatch_kind(g, [&](auto GG, auto MXc) {
         constexpr int G = decltype(GG)::value;
+        constexpr bool MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
             (g.tight ? tight : loose)<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, S, ps, pl);
             ++*count;
         };
-        if (g.nb == 1) run(kb_stage<1, G, false>, kb_stage<1, G, true>);
-        else if (g.nb == 5) run(kb_stage<5, G, false>, kb_stage<5, G, true>);
-        else run(kb_stage<4, G, false>, kb_stage<4, G, true>);
+        if (g.nb == 1) run(kb_stage<1, G, false, MX>, kb_stage<1, G, true, MX>);
+        else if (g.nb == 5) run(kb_stage<5, G, false, MX>, kb_stage<5, G, true, MX>);
+        else run(kb_stage<4, G, false, MX>, kb_stage<4, G, true, MX>);
     });
 }
 
@@ -137,15 +145,16 @@ void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset
 }
 
 void launch_pst(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
-    dispatch_lanes(g.G, [&](auto GG) {
+    dispatch_kind(g, [&](auto GG, auto MXc) {
         constexpr int G = decltype(GG)::value;
+        constexpr bool MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
             (g.tight ? tight : loose)<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, ps, pl);
             ++*count;
         };
-        if (g.nb == 5) run(kb_pst<4, G, false>, kb_pst<4, G, true>);
-        else run(kb_pst<3, G, false>, kb_pst<3, G, true>);
+        if (g.nb == 5) run(kb_pst<4, G, false, MX>, kb_pst<4, G, true, MX>);
+        else run(kb_pst<3, G, false, MX>, kb_pst<3, G, true, MX>);
     });
 }
 
@@ -245,10 +254,10 @@ int rebuild(lssph_batch* b) {
     b->base_sb.assign(n, 0);
     b->base_lb.assign(n, 0);
     b->flip.assign(n, 0);
-    std::map<std::tuple<int, int, int, int>, int> index;
+    std::map<std::tuple<int, int, int, int, int>, int> index;
     for (size_t i = 0; i < n; ++i) {
         const lssph_handle* h = b->members[i];
-        const auto key = std::make_tuple(h->nb_rhs, h->wq, h->p.rk, h->G);
+        const auto key = std::make_tuple(h->nb_rhs, h->wq, h->p.rk, h->G, h->mixed ? 1 : 0);
         auto it = index.find(key);
         if (it == index.end()) {
             BatchGroup g;
@@ -257,6 +266,7 @@ int rebuild(lssph_batch* b) {
             g.wq = h->wq;
             g.rk = h->p.rk;
             g.G = h->G;
+            g.mixed = h->mixed;
             g.p1 = h->p1;
             g.pst_on = h->pst_on;
             g.flip = h->p1 ? 0 : 1;
@@ -410,12 +420,13 @@ int lssph_batch_remove(lssph_batch* b, lssph_handle* h) {
 
 int lssph_batch_size(const lssph_batch* b) { return b ? (int)b->members.size() : 0; }
 
-int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady) {
+int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady, int32_t* steps_taken) {
     if (!b) return bfail(nullptr, LSSPH_E_BAD_PARAM, "null batch");
     const size_t n = b->members.size();
     for (size_t i = 0; i < n; ++i) {
         if (status) status[i] = LSSPH_OK;
         if (steady) steady[i] = 0;
+        if (steps_taken) steps_taken[i] = 0;
     }
     b->last_ms = 0.0;
     b->last_launches = 0;
@@ -429,6 +440,11 @@ int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* s
     if (b->dirty && (rc = rebuild(b)) != LSSPH_OK) return rc;
     if ((rc = gather_scalars(b)) != LSSPH_OK) return rc;
     std::vector<Scalars> s0(b->h_sc, b->h_sc + n);
+    std::vector<int> sb_start(n), lb_start(n);
+    for (size_t i = 0; i < n; ++i) {
+        sb_start[i] = b->members[i]->sb;
+        lb_start[i] = b->members[i]->lb;
+    }
     BATCH_TRY(b, cudaEventRecord(b->ev0, b->stream));
     for (int st = 0; st < nsteps; ++st) {
         cudaGraphExec_t& ge = b->graph[b->t];
@@ -456,6 +472,14 @@ int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* s
             if (first == LSSPH_OK) first = st;
         }
         if (steady && s1.steady && !s0[i].steady) steady[i] = s1.steady_step - s0[i].step_count;
+        // a member that stopped (steady state, step budget, error) ran the remaining steps
+        // as no-ops: its buffers sit where its last executed step left them
+        const int executed = s1.step_count - s0[i].step_count;
+        if (steps_taken) steps_taken[i] = executed;
+        if (executed != nsteps) {
+            b->members[i]->sb = sb_start[i] ^ (b->flip[i] & executed & 1);
+            b->members[i]->lb = lb_start[i] ^ (b->flip[i] & executed & 1);
+        }
     }
     if (first != LSSPH_OK) return bfail(b, first, "a batch member stopped with an error (see the status array)");
     return LSSPH_OK;

@@ -55,8 +55,47 @@ int dalloc(lssph_handle* h, T** ptr, size_t n) {
     const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
     if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     h->allocs.push_back(p);
+    h->alloc_bytes += (int64_t)(n * sizeof(T));
     *ptr = static_cast<T*>(p);
     return LSSPH_OK;
+}
+
+// Virtual markers grouped by the cell tile that holds them, in chunks of at most PPB
+// markers (one pass of a ghost CTA): chunk tile ids, chunk ranges, marker ids.
+void vm_chunks(const CellGrid& g, int ntx, int ntiles, std::vector<int32_t>* tile, std::vector<int32_t>* start,
+               std::vector<int32_t>* vm) {
+    const size_t NE = g.vm_key.size();
+    std::vector<std::vector<int32_t>> by_tile(ntiles);
+    for (size_t me = 0; me < NE; ++me) {
+        const int key = g.vm_key[me];
+        const int cx = key % g.nx, cy = key / g.nx;
+        by_tile[(cx / TX) + (cy / TY) * ntx].push_back((int32_t)me);
+    }
+    tile->clear();
+    start->assign(1, 0);
+    vm->assign(NE, 0);
+    size_t k = 0;
+    for (int t = 0; t < ntiles; ++t) {
+        for (size_t b = 0; b < by_tile[t].size(); b += PPB) {
+            tile->push_back(t);
+            for (size_t e = b; e < std::min(by_tile[t].size(), b + PPB); ++e) (*vm)[k++] = by_tile[t][e];
+            start->push_back((int32_t)k);
+        }
+    }
+}
+
+// Device bytes a solve of these sizes allocates: the same list of arrays as create_impl
+// (every array holds at least one element).
+int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt) {
+    auto n1 = [](size_t n) { return (int64_t)std::max<size_t>(n, 1); };
+    const int64_t d = sizeof(double), i = sizeof(int32_t);
+    int64_t b = 0;
+    b += 2 * (8 * n1(N) * d + n1(NC) * i + n1(NC * (size_t)cap) * i);   // state + cell lists, 2 buffers
+    b += 18 * n1(NI) * d + n1(NI) * i;                                  // RK registers, RHS, f_prev, src, key
+    b += 9 * n1(NE) * d + 3 * n1(NE) * i;                               // virtual markers
+    b += n1(NC + 1) * i + n1(NE) * i + (int64_t)sizeof(Scalars);         // ghost CSR, scalars
+    b += n1((size_t)std::max(nvt, 1)) * i + n1((size_t)nvt + 1) * i + n1(NE) * i;   // marker chunks
+    return b;
 }
 
 inline int blocks_for(long n, int per_block) { return (int)((n + per_block - 1) / per_block); }
@@ -91,29 +130,32 @@ void smem_optin(K kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8, true));
 }
 
-// ---- kernel dispatch on the lane count ---------------------------------------------------
+// ---- kernel dispatch on lanes, register budget and precision ------------------------------
+// The mixed-precision kernels exist for 4 lanes per particle only.
+template <int NB, int GG, bool MX>
+void run_stage(lssph_handle* h, const StageCfg& S) {
+    if (h->preparing) {
+        smem_optin(k_stage<NB, GG, false, MX>);
+        smem_optin(k_stage<NB, GG, true, MX>);
+        return;
+    }
+    auto kern = h->tight ? k_stage<NB, GG, true, MX> : k_stage<NB, GG, false, MX>;
+    kern<<<h->ntiles, PPB * GG, h->smem_bytes, h->stream>>>(h->P, h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb],
+                                                              h->L[h->lb ^ 1], h->gstart, h->glist, h->W, S, h->sc,
+                                                              h->ntx);
+    h->launch_counter++;
+}
+
 template <int NB>
 void launch_stage(lssph_handle* h, const StageCfg& S) {
     ProfScope prof(h, LSSPH_KIND_STAGE);
-    const Fld& cur = h->F[h->sb];
-    const Fld& nxt = h->F[h->sb ^ 1];
-    const Lst& Lc = h->L[h->lb];
-    const Lst& Ln = h->L[h->lb ^ 1];
-    const int G = h->G;
-    const int grid = h->ntiles;
-    const size_t sm = h->smem_bytes;
-#define LSSPH_STAGE(GG)                                                                                 \
-    if (h->preparing) { smem_optin(k_stage<NB, GG, false>); smem_optin(k_stage<NB, GG, true>); return; }   \
-    (h->tight ? k_stage<NB, GG, true> : k_stage<NB, GG, false>)<<<grid, PPB * GG, sm, h->stream>>>(         \
-        h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, S, h->sc, h->ntx)
-    switch (G) {
-        case 1: LSSPH_STAGE(1); break;
-        case 2: LSSPH_STAGE(2); break;
-        case 8: LSSPH_STAGE(8); break;
-        default: LSSPH_STAGE(4); break;
+    if (h->mixed) { run_stage<NB, 4, true>(h, S); return; }
+    switch (h->G) {
+        case 1: run_stage<NB, 1, false>(h, S); break;
+        case 2: run_stage<NB, 2, false>(h, S); break;
+        case 8: run_stage<NB, 8, false>(h, S); break;
+        default: run_stage<NB, 4, false>(h, S); break;
     }
-#undef LSSPH_STAGE
-    h->launch_counter++;
 }
 
 void launch_stage_any(lssph_handle* h, const StageCfg& S) {
@@ -159,27 +201,30 @@ void launch_ghost(lssph_handle* h, int zero_list = -1, int reset_umax = 0) {
     else launch_ghost_nb<3>(h, zero_list, reset_umax);
 }
 
+template <int NB, int GG, bool MX>
+void run_pst(lssph_handle* h) {
+    if (h->preparing) {
+        smem_optin(k_pst<NB, GG, false, MX>);
+        smem_optin(k_pst<NB, GG, true, MX>);
+        return;
+    }
+    auto kern = h->tight ? k_pst<NB, GG, true, MX> : k_pst<NB, GG, false, MX>;
+    kern<<<h->ntiles, PPB * GG, h->smem_bytes, h->stream>>>(h->P, h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb],
+                                                              h->L[h->lb ^ 1], h->gstart, h->glist, h->W, h->sc,
+                                                              h->ntx);
+    h->launch_counter++;
+}
+
 template <int NB>
 void launch_pst_t(lssph_handle* h) {
     ProfScope prof(h, LSSPH_KIND_PST);
-    const Fld& cur = h->F[h->sb];
-    const Fld& nxt = h->F[h->sb ^ 1];
-    const Lst& Lc = h->L[h->lb];
-    const Lst& Ln = h->L[h->lb ^ 1];
-    const int G = h->G;
-    const size_t sm = h->smem_bytes;
-#define LSSPH_PST(GG)                                                                                       \
-    if (h->preparing) { smem_optin(k_pst<NB, GG, false>); smem_optin(k_pst<NB, GG, true>); return; }           \
-    (h->tight ? k_pst<NB, GG, true> : k_pst<NB, GG, false>)<<<h->ntiles, PPB * GG, sm, h->stream>>>(             \
-        h->P, cur, nxt, Lc, Ln, h->gstart, h->glist, h->W, h->sc, h->ntx)
-    switch (G) {
-        case 1: LSSPH_PST(1); break;
-        case 2: LSSPH_PST(2); break;
-        case 8: LSSPH_PST(8); break;
-        default: LSSPH_PST(4); break;
+    if (h->mixed) { run_pst<NB, 4, true>(h); return; }
+    switch (h->G) {
+        case 1: run_pst<NB, 1, false>(h); break;
+        case 2: run_pst<NB, 2, false>(h); break;
+        case 8: run_pst<NB, 8, false>(h); break;
+        default: run_pst<NB, 4, false>(h); break;
     }
-#undef LSSPH_PST
-    h->launch_counter++;
 }
 
 // ---- operator sequences (enqueue only) -----------------------------------------------------
@@ -341,8 +386,10 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (check_param(pin, &msg) != LSSPH_OK) return fail(nullptr, LSSPH_E_BAD_PARAM, msg);
     if (pin->sph_model != 3)
         return fail(nullptr, LSSPH_E_UNSUPPORTED, "the GPU engine implements SPH_MODEL 3 (2nd-order LS-SPH)");
-    if (pin->precision != LSSPH_PRECISION_FP64)
-        return fail(nullptr, LSSPH_E_UNSUPPORTED, "this entry point runs the FP64 path");
+    if (pin->precision != LSSPH_PRECISION_FP64 && pin->precision != LSSPH_PRECISION_MIXED)
+        return fail(nullptr, LSSPH_E_BAD_PARAM, "precision must be LSSPH_PRECISION_FP64 or LSSPH_PRECISION_MIXED");
+    if (pin->precision == LSSPH_PRECISION_MIXED && pin->lanes != 0 && pin->lanes != 4)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs with 4 lanes per particle (lanes = 0 or 4)");
     if (pin->target_problem == 4 && !tem) return fail(nullptr, LSSPH_E_BAD_PARAM, "tem required for problem 4");
     if (num_int <= 0 || num_total <= num_int) return fail(nullptr, LSSPH_E_BAD_PARAM, "bad particle counts");
     for (int i = 0; i < num_total; ++i) {
@@ -362,6 +409,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->nb_rhs = h->p1 ? 1 : (h->has_tem ? 5 : 4);
     h->nb_ghost = h->p1 ? 1 : (h->has_tem ? 4 : 3);
     h->wq = h->p.wall_model == 1 ? 1 : (h->p.wall_model == 3 ? 6 : 3);
+    h->mixed = h->p.precision == LSSPH_PRECISION_MIXED;
     h->G = h->p.lanes > 0 ? h->p.lanes : 4;
     h->Gg = h->p.lanes > 0 ? h->p.lanes : 4;
     h->ptype.assign(ptype, ptype + num_total);
@@ -442,25 +490,9 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->nty = (h->grid.ny + TY - 1) / TY;
     h->ntiles = h->ntx * h->nty;
     h->smem_bytes = std::max(tile_smem_bytes(h->grid.cap, h->G, h->has_tem), tile_smem_bytes(h->grid.cap, h->Gg, h->has_tem));
-    std::vector<int32_t> vt_tile, vt_start, vt_vm(NE);
-    {
-        std::vector<std::vector<int32_t>> by_tile(h->ntiles);
-        for (size_t me = 0; me < NE; ++me) {
-            const int key = h->grid.vm_key[me];
-            const int cx = key % h->grid.nx, cy = key / h->grid.nx;
-            by_tile[(cx / TX) + (cy / TY) * h->ntx].push_back((int32_t)me);
-        }
-        size_t k = 0;
-        vt_start.push_back(0);
-        for (int t = 0; t < h->ntiles; ++t) {   // chunks of at most one pass per CTA
-            for (size_t b = 0; b < by_tile[t].size(); b += PPB) {
-                vt_tile.push_back(t);
-                for (size_t e = b; e < std::min(by_tile[t].size(), b + PPB); ++e) vt_vm[k++] = by_tile[t][e];
-                vt_start.push_back((int32_t)k);
-            }
-        }
-        h->nvt = (int)vt_tile.size();
-    }
+    std::vector<int32_t> vt_tile, vt_start, vt_vm;
+    vm_chunks(h->grid, h->ntx, h->ntiles, &vt_tile, &vt_start, &vt_vm);
+    h->nvt = (int)vt_tile.size();
     A(&h->vt_tile, std::max(h->nvt, 1)); A(&h->vt_start, h->nvt + 1); A(&h->vt_vm, NE);
     if (!ok) { const std::string m = h->err; free_handle(h); return fail(nullptr, LSSPH_E_CUDA, m); }
 
@@ -633,8 +665,9 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
     Scalars s0{};
     int rc = check_scalars(h, &s0);
     if (rc != LSSPH_OK) return rc;
-    if (s0.steady) return LSSPH_OK;   // the reference leaves the time loop at a steady state
+    if (s0.steady || s0.done) return LSSPH_OK;   // the reference leaves the time loop at a steady state
     const int64_t launches0 = h->launch_counter;
+    const int sb_start = h->sb, lb_start = h->lb;
     CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
     for (int st = 0; st < nsteps; ++st) {
         cudaGraphExec_t& ge = h->graph[h->sb][h->lb];
@@ -666,8 +699,77 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->last_ms = ms;
     h->last_launches = h->launch_counter - launches0;
+    // steps after a stop (steady state, step budget, error) ran as no-ops: the buffers
+    // sit where the last executed step left them
+    const int executed = s1.step_count - s0.step_count;
+    if (executed != nsteps) {
+        h->sb = sb_start ^ (((h->step_flip >> 1) & 1) & (executed & 1));
+        h->lb = lb_start ^ ((h->step_flip & 1) & (executed & 1));
+    }
     if (rc != LSSPH_OK) return rc;
     if (s1.steady && steady_step_out) *steady_step_out = s1.steady_step - s0.step_count;
+    return LSSPH_OK;
+}
+
+int lssph_mem_info(int64_t* free_bytes, int64_t* total_bytes) {
+    size_t f = 0, t = 0;
+    const cudaError_t err = cudaMemGetInfo(&f, &t);
+    if (err != cudaSuccess) return fail(nullptr, LSSPH_E_CUDA, std::string("cudaMemGetInfo: ") + cudaGetErrorString(err));
+    if (free_bytes) *free_bytes = (int64_t)f;
+    if (total_bytes) *total_bytes = (int64_t)t;
+    return LSSPH_OK;
+}
+
+int lssph_device_bytes(const lssph_handle* h, int64_t* bytes) {
+    if (!h || !bytes) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    *bytes = h->alloc_bytes;
+    return LSSPH_OK;
+}
+
+int lssph_estimate_device_bytes(const lssph_params* pin, int64_t* bytes) {
+    if (!pin || !bytes) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    std::string msg;
+    lssph_params p = *pin;
+    init_param(&p);
+    if (check_param(&p, &msg) != LSSPH_OK) return fail(nullptr, LSSPH_E_BAD_PARAM, msg);
+    int nt = 0, ni = 0;
+    int rc = closed_box_counts(&p, &nt, &ni);
+    if (rc != LSSPH_OK) return fail(nullptr, rc, "bad particle counts");
+    std::vector<int32_t> ptype(nt);
+    std::vector<double> x(nt), y(nt), u(nt), v(nt), rho(nt), pre(nt), tem(nt);
+    rc = setup_particles(&p, nt, ptype.data(), x.data(), y.data(), u.data(), v.data(), rho.data(), pre.data(),
+                         tem.data(), &msg);
+    VirtualMarkers vm;
+    CellGrid grid;
+    if (rc == LSSPH_OK) rc = build_virtual_markers(&p, nt, ni, ptype.data(), x.data(), y.data(), &vm, &msg);
+    if (rc == LSSPH_OK) rc = build_cell_grid(&p, nt, ni, x.data(), y.data(), vm, &grid, &msg);
+    if (rc != LSSPH_OK) return fail(nullptr, rc, msg);
+    const int ntx = (grid.nx + TX - 1) / TX, nty = (grid.ny + TY - 1) / TY;
+    std::vector<int32_t> vt_tile, vt_start, vt_vm;
+    vm_chunks(grid, ntx, ntx * nty, &vt_tile, &vt_start, &vt_vm);
+    *bytes = solve_bytes(nt, ni, nt - ni, grid.ncell, grid.cap, (int)vt_tile.size());
+    return LSSPH_OK;
+}
+
+int lssph_set_step_budget(lssph_handle* h, int32_t nsteps) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (nsteps < 0) return fail(h, LSSPH_E_BAD_PARAM, "the step budget must be >= 0");
+    Scalars s{};
+    int rc = check_scalars(h, &s);
+    if (rc != LSSPH_OK) return rc;
+    s.step_limit = nsteps > 0 ? s.step_count + nsteps : 0;
+    s.done = 0;
+    CUDA_TRY(h, cudaMemcpy(&h->sc->step_limit, &s.step_limit, 2 * sizeof(int), cudaMemcpyHostToDevice));
+    return LSSPH_OK;
+}
+
+int lssph_get_progress(lssph_handle* h, int32_t* steps_done, int32_t* stopped) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    Scalars s{};
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaMemcpy(&s, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+    if (steps_done) *steps_done = s.step_count;
+    if (stopped) *stopped = s.steady ? 1 : (s.done ? 2 : 0);
     return LSSPH_OK;
 }
 

@@ -18,6 +18,7 @@ struct lssph_handle {
     bool has_tem = false, p1 = false, pst_on = false;
     int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
     int G = 4, Gg = 4;
+    bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
     bool tight = false;                 // register budget of stage/PST kernels (autotuned)
     double tune_us[2] = {0.0, 0.0};     // RHS pass time with the loose / tight budget
     lssph::CellGrid grid;
@@ -27,6 +28,7 @@ struct lssph_handle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<void*> allocs;
+    int64_t alloc_bytes = 0;            // device bytes requested by this handle
     lssph::Fld F[2]{};
     lssph::Lst L[2]{};
     lssph::Work W{};

@@ -1,4 +1,5 @@
-// kernels.cuh -- device code of the FP64 LS-SPH path (sm_100a).
+// kernels.cuh -- device code of the LS-SPH path (sm_100a): FP64, and a mixed-precision
+// variant of the stage and PST kernels (FP32 pair phase, FP64 solve and RK update).
 //
 // Every kernel here replaces one OpenMP region of the reference solver:
 //   k_stage      calculate_RHS (LSSPH_A_mod.f90:26-271) fused with the RK2/RK4 stage
@@ -25,6 +26,9 @@
 // partial sums (identical on every lane, so the G lanes agree bit for bit).
 #pragma once
 
+#include <cstddef>
+#include <type_traits>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -44,10 +48,14 @@ struct Scalars {
     int err;                    // ERR_* bits; any set bit halts later kernels
     int warn;                   // WARN_* bits
     int steady;                 // 1 once the steady state is reached (problem 1)
-    int step_count;             // steps completed (problem 1 epilogue)
+    int step_count;             // time steps completed
     int steady_step;            // step_count value at which steady was reached
-    int pad;
+    int step_limit;             // stop once step_count reaches it (0 = no budget)
+    int done;                   // 1 once the step budget is used up
+    int ctas_done;              // CTAs of the current end-of-step launch that have finished
 };
+static_assert(offsetof(Scalars, done) == offsetof(Scalars, step_limit) + sizeof(int),
+              "step_limit and done are written together");
 
 // Constants of one solve (a subset of lssph_params plus precomputed factors).
 struct Phys {
@@ -100,78 +108,102 @@ enum : int { XM_COPY = 0, XM_K_MINUS = 1, XM_PLUS_K = 2, XM_NEG = 3 };
 
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ bool halted(const Scalars* sc) {
-    return (*(volatile const int*)&sc->err) != 0 || (*(volatile const int*)&sc->steady) != 0;
+    return (*(volatile const int*)&sc->err) != 0 || (*(volatile const int*)&sc->steady) != 0 ||
+           (*(volatile const int*)&sc->done) != 0;
+}
+
+// End of a time step (problems 2-4): the last CTA of the step's final launch to finish
+// counts the step and applies the step budget.  Every CTA of that launch has finished its
+// work by then, so no CTA sees the budget change in the middle of a step.
+__device__ __forceinline__ void end_of_step(Scalars* sc, int nctas) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int prev = atomicAdd(&sc->ctas_done, 1);
+        if (prev == nctas - 1) {
+            __threadfence();
+            sc->ctas_done = 0;
+            if (!halted(sc)) {
+                const int n = sc->step_count + 1;
+                sc->step_count = n;
+                if (sc->step_limit > 0 && n >= sc->step_limit) sc->done = 1;
+            }
+        }
+    }
 }
 
 // cal_W / cal_dW (kernel_functions_mod.f90:26-146); nrm = kernel_norm(kt, h), ih = 1/h.
-__device__ __forceinline__ double dev_W(int kt, double r, double ih, double nrm) {
-    const double q = r * ih;
-    double W = 0.0;
+// R = double: the parity arithmetic; R = float: the mixed-precision pair phase.
+template <class R>
+__device__ __forceinline__ R dev_W(int kt, R r, R ih, R nrm) {
+    const R q = r * ih;
+    R W = R(0);
     if (kt == 3) {
-        if (0.0 <= q && q <= 2.0) {
-            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2;
-            W = t4 * (1.0 + 2.0 * q);
+        if (R(0.0) <= q && q <= R(2.0)) {
+            const R t = R(1.0) - R(0.5) * q, t2 = t * t, t4 = t2 * t2;
+            W = t4 * (R(1.0) + R(2.0) * q);
         }
     } else if (kt == 1) {
-        const double a = 2.0 - q, b = 1.0 - q, a3 = (a * a) * a, b3 = (b * b) * b;
-        if (0.0 <= q && q <= 1.0) W = a3 - 4.0 * b3;
-        else if (1.0 < q && q <= 2.0) W = a3;
+        const R a = R(2.0) - q, b = R(1.0) - q, a3 = (a * a) * a, b3 = (b * b) * b;
+        if (R(0.0) <= q && q <= R(1.0)) W = a3 - R(4.0) * b3;
+        else if (R(1.0) < q && q <= R(2.0)) W = a3;
     } else if (kt == 2) {
-        const double a = 3.0 - q, b = 2.0 - q, c = 1.0 - q;
-        const double a2 = a * a, b2 = b * b, c2 = c * c;
-        const double a5 = (a2 * a2) * a, b5 = (b2 * b2) * b, c5 = (c2 * c2) * c;
-        if (0.0 <= q && q <= 1.0) W = (a5 - 6.0 * b5) + 15.0 * c5;
-        else if (1.0 < q && q <= 2.0) W = a5 - 6.0 * b5;
-        else if (2.0 < q && q <= 3.0) W = a5;
+        const R a = R(3.0) - q, b = R(2.0) - q, c = R(1.0) - q;
+        const R a2 = a * a, b2 = b * b, c2 = c * c;
+        const R a5 = (a2 * a2) * a, b5 = (b2 * b2) * b, c5 = (c2 * c2) * c;
+        if (R(0.0) <= q && q <= R(1.0)) W = (a5 - R(6.0) * b5) + R(15.0) * c5;
+        else if (R(1.0) < q && q <= R(2.0)) W = a5 - R(6.0) * b5;
+        else if (R(2.0) < q && q <= R(3.0)) W = a5;
     } else if (kt == 4) {
-        if (0.0 <= q && q <= 2.0) {
-            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t6 = t4 * t2;
-            W = t6 * ((1.0 + 3.0 * q) + (35.0 * (q * q)) / 12.0);
+        if (R(0.0) <= q && q <= R(2.0)) {
+            const R t = R(1.0) - R(0.5) * q, t2 = t * t, t4 = t2 * t2, t6 = t4 * t2;
+            W = t6 * ((R(1.0) + R(3.0) * q) + (R(35.0) * (q * q)) / R(12.0));
         }
     } else {
-        if (0.0 <= q && q <= 2.0) {
-            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t8 = t4 * t4;
-            const double q2 = q * q, q3 = q2 * q;
-            W = t8 * (((1.0 + 4.0 * q) + (25.0 * q2) / 4.0) + 4.0 * q3);
+        if (R(0.0) <= q && q <= R(2.0)) {
+            const R t = R(1.0) - R(0.5) * q, t2 = t * t, t4 = t2 * t2, t8 = t4 * t4;
+            const R q2 = q * q, q3 = q2 * q;
+            W = t8 * (((R(1.0) + R(4.0) * q) + (R(25.0) * q2) / R(4.0)) + R(4.0) * q3);
         }
     }
     return nrm * W;
 }
 
-__device__ __forceinline__ double dev_dW(int kt, double r, double ih, double m3h, double m5h, double nrm) {
-    const double q = r * ih;
-    double dW = 0.0;
+template <class R>
+__device__ __forceinline__ R dev_dW(int kt, R r, R ih, R m3h, R m5h, R nrm) {
+    const R q = r * ih;
+    R dW = R(0);
     if (kt == 3) {
-        if (0.0 <= q && q <= 2.0) {
-            const double t = 1.0 - 0.5 * q, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
-            dW = -(2.0 * t3) * (1.0 + 2.0 * q) + 2.0 * t4;
+        if (R(0.0) <= q && q <= R(2.0)) {
+            const R t = R(1.0) - R(0.5) * q, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+            dW = -(R(2.0) * t3) * (R(1.0) + R(2.0) * q) + R(2.0) * t4;
         }
         return (nrm * dW) * ih;
     } else if (kt == 1) {
-        const double a = 2.0 - q, b = 1.0 - q;
-        if (0.0 <= q && q <= 1.0) dW = a * a - 4.0 * (b * b);
-        else if (1.0 < q && q <= 2.0) dW = a * a;
+        const R a = R(2.0) - q, b = R(1.0) - q;
+        if (R(0.0) <= q && q <= R(1.0)) dW = a * a - R(4.0) * (b * b);
+        else if (R(1.0) < q && q <= R(2.0)) dW = a * a;
         return (nrm * dW) * m3h;
     } else if (kt == 2) {
-        const double a = 3.0 - q, b = 2.0 - q, c = 1.0 - q;
-        const double a2 = a * a, b2 = b * b, c2 = c * c;
-        const double a4 = a2 * a2, b4 = b2 * b2, c4 = c2 * c2;
-        if (0.0 <= q && q <= 1.0) dW = (a4 - 6.0 * b4) + 15.0 * c4;
-        else if (1.0 < q && q <= 2.0) dW = a4 - 6.0 * b4;
-        else if (2.0 < q && q <= 3.0) dW = a4;
+        const R a = R(3.0) - q, b = R(2.0) - q, c = R(1.0) - q;
+        const R a2 = a * a, b2 = b * b, c2 = c * c;
+        const R a4 = a2 * a2, b4 = b2 * b2, c4 = c2 * c2;
+        if (R(0.0) <= q && q <= R(1.0)) dW = (a4 - R(6.0) * b4) + R(15.0) * c4;
+        else if (R(1.0) < q && q <= R(2.0)) dW = a4 - R(6.0) * b4;
+        else if (R(2.0) < q && q <= R(3.0)) dW = a4;
         return (nrm * dW) * m5h;
     } else if (kt == 4) {
-        if (0.0 <= q && q <= 2.0) {
-            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t5 = t4 * t, t6 = t4 * t2;
-            dW = -(3.0 * t5) * ((1.0 + 3.0 * q) + (35.0 * (q * q)) / 12.0) + t6 * (3.0 + (35.0 * q) / 6.0);
+        if (R(0.0) <= q && q <= R(2.0)) {
+            const R t = R(1.0) - R(0.5) * q, t2 = t * t, t4 = t2 * t2, t5 = t4 * t, t6 = t4 * t2;
+            dW = -(R(3.0) * t5) * ((R(1.0) + R(3.0) * q) + (R(35.0) * (q * q)) / R(12.0)) + t6 * (R(3.0) + (R(35.0) * q) / R(6.0));
         }
         return (nrm * dW) * ih;
     } else {
-        if (0.0 <= q && q <= 2.0) {
-            const double t = 1.0 - 0.5 * q, t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t7 = t6 * t, t8 = t4 * t4;
-            const double q2 = q * q, q3 = q2 * q;
-            dW = -(4.0 * t7) * (((1.0 + 4.0 * q) + (25.0 * q2) / 4.0) + 4.0 * q3) +
-                 t8 * ((4.0 + (25.0 * q) / 2.0) + 12.0 * q2);
+        if (R(0.0) <= q && q <= R(2.0)) {
+            const R t = R(1.0) - R(0.5) * q, t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t7 = t6 * t, t8 = t4 * t4;
+            const R q2 = q * q, q3 = q2 * q;
+            dW = -(R(4.0) * t7) * (((R(1.0) + R(4.0) * q) + (R(25.0) * q2) / R(4.0)) + R(4.0) * q3) +
+                 t8 * ((R(4.0) + (R(25.0) * q) / R(2.0)) + R(12.0) * q2);
         }
         return (nrm * dW) * ih;
     }
@@ -245,6 +277,88 @@ __device__ __forceinline__ void lu_subst(const double (&A)[Q][Q], const double (
 #pragma unroll
         for (int i = 0; i < k; ++i) b[i] = fma(-b[k], A[i][k], b[i]);
     }
+}
+
+// LU with the row interchanges recorded (pv[k] = pivot row of step k) instead of applied
+// to right-hand sides; the mixed-precision solve reuses the factors for its refinement.
+template <int Q>
+__device__ __forceinline__ bool lu_factor_p(double (&A)[Q][Q], double (&rpiv)[Q], int (&pv)[Q]) {
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        int p = k;
+        double amax = fabs(A[k][k]);
+#pragma unroll
+        for (int i = k + 1; i < Q; ++i) {
+            const double a = fabs(A[i][k]);
+            if (a > amax) { amax = a; p = i; }
+        }
+        pv[k] = p;
+        if (p != k) {
+#pragma unroll
+            for (int r = k + 1; r < Q; ++r) {
+                const bool sw = (p == r);
+#pragma unroll
+                for (int c = 0; c < Q; ++c) {
+                    const double t0 = A[k][c], t1 = A[r][c];
+                    A[k][c] = sw ? t1 : t0;
+                    A[r][c] = sw ? t0 : t1;
+                }
+            }
+        }
+        const double piv = A[k][k];
+        if (piv != 0.0) {
+            const double rp = 1.0 / piv;
+#pragma unroll
+            for (int i = k + 1; i < Q; ++i) A[i][k] = A[i][k] * rp;
+        } else {
+            ok = false;
+        }
+        rpiv[k] = 1.0 / piv;
+#pragma unroll
+        for (int j = k + 1; j < Q; ++j)
+#pragma unroll
+            for (int i = k + 1; i < Q; ++i) A[i][j] = fma(-A[i][k], A[k][j], A[i][j]);
+    }
+    return ok;
+}
+
+template <int Q>
+__device__ __forceinline__ void lu_permute(const int (&pv)[Q], double (&b)[Q]) {
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+#pragma unroll
+        for (int r = k + 1; r < Q; ++r) {
+            const bool sw = (pv[k] == r);
+            const double t0 = b[k], t1 = b[r];
+            b[k] = sw ? t1 : t0;
+            b[r] = sw ? t0 : t1;
+        }
+    }
+}
+
+// Mixed-precision LS solve of one right-hand side: FP64 LU of the moment matrix (whose
+// sums were formed in FP32), then one step of iterative refinement against the same
+// FP64 matrix: x = x0 + LU \ (b - M x0).  M is read back from the packed upper triangle.
+template <int Q>
+__device__ __forceinline__ void lu_solve_refined(const double (&LU)[Q][Q], const double (&rpiv)[Q],
+                                                 const int (&pv)[Q], const double* Mu, double (&b)[Q]) {
+    double x[Q], r[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) x[k] = b[k];
+    lu_permute<Q>(pv, x);
+    lu_subst<Q>(LU, rpiv, x);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        double s = b[i];
+#pragma unroll
+        for (int j = 0; j < Q; ++j) s = fma(-(i <= j ? Mu[UT(i, j)] : Mu[UT(j, i)]), x[j], s);
+        r[i] = s;
+    }
+    lu_permute<Q>(pv, r);
+    lu_subst<Q>(LU, rpiv, r);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) b[k] = x[k] + r[k];
 }
 
 template <int Q, int NB>
@@ -540,12 +654,11 @@ __device__ __forceinline__ int tile_pairs(const TileHdr& T, const SmemView& S, b
 
 // Accumulate the LS type-A moment matrix (upper triangle) and b vectors of one pair
 // (LSSPH_A_mod.f90:136-190), df[c] = f_j - f_i.
-template <int NB>
-__device__ __forceinline__ void accumulate_A(double (&Mu)[15], double (&B)[NB][5], double VW, const double (&a)[5],
-                                             const double (&df)[NB]) {
+template <int NB, class R>
+__device__ __forceinline__ void accumulate_A(R (&Mu)[15], R (&B)[NB][5], R VW, const R (&a)[5], const R (&df)[NB]) {
 #pragma unroll
     for (int ii = 0; ii < 5; ++ii) {
-        const double VWa = VW * a[ii];
+        const R VWa = VW * a[ii];
 #pragma unroll
         for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, df[c], B[c][ii]);
 #pragma unroll
@@ -553,13 +666,31 @@ __device__ __forceinline__ void accumulate_A(double (&Mu)[15], double (&B)[NB][5
     }
 }
 
-__device__ __forceinline__ void basis_A(const Phys& P, double x, double y, double (&a)[5]) {
-    a[0] = x * P.ih1;
-    a[1] = y * P.ih1;
-    a[2] = (0.5 * (x * x)) * P.ih2A;
-    a[3] = (0.5 * (y * y)) * P.ih2A;
-    a[4] = (x * y) * P.ih2A;
+template <class R>
+__device__ __forceinline__ void basis_A(R ih1, R ih2A, R x, R y, R (&a)[5]) {
+    a[0] = x * ih1;
+    a[1] = y * ih1;
+    a[2] = (R(0.5) * (x * x)) * ih2A;
+    a[3] = (R(0.5) * (y * y)) * ih2A;
+    a[4] = (x * y) * ih2A;
 }
+
+__device__ __forceinline__ void basis_A(const Phys& P, double x, double y, double (&a)[5]) {
+    basis_A<double>(P.ih1, P.ih2A, x, y, a);
+}
+
+// Constants of the pair phase in its working precision.
+template <class R>
+struct PairConst {
+    R ih1, ih2A, wnorm, iWave, m3h, m5h;
+    __device__ __forceinline__ explicit PairConst(const Phys& P)
+        : ih1(R(P.ih1)), ih2A(R(P.ih2A)), wnorm(R(P.wnorm)), iWave(R(P.iWave)), m3h(R(P.m3h)), m5h(R(P.m5h)) {}
+};
+
+// Reduce G lanes' partial sums; FP32 partials are widened first, so the lanes combine
+// in FP64 (each lane's FP32 sum spans at most ceil(P / G) neighbours).
+template <int G, int N, class R>
+__device__ __forceinline__ void group_reduce_to(const R (&v)[N], double (&out)[N]);
 
 template <int G, int N>
 __device__ __forceinline__ void group_reduce(double (&v)[N]) {
@@ -567,6 +698,13 @@ __device__ __forceinline__ void group_reduce(double (&v)[N]) {
 #pragma unroll
         for (int k = 0; k < N; ++k) v[k] = group_sum<G>(v[k]);
     }
+}
+
+template <int G, int N, class R>
+__device__ __forceinline__ void group_reduce_to(const R (&v)[N], double (&out)[N]) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) out[k] = (double)v[k];
+    group_reduce<G>(out);
 }
 
 // =======================================================================================
@@ -690,7 +828,8 @@ __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, co
 }
 
 // One tile of one solve (the CTA's work in both the single-solve and the batched kernel).
-template <int NB, int G>
+// MIXED: FP32 pair phase (weights, basis, neighbour sums), FP64 solve with refinement.
+template <int NB, int G, bool MIXED>
 __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                            const int* __restrict__ gstart, const int* __restrict__ glist,
                                            const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
@@ -718,43 +857,47 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
             double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
             if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
             if constexpr (NB == 5) my_tem = SM.tem[ki];
-            double Mu[15];
-            double B[NB][Q];
+            using R = typename std::conditional<MIXED, float, double>::type;
+            const PairConst<R> C(P);
+            R Mu[15];
+            R B[NB][Q];
 #pragma unroll
-            for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
+            for (int k = 0; k < 15; ++k) Mu[k] = R(0);
 #pragma unroll
             for (int c = 0; c < NB; ++c)
 #pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+                for (int k = 0; k < Q; ++k) B[c][k] = R(0);
+            // differences are formed in FP64, then rounded to the working precision
             const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
-                const double xji = SM.x[k] - my_x;
-                const double yji = SM.y[k] - my_y;
-                const double r = sqrt(xji * xji + yji * yji);
-                const double Wv = dev_W(P.kt, r, P.ih1, P.wnorm);
-                const double VW = SM.vol[k] * Wv;
-                double a[Q];
-                basis_A(P, xji, yji, a);
-                double df[NB];
-                df[0] = SM.u[k] - my_u;
+                const R xji = R(SM.x[k] - my_x);
+                const R yji = R(SM.y[k] - my_y);
+                const R r = sqrt(xji * xji + yji * yji);
+                const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
+                const R VW = R(SM.vol[k]) * Wv;
+                R a[Q];
+                basis_A<R>(C.ih1, C.ih2A, xji, yji, a);
+                R df[NB];
+                df[0] = R(SM.u[k] - my_u);
                 if constexpr (NB >= 4) {
-                    df[1] = SM.v[k] - my_v;
-                    df[2] = SM.rho[k] - my_rho;
-                    df[3] = SM.pre[k] - my_pre;
+                    df[1] = R(SM.v[k] - my_v);
+                    df[2] = R(SM.rho[k] - my_rho);
+                    df[3] = R(SM.pre[k] - my_pre);
                 }
-                if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
-                accumulate_A<NB>(Mu, B, VW, a, df);
+                if constexpr (NB == 5) df[4] = R(SM.tem[k] - my_tem);
+                accumulate_A<NB, R>(Mu, B, VW, a, df);
             });
-            group_reduce<G>(Mu);
+            double Md[15], Bd[NB][Q];
+            group_reduce_to<G>(Mu, Md);
 #pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
+            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
-                for (int k = 0; k < 15; ++k) sm[k] = Mu[k];
+                for (int k = 0; k < 15; ++k) sm[k] = Md[k];
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = B[c][k];
+                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = Bd[c][k];
                 sm[SR - 1] = (double)cnt;
             }
         }
@@ -763,31 +906,61 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
         double red = 0.0;
         const int o = ob + (int)threadIdx.x;
         if ((int)threadIdx.x < PPB && o < n_own) {
-            const double* sm = SM.sums + threadIdx.x * SR;
+            double* sm = SM.sums + threadIdx.x * SR;
             const int ki = SM.own_k[o];
             const int cnt = (int)sm[SR - 1];
-            double A[Q][Q];
-            double B[NB][Q];
-#pragma unroll
-            for (int r = 0; r < Q; ++r)
-#pragma unroll
-                for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
-#pragma unroll
-            for (int c = 0; c < NB; ++c)
-#pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = sm[15 + 5 * c + k];
             double d[NB][Q];
-            if (cnt >= Q) {
-                if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+            if constexpr (MIXED) {
+                // one right-hand side at a time, solutions written back over the b sums
+                if (cnt >= Q) {
+                    double A[Q][Q];
+#pragma unroll
+                    for (int r = 0; r < Q; ++r)
+#pragma unroll
+                        for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
+                    double rpiv[Q];
+                    int pv[Q];
+                    if (!lu_factor_p<Q>(A, rpiv, pv)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll 1
+                    for (int c = 0; c < NB; ++c) {
+                        double b[Q];
+#pragma unroll
+                        for (int k = 0; k < Q; ++k) b[k] = sm[15 + 5 * c + k];
+                        lu_solve_refined<Q>(A, rpiv, pv, sm, b);
+#pragma unroll
+                        for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = b[k] * (k < 2 ? P.ih1 : P.ih2A);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 15; k < 15 + 5 * NB; ++k) sm[k] = 0.0;
+                }
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) d[c][k] = B[c][k] * (k < 2 ? P.ih1 : P.ih2A);
+                    for (int k = 0; k < Q; ++k) d[c][k] = sm[15 + 5 * c + k];
             } else {
+                double A[Q][Q];
+                double B[NB][Q];
+#pragma unroll
+                for (int r = 0; r < Q; ++r)
+#pragma unroll
+                    for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) d[c][k] = 0.0;
+                    for (int k = 0; k < Q; ++k) B[c][k] = sm[15 + 5 * c + k];
+                if (cnt >= Q) {
+                    if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll
+                    for (int c = 0; c < NB; ++c)
+#pragma unroll
+                        for (int k = 0; k < Q; ++k) d[c][k] = B[c][k] * (k < 2 ? P.ih1 : P.ih2A);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c)
+#pragma unroll
+                        for (int k = 0; k < Q; ++k) d[c][k] = 0.0;
+                }
             }
             double my_v = 0, my_rho = 0, my_tem = 0;
             if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
@@ -801,12 +974,11 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
     }
 }
 
-template <int NB, int G, bool TIGHT = false>
-__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
-                                                   const Lst Ln, const int* __restrict__ gstart,
-                                                   const int* __restrict__ glist, const Work W, const StageCfg S,
-                                                   Scalars* sc, int ntx) {
-    stage_body<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, blockIdx.x);
+template <int NB, int G, bool TIGHT = false, bool MIXED = false>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
+    k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
+            const int* __restrict__ glist, const Work W, const StageCfg S, Scalars* sc, int ntx) {
+    stage_body<NB, G, MIXED>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, blockIdx.x);
 }
 
 // =======================================================================================
@@ -824,14 +996,16 @@ struct VMTiles {
 
 // One chunk (<= PPB markers of one tile) of one solve; nchunk = chunks of this solve.
 template <int NB, int G, int WQ>
-__device__ __forceinline__ void ghost_body(const Phys& P, const Fld& F, const Lst& L, const int* __restrict__ gstart,
+__device__ __forceinline__ void ghost_work(const Phys& P, const Fld& F, const Lst& L, const int* __restrict__ gstart,
                                            const int* __restrict__ glist, const VMd& V, const VMTiles& VT, int ntx,
                                            int* zero_cnt, int reset_umax, Scalars* sc, int chunk, int nchunk) {
-    if (zero_cnt) {
+    // a stopped solve (steady state, step budget, error) keeps its cell lists as they are,
+    // so that it can resume exactly where it stopped
+    const bool stop = halted(sc);
+    if (zero_cnt && !stop) {
         for (int c = chunk * blockDim.x + threadIdx.x; c < P.ncell; c += nchunk * blockDim.x) zero_cnt[c] = 0;
     }
     if (reset_umax && chunk == 0 && threadIdx.x == 0) sc->umax2 = 0ull;
-    const bool stop = halted(sc);   // consumed after staging
     constexpr int Q = (WQ == 1) ? 1 : WQ;
     constexpr int NU = Q * (Q + 1) / 2;
     __shared__ TileHdr T;
@@ -989,6 +1163,15 @@ __device__ __forceinline__ void ghost_body(const Phys& P, const Fld& F, const Ls
     }
 }
 
+// reset_umax marks the ghost launch that ends a time step (after PST).
+template <int NB, int G, int WQ>
+__device__ __forceinline__ void ghost_body(const Phys& P, const Fld& F, const Lst& L, const int* __restrict__ gstart,
+                                           const int* __restrict__ glist, const VMd& V, const VMTiles& VT, int ntx,
+                                           int* zero_cnt, int reset_umax, Scalars* sc, int chunk, int nchunk) {
+    ghost_work<NB, G, WQ>(P, F, L, gstart, glist, V, VT, ntx, zero_cnt, reset_umax, sc, chunk, nchunk);
+    if (reset_umax) end_of_step(sc, nchunk);
+}
+
 template <int NB, int G, int WQ>
 __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, const Lst L,
                                                    const int* __restrict__ gstart, const int* __restrict__ glist,
@@ -1001,7 +1184,7 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
 // k_pst: particle shifting (q = 5) + copy-back + EOS + cell scatter.
 // NB = 3 (u,v,rho) or 4 (+T).  umax2 holds max(u^2+v^2) of the state being shifted.
 // =======================================================================================
-template <int NB, int G>
+template <int NB, int G, bool MIXED>
 __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                          const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
                                          Scalars* sc, int ntx, int tile) {
@@ -1029,53 +1212,56 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
             const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
             double my_tem = 0.0;
             if constexpr (NB == 4) my_tem = SM.tem[ki];
-            double Mu[15];
-            double B[NB][Q];
+            using R = typename std::conditional<MIXED, float, double>::type;
+            const PairConst<R> C(P);
+            R Mu[15];
+            R B[NB][Q];
 #pragma unroll
-            for (int k = 0; k < 15; ++k) Mu[k] = 0.0;
+            for (int k = 0; k < 15; ++k) Mu[k] = R(0);
 #pragma unroll
             for (int c = 0; c < NB; ++c)
 #pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
-            double sxy[2] = {0.0, 0.0};
+                for (int k = 0; k < Q; ++k) B[c][k] = R(0);
+            R sxy[2] = {R(0), R(0)};
             const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
-                const double xji = SM.x[k] - my_x;
-                const double yji = SM.y[k] - my_y;
-                const double r = sqrt(xji * xji + yji * yji);
-                const double Wv = dev_W(P.kt, r, P.ih1, P.wnorm);
-                const double dWdr = dev_dW(P.kt, r, P.ih1, P.m3h, P.m5h, P.wnorm);
-                const double Vj = SM.vol[k];
-                const double VW = Vj * Wv;
-                const double rinv = 1.0 / r;
-                const double gx = ((dWdr * (-xji)) * rinv) * Vj;
-                const double gy = ((dWdr * (-yji)) * rinv) * Vj;
-                const double t = Wv * P.iWave, t2 = t * t, t4 = t2 * t2;
-                const double fac = 1.0 + 0.2 * t4;
+                const R xji = R(SM.x[k] - my_x);
+                const R yji = R(SM.y[k] - my_y);
+                const R r = sqrt(xji * xji + yji * yji);
+                const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
+                const R dWdr = dev_dW<R>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
+                const R Vj = R(SM.vol[k]);
+                const R VW = Vj * Wv;
+                const R rinv = R(1) / r;
+                const R gx = ((dWdr * (-xji)) * rinv) * Vj;
+                const R gy = ((dWdr * (-yji)) * rinv) * Vj;
+                const R t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
+                const R fac = R(1.0) + R(0.2) * t4;
                 sxy[0] = fma(fac, gx, sxy[0]);
                 sxy[1] = fma(fac, gy, sxy[1]);
-                double a[Q];
-                basis_A(P, xji, yji, a);
-                double df[NB];
-                df[0] = SM.u[k] - my_u;
-                df[1] = SM.v[k] - my_v;
-                df[2] = SM.rho[k] - my_rho;
-                if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
-                accumulate_A<NB>(Mu, B, VW, a, df);
+                R a[Q];
+                basis_A<R>(C.ih1, C.ih2A, xji, yji, a);
+                R df[NB];
+                df[0] = R(SM.u[k] - my_u);
+                df[1] = R(SM.v[k] - my_v);
+                df[2] = R(SM.rho[k] - my_rho);
+                if constexpr (NB == 4) df[3] = R(SM.tem[k] - my_tem);
+                accumulate_A<NB, R>(Mu, B, VW, a, df);
             });
-            group_reduce<G>(Mu);
+            double Md[15], Bd[NB][Q], sd[2];
+            group_reduce_to<G>(Mu, Md);
 #pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce<G>(B[c]);
-            group_reduce<G>(sxy);
+            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+            group_reduce_to<G>(sxy, sd);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
-                for (int k = 0; k < 15; ++k) sm[k] = Mu[k];
+                for (int k = 0; k < 15; ++k) sm[k] = Md[k];
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = B[c][k];
-                sm[SR - 3] = sxy[0];
-                sm[SR - 2] = sxy[1];
+                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = Bd[c][k];
+                sm[SR - 3] = sd[0];
+                sm[SR - 2] = sd[1];
                 sm[SR - 1] = (double)cnt;
             }
         }
@@ -1092,23 +1278,54 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
                 dx = ((0.2 * P.h) * dx) / rr;
                 dy = ((0.2 * P.h) * dy) / rr;
             }
-            double A[Q][Q];
             double B[NB][Q];
+            if constexpr (MIXED) {
+                // one right-hand side at a time, solutions written back over the b sums
+                double* smw = SM.sums + threadIdx.x * SR;
+                if (cnt >= Q) {
+                    double A[Q][Q];
 #pragma unroll
-            for (int r = 0; r < Q; ++r)
+                    for (int r = 0; r < Q; ++r)
 #pragma unroll
-                for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
+                        for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? smw[UT(r, c)] : smw[UT(c, r)];
+                    double rpiv[Q];
+                    int pv[Q];
+                    if (!lu_factor_p<Q>(A, rpiv, pv)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll 1
+                    for (int c = 0; c < NB; ++c) {
+                        double b[Q];
 #pragma unroll
-            for (int c = 0; c < NB; ++c)
+                        for (int k = 0; k < Q; ++k) b[k] = smw[15 + 5 * c + k];
+                        lu_solve_refined<Q>(A, rpiv, pv, smw, b);
 #pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = sm[15 + 5 * c + k];
-            if (cnt >= Q) {
-                if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
-            } else {
+                        for (int k = 0; k < Q; ++k) smw[15 + 5 * c + k] = b[k];
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 15; k < 15 + 5 * NB; ++k) smw[k] = 0.0;
+                }
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+                    for (int k = 0; k < Q; ++k) B[c][k] = smw[15 + 5 * c + k];
+            } else {
+                double A[Q][Q];
+#pragma unroll
+                for (int r = 0; r < Q; ++r)
+#pragma unroll
+                    for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) B[c][k] = sm[15 + 5 * c + k];
+                if (cnt >= Q) {
+                    if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c)
+#pragma unroll
+                        for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
+                }
             }
             // interpolation a(dr) . d (shift_interpolate_mod.f90:255-298)
             double a[Q];
@@ -1139,11 +1356,11 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
     }
 }
 
-template <int NB, int G, bool TIGHT = false>
-__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc,
-                                                 const Lst Ln, const int* __restrict__ gstart,
-                                                 const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
-    pst_body<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, blockIdx.x);
+template <int NB, int G, bool TIGHT = false, bool MIXED = false>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
+    k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
+          const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
+    pst_body<NB, G, MIXED>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, blockIdx.x);
 }
 
 // =======================================================================================
@@ -1181,7 +1398,7 @@ __device__ __forceinline__ const SolveDesc& load_desc(const SolveDesc* D, int s,
     return sd;
 }
 
-template <int NB, int G, bool TIGHT = false>
+template <int NB, int G, bool TIGHT = false, bool MIXED = false>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_stage(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
                                                     int ps, int pl) {
     __shared__ SolveDesc sd;
@@ -1190,7 +1407,7 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_stage(c
     const int sb = d.sb ^ ps, lb = d.lb ^ pl;
     S.dt1 = d.dt1[S.stage - 1];
     S.dt2 = d.dt2[S.stage - 1];
-    stage_body<NB, G>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, S, d.sc, d.ntx, m.y);
+    stage_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, S, d.sc, d.ntx, m.y);
 }
 
 template <int NB, int G, int WQ>
@@ -1204,13 +1421,13 @@ __global__ void __launch_bounds__(PPB * G) kb_ghost(const SolveDesc* __restrict_
                           zero_other ? d.L[lb ^ 1].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
 }
 
-template <int NB, int G, bool TIGHT = false>
+template <int NB, int G, bool TIGHT = false, bool MIXED = false>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(const SolveDesc* __restrict__ D, const BatchMap M, int ps, int pl) {
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);
     const int sb = d.sb ^ ps, lb = d.lb ^ pl;
-    pst_body<NB, G>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, d.sc, d.ntx, m.y);
+    pst_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, d.sc, d.ntx, m.y);
 }
 
 // =======================================================================================
@@ -1247,14 +1464,16 @@ static __global__ void k_copy_fprev(const Phys P, const Fld F, const Work W) {
 
 // Problem 1 epilogue of a step (main.f90:139-149 with check_steady_state_mod.f90:39-65):
 // the stage kernel already reduced max|f_previous - u|.
+// End of a time step of problem 1 (one thread): steady check, step count, step budget.
 __device__ __forceinline__ void epilogue_body(double threshold, Scalars* sc) {
-    if (sc->err != 0 || sc->steady != 0) return;
+    if (sc->err != 0 || sc->steady != 0 || sc->done != 0) return;
     sc->step_count += 1;
     const double df = __longlong_as_double((long long)sc->dfmax);
     if (df < threshold) {
         sc->steady = 1;
         sc->steady_step = sc->step_count;
     }
+    if (sc->step_limit > 0 && sc->step_count >= sc->step_limit) sc->done = 1;
     sc->dfmax = 0ull;
 }
 

@@ -3,12 +3,14 @@ from ._abi import (LIB_PATH, PRECISION_FP64, PRECISION_MIXED, LssphError, Params
                    load)
 from .params import (boussinesq_params, cavity_params, check_param, default_params, diffusion_params,
                      from_config, init_param, make_params, taylor_green_params, write_config_h)
-from .simulation import Simulation, State, read_data, setup_particles
+from .simulation import Simulation, State, estimate_device_bytes, read_data, setup_particles
 from .batch import Batch
+from .serving import Request, Server, ServerStats, device_memory
 
 __all__ = [
     "LIB_PATH", "PRECISION_FP64", "PRECISION_MIXED", "LssphError", "Params", "exported_names", "load",
     "boussinesq_params", "cavity_params", "check_param", "default_params", "diffusion_params",
     "from_config", "init_param", "make_params", "taylor_green_params", "write_config_h",
-    "Simulation", "State", "read_data", "setup_particles", "Batch",
+    "Simulation", "State", "estimate_device_bytes", "read_data", "setup_particles", "Batch",
+    "Request", "Server", "ServerStats", "device_memory",
 ]

@@ -158,6 +158,11 @@ _PROTOS = {
     "lssph_write_parameters": (C.c_int, [_P(Params), C.c_int32, C.c_int32, C.c_char_p]),
     "lssph_read_data": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _i, _d, _d, _d, _d, _d, _d, _d]),
     "lssph_last_step_stats": (C.c_int, [_H, _P(C.c_double), _P(C.c_int64)]),
+    "lssph_mem_info": (C.c_int, [_P(C.c_int64), _P(C.c_int64)]),
+    "lssph_device_bytes": (C.c_int, [_H, _P(C.c_int64)]),
+    "lssph_estimate_device_bytes": (C.c_int, [_P(Params), _P(C.c_int64)]),
+    "lssph_set_step_budget": (C.c_int, [_H, C.c_int32]),
+    "lssph_get_progress": (C.c_int, [_H, _i, _i]),
     "lssph_get_tuning": (C.c_int, [_H, _i, _i, _P(C.c_double), _P(C.c_double)]),
     "lssph_step_profiled": (C.c_int, [_H, C.c_int32, _d, _P(C.c_int64)]),
     "lssph_batch_create": (C.c_int, [_P(C.c_void_p)]),
@@ -166,7 +171,7 @@ _PROTOS = {
     "lssph_batch_add": (C.c_int, [_H, _H]),
     "lssph_batch_remove": (C.c_int, [_H, _H]),
     "lssph_batch_size": (C.c_int, [_H]),
-    "lssph_batch_step": (C.c_int, [_H, C.c_int32, _i, _i]),
+    "lssph_batch_step": (C.c_int, [_H, C.c_int32, _i, _i, _i]),
     "lssph_batch_last_step_stats": (C.c_int, [_H, _P(C.c_double), _P(C.c_int64)]),
     # device pointers (caller-owned device memory), stream handle
     "lssph_rhs_noalloc": (C.c_int, [_P(Params), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,

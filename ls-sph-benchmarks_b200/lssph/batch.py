@@ -64,21 +64,23 @@ class Batch:
         self._chk(self._lib.lssph_batch_remove(self._b, sim._h))
         self.members = [m for m in self.members if m is not sim]
 
-    def step(self, nsteps: int = 1, raise_on_error: bool = True) -> tuple[np.ndarray, np.ndarray]:
+    def step(self, nsteps: int = 1, raise_on_error: bool = True) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         """Advance every member nsteps steps.
 
-        Returns (status, steady): per-member status codes and the 1-based step within
-        this call at which each member reached a steady state (0 = not reached).  With
-        raise_on_error, a member error raises LssphError after the call.
+        Returns (status, steady, steps): per-member status codes, the 1-based step within
+        this call at which each member reached a steady state (0 = not reached), and the
+        steps each member actually advanced (fewer once it stopped).  With raise_on_error,
+        a member error raises LssphError after the call.
         """
         n = len(self.members)
         status = np.zeros(n, dtype=np.int32)
         steady = np.zeros(n, dtype=np.int32)
+        steps = np.zeros(n, dtype=np.int32)
         rc = self._lib.lssph_batch_step(self._b, int(nsteps), iptr(status) if n else None,
-                                        iptr(steady) if n else None)
+                                        iptr(steady) if n else None, iptr(steps) if n else None)
         if rc == _abi.E_CUDA or (raise_on_error and rc != _abi.OK):
             self._chk(rc)
-        return status, steady
+        return status, steady, steps
 
     def last_step_stats(self) -> tuple[float, int]:
         ms = C.c_double()

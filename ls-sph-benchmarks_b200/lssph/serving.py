@@ -1,0 +1,207 @@
+"""Request loop: continuous batching of independent solves on one GPU.
+
+Requests (a parameter set and a number of time steps) arrive over time.  The server keeps
+every admitted solve resident on the device and advances all of them together through
+one :class:`~lssph.batch.Batch` (one graph launch per step for all members).  Between
+batch calls it
+  * admits waiting requests, in arrival order, whose device footprint (computed exactly
+    by lssph_estimate_device_bytes) fits the remaining HBM budget and a free slot;
+    a request that does not fit does not block smaller ones behind it (first fit);
+  * gives each new member a step budget equal to its remaining steps, so it stops on the
+    device exactly where a solo run of that many steps stops, whatever the chunk size;
+  * retires members that finished (budget used up, steady state or error): downloads the
+    final state, frees the device memory and records the time to solution.
+Each result is bit-identical to running the same request alone (the batched kernels run
+the solo arithmetic per member); the serving test checks this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import Params, check
+from .batch import Batch
+from .simulation import Simulation, State, estimate_device_bytes, setup_counts
+
+
+def device_memory() -> tuple[int, int]:
+    """(free, total) bytes of the current device."""
+    lib = _abi.load()
+    f, t = C.c_int64(), C.c_int64()
+    check(lib.lssph_mem_info(C.byref(f), C.byref(t)))
+    return f.value, t.value
+
+
+@dataclass
+class Request:
+    rid: int
+    params: Params
+    nsteps: int
+    arrival: float = 0.0                 # seconds on the server clock
+    tag: str = ""
+    state: State | None = None           # initial state (default: the fresh-start setup)
+    # filled in by the server
+    footprint: int = 0
+    admitted: float | None = None
+    finished: float | None = None
+    steps_done: int = 0
+    status: int = 0
+    stopped: str = ""                    # "budget" | "steady" | "error"
+    result: State | None = None
+
+    @property
+    def latency(self) -> float | None:
+        return None if self.finished is None else self.finished - self.arrival
+
+
+@dataclass
+class ServerStats:
+    completed: int
+    makespan_s: float
+    solves_per_s: float
+    p50_s: float
+    p99_s: float
+    particle_updates_per_s: float
+    device_ms: float
+    max_active: int
+    batch_calls: int
+    latencies_s: list = field(default_factory=list)
+
+
+class Server:
+    """Continuous-batching request loop (single thread, one device)."""
+
+    def __init__(self, hbm_budget: int | None = None, max_active: int = 64, chunk_steps: int = 50,
+                 keep_results: bool = True, clock=time.perf_counter):
+        if hbm_budget is None:
+            free, _ = device_memory()
+            hbm_budget = int(0.8 * free)
+        self.hbm_budget = int(hbm_budget)
+        self.max_active = int(max_active)
+        self.chunk_steps = int(chunk_steps)
+        self.keep_results = keep_results
+        self.clock = clock
+        self.batch = Batch()
+        self.waiting: deque[Request] = deque()
+        self.active: list[tuple[Request, Simulation]] = []
+        self.done: list[Request] = []
+        self.used = 0
+        self.peak_used = 0
+        self.t0 = clock()
+        self.device_ms = 0.0
+        self.batch_calls = 0
+        self.peak_active = 0
+        self.particle_steps = 0
+
+    # ---- request intake ---------------------------------------------------------------
+    def now(self) -> float:
+        return self.clock() - self.t0
+
+    def submit(self, req: Request) -> None:
+        if req.footprint == 0:
+            req.footprint = estimate_device_bytes(req.params)
+        if req.footprint > self.hbm_budget:
+            raise ValueError(f"request {req.rid} needs {req.footprint} bytes, over the HBM budget")
+        self.waiting.append(req)
+
+    def _admit(self) -> int:
+        now = self.now()
+        admitted = 0
+        keep: deque[Request] = deque()
+        while self.waiting:
+            req = self.waiting.popleft()
+            if (req.arrival <= now and len(self.active) < self.max_active
+                    and self.used + req.footprint <= self.hbm_budget):
+                if req.state is None:
+                    sim = Simulation.new(req.params)
+                else:
+                    sim = Simulation(req.params, req.state, setup_counts(req.params)[1])
+                    sim.ghost()
+                sim.set_step_budget(req.nsteps)
+                self.batch.add(sim)
+                self.active.append((req, sim))
+                self.used += req.footprint
+                self.peak_used = max(self.peak_used, self.used)
+                req.admitted = self.now()
+                admitted += 1
+            else:
+                keep.append(req)
+        self.waiting = keep
+        self.peak_active = max(self.peak_active, len(self.active))
+        return admitted
+
+    # ---- one batch call ---------------------------------------------------------------
+    def step_once(self) -> int:
+        """Admit, advance every member by up to chunk_steps, retire finished members.
+        Returns the number of members retired."""
+        self._admit()
+        if not self.active:
+            return 0
+        status, steady, steps = self.batch.step(self.chunk_steps, raise_on_error=False)
+        ms, _ = self.batch.last_step_stats()
+        self.device_ms += ms
+        self.batch_calls += 1
+        retired = []
+        for i, (req, sim) in enumerate(self.active):
+            req.steps_done += int(steps[i])
+            self.particle_steps += int(steps[i]) * sim.num_int
+            if status[i] != _abi.OK:
+                req.status, req.stopped = int(status[i]), "error"
+            elif steady[i] > 0:
+                req.stopped = "steady"
+            elif req.steps_done >= req.nsteps:
+                req.stopped = "budget"
+            if req.stopped:
+                retired.append(i)
+        for i in reversed(retired):
+            req, sim = self.active.pop(i)
+            if self.keep_results and req.status == _abi.OK:
+                req.result = sim.download()
+            self.batch.remove(sim)
+            sim.close()
+            self.used -= req.footprint
+            req.finished = self.now()
+            self.done.append(req)
+        return len(retired)
+
+    def run(self, requests: list[Request], realtime: bool = True) -> ServerStats:
+        """Serve `requests` (arrival times relative to the start of this call).  With
+        realtime=False every request is available at once."""
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        self.t0 = self.clock()
+        total = len(pending)
+        while len(self.done) < total:
+            now = self.now()
+            while pending and (not realtime or pending[0].arrival <= now):
+                r = pending.popleft()
+                if not realtime:
+                    r.arrival = 0.0
+                self.submit(r)
+            if not self.active and not self.waiting and pending:
+                time.sleep(max(0.0, min(pending[0].arrival - self.now(), 0.05)))
+                continue
+            self.step_once()
+        return self.stats()
+
+    def stats(self) -> ServerStats:
+        lat = sorted(r.latency for r in self.done if r.latency is not None)
+        span = max((r.finished for r in self.done), default=0.0) - min((r.arrival for r in self.done), default=0.0)
+        q = lambda f: float(np.quantile(lat, f)) if lat else math.nan   # noqa: E731
+        return ServerStats(completed=len(self.done), makespan_s=span,
+                           solves_per_s=len(self.done) / span if span > 0 else math.nan,
+                           p50_s=q(0.5), p99_s=q(0.99),
+                           particle_updates_per_s=self.particle_steps / span if span > 0 else math.nan,
+                           device_ms=self.device_ms, max_active=self.peak_active, batch_calls=self.batch_calls,
+                           latencies_s=lat)
+
+    def close(self) -> None:
+        for _, sim in self.active:
+            sim.close()
+        self.active = []
+        self.batch.close()

@@ -213,6 +213,22 @@ class Simulation:
         self._chk(self._lib.lssph_step_profiled(self._h, int(nsteps), ms, nl))
         return {k: (ms[i], nl[i]) for i, k in enumerate(_abi.KIND_NAMES)}
 
+    def device_bytes(self) -> int:
+        """Device memory this solve holds (requested bytes)."""
+        n = C.c_int64()
+        self._chk(self._lib.lssph_device_bytes(self._h, C.byref(n)))
+        return n.value
+
+    def set_step_budget(self, nsteps: int) -> None:
+        """Stop advancing after nsteps more steps (0 removes the budget)."""
+        self._chk(self._lib.lssph_set_step_budget(self._h, int(nsteps)))
+
+    def progress(self) -> tuple[int, str]:
+        """(steps completed since creation, "running" | "steady" | "budget")."""
+        n, st = C.c_int32(), C.c_int32()
+        self._chk(self._lib.lssph_get_progress(self._h, C.byref(n), C.byref(st)))
+        return n.value, ("running", "steady", "budget")[st.value]
+
     def tuning(self) -> dict:
         """Kernel configuration picked for this solve (lanes, register budget, timings)."""
         lanes, tight = C.c_int32(), C.c_int32()
@@ -234,6 +250,22 @@ class Simulation:
 
     def write_data(self, results_root: str, step: int) -> None:
         self._chk(self._lib.lssph_write_data(self._h, results_root.encode(), int(step)))
+
+
+def setup_counts(params: Params) -> tuple[int, int]:
+    """(num_total, num_int) of the closed box described by params."""
+    lib = _abi.load()
+    nt, ni = C.c_int32(), C.c_int32()
+    check(lib.lssph_setup_counts(C.byref(params), C.byref(nt), C.byref(ni)))
+    return nt.value, ni.value
+
+
+def estimate_device_bytes(params: Params) -> int:
+    """Device bytes Simulation.new(params) will allocate (host-side computation)."""
+    lib = _abi.load()
+    n = C.c_int64()
+    check(lib.lssph_estimate_device_bytes(C.byref(params), C.byref(n)))
+    return n.value
 
 
 def read_data(path: str, params: Params) -> State:

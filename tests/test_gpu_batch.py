@@ -59,7 +59,8 @@ def test_batch_equals_solo_bit_exact():
         for m in mem:
             b.add(m)
         for _ in range(2):          # two calls: both step parities and descriptor reuse
-            status, steady = b.step(3)
+            status, steady, steps = b.step(3)
+            assert (steps == 3).all()
             assert (status == 0).all() and (steady == 0).all()
         ms, launches = b.last_step_stats()
         assert ms > 0 and launches > 0
@@ -115,9 +116,10 @@ def test_steady_state_per_member():
     with lssph.Batch() as bt:
         bt.add(d)
         bt.add(t)
-        status, steady = bt.step(s_ref + 7)
+        status, steady, steps = bt.step(s_ref + 7)
     assert (status == 0).all()
     assert steady[0] == s_ref and steady[1] == 0
+    assert steps[0] == s_ref and steps[1] == s_ref + 7
     rt.step(s_ref + 7)
     _same(d, ref, "diffusion")     # frozen at its steady state while the other ran on
     _same(t, rt, "taylor_green")
@@ -133,7 +135,7 @@ def test_error_is_isolated_to_its_member():
     with lssph.Batch() as bt:
         bt.add(bad)
         bt.add(good)
-        status, _ = bt.step(3, raise_on_error=False)
+        status, _, _ = bt.step(3, raise_on_error=False)
         with pytest.raises(lssph.LssphError):
             bt.step(1)
     assert status[0] == lssph._abi.E_NONFINITE and status[1] == 0
@@ -169,3 +171,49 @@ def test_destroyed_member_leaves_the_batch():
     bt.close()
     rb.step(3)
     _same(b_, rb, "b")
+
+
+def test_step_budget_alone():
+    p = MEMBERS[2]()
+    a, ref = _sim(p, seed=11), _sim(p, seed=11)
+    a.set_step_budget(7)
+    a.step(10)
+    assert a.progress() == (7, "budget")
+    ref.step(7)
+    _same(a, ref, "stopped at the budget")
+    a.step(5)                       # no-op once stopped
+    _same(a, ref, "still stopped")
+    a.set_step_budget(0)            # resume
+    a.step(3)
+    ref.step(3)
+    assert a.progress() == (10, "running")
+    _same(a, ref, "resumed")
+
+
+def test_step_budgets_in_a_batch():
+    mk = [MEMBERS[1], MEMBERS[2], MEMBERS[3], MEMBERS[0], MEMBERS[6]]
+    budgets = [3, 5, 8, 4, 6]
+    mem = [_sim(f(), seed=20 + i) for i, f in enumerate(mk)]
+    ref = [_sim(f(), seed=20 + i) for i, f in enumerate(mk)]
+    with lssph.Batch() as bt:
+        for m, n in zip(mem, budgets):
+            m.set_step_budget(n)
+            bt.add(m)
+        status, _, steps = bt.step(10)
+        assert (status == 0).all()
+        assert list(steps) == budgets
+        mem[2].set_step_budget(2)   # two more for one member, the others stay stopped
+        _, _, steps = bt.step(4)
+        assert list(steps) == [0, 0, 2, 0, 0]
+    for r, n in zip(ref, budgets):
+        r.step(n)
+    ref[2].step(2)
+    for i, (m, r) in enumerate(zip(mem, ref)):
+        _same(m, r, i)
+
+
+@pytest.mark.parametrize("k", range(len(MEMBERS)))
+def test_footprint_estimate_matches_allocation(k):
+    p = MEMBERS[k]()
+    sim = lssph.Simulation.new(p)
+    assert sim.device_bytes() == lssph.estimate_device_bytes(p)

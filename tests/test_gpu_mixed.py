@@ -1,0 +1,110 @@
+"""Mixed precision: FP32 kernel weights, basis and neighbour sums (over FP64-formed,
+FP32-rounded offsets and field differences), FP64 moment-matrix factorisation with one
+refinement step, FP64 RK update.
+
+Bound (stated): every field within relative L2 1e-5 of the FP64 path on the same inputs
+after the stated step count, and analytical-solution errors unchanged.  Needs a B200.
+"""
+import numpy as np
+import pytest
+
+import lssph
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+CASES = {
+    "diffusion": (lambda: lssph.diffusion_params(num=50, seed=1), 1000),
+    "taylor_green": (lambda: lssph.taylor_green_params(num=64), 400),
+    "cavity": (lambda: lssph.cavity_params(num=64), 400),
+    "boussinesq": (lambda: lssph.boussinesq_params(num=48, ra=1e5), 400),
+}
+
+
+def _fields(p):
+    return ("x", "y", "u", "v", "rho", "pre") + (("tem",) if p.target_problem == 4 else ())
+
+
+def _sim(p, precision, amp=0.1, seed=0):
+    q = lssph.make_params(p, precision=precision)
+    st, ni = lssph.setup_particles(q)
+    rng = np.random.default_rng(seed)
+    if q.target_problem != 1:
+        st.x[:ni] += amp * q.dx * (2 * rng.random(ni) - 1)
+        st.y[:ni] += amp * q.dx * (2 * rng.random(ni) - 1)
+    sim = lssph.Simulation(q, st, ni)
+    sim.ghost()
+    return sim
+
+
+def _rel(a, b):
+    n = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / n if n > 0 else np.linalg.norm(a - b)
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_mixed_within_bound_of_fp64(case):
+    mk, steps = CASES[case]
+    p = mk()
+    s64 = _sim(p, lssph.PRECISION_FP64)
+    smx = _sim(p, lssph.PRECISION_MIXED)
+    assert s64.step(steps) == smx.step(steps) == 0
+    g64, gmx = s64.download(), smx.download()
+    ni = s64.num_int
+    for k in _fields(p):
+        err = _rel(getattr(gmx, k)[:ni], getattr(g64, k)[:ni])
+        assert err <= TOL, (k, err)
+    assert not np.array_equal(gmx.u, g64.u)   # it is a different arithmetic
+
+
+def test_mixed_against_the_oracle():
+    p = lssph.cavity_params(num=48)
+    smx = _sim(p, lssph.PRECISION_MIXED, seed=3)
+    st, ni = lssph.setup_particles(p)
+    rng = np.random.default_rng(3)
+    st.x[:ni] += 0.1 * p.dx * (2 * rng.random(ni) - 1)
+    st.y[:ni] += 0.1 * p.dx * (2 * rng.random(ni) - 1)
+    orc = O.Oracle(p, st, ni, ghost=True)
+    smx.step(50)
+    orc.run(50)
+    g, o = smx.download(), orc.get()
+    for k in _fields(p):
+        assert _rel(getattr(g, k)[:ni], o[k][:ni]) <= TOL, k
+
+
+def test_mixed_taylor_green_decay_error_unchanged():
+    # velocity amplitude decays as exp(-8 pi^2 t / Re) (TG_A = TG_B = 2)
+    p = lssph.taylor_green_params(num=64, re=100.0)
+    errs = {}
+    for prec in (lssph.PRECISION_FP64, lssph.PRECISION_MIXED):
+        sim = _sim(p, prec, amp=0.0)
+        u0 = sim.download()
+        n = 800
+        sim.step(n)
+        g = sim.download()
+        ni = sim.num_int
+        decay = np.exp(-8.0 * np.pi ** 2 * (n * p.dt) / 100.0)
+        ref = np.hypot(u0.u[:ni], u0.v[:ni]) * decay
+        errs[prec] = np.linalg.norm(np.hypot(g.u[:ni], g.v[:ni]) - ref) / np.linalg.norm(ref)
+    # the discretisation error dominates; mixed precision moves it by well under 1%
+    assert abs(errs[lssph.PRECISION_MIXED] - errs[lssph.PRECISION_FP64]) <= 1e-2 * errs[lssph.PRECISION_FP64], errs
+
+
+def test_mixed_members_identical_alone_and_batched():
+    mk = [lambda: lssph.taylor_green_params(num=48), lambda: lssph.boussinesq_params(num=40),
+          lambda: lssph.diffusion_params(num=30)]
+    solo = [_sim(f(), lssph.PRECISION_MIXED, seed=i) for i, f in enumerate(mk)]
+    mem = [_sim(f(), lssph.PRECISION_MIXED, seed=i) for i, f in enumerate(mk)]
+    fp64 = _sim(lssph.cavity_params(num=32), lssph.PRECISION_FP64, seed=9)
+    ref64 = _sim(lssph.cavity_params(num=32), lssph.PRECISION_FP64, seed=9)
+    with lssph.Batch() as b:
+        for m in mem + [fp64]:
+            b.add(m)
+        b.step(5)
+    for s in solo + [ref64]:
+        s.step(5)
+    for s, m in zip(solo + [ref64], mem + [fp64]):
+        gs, gm = s.download(), m.download()
+        for k in _fields(s.params):
+            assert np.array_equal(getattr(gs, k), getattr(gm, k)), k

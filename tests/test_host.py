@@ -183,3 +183,22 @@ def test_status_strings():
     lib = lssph.load()
     for code in range(0, -11, -1):
         assert lib.lssph_status_string(code)
+
+
+def test_mixed_precision_requires_four_lanes():
+    import lssph
+    p = lssph.make_params(lssph.taylor_green_params(num=16), precision=lssph.PRECISION_MIXED, lanes=2)
+    st, ni = lssph.setup_particles(p)
+    with pytest.raises(lssph.LssphError) as e:
+        lssph.Simulation(p, st, ni)
+    assert e.value.status == lssph._abi.E_UNSUPPORTED
+
+
+def test_device_footprint_estimate_is_host_only_and_grows_with_size():
+    import lssph
+    sizes = [lssph.estimate_device_bytes(lssph.taylor_green_params(num=n)) for n in (32, 64, 128)]
+    assert 0 < sizes[0] < sizes[1] < sizes[2]
+    # FP64 state, RK registers and cell lists: a few hundred bytes per particle
+    p = lssph.taylor_green_params(num=128)
+    nt, ni = lssph.setup_particles(p)[0].num_total, 128 * 128
+    assert 200 * nt < sizes[2] < 2000 * nt
