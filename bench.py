@@ -231,6 +231,175 @@ def run_reference(args) -> int:
     return 0
 
 
+# ---------------------------------------------------------------------------------------
+# The other configurations of the metric, reported beside the headline number
+# ---------------------------------------------------------------------------------------
+def _jittered(p, seed, amp=0.05):
+    """Fresh-start state with seeded uniform position jitter of +-amp dx (interior)."""
+    import numpy as np
+
+    import lssph
+    st, ni = lssph.setup_particles(p)
+    rng = np.random.default_rng(seed)
+    if p.target_problem != 1:   # problem 1 applies POS_PERT in its own setup
+        st.x[:ni] += amp * p.dx * (2 * rng.random(ni) - 1)
+        st.y[:ni] += amp * p.dx * (2 * rng.random(ni) - 1)
+    return st, ni
+
+
+def bench_mixed(steps: int = 100, acc_steps: int = 500) -> dict:
+    """Lid-driven cavity, Re = 1000, 256^2, RK4 + PST: FP64 vs mixed precision, and the
+    per-field relative L2 of mixed against FP64 after acc_steps steps (same inputs)."""
+    import numpy as np
+
+    import lssph
+    out = {"workload": "cavity_re1000_256x256_rk4_pst", "steps": steps,
+           "l2": "inputs larger than L2 not required: per-step working set ~45 MB, warm"}
+    states = {}
+    for name, prec in (("fp64", lssph.PRECISION_FP64), ("mixed", lssph.PRECISION_MIXED)):
+        p = lssph.make_params(lssph.cavity_params(num=256, re=1000.0), precision=prec)
+        sim = lssph.Simulation.new(p)
+        sim.step(5)
+        sim.step(steps)
+        ms, _ = sim.last_step_stats()
+        out[f"{name}_value"] = sim.num_int * steps / (ms * 1e-3)
+        out[f"{name}_register_budget"] = sim.tuning()["register_budget"]
+        sim.step(acc_steps - 5 - steps)
+        states[name] = (sim.download(), sim.num_int)
+        sim.close()
+    out["value"] = out["mixed_value"]
+    out["unit"] = UNIT
+    out["speedup_vs_fp64"] = out["mixed_value"] / out["fp64_value"]
+    (g64, ni), (gmx, _) = states["fp64"], states["mixed"]
+    out["rel_l2_vs_fp64"] = {k: float(np.linalg.norm(getattr(gmx, k)[:ni] - getattr(g64, k)[:ni]) /
+                                      np.linalg.norm(getattr(g64, k)[:ni])) for k in ("x", "y", "u", "v", "rho", "pre")}
+    out["rel_l2_after_steps"] = acc_steps
+    return out
+
+
+def batched_mix(seed: int = 4, n: int = 64, precision: int = 0):
+    """64 solves: half diffusion, half Taylor-Green; lattice side uniform over
+    {32,48,64,96,128,192,256}; Re log-uniform in [50, 1000]; jitter +-0.05 dx."""
+    import numpy as np
+
+    import lssph
+    rng = np.random.default_rng(seed)
+    sides = [32, 48, 64, 96, 128, 192, 256]
+    specs = []
+    for k in range(n):
+        side = int(rng.choice(sides))
+        re = float(np.exp(rng.uniform(np.log(50.0), np.log(1000.0))))
+        s = int(rng.integers(1 << 30))
+        if k % 2 == 0:
+            p = lssph.diffusion_params(num=side, pos_pert=0.05, seed=s)
+        else:
+            p = lssph.taylor_green_params(num=side, re=re)
+        specs.append((lssph.make_params(p, precision=precision), s))
+    return specs
+
+
+def bench_batched(steps: int = 20) -> dict:
+    import lssph
+    out = {"workload": "64 solves: 32 diffusion + 32 Taylor-Green, sides {32..256}, Re log-uniform [50,1000]",
+           "steps": steps, "l2": "batched working set > L2 (126 MB); sequential runs are L2-warm"}
+    # 64 sequential plain-FP64 runs, one after the other
+    seq_ms, seq_units = 0.0, 0
+    for p, s in batched_mix(precision=lssph.PRECISION_FP64):
+        st, ni = _jittered(p, s)
+        sim = lssph.Simulation(p, st, ni)
+        sim.ghost()
+        sim.step(3)
+        sim.step(steps)
+        seq_ms += sim.last_step_stats()[0]
+        seq_units += ni * steps
+        sim.close()
+    out["sequential_fp64_value"] = seq_units / (seq_ms * 1e-3)
+    for name, prec in (("batched_fp64", lssph.PRECISION_FP64), ("batched_mixed", lssph.PRECISION_MIXED)):
+        sims = []
+        units = 0
+        with lssph.Batch() as b:
+            for p, s in batched_mix(precision=prec):
+                st, ni = _jittered(p, s)
+                sim = lssph.Simulation(p, st, ni)
+                sim.ghost()
+                sims.append(sim)
+                b.add(sim)
+                units += ni
+            b.step(3)
+            b.step(steps)
+            ms, launches = b.last_step_stats()
+        out[f"{name}_value"] = units * steps / (ms * 1e-3)
+        out[f"{name}_launches_per_step"] = launches // steps
+        for sim in sims:
+            sim.close()
+    out["total_particles"] = units
+    out["value"] = out["batched_mixed_value"]
+    out["unit"] = UNIT
+    out["speedup_vs_sequential_fp64"] = out["batched_mixed_value"] / out["sequential_fp64_value"]
+    return out
+
+
+def _perturbed_temperature(p, seed: int, amp: float = 1e-3):
+    """Initial state builder: fresh start plus a seeded uniform T perturbation of +-amp."""
+    def init():
+        import numpy as np
+
+        import lssph
+        st, ni = lssph.setup_particles(p)
+        st.tem[:ni] += amp * (2.0 * np.random.default_rng(seed).random(ni) - 1.0)
+        return st
+    return init
+
+
+def serving_requests(seed: int = 5, rate: float = 20.0, window_s: float = 8.0, median_steps: int = 60):
+    """Poisson arrivals; 50% bottom-heated Boussinesq (Ra log-uniform [1e4, 1e6], Pr 0.71,
+    seeded initial T perturbation of amplitude 1e-3), 50% lid-driven cavity (Re log-uniform
+    [100, 3200]); lattice side uniform over 64..384 in steps of 32; mixed precision.  The
+    simulated time of every request is t_end = 20 scaled by one factor, chosen so that the
+    median request runs median_steps steps."""
+    import numpy as np
+
+    import lssph
+    from lssph import Request
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > window_s:
+            break
+        side = int(rng.choice(np.arange(64, 385, 32)))
+        if rng.random() < 0.5:
+            ra = float(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
+            p = lssph.make_params(lssph.boussinesq_params(num=side, ra=ra, pr=0.71), precision=lssph.PRECISION_MIXED)
+            init, tag = _perturbed_temperature(p, int(rng.integers(1 << 30))), "boussinesq"
+        else:
+            re = float(np.exp(rng.uniform(np.log(100.0), np.log(3200.0))))
+            p = lssph.make_params(lssph.cavity_params(num=side, re=re), precision=lssph.PRECISION_MIXED)
+            init, tag = None, "cavity"
+        reqs.append(Request(rid=len(reqs), params=p, nsteps=0, arrival=t, tag=tag, init=init))
+    steps20 = np.array([20.0 / r.params.dt for r in reqs])
+    scale = median_steps / float(np.median(steps20))
+    for r, n20 in zip(reqs, steps20):
+        r.nsteps = max(1, int(round(n20 * scale)))
+    return reqs, scale
+
+
+def bench_serving() -> dict:
+    from lssph import Server
+    reqs, scale = serving_requests()
+    srv = Server(max_active=64, chunk_steps=20, keep_results=False)
+    st = srv.run(reqs)
+    srv.close()
+    return {"workload": "Poisson 20/s for 8 s; 50% Boussinesq Ra [1e4,1e6], 50% cavity Re [100,3200]; "
+                        "sides 64..384 step 32; mixed precision",
+            "t_end_scale": scale, "t_end": 20.0 * scale, "requests": len(reqs), "completed": st.completed,
+            "p50_s": st.p50_s, "p99_s": st.p99_s, "solves_per_s": st.solves_per_s,
+            "particle_updates_per_s": st.particle_updates_per_s, "device_busy_s": st.device_ms * 1e-3,
+            "makespan_s": st.makespan_s, "max_active": st.max_active, "batch_calls": st.batch_calls,
+            "host_setup_s": st.host_create_s, "host_wait_s": st.wait_s, "host_retire_s": st.host_retire_s,
+            "admission": "first fit by exact device footprint within 80% of free HBM, 64 slots"}
+
+
 def run_engine(args) -> int:
     import numpy as np
     import torch
@@ -326,6 +495,11 @@ def run_engine(args) -> int:
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
+    extras = {}
+    if rank == 0 and ws == 1 and not args.no_extras:
+        extras["mixed"] = bench_mixed()
+        extras["batched"] = bench_batched()
+        extras["serving"] = bench_serving()
 
     if dist:
         dist.barrier()
@@ -339,7 +513,7 @@ def run_engine(args) -> int:
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks.summary()}
+            "clocks": clocks.summary(), **extras}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -352,6 +526,8 @@ def main() -> int:
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision, batched and serving configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

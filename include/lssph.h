@@ -247,6 +247,12 @@ int  lssph_batch_size(const lssph_batch* b);
    LSSPH_E_CUDA for a failure of the batch itself. */
 int  lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady,
                       int32_t* steps_taken);
+/* lssph_batch_step in two halves, so that the host can prepare new solves while the GPU
+   steps the batch: lssph_batch_launch enqueues the nsteps steps and returns; the batch
+   and its members must not be used (no add/remove, no solo calls) until lssph_batch_wait
+   has returned the same outputs as lssph_batch_step.  lssph_batch_step = launch + wait. */
+int  lssph_batch_launch(lssph_batch* b, int32_t nsteps);
+int  lssph_batch_wait(lssph_batch* b, int32_t* status, int32_t* steady, int32_t* steps_taken);
 /* Device time and kernel launches of the last lssph_batch_step (all members). */
 int  lssph_batch_last_step_stats(const lssph_batch* b, double* device_ms, int64_t* kernel_launches);
 

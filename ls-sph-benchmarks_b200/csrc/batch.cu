@@ -59,9 +59,13 @@ struct lssph_batch {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_launches = 0;
     SolveDesc* all_desc = nullptr;       // device, every member in member order (scalar gather)
-    Scalars* d_sc = nullptr;             // device gather buffer
-    Scalars* h_sc = nullptr;             // pinned host copy
+    Scalars* d_sc = nullptr;             // device gather buffer: [0, n) before, [n, 2n) after a step call
+    Scalars* h_sc = nullptr;             // pinned host copy of it
     size_t sc_cap = 0;
+    // the step call in flight (lssph_batch_launch .. lssph_batch_wait)
+    bool in_flight = false;
+    int flight_steps = 0;
+    std::vector<int> sb_start, lb_start;
     double last_ms = 0.0;
     int64_t last_launches = 0;
     std::string err;
@@ -313,8 +317,8 @@ int rebuild(lssph_batch* b) {
         b->d_sc = nullptr;
         b->h_sc = nullptr;
         b->sc_cap = 0;
-        BATCH_TRY(b, cudaMalloc(&b->d_sc, sizeof(Scalars) * n));
-        BATCH_TRY(b, cudaMallocHost(&b->h_sc, sizeof(Scalars) * n));
+        BATCH_TRY(b, cudaMalloc(&b->d_sc, 2 * sizeof(Scalars) * n));
+        BATCH_TRY(b, cudaMallocHost(&b->h_sc, 2 * sizeof(Scalars) * n));
         b->sc_cap = n;
     }
     BATCH_TRY(b, cudaStreamSynchronize(b->stream));
@@ -323,13 +327,14 @@ int rebuild(lssph_batch* b) {
     return LSSPH_OK;
 }
 
-// Every member's scalars, read back in one copy (the batch stream is idle afterwards).
-int gather_scalars(lssph_batch* b) {
+// Enqueue a read-back of every member's scalars into slot `which` (0: before, 1: after).
+int gather_scalars(lssph_batch* b, int which) {
     const int n = (int)b->members.size();
-    kb_gather_scalars<<<(n + 127) / 128, 128, 0, b->stream>>>(b->all_desc, n, b->d_sc);
+    Scalars* d = b->d_sc + (size_t)which * n;
+    kb_gather_scalars<<<(n + 127) / 128, 128, 0, b->stream>>>(b->all_desc, n, d);
     BATCH_TRY(b, cudaGetLastError());
-    BATCH_TRY(b, cudaMemcpyAsync(b->h_sc, b->d_sc, sizeof(Scalars) * n, cudaMemcpyDeviceToHost, b->stream));
-    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    BATCH_TRY(b, cudaMemcpyAsync(b->h_sc + (size_t)which * n, d, sizeof(Scalars) * n, cudaMemcpyDeviceToHost,
+                                 b->stream));
     return LSSPH_OK;
 }
 
@@ -401,6 +406,7 @@ const char* lssph_batch_error(const lssph_batch* b) { return b ? b->err.c_str() 
 int lssph_batch_add(lssph_batch* b, lssph_handle* h) {
     if (!b || !h) return bfail(b, LSSPH_E_BAD_PARAM, "null argument");
     if (h->batch) return bfail(b, LSSPH_E_BAD_PARAM, "the handle is already a member of a batch");
+    if (b->in_flight) return bfail(b, LSSPH_E_BAD_PARAM, "a batch step call is in flight");
     b->members.push_back(h);
     h->batch = b;
     b->dirty = true;
@@ -411,6 +417,10 @@ int lssph_batch_remove(lssph_batch* b, lssph_handle* h) {
     if (!b || !h) return bfail(b, LSSPH_E_BAD_PARAM, "null argument");
     auto it = std::find(b->members.begin(), b->members.end(), h);
     if (it == b->members.end()) return bfail(b, LSSPH_E_BAD_PARAM, "the handle is not a member of this batch");
+    if (b->in_flight) {   // a member destroyed mid-call: finish the call first
+        b->in_flight = false;
+        cudaStreamSynchronize(b->stream);
+    }
     cudaStreamSynchronize(b->stream);
     b->members.erase(it);
     h->batch = nullptr;
@@ -420,17 +430,14 @@ int lssph_batch_remove(lssph_batch* b, lssph_handle* h) {
 
 int lssph_batch_size(const lssph_batch* b) { return b ? (int)b->members.size() : 0; }
 
-int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady, int32_t* steps_taken) {
+int lssph_batch_launch(lssph_batch* b, int32_t nsteps) {
     if (!b) return bfail(nullptr, LSSPH_E_BAD_PARAM, "null batch");
+    if (b->in_flight) return bfail(b, LSSPH_E_BAD_PARAM, "a batch step call is already in flight");
     const size_t n = b->members.size();
-    for (size_t i = 0; i < n; ++i) {
-        if (status) status[i] = LSSPH_OK;
-        if (steady) steady[i] = 0;
-        if (steps_taken) steps_taken[i] = 0;
-    }
     b->last_ms = 0.0;
     b->last_launches = 0;
-    if (nsteps <= 0 || n == 0) return LSSPH_OK;
+    b->flight_steps = nsteps > 0 ? nsteps : 0;
+    if (b->flight_steps == 0 || n == 0) { b->in_flight = true; return LSSPH_OK; }
     // a member stepped on its own since the last batch call: rewrite the descriptors
     for (size_t i = 0; i < n && !b->dirty; ++i) {
         const int par = b->flip[i] & b->t;
@@ -438,12 +445,12 @@ int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* s
     }
     int rc;
     if (b->dirty && (rc = rebuild(b)) != LSSPH_OK) return rc;
-    if ((rc = gather_scalars(b)) != LSSPH_OK) return rc;
-    std::vector<Scalars> s0(b->h_sc, b->h_sc + n);
-    std::vector<int> sb_start(n), lb_start(n);
+    if ((rc = gather_scalars(b, 0)) != LSSPH_OK) return rc;
+    b->sb_start.resize(n);
+    b->lb_start.resize(n);
     for (size_t i = 0; i < n; ++i) {
-        sb_start[i] = b->members[i]->sb;
-        lb_start[i] = b->members[i]->lb;
+        b->sb_start[i] = b->members[i]->sb;
+        b->lb_start[i] = b->members[i]->lb;
     }
     BATCH_TRY(b, cudaEventRecord(b->ev0, b->stream));
     for (int st = 0; st < nsteps; ++st) {
@@ -457,14 +464,33 @@ int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* s
         }
     }
     BATCH_TRY(b, cudaEventRecord(b->ev1, b->stream));
-    if ((rc = gather_scalars(b)) != LSSPH_OK) return rc;
+    if ((rc = gather_scalars(b, 1)) != LSSPH_OK) return rc;
+    b->in_flight = true;
+    return LSSPH_OK;
+}
+
+int lssph_batch_wait(lssph_batch* b, int32_t* status, int32_t* steady, int32_t* steps_taken) {
+    if (!b) return bfail(nullptr, LSSPH_E_BAD_PARAM, "null batch");
+    if (!b->in_flight) return bfail(b, LSSPH_E_BAD_PARAM, "no batch step call in flight");
+    b->in_flight = false;
+    const size_t n = b->members.size();
+    for (size_t i = 0; i < n; ++i) {
+        if (status) status[i] = LSSPH_OK;
+        if (steady) steady[i] = 0;
+        if (steps_taken) steps_taken[i] = 0;
+    }
+    const int nsteps = b->flight_steps;
+    if (nsteps == 0 || n == 0) return LSSPH_OK;
+    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->last_ms = ms;
     b->last_launches = (int64_t)nsteps * b->graph_launches;
+    const Scalars* s0 = b->h_sc;
+    const Scalars* s1v = b->h_sc + n;
     int first = LSSPH_OK;
     for (size_t i = 0; i < n; ++i) {
-        const Scalars& s1 = b->h_sc[i];
+        const Scalars& s1 = s1v[i];
         const int st = member_status(s1);
         if (status) status[i] = st;
         if (st != LSSPH_OK) {
@@ -477,12 +503,18 @@ int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* s
         const int executed = s1.step_count - s0[i].step_count;
         if (steps_taken) steps_taken[i] = executed;
         if (executed != nsteps) {
-            b->members[i]->sb = sb_start[i] ^ (b->flip[i] & executed & 1);
-            b->members[i]->lb = lb_start[i] ^ (b->flip[i] & executed & 1);
+            b->members[i]->sb = b->sb_start[i] ^ (b->flip[i] & executed & 1);
+            b->members[i]->lb = b->lb_start[i] ^ (b->flip[i] & executed & 1);
         }
     }
     if (first != LSSPH_OK) return bfail(b, first, "a batch member stopped with an error (see the status array)");
     return LSSPH_OK;
+}
+
+int lssph_batch_step(lssph_batch* b, int32_t nsteps, int32_t* status, int32_t* steady, int32_t* steps_taken) {
+    const int rc = lssph_batch_launch(b, nsteps);
+    if (rc != LSSPH_OK) return rc;
+    return lssph_batch_wait(b, status, steady, steps_taken);
 }
 
 int lssph_batch_last_step_stats(const lssph_batch* b, double* device_ms, int64_t* kernel_launches) {

@@ -47,18 +47,34 @@ int fail(lssph_handle* h, int code, const std::string& msg) {
             return fail((h), LSSPH_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-template <class T>
-int dalloc(lssph_handle* h, T** ptr, size_t n) {
-    *ptr = nullptr;
-    if (n == 0) n = 1;
-    void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
-    if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    h->allocs.push_back(p);
-    h->alloc_bytes += (int64_t)(n * sizeof(T));
-    *ptr = static_cast<T*>(p);
-    return LSSPH_OK;
+// Every device array of a solve, in one place: the visitor gets (&pointer, element count)
+// for each.  Used to size the solve's single device block and to carve it up.
+template <class Vis>
+void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, Vis&& A) {
+    for (int b = 0; b < 2; ++b) {
+        Fld& F = h->F[b];
+        A(&F.x, N); A(&F.y, N); A(&F.u, N); A(&F.v, N); A(&F.rho, N); A(&F.pre, N); A(&F.tem, N); A(&F.vol, N);
+        Lst& L = h->L[b];
+        A(&L.cnt, NC); A(&L.slots, NC * (size_t)cap);
+    }
+    Work& W = h->W;
+    A(&W.x_old, NI); A(&W.y_old, NI); A(&W.u_old, NI); A(&W.v_old, NI); A(&W.rho_old, NI); A(&W.tem_old, NI);
+    A(&W.x_acc, NI); A(&W.y_acc, NI); A(&W.u_acc, NI); A(&W.v_acc, NI); A(&W.rho_acc, NI); A(&W.tem_acc, NI);
+    A(&W.rhs_u, NI); A(&W.rhs_v, NI); A(&W.rhs_rho, NI); A(&W.rhs_tem, NI);
+    A(&W.f_prev, NI); A(&W.src, NI); A(&W.key, NI);
+    VMd& V = h->V;
+    A(&V.x, NE); A(&V.y, NE); A(&V.nx, NE); A(&V.ny, NE); A(&V.u, NE); A(&V.v, NE); A(&V.pre, NE); A(&V.tem, NE);
+    A(&V.K, NE); A(&V.ptype, NE); A(&V.key, NE); A(&V.mode, NE);
+    A(&h->gstart, NC + 1); A(&h->glist, NE);
+    A(&h->sc, 1);
+    A(&h->vt_tile, (size_t)std::max(nvt, 1)); A(&h->vt_start, (size_t)nvt + 1); A(&h->vt_vm, NE);
 }
+
+constexpr size_t kArrayAlign = 256;   // every array starts on a 256-byte boundary
+inline size_t align_up(size_t v) { return (v + kArrayAlign - 1) / kArrayAlign * kArrayAlign; }
+
+template <class T>
+size_t array_bytes(T**, size_t n) { return align_up(std::max<size_t>(n, 1) * sizeof(T)); }
 
 // Virtual markers grouped by the cell tile that holds them, in chunks of at most PPB
 // markers (one pass of a ghost CTA): chunk tile ids, chunk ranges, marker ids.
@@ -84,18 +100,13 @@ void vm_chunks(const CellGrid& g, int ntx, int ntiles, std::vector<int32_t>* til
     }
 }
 
-// Device bytes a solve of these sizes allocates: the same list of arrays as create_impl
-// (every array holds at least one element).
+// Size of the single device block of a solve of these sizes (every array holds at least
+// one element and starts on a 256-byte boundary).
 int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt) {
-    auto n1 = [](size_t n) { return (int64_t)std::max<size_t>(n, 1); };
-    const int64_t d = sizeof(double), i = sizeof(int32_t);
-    int64_t b = 0;
-    b += 2 * (8 * n1(N) * d + n1(NC) * i + n1(NC * (size_t)cap) * i);   // state + cell lists, 2 buffers
-    b += 18 * n1(NI) * d + n1(NI) * i;                                  // RK registers, RHS, f_prev, src, key
-    b += 9 * n1(NE) * d + 3 * n1(NE) * i;                               // virtual markers
-    b += n1(NC + 1) * i + n1(NE) * i + (int64_t)sizeof(Scalars);         // ghost CSR, scalars
-    b += n1((size_t)std::max(nvt, 1)) * i + n1((size_t)nvt + 1) * i + n1(NE) * i;   // marker chunks
-    return b;
+    lssph_handle layout;
+    size_t total = 0;
+    visit_solve_arrays(&layout, N, NI, NE, NC, cap, nvt, [&](auto** p, size_t n) { total += array_bytes(p, n); });
+    return (int64_t)total;
 }
 
 inline int blocks_for(long n, int per_block) { return (int)((n + per_block - 1) / per_block); }
@@ -294,6 +305,7 @@ int sync_check(lssph_handle* h);
 // current state (writes only the RHS arrays) with each budget, keep the faster.  Both
 // budgets give bit-identical results, so the choice never changes an answer.
 int autotune(lssph_handle* h) {
+    h->tuned = true;
     StageCfg S{};
     S.mode = MODE_RHS_ONLY;
     S.stage = 1;
@@ -319,6 +331,10 @@ int autotune(lssph_handle* h) {
     h->launch_counter = c0;
     return sync_check(h);
 }
+
+// The handle's own launches use the measured register budget; batches choose per group
+// and never need it, so the measurement waits for the first solo launch.
+int ensure_tuned(lssph_handle* h) { return h->tuned ? LSSPH_OK : autotune(h); }
 
 int check_scalars(lssph_handle* h, Scalars* out) {
     Scalars s{};
@@ -369,7 +385,7 @@ void free_handle(lssph_handle* h) {
     for (auto& row : h->graph)
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);
-    for (void* p : h->allocs) cudaFree(p);
+    if (h->block) cudaFree(h->block);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -467,24 +483,6 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         return rc;
     }
     const size_t N = num_total, NI = num_int, NE = h->num_ext, NC = h->grid.ncell;
-    bool ok = true;
-    auto A = [&](auto** ptr, size_t n) { if (ok && dalloc(h, ptr, n) != LSSPH_OK) ok = false; };
-    for (int b = 0; b < 2; ++b) {
-        Fld& F = h->F[b];
-        A(&F.x, N); A(&F.y, N); A(&F.u, N); A(&F.v, N); A(&F.rho, N); A(&F.pre, N); A(&F.tem, N); A(&F.vol, N);
-        Lst& L = h->L[b];
-        A(&L.cnt, NC); A(&L.slots, NC * h->grid.cap);
-    }
-    Work& W = h->W;
-    A(&W.x_old, NI); A(&W.y_old, NI); A(&W.u_old, NI); A(&W.v_old, NI); A(&W.rho_old, NI); A(&W.tem_old, NI);
-    A(&W.x_acc, NI); A(&W.y_acc, NI); A(&W.u_acc, NI); A(&W.v_acc, NI); A(&W.rho_acc, NI); A(&W.tem_acc, NI);
-    A(&W.rhs_u, NI); A(&W.rhs_v, NI); A(&W.rhs_rho, NI); A(&W.rhs_tem, NI);
-    A(&W.f_prev, NI); A(&W.src, NI); A(&W.key, NI);
-    VMd& V = h->V;
-    A(&V.x, NE); A(&V.y, NE); A(&V.nx, NE); A(&V.ny, NE); A(&V.u, NE); A(&V.v, NE); A(&V.pre, NE); A(&V.tem, NE);
-    A(&V.K, NE); A(&V.ptype, NE); A(&V.key, NE); A(&V.mode, NE);
-    A(&h->gstart, NC + 1); A(&h->glist, NE);
-    A(&h->sc, 1);
     // cell tiles and the tiles that hold virtual markers (grouped, ascending marker id)
     h->ntx = (h->grid.nx + TX - 1) / TX;
     h->nty = (h->grid.ny + TY - 1) / TY;
@@ -493,8 +491,26 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     std::vector<int32_t> vt_tile, vt_start, vt_vm;
     vm_chunks(h->grid, h->ntx, h->ntiles, &vt_tile, &vt_start, &vt_vm);
     h->nvt = (int)vt_tile.size();
-    A(&h->vt_tile, std::max(h->nvt, 1)); A(&h->vt_start, h->nvt + 1); A(&h->vt_vm, NE);
-    if (!ok) { const std::string m = h->err; free_handle(h); return fail(nullptr, LSSPH_E_CUDA, m); }
+    // one device block for every array of the solve (one cudaMalloc, one cudaFree)
+    const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt);
+    {
+        const cudaError_t e = cudaMalloc(&h->block, block);
+        if (e != cudaSuccess) {
+            free_handle(h);
+            return fail(nullptr, LSSPH_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        h->alloc_bytes = (int64_t)block;
+        size_t off = 0;
+        char* base = static_cast<char*>(h->block);
+        visit_solve_arrays(h, N, NI, NE, NC, h->grid.cap, h->nvt, [&](auto** p, size_t n) {
+            using T = std::remove_reference_t<decltype(**p)>;
+            *p = reinterpret_cast<T*>(base + off);
+            off += array_bytes(p, n);
+        });
+    }
+    bool ok = true;
+    Work& W = h->W;
+    VMd& V = h->V;
 
     // ---- host-side constant arrays ----
     std::vector<double> src(NI, 0.0), K(NE, 0.0), zeros(std::max(NI, NE), 0.0), ones(NI, 1.0);
@@ -553,8 +569,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (!ok) { free_handle(h); return fail(nullptr, LSSPH_E_CUDA, "device initialisation failed"); }
     prepare_kernels(h);
     if ((rc = upload_fields(h, x, y, u, v, rho, pre, tem)) != LSSPH_OK ||
-        (rc = rebuild_cells(h)) != LSSPH_OK || (rc = sync_check(h)) != LSSPH_OK ||
-        (rc = autotune(h)) != LSSPH_OK) {
+        (rc = rebuild_cells(h)) != LSSPH_OK || (rc = sync_check(h)) != LSSPH_OK) {
         const std::string m = h->err;
         free_handle(h);
         return fail(nullptr, rc, m);
@@ -597,6 +612,7 @@ int lssph_counts(const lssph_handle* h, int32_t* num_total, int32_t* num_int, in
 
 int lssph_calculate_rhs(lssph_handle* h) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (const int rc_t = ensure_tuned(h)) return rc_t;
     StageCfg S{};
     S.mode = MODE_RHS_ONLY;
     S.stage = 1;
@@ -623,6 +639,7 @@ int lssph_ghost(lssph_handle* h) {
 
 int lssph_rk2(lssph_handle* h) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (const int rc_t = ensure_tuned(h)) return rc_t;
     if (h->p.rk != 2) return fail(h, LSSPH_E_BAD_PARAM, "handle was configured with RK = 4");
     for (int s = 1; s <= 2; ++s) enq_stage(h, s, false);
     return sync_check(h);
@@ -630,6 +647,7 @@ int lssph_rk2(lssph_handle* h) {
 
 int lssph_rk4(lssph_handle* h) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (const int rc_t = ensure_tuned(h)) return rc_t;
     if (h->p.rk != 4) return fail(h, LSSPH_E_BAD_PARAM, "handle was configured with RK = 2");
     for (int s = 1; s <= 4; ++s) enq_stage(h, s, false);
     return sync_check(h);
@@ -637,6 +655,7 @@ int lssph_rk4(lssph_handle* h) {
 
 int lssph_pst(lssph_handle* h) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (const int rc_t = ensure_tuned(h)) return rc_t;
     CUDA_TRY(h, cudaMemsetAsync(&h->sc->umax2, 0, sizeof(unsigned long long), h->stream));
     k_umax<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->sc);
     enq_pst(h);
@@ -666,6 +685,7 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
     int rc = check_scalars(h, &s0);
     if (rc != LSSPH_OK) return rc;
     if (s0.steady || s0.done) return LSSPH_OK;   // the reference leaves the time loop at a steady state
+    if ((rc = ensure_tuned(h)) != LSSPH_OK) return rc;
     const int64_t launches0 = h->launch_counter;
     const int sb_start = h->sb, lb_start = h->lb;
     CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
@@ -915,6 +935,7 @@ int lssph_write_param(lssph_handle* h, const char* results_root, const char* con
 
 int lssph_step_profiled(lssph_handle* h, int32_t nsteps, double* ms_by_kind, int64_t* launches_by_kind) {
     if (!h || !ms_by_kind || !launches_by_kind) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    if (const int rc_t = ensure_tuned(h)) return rc_t;
     for (int k = 0; k < LSSPH_KIND_COUNT; ++k) { ms_by_kind[k] = 0.0; launches_by_kind[k] = 0; }
     int rc = check_scalars(h, nullptr);
     if (rc != LSSPH_OK) return rc;
@@ -933,9 +954,11 @@ int lssph_step_profiled(lssph_handle* h, int32_t nsteps, double* ms_by_kind, int
     return check_scalars(h, nullptr);
 }
 
-int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
+int lssph_get_tuning(const lssph_handle* hc, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
                      double* rhs_us_tight) {
-    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (!hc) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    lssph_handle* h = const_cast<lssph_handle*>(hc);   // the measurement is a cache
+    if (const int rc = ensure_tuned(h)) return rc;
     if (lanes) *lanes = h->G;
     if (tight) *tight = h->tight ? 1 : 0;
     if (rhs_us_loose) *rhs_us_loose = h->tune_us[0];

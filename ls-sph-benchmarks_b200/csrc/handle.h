@@ -19,6 +19,7 @@ struct lssph_handle {
     int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
     int G = 4, Gg = 4;
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
+    bool tuned = false;                 // register budget measured (first solo launch)
     bool tight = false;                 // register budget of stage/PST kernels (autotuned)
     double tune_us[2] = {0.0, 0.0};     // RHS pass time with the loose / tight budget
     lssph::CellGrid grid;
@@ -27,8 +28,8 @@ struct lssph_handle {
     lssph::Phys P{};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<void*> allocs;
-    int64_t alloc_bytes = 0;            // device bytes requested by this handle
+    void* block = nullptr;              // the one device allocation all arrays live in
+    int64_t alloc_bytes = 0;            // its size
     lssph::Fld F[2]{};
     lssph::Lst L[2]{};
     lssph::Work W{};

@@ -82,6 +82,22 @@ class Batch:
             self._chk(rc)
         return status, steady, steps
 
+    def launch(self, nsteps: int = 1) -> None:
+        """Start a step call; the host is free until wait().  No add/remove meanwhile."""
+        self._chk(self._lib.lssph_batch_launch(self._b, int(nsteps)))
+
+    def wait(self, raise_on_error: bool = True) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Finish the call started by launch(); returns what step() returns."""
+        n = len(self.members)
+        status = np.zeros(n, dtype=np.int32)
+        steady = np.zeros(n, dtype=np.int32)
+        steps = np.zeros(n, dtype=np.int32)
+        rc = self._lib.lssph_batch_wait(self._b, iptr(status) if n else None, iptr(steady) if n else None,
+                                        iptr(steps) if n else None)
+        if rc == _abi.E_CUDA or (raise_on_error and rc != _abi.OK):
+            self._chk(rc)
+        return status, steady, steps
+
     def last_step_stats(self) -> tuple[float, int]:
         ms = C.c_double()
         n = C.c_int64()

@@ -21,6 +21,7 @@ import math
 import time
 from collections import deque
 from dataclasses import dataclass, field
+from typing import Callable
 
 import numpy as np
 
@@ -45,7 +46,7 @@ class Request:
     nsteps: int
     arrival: float = 0.0                 # seconds on the server clock
     tag: str = ""
-    state: State | None = None           # initial state (default: the fresh-start setup)
+    init: Callable[[], State] | None = None   # builds the initial state (default: fresh start)
     # filled in by the server
     footprint: int = 0
     admitted: float | None = None
@@ -71,6 +72,9 @@ class ServerStats:
     device_ms: float
     max_active: int
     batch_calls: int
+    host_create_s: float = 0.0
+    wait_s: float = 0.0
+    host_retire_s: float = 0.0
     latencies_s: list = field(default_factory=list)
 
 
@@ -95,6 +99,9 @@ class Server:
         self.peak_used = 0
         self.t0 = clock()
         self.device_ms = 0.0
+        self.host_create_s = 0.0     # setting up admitted solves (overlaps batch calls)
+        self.wait_s = 0.0            # waiting for batch calls after the set-up work
+        self.host_retire_s = 0.0     # downloading results, freeing solves
         self.batch_calls = 0
         self.peak_active = 0
         self.particle_steps = 0
@@ -110,64 +117,80 @@ class Server:
             raise ValueError(f"request {req.rid} needs {req.footprint} bytes, over the HBM budget")
         self.waiting.append(req)
 
-    def _admit(self) -> int:
+    def _pick(self) -> list[Request]:
+        """Waiting requests that have arrived and fit (first fit, arrival order); their
+        footprint and slot are reserved here."""
         now = self.now()
-        admitted = 0
+        picked: list[Request] = []
         keep: deque[Request] = deque()
+        slots = self.max_active - len(self.active)
         while self.waiting:
             req = self.waiting.popleft()
-            if (req.arrival <= now and len(self.active) < self.max_active
-                    and self.used + req.footprint <= self.hbm_budget):
-                if req.state is None:
-                    sim = Simulation.new(req.params)
-                else:
-                    sim = Simulation(req.params, req.state, setup_counts(req.params)[1])
-                    sim.ghost()
-                sim.set_step_budget(req.nsteps)
-                self.batch.add(sim)
-                self.active.append((req, sim))
+            if req.arrival <= now and len(picked) < slots and self.used + req.footprint <= self.hbm_budget:
                 self.used += req.footprint
                 self.peak_used = max(self.peak_used, self.used)
                 req.admitted = self.now()
-                admitted += 1
+                picked.append(req)
             else:
                 keep.append(req)
         self.waiting = keep
-        self.peak_active = max(self.peak_active, len(self.active))
-        return admitted
+        return picked
+
+    def _create(self, req: Request) -> Simulation:
+        if req.init is None:
+            sim = Simulation.new(req.params)
+        else:
+            sim = Simulation(req.params, req.init(), setup_counts(req.params)[1])
+            sim.ghost()
+        sim.set_step_budget(req.nsteps)
+        return sim
 
     # ---- one batch call ---------------------------------------------------------------
     def step_once(self) -> int:
-        """Admit, advance every member by up to chunk_steps, retire finished members.
-        Returns the number of members retired."""
-        self._admit()
-        if not self.active:
-            return 0
-        status, steady, steps = self.batch.step(self.chunk_steps, raise_on_error=False)
-        ms, _ = self.batch.last_step_stats()
-        self.device_ms += ms
-        self.batch_calls += 1
+        """One batch call of up to chunk_steps steps.  Requests admitted now are set up on
+        the host and copied to the device while the GPU steps the current members; they
+        join the batch for the next call.  Returns the number of members retired."""
+        picked = self._pick()
+        launched = bool(self.active)
+        t0 = self.clock()
+        if launched:
+            self.batch.launch(self.chunk_steps)
+        created = [(req, self._create(req)) for req in picked]     # overlaps the batch call
+        t1 = self.clock()
+        self.host_create_s += t1 - t0
         retired = []
-        for i, (req, sim) in enumerate(self.active):
-            req.steps_done += int(steps[i])
-            self.particle_steps += int(steps[i]) * sim.num_int
-            if status[i] != _abi.OK:
-                req.status, req.stopped = int(status[i]), "error"
-            elif steady[i] > 0:
-                req.stopped = "steady"
-            elif req.steps_done >= req.nsteps:
-                req.stopped = "budget"
-            if req.stopped:
-                retired.append(i)
-        for i in reversed(retired):
-            req, sim = self.active.pop(i)
-            if self.keep_results and req.status == _abi.OK:
-                req.result = sim.download()
-            self.batch.remove(sim)
-            sim.close()
-            self.used -= req.footprint
-            req.finished = self.now()
-            self.done.append(req)
+        if launched:
+            status, steady, steps = self.batch.wait(raise_on_error=False)
+            t2 = self.clock()
+            self.wait_s += t2 - t1
+            ms, _ = self.batch.last_step_stats()
+            self.device_ms += ms
+            self.batch_calls += 1
+            for i, (req, sim) in enumerate(self.active):
+                req.steps_done += int(steps[i])
+                self.particle_steps += int(steps[i]) * sim.num_int
+                if status[i] != _abi.OK:
+                    req.status, req.stopped = int(status[i]), "error"
+                elif steady[i] > 0:
+                    req.stopped = "steady"
+                elif req.steps_done >= req.nsteps:
+                    req.stopped = "budget"
+                if req.stopped:
+                    retired.append(i)
+            for i in reversed(retired):
+                req, sim = self.active.pop(i)
+                if self.keep_results and req.status == _abi.OK:
+                    req.result = sim.download()
+                self.batch.remove(sim)
+                sim.close()
+                self.used -= req.footprint
+                req.finished = self.now()
+                self.done.append(req)
+            self.host_retire_s += self.clock() - t2
+        for req, sim in created:
+            self.batch.add(sim)
+            self.active.append((req, sim))
+        self.peak_active = max(self.peak_active, len(self.active))
         return len(retired)
 
     def run(self, requests: list[Request], realtime: bool = True) -> ServerStats:
@@ -183,7 +206,7 @@ class Server:
                 if not realtime:
                     r.arrival = 0.0
                 self.submit(r)
-            if not self.active and not self.waiting and pending:
+            if not self.active and pending and not any(r.arrival <= self.now() for r in self.waiting):
                 time.sleep(max(0.0, min(pending[0].arrival - self.now(), 0.05)))
                 continue
             self.step_once()
@@ -198,6 +221,7 @@ class Server:
                            p50_s=q(0.5), p99_s=q(0.99),
                            particle_updates_per_s=self.particle_steps / span if span > 0 else math.nan,
                            device_ms=self.device_ms, max_active=self.peak_active, batch_calls=self.batch_calls,
+                           host_create_s=self.host_create_s, wait_s=self.wait_s, host_retire_s=self.host_retire_s,
                            latencies_s=lat)
 
     def close(self) -> None:
