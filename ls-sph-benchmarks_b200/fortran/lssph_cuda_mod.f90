@@ -126,6 +126,53 @@ module lssph_cuda_mod
             real(c_double), intent(out) :: x(*), y(*), u(*), v(*), rho(*), pre(*), tem(*)
         end function
 
+        ! ---- batched time loop, step budgets, device memory (no reference counterpart) ----
+        integer(c_int) function lssph_batch_create(b) bind(c, name="lssph_batch_create")
+            import :: c_int, c_ptr
+            type(c_ptr), intent(out) :: b
+        end function
+
+        subroutine lssph_batch_destroy(b) bind(c, name="lssph_batch_destroy")
+            import :: c_ptr
+            type(c_ptr), value :: b
+        end subroutine
+
+        integer(c_int) function lssph_batch_add(b, h) bind(c, name="lssph_batch_add")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: b, h
+        end function
+
+        integer(c_int) function lssph_batch_remove(b, h) bind(c, name="lssph_batch_remove")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: b, h
+        end function
+
+        integer(c_int) function lssph_batch_step(b, nsteps, status, steady, steps_taken) &
+                bind(c, name="lssph_batch_step")
+            import :: c_int, c_int32_t, c_ptr
+            type(c_ptr), value :: b
+            integer(c_int32_t), value :: nsteps
+            integer(c_int32_t), intent(out) :: status(*), steady(*), steps_taken(*)
+        end function
+
+        integer(c_int) function lssph_set_step_budget(h, nsteps) bind(c, name="lssph_set_step_budget")
+            import :: c_int, c_int32_t, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: nsteps
+        end function
+
+        integer(c_int) function lssph_get_progress(h, steps_done, stopped) bind(c, name="lssph_get_progress")
+            import :: c_int, c_int32_t, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int32_t), intent(out) :: steps_done, stopped
+        end function
+
+        integer(c_int) function lssph_estimate_device_bytes(p, bytes) bind(c, name="lssph_estimate_device_bytes")
+            import :: c_int, c_int64_t, lssph_params
+            type(lssph_params), intent(in) :: p
+            integer(c_int64_t), intent(out) :: bytes
+        end function
+
         type(c_ptr) function lssph_last_error_c() bind(c, name="lssph_last_error")
             import :: c_ptr
         end function
