@@ -33,6 +33,7 @@ namespace {
 struct BatchGroup {
     int nb = 4, nbg = 3, wq = 3, rk = 4, G = 4;
     bool p1 = false, pst_on = true, mixed = false;
+    bool pdl = true;               // programmatic dependent launches between the group's kernels
     int flip = 1;                  // both parities flip once per step (problems 2-4)
     std::vector<int> members;      // indices into lssph_batch::members
     SolveDesc* D = nullptr;        // device, one descriptor per member
@@ -119,7 +120,8 @@ void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool p
         constexpr bool MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
-            (g.tight ? tight : loose)<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, S, ps, pl);
+            launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles}, S,
+                          ps, pl);
             ++*count;
         };
         if (g.nb == 1) run(kb_stage<1, G, false, MX>, kb_stage<1, G, true, MX>);
@@ -133,7 +135,8 @@ void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset
         constexpr int G = decltype(GG)::value;
         auto run = [&](auto kern) {
             if (prep) { optin(kern); return; }
-            kern<<<g.nchunks, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.chunks}, ps, pl, zero_other, reset_umax);
+            launch_kernel(g.pdl, kern, g.nchunks, PPB * G, g.smem, g.stream, g.D, BatchMap{g.chunks}, ps, pl, zero_other,
+                          reset_umax);
             ++*count;
         };
         auto by_wq = [&](auto NBc) {
@@ -154,7 +157,8 @@ void launch_pst(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
         constexpr bool MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
-            (g.tight ? tight : loose)<<<g.ntiles, PPB * G, g.smem, g.stream>>>(g.D, BatchMap{g.tiles}, ps, pl);
+            launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles}, ps,
+                          pl);
             ++*count;
         };
         if (g.nb == 5) run(kb_pst<4, G, false, MX>, kb_pst<4, G, true, MX>);
@@ -191,7 +195,8 @@ void enq_group_step(const BatchGroup& g, int ps, int pl, bool prep, int* count) 
         launch_ghost(g, ps, pl, 1, 1, prep, count);
     }
     if (g.p1 && !prep) {
-        kb_epilogue<<<(int)((g.members.size() + 127) / 128), 128, 0, g.stream>>>(g.D, (int)g.members.size());
+        launch_kernel(g.pdl, kb_epilogue, (unsigned)((g.members.size() + 127) / 128), 128, 0, g.stream, g.D,
+                      (int)g.members.size());
         ++*count;
     }
 }
@@ -271,6 +276,7 @@ int rebuild(lssph_batch* b) {
             g.rk = h->p.rk;
             g.G = h->G;
             g.mixed = h->mixed;
+            g.pdl = pdl_enabled();
             g.p1 = h->p1;
             g.pst_on = h->pst_on;
             g.flip = h->p1 ? 0 : 1;

@@ -151,9 +151,8 @@ void run_stage(lssph_handle* h, const StageCfg& S) {
         return;
     }
     auto kern = h->tight ? k_stage<NB, GG, true, MX> : k_stage<NB, GG, false, MX>;
-    kern<<<h->ntiles, PPB * GG, h->smem_bytes, h->stream>>>(h->P, h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb],
-                                                              h->L[h->lb ^ 1], h->gstart, h->glist, h->W, S, h->sc,
-                                                              h->ntx);
+    launch_kernel(h->pdl, kern, h->ntiles, PPB * GG, h->smem_bytes, h->stream, h->P, h->F[h->sb], h->F[h->sb ^ 1],
+                  h->L[h->lb], h->L[h->lb ^ 1], h->gstart, h->glist, h->W, S, h->sc, h->ntx);
     h->launch_counter++;
 }
 
@@ -187,7 +186,7 @@ void launch_ghost_t(lssph_handle* h, int zero_list, int reset_umax) {
     const size_t sm = h->smem_bytes;
 #define LSSPH_GHOST(GG)                                                                                    \
     if (h->preparing) { smem_optin(k_ghost<NB, GG, WQ>); return; }                                        \
-    k_ghost<NB, GG, WQ><<<h->nvt, PPB * GG, sm, h->stream>>>(h->P, F, L, h->gstart, h->glist, h->V, VT, h->ntx, zc, \
+    launch_kernel(h->pdl, k_ghost<NB, GG, WQ>, h->nvt, PPB * GG, sm, h->stream, h->P, F, L, h->gstart, h->glist, h->V, VT, h->ntx, zc, \
                                                           reset_umax, h->sc)
     switch (G) {
         case 1: LSSPH_GHOST(1); break;
@@ -220,9 +219,8 @@ void run_pst(lssph_handle* h) {
         return;
     }
     auto kern = h->tight ? k_pst<NB, GG, true, MX> : k_pst<NB, GG, false, MX>;
-    kern<<<h->ntiles, PPB * GG, h->smem_bytes, h->stream>>>(h->P, h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb],
-                                                              h->L[h->lb ^ 1], h->gstart, h->glist, h->W, h->sc,
-                                                              h->ntx);
+    launch_kernel(h->pdl, kern, h->ntiles, PPB * GG, h->smem_bytes, h->stream, h->P, h->F[h->sb], h->F[h->sb ^ 1],
+                  h->L[h->lb], h->L[h->lb ^ 1], h->gstart, h->glist, h->W, h->sc, h->ntx);
     h->launch_counter++;
 }
 
@@ -294,7 +292,7 @@ void enq_step(lssph_handle* h) {
     if (h->pst_on) enq_pst(h);
     if (h->p1) {
         ProfScope prof(h, LSSPH_KIND_OTHER);
-        k_epilogue<<<1, 1, 0, h->stream>>>(h->P, h->sc);
+        launch_kernel(h->pdl, k_epilogue, 1, 1, 0, h->stream, h->P, h->sc);
         h->launch_counter++;
     }
 }
@@ -335,6 +333,15 @@ int autotune(lssph_handle* h) {
 // The handle's own launches use the measured register budget; batches choose per group
 // and never need it, so the measurement waits for the first solo launch.
 int ensure_tuned(lssph_handle* h) { return h->tuned ? LSSPH_OK : autotune(h); }
+
+}  // namespace
+
+bool lssph::pdl_enabled() {
+    const char* v = std::getenv("LSSPH_PDL");
+    return !(v && std::strcmp(v, "0") == 0);
+}
+
+namespace {
 
 int check_scalars(lssph_handle* h, Scalars* out) {
     Scalars s{};
@@ -426,6 +433,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->nb_ghost = h->p1 ? 1 : (h->has_tem ? 4 : 3);
     h->wq = h->p.wall_model == 1 ? 1 : (h->p.wall_model == 3 ? 6 : 3);
     h->mixed = h->p.precision == LSSPH_PRECISION_MIXED;
+    h->pdl = pdl_enabled();
     h->G = h->p.lanes > 0 ? h->p.lanes : 4;
     h->Gg = h->p.lanes > 0 ? h->p.lanes : 4;
     h->ptype.assign(ptype, ptype + num_total);

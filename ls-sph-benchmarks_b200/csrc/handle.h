@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "engine.h"
@@ -19,6 +20,7 @@ struct lssph_handle {
     int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
     int G = 4, Gg = 4;
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
+    bool pdl = true;                    // programmatic dependent launches in the time step
     bool tuned = false;                 // register budget measured (first solo launch)
     bool tight = false;                 // register budget of stage/PST kernels (autotuned)
     double tune_us[2] = {0.0, 0.0};     // RHS pass time with the loose / tight budget
@@ -59,6 +61,28 @@ struct lssph_handle {
 };
 
 namespace lssph {
+// Launch a kernel, optionally as a programmatic dependent launch (the kernel may be
+// scheduled while the previous kernel in the stream drains; it calls pdl_wait() before
+// touching that kernel's results).  Captured into CUDA graphs as programmatic edges.
+template <class... KArgs, class... Args>
+inline cudaError_t launch_kernel(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                 cudaStream_t stream, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
+// LSSPH_PDL=0 turns programmatic dependent launches off (default on).
+bool pdl_enabled();
+
 // Drop a handle that is being destroyed from the batch that holds it (batch.cu).
 void batch_forget(lssph_batch* b, lssph_handle* h);
 }  // namespace lssph

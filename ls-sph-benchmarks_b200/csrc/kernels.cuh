@@ -107,6 +107,13 @@ struct StageCfg {
 enum : int { XM_COPY = 0, XM_K_MINUS = 1, XM_PLUS_K = 2, XM_NEG = 3 };
 
 // ---------------------------------------------------------------------------------------
+// Programmatic dependent launch: a kernel launched with programmatic stream serialisation
+// can be scheduled while its predecessor drains; pdl_wait() holds it until the predecessor
+// has completed and its writes are visible, pdl_release() lets the successor be scheduled.
+// Both are no-ops for an ordinary launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ bool halted(const Scalars* sc) {
     return (*(volatile const int*)&sc->err) != 0 || (*(volatile const int*)&sc->steady) != 0 ||
            (*(volatile const int*)&sc->done) != 0;
@@ -833,6 +840,7 @@ template <int NB, int G, bool MIXED>
 __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                            const int* __restrict__ gstart, const int* __restrict__ glist,
                                            const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
+    pdl_wait();
     const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
     constexpr int SR = sums_stride(15 + 5 * NB + 1);
@@ -842,6 +850,7 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
     const SmemView SM = smem_view<NB == 5>(smem_raw, P.cap);
     const int tx = tile % ntx, ty = tile / ntx;
     stage_halo<false, NB == 5>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    pdl_release();
     if (stop) return;
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
@@ -1001,6 +1010,7 @@ __device__ __forceinline__ void ghost_work(const Phys& P, const Fld& F, const Ls
                                            int* zero_cnt, int reset_umax, Scalars* sc, int chunk, int nchunk) {
     // a stopped solve (steady state, step budget, error) keeps its cell lists as they are,
     // so that it can resume exactly where it stopped
+    pdl_wait();
     const bool stop = halted(sc);
     if (zero_cnt && !stop) {
         for (int c = chunk * blockDim.x + threadIdx.x; c < P.ncell; c += nchunk * blockDim.x) zero_cnt[c] = 0;
@@ -1015,6 +1025,7 @@ __device__ __forceinline__ void ghost_work(const Phys& P, const Fld& F, const Ls
     const int tx = tile % ntx, ty = tile / ntx;
     const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
     stage_halo<true, NB == 4>(P, F, L, gstart, glist, cx0, cy0, T, SM);
+    pdl_release();
     if (stop) return;
     const int v0 = VT.start[chunk], nvm = VT.start[chunk + 1] - v0;
     const int lane = threadIdx.x & (G - 1);
@@ -1188,6 +1199,7 @@ template <int NB, int G, bool MIXED>
 __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                          const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
                                          Scalars* sc, int ntx, int tile) {
+    pdl_wait();
     const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
     constexpr int Q = 5;
     constexpr int SR = sums_stride(15 + 5 * NB + 3);
@@ -1197,6 +1209,7 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
     const SmemView SM = smem_view<NB == 4>(smem_raw, P.cap);
     const int tx = tile % ntx, ty = tile / ntx;
     stage_halo<false, NB == 4>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    pdl_release();
     if (stop) return;
     const int n_own = T.own_off[OC];
     const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
@@ -1466,6 +1479,7 @@ static __global__ void k_copy_fprev(const Phys P, const Fld F, const Work W) {
 // the stage kernel already reduced max|f_previous - u|.
 // End of a time step of problem 1 (one thread): steady check, step count, step budget.
 __device__ __forceinline__ void epilogue_body(double threshold, Scalars* sc) {
+    pdl_wait();
     if (sc->err != 0 || sc->steady != 0 || sc->done != 0) return;
     sc->step_count += 1;
     const double df = __longlong_as_double((long long)sc->dfmax);
