@@ -41,7 +41,7 @@ struct BatchGroup {
     int2* chunks = nullptr;        // (solve, chunk) per CTA of ghost launches
     int ntiles = 0, nchunks = 0;
     bool tight = false;            // register budget of the stage / PST kernels
-    size_t smem = 0;
+    size_t smem = 0, smem_ghost = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t join = nullptr;
 };
@@ -135,7 +135,7 @@ void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset
         constexpr int G = decltype(GG)::value;
         auto run = [&](auto kern) {
             if (prep) { optin(kern); return; }
-            launch_kernel(g.pdl, kern, g.nchunks, PPB * G, g.smem, g.stream, g.D, BatchMap{g.chunks}, ps, pl, zero_other,
+            launch_kernel(g.pdl, kern, g.nchunks, PPB * G, g.smem_ghost, g.stream, g.D, BatchMap{g.chunks}, ps, pl, zero_other,
                           reset_umax);
             ++*count;
         };
@@ -298,6 +298,7 @@ int rebuild(lssph_batch* b) {
             for (int t = 0; t < h->ntiles; ++t) tiles.push_back(make_int2((int)s, t));
             for (int c = 0; c < h->nvt; ++c) chunks.push_back(make_int2((int)s, c));
             g.smem = std::max(g.smem, h->smem_bytes);
+            g.smem_ghost = std::max(g.smem_ghost, h->smem_ghost);
             g.tight = g.tight || h->tight;
         }
         // the tight budget wins once a launch has more tiles than fit at the loose one

@@ -183,7 +183,7 @@ void launch_ghost_t(lssph_handle* h, int zero_list, int reset_umax) {
     const int G = h->Gg;
     const VMTiles VT{h->vt_tile, h->vt_start, h->vt_vm};
     int* zc = zero_list >= 0 ? h->L[zero_list].cnt : nullptr;
-    const size_t sm = h->smem_bytes;
+    const size_t sm = h->smem_ghost;
 #define LSSPH_GHOST(GG)                                                                                    \
     if (h->preparing) { smem_optin(k_ghost<NB, GG, WQ>); return; }                                        \
     launch_kernel(h->pdl, k_ghost<NB, GG, WQ>, h->nvt, PPB * GG, sm, h->stream, h->P, F, L, h->gstart, h->glist, h->V, VT, h->ntx, zc, \
@@ -495,7 +495,9 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->ntx = (h->grid.nx + TX - 1) / TX;
     h->nty = (h->grid.ny + TY - 1) / TY;
     h->ntiles = h->ntx * h->nty;
-    h->smem_bytes = std::max(tile_smem_bytes(h->grid.cap, h->G, h->has_tem), tile_smem_bytes(h->grid.cap, h->Gg, h->has_tem));
+    h->smem_bytes = h->mixed ? tile_smem_bytes_mx(h->grid.cap, h->G, h->has_tem)
+                             : tile_smem_bytes(h->grid.cap, h->G, h->has_tem);
+    h->smem_ghost = tile_smem_bytes(h->grid.cap, h->Gg, h->has_tem);   // ghosts stay FP64
     std::vector<int32_t> vt_tile, vt_start, vt_vm;
     vm_chunks(h->grid, h->ntx, h->ntiles, &vt_tile, &vt_start, &vt_vm);
     h->nvt = (int)vt_tile.size();

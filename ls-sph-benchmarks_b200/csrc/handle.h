@@ -41,7 +41,8 @@ struct lssph_handle {
     int ntx = 0, nty = 0, ntiles = 0;   // cell tiles
     int nvt = 0;                        // tiles holding virtual markers
     int *vt_tile = nullptr, *vt_start = nullptr, *vt_vm = nullptr;
-    size_t smem_bytes = 0;
+    size_t smem_bytes = 0;              // dynamic shared memory of stage / PST CTAs
+    size_t smem_ghost = 0;              // ... of ghost CTAs
     bool preparing = false;             // launch helpers only set kernel attributes
     lssph::Scalars* sc = nullptr;
     int sb = 0, lb = 0;

@@ -466,7 +466,17 @@ struct TileHdr {
     int nf[HC];         // interior prefix of each halo cell
     int off[HC + 1];    // smem offset of each halo cell
     int own_off[OC + 1];
+    int cell[HC];       // global cell of each halo cell (-1 outside the grid)
+    int g0[HC];         // start of its ghost list
 };
+
+// Halo cell holding staged position k (cells in staging order; empty cells skipped).
+__device__ __forceinline__ int halo_cell_of(const TileHdr& T, int k) {
+    int h = 0;
+#pragma unroll
+    for (int q = 1; q < HC; ++q) h += (k >= T.off[q]) ? 1 : 0;
+    return h;
+}
 
 // Dynamic shared memory: SoA fields of up to HC*cap staged particles, their global
 // indices, and the own-particle list.
@@ -519,14 +529,14 @@ __device__ __forceinline__ int warp_incl_scan(int v) {
     return v;
 }
 
-// Stage the halo of the tile whose halo cell (0,0) is global cell (cx0, cy0): counts,
-// reference-order index lists (interior particles ascending, then the ghost list) and
-// the SoA fields of every staged particle.  Own particles are the interior particles of
-// the TX x TY own cells.  All global loads of a phase are independent of each other.
-template <bool FLUID_ONLY, bool WITH_TEM>
-__device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Lst& L, const int* __restrict__ gstart,
-                                           const int* __restrict__ glist, int cx0, int cy0, TileHdr& T,
-                                           const SmemView& S) {
+// Stage the lists of the tile whose halo cell (0,0) is global cell (cx0, cy0): counts,
+// reference-order index lists (interior particles ascending, then the ghost list) and the
+// own-particle list.  Own particles are the interior particles of the TX x TY own cells.
+// All global loads of a phase are independent of each other.  Ends with a barrier.
+template <bool FLUID_ONLY, class View>
+__device__ __forceinline__ void stage_lists(const Phys& P, const Lst& L, const int* __restrict__ gstart,
+                                            const int* __restrict__ glist, int cx0, int cy0, TileHdr& T,
+                                            const View& S) {
     const int tid = threadIdx.x;
     int c = -1, g0 = 0;
     if (tid < HC) {
@@ -541,6 +551,8 @@ __device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Ls
         }
         T.nf[tid] = nf;
         T.cnt[tid] = nf + ng;
+        T.cell[tid] = c;
+        T.g0[tid] = g0;
     }
     __syncthreads();
     if (tid < 32) {
@@ -555,12 +567,17 @@ __device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Ls
         if (tid == 0) T.own_off[0] = 0;
     }
     __syncthreads();
+    // every staged index is one independent load, spread over all threads
+    const int n = T.off[HC];
+    for (int k = tid; k < n; k += blockDim.x) {
+        const int h = halo_cell_of(T, k);
+        const int sl = k - T.off[h], nfh = T.nf[h], ch = T.cell[h];
+        S.idx[k] = sl < nfh ? __ldg(L.slots + (size_t)ch * P.cap + sl) : __ldg(glist + T.g0[h] + (sl - nfh));
+    }
+    __syncthreads();
     if (tid < HC && c >= 0) {
-        const int nf = T.nf[tid], ng = T.cnt[tid] - nf, base = T.off[tid];
-        const int* src = L.slots + (size_t)c * P.cap;
-        for (int k = 0; k < nf; ++k) S.idx[base + k] = __ldg(src + k);                // independent loads
-        for (int g = 0; g < ng; ++g) S.idx[base + nf + g] = __ldg(glist + g0 + g);
-        for (int k = 1; k < nf; ++k) {                                                  // then sort in smem
+        const int nf = T.nf[tid], base = T.off[tid];
+        for (int k = 1; k < nf; ++k) {   // interior particles of the cell in ascending order
             const int v = S.idx[base + k];
             int t = k;
             while (t > 0 && S.idx[base + t - 1] > v) { S.idx[base + t] = S.idx[base + t - 1]; --t; }
@@ -574,8 +591,16 @@ __device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Ls
         }
     }
     __syncthreads();
+}
+
+// Lists, then the SoA FP64 fields of every staged particle.
+template <bool FLUID_ONLY, bool WITH_TEM>
+__device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Lst& L, const int* __restrict__ gstart,
+                                           const int* __restrict__ glist, int cx0, int cy0, TileHdr& T,
+                                           const SmemView& S) {
+    stage_lists<FLUID_ONLY>(P, L, gstart, glist, cx0, cy0, T, S);
     const int n = T.off[HC];
-    for (int k = tid; k < n; k += blockDim.x) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int j = S.idx[k];
         S.x[k] = __ldg(F.x + j);
         S.y[k] = __ldg(F.y + j);
@@ -589,22 +614,162 @@ __device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Ls
     __syncthreads();
 }
 
+// ---- mixed-precision staging -------------------------------------------------------------
+// Positions as FP32 offsets from the FP64 origin of the particle's halo cell (cell width
+// cw = h_eff); fields as FP32 offsets from FP64 reference values (those of the first staged
+// particle); volumes in FP32.  The pair phase rebuilds x_j - x_i = ddx cw + (o_j - o_i) from
+// the cell delta (ddx, ddy) of the candidate's cell, so no FP32 value carries more than
+// the spread of one tile.  Hit lists are 16-bit: staged index (10 bits) and cell delta.
+struct SmemMx {
+    double* sums;                                       // [PPB][row stride], as in SmemView
+    float *ox, *oy, *u, *v, *rho, *pre, *vol, *tem;
+    int *idx, *own_k, *own_hc;
+    unsigned short* nbr;
+};
+
+__host__ __device__ inline size_t tile_smem_bytes_mx(int cap, int G, bool tem) {
+    const size_t maxp = (size_t)HC * cap, maxo = (size_t)OC * cap;
+    const size_t lists = (size_t)PPB * G * nbr_list_len(cap, G);
+    return (size_t)PPB * SUMS_MAX * sizeof(double) + maxp * ((tem ? 8 : 7) * sizeof(float) + sizeof(int)) +
+           2 * maxo * sizeof(int) + lists * sizeof(unsigned short);
+}
+
+template <bool TEM>
+__device__ __forceinline__ SmemMx smem_view_mx(void* raw, int cap) {
+    SmemMx S;
+    const int maxp = HC * cap, maxo = OC * cap;
+    double* d = static_cast<double*>(raw);
+    S.sums = d;
+    float* f = reinterpret_cast<float*>(d + PPB * SUMS_MAX);
+    S.ox = f; S.oy = f + maxp; S.u = f + 2 * maxp; S.v = f + 3 * maxp; S.rho = f + 4 * maxp;
+    S.pre = f + 5 * maxp; S.vol = f + 6 * maxp; S.tem = TEM ? f + 7 * maxp : nullptr;
+    int* q = reinterpret_cast<int*>(f + (TEM ? 8 : 7) * maxp);
+    S.idx = q; S.own_k = q + maxp; S.own_hc = q + maxp + maxo;
+    S.nbr = reinterpret_cast<unsigned short*>(q + maxp + 2 * maxo);
+    return S;
+}
+
+// Field reference values of a staged tile (FP64); offsets are taken against them.
+struct TileRef {
+    double u, v, rho, pre, tem;
+};
+
+template <bool WITH_TEM>
+__device__ __forceinline__ TileRef stage_fields_mx(const Phys& P, const Fld& F, int cx0, int cy0, const TileHdr& T,
+                                                   const SmemMx& S) {
+    TileRef R{0.0, 0.0, 0.0, 0.0, 0.0};
+    const int n = T.off[HC];
+    if (n > 0) {
+        const int j0 = S.idx[0];
+        R.u = __ldg(F.u + j0); R.v = __ldg(F.v + j0); R.rho = __ldg(F.rho + j0); R.pre = __ldg(F.pre + j0);
+        if (WITH_TEM) R.tem = __ldg(F.tem + j0);
+    }
+    const double cw = sqrt(P.h_eff_sq);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int h = halo_cell_of(T, k);
+        const double x0 = (double)(cx0 + h % HX) * cw, y0 = (double)(cy0 + h / HX) * cw;
+        const int j = S.idx[k];
+        S.ox[k] = (float)(__ldg(F.x + j) - x0);
+        S.oy[k] = (float)(__ldg(F.y + j) - y0);
+        S.u[k] = (float)(__ldg(F.u + j) - R.u);
+        S.v[k] = (float)(__ldg(F.v + j) - R.v);
+        S.rho[k] = (float)(__ldg(F.rho + j) - R.rho);
+        S.pre[k] = (float)(__ldg(F.pre + j) - R.pre);
+        S.vol[k] = (float)__ldg(F.vol + j);
+        if (WITH_TEM) S.tem[k] = (float)(__ldg(F.tem + j) - R.tem);
+    }
+    __syncthreads();
+    return R;
+}
+
+// Candidates of an own particle in halo cell hc with the code of their cell delta
+// (ddx + 1) + 3 (ddy + 1); the same visiting order as for_tile_candidates.
+template <int G, class Fn>
+__device__ __forceinline__ void for_tile_candidates_code(const TileHdr& T, int hc, int lane, Fn&& f) {
+    int base = 0;
+#pragma unroll 1
+    for (int dy = -1; dy <= 1; ++dy) {
+        const int h0 = hc - 1 + dy * HX;
+        const int lo = T.off[h0], m1 = T.off[h0 + 1], m2 = T.off[h0 + 2], hi = T.off[h0 + 3];
+        const int row = 3 * (dy + 1);
+        int k = lo + ((G == 1) ? 0 : ((lane - base) & (G - 1)));
+#pragma unroll 4
+        for (; k < hi; k += G) f(k, row + (k >= m1 ? 1 : 0) + (k >= m2 ? 1 : 0));
+        base += hi - lo;
+    }
+}
+
+// Mixed-precision two-phase neighbour loop (see tile_pairs): FP32 cutoff test on the
+// rebuilt offsets, 16-bit hits, f(k, x_j - x_i, y_j - y_i) over the hits.  xs[d + 1] =
+// o_x,i - d cw (and ys for y) are the own particle's offsets seen from the three cell
+// columns (rows).  At the cutoff W and its gradient are zero, so a pair that the FP32
+// test classifies differently from FP64 contributes nothing either way.
+template <int G, class Fn>
+__device__ __forceinline__ int tile_pairs_mx(const TileHdr& T, const SmemMx& S, bool active, int hc, int lane,
+                                             int skip, const float (&xs)[3], const float (&ys)[3], float heff2,
+                                             Fn&& f) {
+    int nl = 0;
+    const int stride = blockDim.x;
+    unsigned short* list = S.nbr + threadIdx.x;
+    if (active) {
+        for_tile_candidates_code<G>(T, hc, lane, [&](int k, int code) {
+            const float xji = S.ox[k] - xs[code % 3];
+            const float yji = S.oy[k] - ys[code / 3];
+            if (k != skip && !(xji * xji + yji * yji > heff2)) {
+                list[nl * stride] = (unsigned short)(k | (code << 10));
+                ++nl;
+            }
+        });
+    }
+    auto body = [&](unsigned e) {
+        const int k = (int)(e & 1023u), code = (int)(e >> 10);
+        f(k, S.ox[k] - xs[code % 3], S.oy[k] - ys[code / 3]);
+    };
+    if constexpr (G == 1) {
+#pragma unroll 2
+        for (int t = 0; t < nl; ++t) body(list[t * stride]);
+        return nl;
+    } else {
+        int incl = nl;
+#pragma unroll
+        for (int off = 1; off < G; off <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, off, G);
+            if (lane >= off) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, G - 1, G);
+        int bases[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) bases[q] = __shfl_sync(0xffffffffu, incl - nl, q, G);
+        const int lane0 = (int)threadIdx.x - lane;
+#pragma unroll 2
+        for (int pidx = lane; pidx < total; pidx += G) {
+            int o = 0, bo = bases[0];
+#pragma unroll
+            for (int q = 1; q < G; ++q) {
+                const bool ge = pidx >= bases[q];
+                o = ge ? q : o;
+                bo = ge ? bases[q] : bo;
+            }
+            body(S.nbr[(pidx - bo) * stride + lane0 + o]);
+        }
+        return total;
+    }
+}
+
 // Visit the staged candidates of an own particle in halo cell hc: 3x3 cells in reference
 // order; lane `lane` of a G-lane group takes every G-th candidate of the concatenation.
+// The three cells of a halo row are staged next to each other, so each row is one
+// contiguous range of staged positions (in the reference's dx order).
 template <int G, class Fn>
 __device__ __forceinline__ void for_tile_candidates(const TileHdr& T, int hc, int lane, Fn&& f) {
     int base = 0;
 #pragma unroll 1
     for (int dy = -1; dy <= 1; ++dy) {
-#pragma unroll 1
-        for (int dx = -1; dx <= 1; ++dx) {
-            const int h = hc + dx + dy * HX;
-            const int n = T.cnt[h], o = T.off[h];
-            int t = (G == 1) ? 0 : ((lane - base) & (G - 1));
+        const int lo = T.off[hc - 1 + dy * HX], hi = T.off[hc + 2 + dy * HX];
+        int k = lo + ((G == 1) ? 0 : ((lane - base) & (G - 1)));
 #pragma unroll 4
-            for (; t < n; t += G) f(o + t);
-            base += n;
-        }
+        for (; k < hi; k += G) f(k);
+        base += hi - lo;
     }
 }
 
@@ -837,7 +1002,7 @@ __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, co
 // One tile of one solve (the CTA's work in both the single-solve and the batched kernel).
 // MIXED: FP32 pair phase (weights, basis, neighbour sums), FP64 solve with refinement.
 template <int NB, int G, bool MIXED>
-__device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
+__device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                            const int* __restrict__ gstart, const int* __restrict__ glist,
                                            const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
     pdl_wait();
@@ -981,6 +1146,150 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
             warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
         __syncthreads();
     }
+}
+
+
+// ---- mixed precision: LS solve of one particle's sums row in place ----------------------
+// FP64 LU of the moment matrix (packed upper triangle at row[0..14]), then per right-hand
+// side the DGESV substitutions plus one refinement step; the solution replaces the b sums
+// (scaled by the basis factors when SCALE).  cnt < Q leaves zeros, as the FP64 path does.
+template <int Q, int NB, bool SCALE>
+__device__ __forceinline__ void solve_row_refined(const Phys& P, double* row, int cnt, Scalars* sc) {
+    if (cnt >= Q) {
+        double A[Q][Q];
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+#pragma unroll
+            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? row[UT(r, c)] : row[UT(c, r)];
+        double rpiv[Q];
+        int pv[Q];
+        if (!lu_factor_p<Q>(A, rpiv, pv)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll 1
+        for (int c = 0; c < NB; ++c) {
+            double b[Q];
+#pragma unroll
+            for (int k = 0; k < Q; ++k) b[k] = row[15 + 5 * c + k];
+            lu_solve_refined<Q>(A, rpiv, pv, row, b);
+#pragma unroll
+            for (int k = 0; k < Q; ++k) row[15 + 5 * c + k] = SCALE ? b[k] * (k < 2 ? P.ih1 : P.ih2A) : b[k];
+        }
+    } else {
+#pragma unroll
+        for (int k = 15; k < 15 + 5 * NB; ++k) row[k] = 0.0;
+    }
+}
+
+// Mixed-precision stage: FP32 staging and pair phase (offsets from FP64 cell origins and
+// field references), lanes combined in FP64, FP64 solve with refinement, FP64 update.
+template <int NB, int G>
+__device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
+                                              const Lst& Ln, const int* __restrict__ gstart,
+                                              const int* __restrict__ glist, const Work& W, const StageCfg& S,
+                                              Scalars* sc, int ntx, int tile) {
+    pdl_wait();
+    const bool stop = halted(sc);
+    constexpr int Q = 5;
+    constexpr int SR = sums_stride(15 + 5 * NB + 1);
+    static_assert(SR <= SUMS_MAX, "reduced sums overflow");
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemMx SM = smem_view_mx<NB == 5>(smem_raw, P.cap);
+    const int tx = tile % ntx, ty = tile / ntx;
+    const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
+    stage_lists<false>(P, Lc, gstart, glist, cx0, cy0, T, SM);
+    stage_fields_mx<NB == 5>(P, cur, cx0, cy0, T, SM);
+    pdl_release();
+    if (stop) return;
+    const int n_own = T.own_off[OC];
+    const int lane = threadIdx.x & (G - 1);
+    const float cw = (float)sqrt(P.h_eff_sq);
+    const float heff2 = (float)P.h_eff_sq;
+    const PairConst<float> C(P);
+    for (int ob = 0; ob < n_own; ob += PPB) {
+        {
+            const int slot = (int)threadIdx.x / G;
+            const int o = ob + slot;
+            const bool active = o < n_own;
+            int ki = 0, hc = 0;
+            if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+            const float oxi = SM.ox[ki], oyi = SM.oy[ki];
+            const float xs[3] = {oxi + cw, oxi, oxi - cw};
+            const float ys[3] = {oyi + cw, oyi, oyi - cw};
+            const float my_u = SM.u[ki];
+            float my_v = 0.f, my_rho = 0.f, my_pre = 0.f, my_tem = 0.f;
+            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
+            if constexpr (NB == 5) my_tem = SM.tem[ki];
+            float Mu[15];
+            float B[NB][Q];
+#pragma unroll
+            for (int k = 0; k < 15; ++k) Mu[k] = 0.f;
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+#pragma unroll
+                for (int k = 0; k < Q; ++k) B[c][k] = 0.f;
+            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, xs, ys, heff2,
+                                             [&](int k, float xji, float yji) {
+                const float r = sqrtf(xji * xji + yji * yji);
+                const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
+                const float VW = SM.vol[k] * Wv;
+                float a[Q];
+                basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
+                float df[NB];
+                df[0] = SM.u[k] - my_u;
+                if constexpr (NB >= 4) {
+                    df[1] = SM.v[k] - my_v;
+                    df[2] = SM.rho[k] - my_rho;
+                    df[3] = SM.pre[k] - my_pre;
+                }
+                if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
+                accumulate_A<NB, float>(Mu, B, VW, a, df);
+            });
+            double Md[15], Bd[NB][Q];
+            group_reduce_to<G>(Mu, Md);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+            if (active && lane == 0) {
+                double* sm = SM.sums + slot * SR;
+#pragma unroll
+                for (int k = 0; k < 15; ++k) sm[k] = Md[k];
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = Bd[c][k];
+                sm[SR - 1] = (double)cnt;
+            }
+        }
+        __syncthreads();
+        double red = 0.0;
+        const int o = ob + (int)threadIdx.x;
+        if ((int)threadIdx.x < PPB && o < n_own) {
+            double* sm = SM.sums + threadIdx.x * SR;
+            const int i = SM.idx[SM.own_k[o]];
+            // the particle's own FP64 state (loads issued before the solve they do not need)
+            const double my_x = cur.x[i], my_y = cur.y[i], my_u = cur.u[i];
+            double my_v = 0, my_rho = 0, my_tem = 0;
+            if constexpr (NB >= 4) { my_v = cur.v[i]; my_rho = cur.rho[i]; }
+            if constexpr (NB == 5) my_tem = cur.tem[i];
+            solve_row_refined<Q, NB, true>(P, sm, (int)sm[SR - 1], sc);
+            double d[NB][Q];
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+#pragma unroll
+                for (int k = 0; k < Q; ++k) d[c][k] = sm[15 + 5 * c + k];
+            red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem, d);
+        }
+        if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
+            warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
+        __syncthreads();
+    }
+}
+
+template <int NB, int G, bool MIXED>
+__device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
+                                           const int* __restrict__ gstart, const int* __restrict__ glist,
+                                           const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
+    if constexpr (MIXED) stage_body_mx<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
+    else stage_body_fp64<NB, G, false>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
 }
 
 template <int NB, int G, bool TIGHT = false, bool MIXED = false>
@@ -1196,7 +1505,7 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
 // NB = 3 (u,v,rho) or 4 (+T).  umax2 holds max(u^2+v^2) of the state being shifted.
 // =======================================================================================
 template <int NB, int G, bool MIXED>
-__device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
+__device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                          const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
                                          Scalars* sc, int ntx, int tile) {
     pdl_wait();
@@ -1367,6 +1676,148 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
         }
         __syncthreads();
     }
+}
+
+
+// Mixed-precision PST: FP32 staging and pair phase, FP64 solve with refinement and update.
+template <int NB, int G>
+__device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
+                                            const Lst& Ln, const int* __restrict__ gstart,
+                                            const int* __restrict__ glist, const Work& W, Scalars* sc, int ntx,
+                                            int tile) {
+    pdl_wait();
+    const bool stop = halted(sc);
+    constexpr int Q = 5;
+    constexpr int SR = sums_stride(15 + 5 * NB + 3);
+    static_assert(SR <= SUMS_MAX, "reduced sums overflow");
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemMx SM = smem_view_mx<NB == 4>(smem_raw, P.cap);
+    const int tx = tile % ntx, ty = tile / ntx;
+    const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
+    stage_lists<false>(P, Lc, gstart, glist, cx0, cy0, T, SM);
+    stage_fields_mx<NB == 4>(P, cur, cx0, cy0, T, SM);
+    pdl_release();
+    if (stop) return;
+    const int n_own = T.own_off[OC];
+    const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
+    const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
+    const int lane = threadIdx.x & (G - 1);
+    const float cw = (float)sqrt(P.h_eff_sq);
+    const float heff2 = (float)P.h_eff_sq;
+    const PairConst<float> C(P);
+    for (int ob = 0; ob < n_own; ob += PPB) {
+        {
+            const int slot = (int)threadIdx.x / G;
+            const int o = ob + slot;
+            const bool active = o < n_own;
+            int ki = 0, hc = 0;
+            if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+            const float oxi = SM.ox[ki], oyi = SM.oy[ki];
+            const float xs[3] = {oxi + cw, oxi, oxi - cw};
+            const float ys[3] = {oyi + cw, oyi, oyi - cw};
+            const float my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
+            float my_tem = 0.f;
+            if constexpr (NB == 4) my_tem = SM.tem[ki];
+            float Mu[15];
+            float B[NB][Q];
+#pragma unroll
+            for (int k = 0; k < 15; ++k) Mu[k] = 0.f;
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+#pragma unroll
+                for (int k = 0; k < Q; ++k) B[c][k] = 0.f;
+            float sxy[2] = {0.f, 0.f};
+            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, xs, ys, heff2,
+                                             [&](int k, float xji, float yji) {
+                const float r = sqrtf(xji * xji + yji * yji);
+                const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
+                const float dWdr = dev_dW<float>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
+                const float Vj = SM.vol[k];
+                const float VW = Vj * Wv;
+                const float rinv = 1.f / r;
+                const float gx = ((dWdr * (-xji)) * rinv) * Vj;
+                const float gy = ((dWdr * (-yji)) * rinv) * Vj;
+                const float t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
+                const float fac = 1.f + 0.2f * t4;
+                sxy[0] = fmaf(fac, gx, sxy[0]);
+                sxy[1] = fmaf(fac, gy, sxy[1]);
+                float a[Q];
+                basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
+                float df[NB];
+                df[0] = SM.u[k] - my_u;
+                df[1] = SM.v[k] - my_v;
+                df[2] = SM.rho[k] - my_rho;
+                if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
+                accumulate_A<NB, float>(Mu, B, VW, a, df);
+            });
+            double Md[15], Bd[NB][Q], sd[2];
+            group_reduce_to<G>(Mu, Md);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+            group_reduce_to<G>(sxy, sd);
+            if (active && lane == 0) {
+                double* sm = SM.sums + slot * SR;
+#pragma unroll
+                for (int k = 0; k < 15; ++k) sm[k] = Md[k];
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = Bd[c][k];
+                sm[SR - 3] = sd[0];
+                sm[SR - 2] = sd[1];
+                sm[SR - 1] = (double)cnt;
+            }
+        }
+        __syncthreads();
+        const int o = ob + (int)threadIdx.x;
+        if ((int)threadIdx.x < PPB && o < n_own) {
+            double* sm = SM.sums + threadIdx.x * SR;
+            const int i = SM.idx[SM.own_k[o]];
+            const double my_x = cur.x[i], my_y = cur.y[i], my_u = cur.u[i], my_v = cur.v[i], my_rho = cur.rho[i];
+            double my_tem = 0.0;
+            if constexpr (NB == 4) my_tem = cur.tem[i];
+            // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
+            double dx = -coe * sm[SR - 3], dy = -coe * sm[SR - 2];
+            const double rr = sqrt(dx * dx + dy * dy);
+            if (rr > 0.2 * P.h) {
+                dx = ((0.2 * P.h) * dx) / rr;
+                dy = ((0.2 * P.h) * dy) / rr;
+            }
+            solve_row_refined<Q, NB, false>(P, sm, (int)sm[SR - 1], sc);
+            // interpolation a(dr) . d (shift_interpolate_mod.f90:255-298)
+            double a[Q];
+            basis_A(P, dx, dy, a);
+            double acc[NB];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                double sacc = 0.0;
+#pragma unroll
+                for (int k = 0; k < Q; ++k) sacc = fma(a[k], sm[15 + 5 * c + k], sacc);
+                acc[c] = sacc;
+            }
+            const double xn = my_x + dx, yn = my_y + dy;
+            const double un = my_u + acc[0], vn = my_v + acc[1], rn = my_rho + acc[2];
+            nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
+            nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
+            nxt.vol[i] = P.SP_mass / rn;
+            bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
+            if constexpr (NB == 4) { const double tn = my_tem + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
+            if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
+            const int nk = cell_key_mul(P, xn, yn, sc);
+            if (nk >= 0) W.key[i] = nk;
+            scatter_to_cell(P, Ln, gstart, nk, i, sc);
+        }
+        __syncthreads();
+    }
+}
+
+template <int NB, int G, bool MIXED>
+__device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
+                                         const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
+                                         Scalars* sc, int ntx, int tile) {
+    if constexpr (MIXED) pst_body_mx<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
+    else pst_body_fp64<NB, G, false>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
 }
 
 template <int NB, int G, bool TIGHT = false, bool MIXED = false>
