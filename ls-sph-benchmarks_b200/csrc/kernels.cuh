@@ -567,27 +567,33 @@ __device__ __forceinline__ void stage_lists(const Phys& P, const Lst& L, const i
         if (tid == 0) T.own_off[0] = 0;
     }
     __syncthreads();
-    // every staged index is one independent load, spread over all threads
+    // every staged index is one independent load, spread over all threads; interior
+    // indices go to a scratch list (the hit-list area, idle while staging) to be ranked
     const int n = T.off[HC];
+    int* tmp = reinterpret_cast<int*>(S.nbr);
     for (int k = tid; k < n; k += blockDim.x) {
         const int h = halo_cell_of(T, k);
         const int sl = k - T.off[h], nfh = T.nf[h], ch = T.cell[h];
-        S.idx[k] = sl < nfh ? __ldg(L.slots + (size_t)ch * P.cap + sl) : __ldg(glist + T.g0[h] + (sl - nfh));
+        if (sl < nfh) tmp[k] = __ldg(L.slots + (size_t)ch * P.cap + sl);
+        else S.idx[k] = __ldg(glist + T.g0[h] + (sl - nfh));
     }
     __syncthreads();
-    if (tid < HC && c >= 0) {
-        const int nf = T.nf[tid], base = T.off[tid];
-        for (int k = 1; k < nf; ++k) {   // interior particles of the cell in ascending order
-            const int v = S.idx[base + k];
-            int t = k;
-            while (t > 0 && S.idx[base + t - 1] > v) { S.idx[base + t] = S.idx[base + t - 1]; --t; }
-            S.idx[base + t] = v;
-        }
-        const int hx = tid % HX, hy = tid / HX;
-        if (hx >= 1 && hx <= TX && hy >= 1 && hy <= TY) {
-            const int o = (hx - 1) + (hy - 1) * TX;
-            const int ob = T.own_off[o];
-            for (int k = 0; k < nf; ++k) { S.own_k[ob + k] = base + k; S.own_hc[ob + k] = tid; }
+    // each cell's interior indices in ascending order (the reference's list order): every
+    // index counts the smaller ones of its cell and goes to that rank
+    for (int k = tid; k < n; k += blockDim.x) {
+        const int h = halo_cell_of(T, k);
+        const int base = T.off[h], sl = k - base, nfh = T.nf[h];
+        if (sl < nfh) {
+            const int v = tmp[k];
+            int r = 0;
+            for (int q = 0; q < nfh; ++q) r += (tmp[base + q] < v) ? 1 : 0;
+            S.idx[base + r] = v;
+            const int hx = h % HX, hy = h / HX;
+            if (hx >= 1 && hx <= TX && hy >= 1 && hy <= TY) {
+                const int ob = T.own_off[(hx - 1) + (hy - 1) * TX];
+                S.own_k[ob + sl] = k;
+                S.own_hc[ob + sl] = h;
+            }
         }
     }
     __syncthreads();
@@ -699,6 +705,9 @@ __device__ __forceinline__ void for_tile_candidates_code(const TileHdr& T, int h
     }
 }
 
+// v[i] for i in 0..2 by selects (a dynamic index would put v in local memory).
+__device__ __forceinline__ float pick3(const float (&v)[3], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+
 // Mixed-precision two-phase neighbour loop (see tile_pairs): FP32 cutoff test on the
 // rebuilt offsets, 16-bit hits, f(k, x_j - x_i, y_j - y_i) over the hits.  xs[d + 1] =
 // o_x,i - d cw (and ys for y) are the own particle's offsets seen from the three cell
@@ -713,8 +722,8 @@ __device__ __forceinline__ int tile_pairs_mx(const TileHdr& T, const SmemMx& S, 
     unsigned short* list = S.nbr + threadIdx.x;
     if (active) {
         for_tile_candidates_code<G>(T, hc, lane, [&](int k, int code) {
-            const float xji = S.ox[k] - xs[code % 3];
-            const float yji = S.oy[k] - ys[code / 3];
+            const float xji = S.ox[k] - pick3(xs, code % 3);
+            const float yji = S.oy[k] - pick3(ys, code / 3);
             if (k != skip && !(xji * xji + yji * yji > heff2)) {
                 list[nl * stride] = (unsigned short)(k | (code << 10));
                 ++nl;
@@ -723,7 +732,7 @@ __device__ __forceinline__ int tile_pairs_mx(const TileHdr& T, const SmemMx& S, 
     }
     auto body = [&](unsigned e) {
         const int k = (int)(e & 1023u), code = (int)(e >> 10);
-        f(k, S.ox[k] - xs[code % 3], S.oy[k] - ys[code / 3]);
+        f(k, S.ox[k] - pick3(xs, code % 3), S.oy[k] - pick3(ys, code / 3));
     };
     if constexpr (G == 1) {
 #pragma unroll 2
