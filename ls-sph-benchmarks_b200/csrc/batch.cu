@@ -7,12 +7,13 @@
 // their own streams, forked from and joined back into the batch stream inside the
 // captured step, so small solves of one kind overlap large solves of another.
 //
-// Parities.  A solo step flips the state/list parities of problems 2-4 once per stage
-// plus once for PST (an odd count for RK2 and RK4) and leaves problem 1's unchanged
-// (an even number of state flips, no list flips).  So after k batch steps every member
-// of a group sits at (descriptor parity) xor (flip_g & k & 1), and two graphs (k even,
-// k odd) cover every step.  Descriptors are rewritten whenever the membership changes
-// or a member was advanced on its own between batch calls.
+// Parities.  A solo step of problems 2-4 flips the state buffers and advances the cell
+// list rotation once per stage and once for PST (RK4: 5 times, RK2: 3); problem 1 flips
+// its state buffers once per stage and never scatters.  So after k batch steps a member of
+// a group sits at state parity (descriptor's) xor (sbf_g & k) and list index
+// (descriptor's) + lba_g k (mod 3), and six graphs (k mod 6) cover every step.
+// Descriptors are rewritten whenever the membership changes or a member was advanced on
+// its own between batch calls.
 
 #include <cuda_runtime.h>
 
@@ -30,11 +31,14 @@ using namespace lssph;
 
 namespace {
 
+constexpr int kPeriod = 2 * kLists;   // step period of (state parity, list index)
+
 struct BatchGroup {
     int nb = 4, nbg = 3, wq = 3, rk = 4, G = 4;
     bool p1 = false, pst_on = true, mixed = false;
     bool pdl = true;               // programmatic dependent launches between the group's kernels
-    int flip = 1;                  // both parities flip once per step (problems 2-4)
+    int sbf = 1;                   // state-buffer flip per step (0/1)
+    int lba = 2;                   // list advance per step (mod kLists)
     std::vector<int> members;      // indices into lssph_batch::members
     SolveDesc* D = nullptr;        // device, one descriptor per member
     int2* tiles = nullptr;         // (solve, tile) per CTA of stage / PST launches
@@ -51,13 +55,13 @@ struct BatchGroup {
 struct lssph_batch {
     std::vector<lssph_handle*> members;
     std::vector<int> base_sb, base_lb;   // member parities the descriptors were written with
-    std::vector<int> flip;               // per member: its group's per-step flip
+    std::vector<int> sbf, lba;           // per member: its group's per-step flip and list advance
     std::vector<BatchGroup> groups;
     bool dirty = true;
-    int t = 0;                           // steps since the descriptors were written, mod 2
+    int t = 0;                           // steps since the descriptors were written, mod kPeriod
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[kPeriod] = {};
     int graph_launches = 0;
     SolveDesc* all_desc = nullptr;       // device, every member in member order (scalar gather)
     Scalars* d_sc = nullptr;             // device gather buffer: [0, n) before, [n, 2n) after a step call
@@ -182,7 +186,7 @@ void enq_group_step(const BatchGroup& g, int ps, int pl, bool prep, int* count) 
         launch_stage(g, S, ps, pl, prep, count);
         ps ^= 1;
         if (!g.p1) {
-            pl ^= 1;
+            pl = next_list(pl);
             launch_ghost(g, ps, pl, 1, 0, prep, count);
         } else {
             launch_ghost(g, ps, pl, 0, 0, prep, count);
@@ -191,7 +195,7 @@ void enq_group_step(const BatchGroup& g, int ps, int pl, bool prep, int* count) 
     if (g.pst_on) {
         launch_pst(g, ps, pl, prep, count);
         ps ^= 1;
-        pl ^= 1;
+        pl = next_list(pl);
         launch_ghost(g, ps, pl, 1, 1, prep, count);
     }
     if (g.p1 && !prep) {
@@ -207,8 +211,7 @@ SolveDesc make_desc(const lssph_handle* h) {
     d.P = h->P;
     d.F[0] = h->F[0];
     d.F[1] = h->F[1];
-    d.L[0] = h->L[0];
-    d.L[1] = h->L[1];
+    for (int l = 0; l < kLists; ++l) d.L[l] = h->L[l];
     d.W = h->W;
     d.V = h->V;
     d.VT = VMTiles{h->vt_tile, h->vt_start, h->vt_vm};
@@ -262,7 +265,8 @@ int rebuild(lssph_batch* b) {
     const size_t n = b->members.size();
     b->base_sb.assign(n, 0);
     b->base_lb.assign(n, 0);
-    b->flip.assign(n, 0);
+    b->sbf.assign(n, 0);
+    b->lba.assign(n, 0);
     std::map<std::tuple<int, int, int, int, int>, int> index;
     for (size_t i = 0; i < n; ++i) {
         const lssph_handle* h = b->members[i];
@@ -279,14 +283,17 @@ int rebuild(lssph_batch* b) {
             g.pdl = pdl_enabled();
             g.p1 = h->p1;
             g.pst_on = h->pst_on;
-            g.flip = h->p1 ? 0 : 1;
+            const int ns = h->p.rk == 2 ? 2 : 4;
+            g.sbf = h->p1 ? (ns & 1) : ((ns + 1) & 1);
+            g.lba = h->p1 ? 0 : (ns + 1) % kLists;
             it = index.emplace(key, (int)b->groups.size()).first;
             b->groups.push_back(g);
         }
         b->groups[it->second].members.push_back((int)i);
         b->base_sb[i] = b->members[i]->sb;
         b->base_lb[i] = b->members[i]->lb;
-        b->flip[i] = b->groups[it->second].flip;
+        b->sbf[i] = b->groups[it->second].sbf;
+        b->lba[i] = b->groups[it->second].lba;
     }
     std::vector<SolveDesc> all;
     for (auto& g : b->groups) {
@@ -351,8 +358,7 @@ int capture(lssph_batch* b, int t, cudaGraphExec_t* out) {
     int count = 0;
     for (auto& g : b->groups) {
         cudaStreamWaitEvent(g.stream, b->fork, 0);
-        const int par = g.flip & t;
-        enq_group_step(g, par, par, false, &count);
+        enq_group_step(g, g.sbf & t & 1, (g.lba * t) % kLists, false, &count);
         cudaEventRecord(g.join, g.stream);
         cudaStreamWaitEvent(b->stream, g.join, 0);
     }
@@ -447,8 +453,8 @@ int lssph_batch_launch(lssph_batch* b, int32_t nsteps) {
     if (b->flight_steps == 0 || n == 0) { b->in_flight = true; return LSSPH_OK; }
     // a member stepped on its own since the last batch call: rewrite the descriptors
     for (size_t i = 0; i < n && !b->dirty; ++i) {
-        const int par = b->flip[i] & b->t;
-        if (b->members[i]->sb != (b->base_sb[i] ^ par) || b->members[i]->lb != (b->base_lb[i] ^ par)) b->dirty = true;
+        const int sb = b->base_sb[i] ^ (b->sbf[i] & b->t & 1), lb = (b->base_lb[i] + b->lba[i] * b->t) % kLists;
+        if (b->members[i]->sb != sb || b->members[i]->lb != lb) b->dirty = true;
     }
     int rc;
     if (b->dirty && (rc = rebuild(b)) != LSSPH_OK) return rc;
@@ -464,10 +470,10 @@ int lssph_batch_launch(lssph_batch* b, int32_t nsteps) {
         cudaGraphExec_t& ge = b->graph[b->t];
         if (!ge && (rc = capture(b, b->t, &ge)) != LSSPH_OK) return rc;
         BATCH_TRY(b, cudaGraphLaunch(ge, b->stream));
-        b->t ^= 1;
+        b->t = (b->t + 1) % kPeriod;
         for (size_t i = 0; i < n; ++i) {   // members follow the batch's parity
-            b->members[i]->sb ^= b->flip[i];
-            b->members[i]->lb ^= b->flip[i];
+            b->members[i]->sb ^= b->sbf[i];
+            b->members[i]->lb = (b->members[i]->lb + b->lba[i]) % kLists;
         }
     }
     BATCH_TRY(b, cudaEventRecord(b->ev1, b->stream));
@@ -510,8 +516,8 @@ int lssph_batch_wait(lssph_batch* b, int32_t* status, int32_t* steady, int32_t* 
         const int executed = s1.step_count - s0[i].step_count;
         if (steps_taken) steps_taken[i] = executed;
         if (executed != nsteps) {
-            b->members[i]->sb = b->sb_start[i] ^ (b->flip[i] & executed & 1);
-            b->members[i]->lb = b->lb_start[i] ^ (b->flip[i] & executed & 1);
+            b->members[i]->sb = b->sb_start[i] ^ (b->sbf[i] & executed & 1);
+            b->members[i]->lb = (b->lb_start[i] + b->lba[i] * executed) % kLists;
         }
     }
     if (first != LSSPH_OK) return bfail(b, first, "a batch member stopped with an error (see the status array)");

@@ -54,6 +54,8 @@ void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t 
     for (int b = 0; b < 2; ++b) {
         Fld& F = h->F[b];
         A(&F.x, N); A(&F.y, N); A(&F.u, N); A(&F.v, N); A(&F.rho, N); A(&F.pre, N); A(&F.tem, N); A(&F.vol, N);
+    }
+    for (int b = 0; b < kLists; ++b) {
         Lst& L = h->L[b];
         A(&L.cnt, NC); A(&L.slots, NC * (size_t)cap);
     }
@@ -152,7 +154,7 @@ void run_stage(lssph_handle* h, const StageCfg& S) {
     }
     auto kern = h->tight ? k_stage<NB, GG, true, MX> : k_stage<NB, GG, false, MX>;
     launch_kernel(h->pdl, kern, h->ntiles, PPB * GG, h->smem_bytes, h->stream, h->P, h->F[h->sb], h->F[h->sb ^ 1],
-                  h->L[h->lb], h->L[h->lb ^ 1], h->gstart, h->glist, h->W, S, h->sc, h->ntx);
+                  h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, S, h->sc, h->ntx);
     h->launch_counter++;
 }
 
@@ -220,7 +222,7 @@ void run_pst(lssph_handle* h) {
     }
     auto kern = h->tight ? k_pst<NB, GG, true, MX> : k_pst<NB, GG, false, MX>;
     launch_kernel(h->pdl, kern, h->ntiles, PPB * GG, h->smem_bytes, h->stream, h->P, h->F[h->sb], h->F[h->sb ^ 1],
-                  h->L[h->lb], h->L[h->lb ^ 1], h->gstart, h->glist, h->W, h->sc, h->ntx);
+                  h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, h->sc, h->ntx);
     h->launch_counter++;
 }
 
@@ -260,8 +262,8 @@ void enq_stage(lssph_handle* h, int stage, bool fused_step) {
     launch_stage_any(h, S);
     h->sb ^= 1;
     if (!h->p1) {
-        h->lb ^= 1;
-        launch_ghost(h, h->lb ^ 1, 0);   // also clears the list the stage just consumed
+        h->lb = next_list(h->lb);
+        launch_ghost(h, prev_list(h->lb), 0);   // also clears the list the stage just consumed
     } else {
         launch_ghost(h);
     }
@@ -271,8 +273,8 @@ void enq_pst(lssph_handle* h) {
     if (h->has_tem) launch_pst_t<4>(h);
     else launch_pst_t<3>(h);
     h->sb ^= 1;
-    h->lb ^= 1;
-    launch_ghost(h, h->lb ^ 1, 1);
+    h->lb = next_list(h->lb);
+    launch_ghost(h, prev_list(h->lb), 1);
 }
 
 // Set the shared-memory opt-in of every kernel instantiation this handle launches.
@@ -363,7 +365,7 @@ int sync_check(lssph_handle* h) {
 
 // Build the cell list of the current positions into list buffer lb (fresh).
 int rebuild_cells(lssph_handle* h) {
-    for (int b = 0; b < 2; ++b) CUDA_TRY(h, cudaMemsetAsync(h->L[b].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
+    for (int b = 0; b < kLists; ++b) CUDA_TRY(h, cudaMemsetAsync(h->L[b].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
     k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->gstart, h->W.key, h->sc);
     return LSSPH_OK;
 }
@@ -572,10 +574,10 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     H2D(h->vt_vm, vt_vm.data(), sizeof(int32_t) * NE);
     if (ok && cudaMemsetAsync(h->sc, 0, sizeof(Scalars), h->stream) != cudaSuccess) ok = false;
     if (ok && cudaMemsetAsync(W.key, 0, sizeof(int32_t) * NI, h->stream) != cudaSuccess) ok = false;
-    for (int b = 0; b < 2 && ok; ++b) {
+    for (int b = 0; b < 2 && ok; ++b)
         if (cudaMemsetAsync(h->F[b].tem, 0, sizeof(double) * N, h->stream) != cudaSuccess) ok = false;
+    for (int b = 0; b < kLists && ok; ++b)
         if (cudaMemsetAsync(h->L[b].slots, 0xff, sizeof(int) * NC * h->grid.cap, h->stream) != cudaSuccess) ok = false;
-    }
     if (!ok) { free_handle(h); return fail(nullptr, LSSPH_E_CUDA, "device initialisation failed"); }
     prepare_kernels(h);
     if ((rc = upload_fields(h, x, y, u, v, rho, pre, tem)) != LSSPH_OK ||
@@ -633,11 +635,11 @@ int lssph_calculate_rhs(lssph_handle* h) {
 
 int lssph_update_cell(lssph_handle* h) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
-    CUDA_TRY(h, cudaMemsetAsync(h->L[h->lb ^ 1].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
-    k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb ^ 1], h->gstart,
+    CUDA_TRY(h, cudaMemsetAsync(h->L[next_list(h->lb)].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
+    k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[next_list(h->lb)], h->gstart,
                                                                      h->W.key, h->sc);
-    h->lb ^= 1;
-    CUDA_TRY(h, cudaMemsetAsync(h->L[h->lb ^ 1].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
+    h->lb = next_list(h->lb);
+    CUDA_TRY(h, cudaMemsetAsync(h->L[prev_list(h->lb)].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
     return sync_check(h);
 }
 
@@ -713,14 +715,15 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
             if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
             h->graph_launches = (int)(h->launch_counter - c0);
             h->launch_counter = c0;
-            h->step_flip = ((h->sb ^ sb0) << 1) | (h->lb ^ lb0);
+            h->step_sbf = h->sb ^ sb0;
+            h->step_lba = (h->lb - lb0 + kLists) % kLists;
             h->sb = sb0;
             h->lb = lb0;
         }
         CUDA_TRY(h, cudaGraphLaunch(ge, h->stream));
         h->launch_counter += h->graph_launches;
-        h->sb ^= (h->step_flip >> 1) & 1;
-        h->lb ^= h->step_flip & 1;
+        h->sb ^= h->step_sbf;
+        h->lb = (h->lb + h->step_lba) % kLists;
     }
     CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
     Scalars s1{};
@@ -733,8 +736,8 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
     // sit where the last executed step left them
     const int executed = s1.step_count - s0.step_count;
     if (executed != nsteps) {
-        h->sb = sb_start ^ (((h->step_flip >> 1) & 1) & (executed & 1));
-        h->lb = lb_start ^ ((h->step_flip & 1) & (executed & 1));
+        h->sb = sb_start ^ (h->step_sbf & executed & 1);
+        h->lb = (lb_start + h->step_lba * executed) % kLists;
     }
     if (rc != LSSPH_OK) return rc;
     if (s1.steady && steady_step_out) *steady_step_out = s1.steady_step - s0.step_count;

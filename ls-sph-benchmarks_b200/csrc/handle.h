@@ -33,7 +33,7 @@ struct lssph_handle {
     void* block = nullptr;              // the one device allocation all arrays live in
     int64_t alloc_bytes = 0;            // its size
     lssph::Fld F[2]{};
-    lssph::Lst L[2]{};
+    lssph::Lst L[lssph::kLists]{};      // cell lists in rotation: read one, scatter into the next
     lssph::Work W{};
     lssph::VMd V{};
     int* gstart = nullptr;
@@ -46,9 +46,10 @@ struct lssph_handle {
     bool preparing = false;             // launch helpers only set kernel attributes
     lssph::Scalars* sc = nullptr;
     int sb = 0, lb = 0;
-    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaGraphExec_t graph[2][lssph::kLists] = {};   // per (state parity, list index)
     int graph_launches = 0;   // kernels per captured step
-    int step_flip = 0;        // parity change per step
+    int step_sbf = 0;         // state-buffer flip per step (0/1)
+    int step_lba = 0;         // list advance per step (mod kLists)
     int64_t launch_counter = 0;
     double last_ms = 0.0;
     int64_t last_launches = 0;

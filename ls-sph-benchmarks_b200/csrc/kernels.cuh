@@ -75,6 +75,14 @@ struct Phys {
 struct Fld {   // SoA particle state over num_total
     double *x, *y, *u, *v, *rho, *pre, *tem, *vol;
 };
+// Cell lists rotate through three buffers: a stage reads list l and scatters into list
+// l + 1 while the ghost launch after it clears list l - 1, so a list is cleared well
+// before the next scatter into it and no clearing sits between two launches that read
+// the same buffers.
+constexpr int kLists = 3;
+__host__ __device__ constexpr int next_list(int l) { return l == kLists - 1 ? 0 : l + 1; }
+__host__ __device__ constexpr int prev_list(int l) { return l == 0 ? kLists - 1 : l - 1; }
+
 struct Lst {   // interior particles per cell, scatter order: slots[c*cap + k], k < cnt[c]
     int *cnt, *slots;
 };
@@ -1845,7 +1853,7 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
 struct SolveDesc {
     Phys P;
     Fld F[2];
-    Lst L[2];
+    Lst L[kLists];
     Work W;
     VMd V;
     VMTiles VT;
@@ -1877,10 +1885,11 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_stage(c
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);
-    const int sb = d.sb ^ ps, lb = d.lb ^ pl;
+    const int sb = d.sb ^ ps, lb = (d.lb + pl) % kLists;
     S.dt1 = d.dt1[S.stage - 1];
     S.dt2 = d.dt2[S.stage - 1];
-    stage_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, S, d.sc, d.ntx, m.y);
+    stage_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[next_list(lb)], d.gstart, d.glist, d.W, S, d.sc,
+                             d.ntx, m.y);
 }
 
 template <int NB, int G, int WQ>
@@ -1889,9 +1898,9 @@ __global__ void __launch_bounds__(PPB * G) kb_ghost(const SolveDesc* __restrict_
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);
-    const int sb = d.sb ^ ps, lb = d.lb ^ pl;
+    const int sb = d.sb ^ ps, lb = (d.lb + pl) % kLists;
     ghost_body<NB, G, WQ>(d.P, d.F[sb], d.L[lb], d.gstart, d.glist, d.V, d.VT, d.ntx,
-                          zero_other ? d.L[lb ^ 1].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
+                          zero_other ? d.L[prev_list(lb)].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
 }
 
 template <int NB, int G, bool TIGHT = false, bool MIXED = false>
@@ -1899,8 +1908,9 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(con
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);
-    const int sb = d.sb ^ ps, lb = d.lb ^ pl;
-    pst_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[lb ^ 1], d.gstart, d.glist, d.W, d.sc, d.ntx, m.y);
+    const int sb = d.sb ^ ps, lb = (d.lb + pl) % kLists;
+    pst_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[next_list(lb)], d.gstart, d.glist, d.W, d.sc,
+                           d.ntx, m.y);
 }
 
 // =======================================================================================
