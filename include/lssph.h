@@ -206,6 +206,12 @@ int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32
 int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
                      double* rhs_us_tight);
 
+/* Time-step schedule (no counterpart in the reference): cell tiles, the tiles whose halo
+   holds no ghost particle, and whether lssph_step runs each ghost launch beside the next
+   stage's interior tiles (1) or alone (0; LSSPH_OVERLAP=0 forces it).  Never changes a
+   result. */
+int lssph_get_schedule(const lssph_handle* h, int32_t* tiles, int32_t* interior_tiles, int32_t* overlapped);
+
 /* Device time of the kernels launched by the last lssph_step call, in milliseconds
    (CUDA events on the handle's stream), and the number of kernel launches it made. */
 int lssph_last_step_stats(const lssph_handle* h, double* device_ms, int64_t* kernel_launches);

@@ -50,7 +50,8 @@ int fail(lssph_handle* h, int code, const std::string& msg) {
 // Every device array of a solve, in one place: the visitor gets (&pointer, element count)
 // for each.  Used to size the solve's single device block and to carve it up.
 template <class Vis>
-void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, Vis&& A) {
+void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, int ntiles,
+                        Vis&& A) {
     for (int b = 0; b < 2; ++b) {
         Fld& F = h->F[b];
         A(&F.x, N); A(&F.y, N); A(&F.u, N); A(&F.v, N); A(&F.rho, N); A(&F.pre, N); A(&F.tem, N); A(&F.vol, N);
@@ -70,6 +71,7 @@ void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t 
     A(&h->gstart, NC + 1); A(&h->glist, NE);
     A(&h->sc, 1);
     A(&h->vt_tile, (size_t)std::max(nvt, 1)); A(&h->vt_start, (size_t)nvt + 1); A(&h->vt_vm, NE);
+    A(&h->tile_int, (size_t)ntiles); A(&h->tile_wall, (size_t)ntiles);
 }
 
 constexpr size_t kArrayAlign = 256;   // every array starts on a 256-byte boundary
@@ -104,10 +106,10 @@ void vm_chunks(const CellGrid& g, int ntx, int ntiles, std::vector<int32_t>* til
 
 // Size of the single device block of a solve of these sizes (every array holds at least
 // one element and starts on a 256-byte boundary).
-int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt) {
+int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, int ntiles) {
     lssph_handle layout;
     size_t total = 0;
-    visit_solve_arrays(&layout, N, NI, NE, NC, cap, nvt, [&](auto** p, size_t n) { total += array_bytes(p, n); });
+    visit_solve_arrays(&layout, N, NI, NE, NC, cap, nvt, ntiles, [&](auto** p, size_t n) { total += array_bytes(p, n); });
     return (int64_t)total;
 }
 
@@ -143,42 +145,56 @@ void smem_optin(K kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8, true));
 }
 
+// Where a launch goes: its tile map (NULL: every tile in order), CTA count, stream, and
+// whether it may be a programmatic dependent launch (not right after a fork or join).
+struct Where {
+    const int* tiles;
+    int count;
+    cudaStream_t stream;
+    bool pdl;
+    int priority;   // 0: default
+};
+Where all_tiles(const lssph_handle* h) { return Where{nullptr, h->ntiles, h->stream, h->pdl, 0}; }
+
 // ---- kernel dispatch on lanes, register budget and precision ------------------------------
 // The mixed-precision kernels exist for 4 lanes per particle only.
 template <int NB, int GG, bool MX>
-void run_stage(lssph_handle* h, const StageCfg& S) {
+void run_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     if (h->preparing) {
         smem_optin(k_stage<NB, GG, false, MX>);
         smem_optin(k_stage<NB, GG, true, MX>);
         return;
     }
     auto kern = h->tight ? k_stage<NB, GG, true, MX> : k_stage<NB, GG, false, MX>;
-    launch_kernel(h->pdl, kern, h->ntiles, PPB * GG, h->smem_bytes, h->stream, h->P, h->F[h->sb], h->F[h->sb ^ 1],
-                  h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, S, h->sc, h->ntx);
+    launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P, h->F[h->sb],
+                    h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, S, h->sc, h->ntx,
+                    w.tiles);
     h->launch_counter++;
 }
 
 template <int NB>
-void launch_stage(lssph_handle* h, const StageCfg& S) {
+void launch_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_STAGE);
-    if (h->mixed) { run_stage<NB, 4, true>(h, S); return; }
+    if (h->mixed) { run_stage<NB, 4, true>(h, S, w); return; }
     switch (h->G) {
-        case 1: run_stage<NB, 1, false>(h, S); break;
-        case 2: run_stage<NB, 2, false>(h, S); break;
-        case 8: run_stage<NB, 8, false>(h, S); break;
-        default: run_stage<NB, 4, false>(h, S); break;
+        case 1: run_stage<NB, 1, false>(h, S, w); break;
+        case 2: run_stage<NB, 2, false>(h, S, w); break;
+        case 8: run_stage<NB, 8, false>(h, S, w); break;
+        default: run_stage<NB, 4, false>(h, S, w); break;
     }
 }
 
-void launch_stage_any(lssph_handle* h, const StageCfg& S) {
-    if (h->nb_rhs == 1) launch_stage<1>(h, S);
-    else if (h->nb_rhs == 5) launch_stage<5>(h, S);
-    else launch_stage<4>(h, S);
+void launch_stage_any(lssph_handle* h, const StageCfg& S, const Where& w) {
+    if (h->nb_rhs == 1) launch_stage<1>(h, S, w);
+    else if (h->nb_rhs == 5) launch_stage<5>(h, S, w);
+    else launch_stage<4>(h, S, w);
 }
+
+void launch_stage_any(lssph_handle* h, const StageCfg& S) { launch_stage_any(h, S, all_tiles(h)); }
 
 // zero_list >= 0: clear that list's scatter counters (the list the preceding stage read).
 template <int NB, int WQ>
-void launch_ghost_t(lssph_handle* h, int zero_list, int reset_umax) {
+void launch_ghost_t(lssph_handle* h, int zero_list, int reset_umax, cudaStream_t stream, bool pdl, int priority) {
     ProfScope prof(h, LSSPH_KIND_GHOST);
     const Fld& F = h->F[h->sb];
     const Lst& L = h->L[h->lb];
@@ -188,7 +204,7 @@ void launch_ghost_t(lssph_handle* h, int zero_list, int reset_umax) {
     const size_t sm = h->smem_ghost;
 #define LSSPH_GHOST(GG)                                                                                    \
     if (h->preparing) { smem_optin(k_ghost<NB, GG, WQ>); return; }                                        \
-    launch_kernel(h->pdl, k_ghost<NB, GG, WQ>, h->nvt, PPB * GG, sm, h->stream, h->P, F, L, h->gstart, h->glist, h->V, VT, h->ntx, zc, \
+    launch_kernel_p(pdl, priority, k_ghost<NB, GG, WQ>, h->nvt, PPB * GG, sm, stream, h->P, F, L, h->gstart, h->glist, h->V, VT, h->ntx, zc, \
                                                           reset_umax, h->sc)
     switch (G) {
         case 1: LSSPH_GHOST(1); break;
@@ -201,46 +217,57 @@ void launch_ghost_t(lssph_handle* h, int zero_list, int reset_umax) {
 }
 
 template <int NB>
-void launch_ghost_nb(lssph_handle* h, int zero_list, int reset_umax) {
-    if (h->wq == 1) launch_ghost_t<NB, 1>(h, zero_list, reset_umax);
-    else if (h->wq == 6) launch_ghost_t<NB, 6>(h, zero_list, reset_umax);
-    else launch_ghost_t<NB, 3>(h, zero_list, reset_umax);
+void launch_ghost_nb(lssph_handle* h, int zero_list, int reset_umax, cudaStream_t stream, bool pdl, int priority) {
+    if (h->wq == 1) launch_ghost_t<NB, 1>(h, zero_list, reset_umax, stream, pdl, priority);
+    else if (h->wq == 6) launch_ghost_t<NB, 6>(h, zero_list, reset_umax, stream, pdl, priority);
+    else launch_ghost_t<NB, 3>(h, zero_list, reset_umax, stream, pdl, priority);
+}
+
+void launch_ghost_on(lssph_handle* h, int zero_list, int reset_umax, cudaStream_t stream, bool pdl,
+                     int priority = 0) {
+    if (h->nb_ghost == 1) launch_ghost_nb<1>(h, zero_list, reset_umax, stream, pdl, priority);
+    else if (h->nb_ghost == 4) launch_ghost_nb<4>(h, zero_list, reset_umax, stream, pdl, priority);
+    else launch_ghost_nb<3>(h, zero_list, reset_umax, stream, pdl, priority);
 }
 
 void launch_ghost(lssph_handle* h, int zero_list = -1, int reset_umax = 0) {
-    if (h->nb_ghost == 1) launch_ghost_nb<1>(h, zero_list, reset_umax);
-    else if (h->nb_ghost == 4) launch_ghost_nb<4>(h, zero_list, reset_umax);
-    else launch_ghost_nb<3>(h, zero_list, reset_umax);
+    launch_ghost_on(h, zero_list, reset_umax, h->stream, h->pdl);
 }
 
 template <int NB, int GG, bool MX>
-void run_pst(lssph_handle* h) {
+void run_pst(lssph_handle* h, const Where& w) {
     if (h->preparing) {
         smem_optin(k_pst<NB, GG, false, MX>);
         smem_optin(k_pst<NB, GG, true, MX>);
         return;
     }
     auto kern = h->tight ? k_pst<NB, GG, true, MX> : k_pst<NB, GG, false, MX>;
-    launch_kernel(h->pdl, kern, h->ntiles, PPB * GG, h->smem_bytes, h->stream, h->P, h->F[h->sb], h->F[h->sb ^ 1],
-                  h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, h->sc, h->ntx);
+    launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P, h->F[h->sb],
+                    h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, h->sc, h->ntx,
+                    w.tiles);
     h->launch_counter++;
 }
 
 template <int NB>
-void launch_pst_t(lssph_handle* h) {
+void launch_pst_t(lssph_handle* h, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_PST);
-    if (h->mixed) { run_pst<NB, 4, true>(h); return; }
+    if (h->mixed) { run_pst<NB, 4, true>(h, w); return; }
     switch (h->G) {
-        case 1: run_pst<NB, 1, false>(h); break;
-        case 2: run_pst<NB, 2, false>(h); break;
-        case 8: run_pst<NB, 8, false>(h); break;
-        default: run_pst<NB, 4, false>(h); break;
+        case 1: run_pst<NB, 1, false>(h, w); break;
+        case 2: run_pst<NB, 2, false>(h, w); break;
+        case 8: run_pst<NB, 8, false>(h, w); break;
+        default: run_pst<NB, 4, false>(h, w); break;
     }
+}
+
+void launch_pst_any(lssph_handle* h, const Where& w) {
+    if (h->has_tem) launch_pst_t<4>(h, w);
+    else launch_pst_t<3>(h, w);
 }
 
 // ---- operator sequences (enqueue only) -----------------------------------------------------
 // One RK stage: RHS + update (+ scatter), cell list finish, ghost.
-void enq_stage(lssph_handle* h, int stage, bool fused_step) {
+StageCfg stage_cfg(const lssph_handle* h, int stage, bool fused_step) {
     StageCfg S{};
     S.mode = MODE_STAGE;
     S.stage = stage;
@@ -259,7 +286,11 @@ void enq_stage(lssph_handle* h, int stage, bool fused_step) {
     S.do_umax = (fused_step && h->pst_on) ? 1 : 0;
     S.do_steady = (fused_step && h->p1) ? 1 : 0;
     S.write_rhs = 1;
-    launch_stage_any(h, S);
+    return S;
+}
+
+void enq_stage(lssph_handle* h, int stage, bool fused_step) {
+    launch_stage_any(h, stage_cfg(h, stage, fused_step));
     h->sb ^= 1;
     if (!h->p1) {
         h->lb = next_list(h->lb);
@@ -270,8 +301,7 @@ void enq_stage(lssph_handle* h, int stage, bool fused_step) {
 }
 
 void enq_pst(lssph_handle* h) {
-    if (h->has_tem) launch_pst_t<4>(h);
-    else launch_pst_t<3>(h);
+    launch_pst_any(h, all_tiles(h));
     h->sb ^= 1;
     h->lb = next_list(h->lb);
     launch_ghost(h, prev_list(h->lb), 1);
@@ -283,20 +313,77 @@ void prepare_kernels(lssph_handle* h) {
     StageCfg S{};
     launch_stage_any(h, S);
     launch_ghost(h);
-    if (h->has_tem) launch_pst_t<4>(h);
-    else launch_pst_t<3>(h);
+    launch_pst_any(h, all_tiles(h));
     h->preparing = false;
+}
+
+void enq_epilogue(lssph_handle* h, bool pdl) {
+    ProfScope prof(h, LSSPH_KIND_OTHER);
+    launch_kernel(pdl, k_epilogue, 1, 1, 0, h->stream, h->P, h->sc);
+    h->launch_counter++;
 }
 
 void enq_step(lssph_handle* h) {
     const int ns = h->p.rk == 2 ? 2 : 4;
     for (int s = 1; s <= ns; ++s) enq_stage(h, s, true);
     if (h->pst_on) enq_pst(h);
-    if (h->p1) {
-        ProfScope prof(h, LSSPH_KIND_OTHER);
-        launch_kernel(h->pdl, k_epilogue, 1, 1, 0, h->stream, h->P, h->sc);
-        h->launch_counter++;
+    if (h->p1) enq_epilogue(h, h->pdl);
+}
+
+// The same time step with each ghost launch beside the next stage's interior tiles
+// (tiles whose halo holds no ghost particle need no ghost values).  On the side stream
+// the ghost launch is followed by the wall tiles; both streams join before the next
+// stage.  Every launch reads and writes exactly what it does in enq_step: the ghost
+// launch touches ghost entries, virtual markers and the list two rotations back, the
+// interior tiles read interior entries and the current list and write the next list and
+// the other state buffer.  Stage 1 still follows the previous step's last ghost launch,
+// which counts the step and applies the step budget.
+void enq_step_overlap(lssph_handle* h) {
+    const int ns = h->p.rk == 2 ? 2 : 4;
+    // the ghost launch and the wall tiles are the critical path: their CTAs go first
+    const Where interior{h->tile_int, h->n_int, h->stream, false, 0};
+    const Where wall{h->tile_wall, h->n_wall, h->aux, h->pdl, h->high_priority};
+    launch_stage_any(h, stage_cfg(h, 1, true));
+    h->sb ^= 1;
+    int zero = -1;
+    if (!h->p1) {
+        h->lb = next_list(h->lb);
+        zero = prev_list(h->lb);
     }
+    auto fork = [&]() {
+        cudaEventRecord(h->fork_ev, h->stream);
+        cudaStreamWaitEvent(h->aux, h->fork_ev, 0);
+    };
+    auto join = [&]() {
+        cudaEventRecord(h->join_ev, h->aux);
+        cudaStreamWaitEvent(h->stream, h->join_ev, 0);
+    };
+    for (int s = 2; s <= ns; ++s) {
+        const StageCfg S = stage_cfg(h, s, true);
+        fork();
+        launch_ghost_on(h, zero, 0, h->aux, false, h->high_priority);
+        launch_stage_any(h, S, interior);
+        launch_stage_any(h, S, wall);
+        join();
+        h->sb ^= 1;
+        if (!h->p1) {
+            h->lb = next_list(h->lb);
+            zero = prev_list(h->lb);
+        }
+    }
+    if (h->pst_on) {
+        fork();
+        launch_ghost_on(h, zero, 0, h->aux, false, h->high_priority);
+        launch_pst_any(h, interior);
+        launch_pst_any(h, wall);
+        join();
+        h->sb ^= 1;
+        h->lb = next_list(h->lb);
+        launch_ghost_on(h, prev_list(h->lb), 1, h->stream, false);
+    } else {
+        launch_ghost_on(h, zero, 0, h->stream, false);
+    }
+    if (h->p1) enq_epilogue(h, h->pdl);
 }
 
 int sync_check(lssph_handle* h);
@@ -327,7 +414,10 @@ int autotune(lssph_handle* h) {
         CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
         h->tune_us[t] = 1e3 * ms / 3.0;
     }
-    h->tight = h->tune_us[1] < h->tune_us[0];
+    // In the overlapped step the interior tiles share the SMs with the ghost launch: four
+    // CTAs per SM (the tight budget) leave room for it where three do not, which an RHS
+    // pass alone does not show, so the overlapped step always takes the tight budget.
+    h->tight = h->overlap ? true : (h->tune_us[1] < h->tune_us[0]);
     h->launch_counter = c0;
     return sync_check(h);
 }
@@ -398,6 +488,9 @@ void free_handle(lssph_handle* h) {
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+    if (h->join_ev) cudaEventDestroy(h->join_ev);
+    if (h->aux) cudaStreamDestroy(h->aux);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -436,6 +529,14 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->wq = h->p.wall_model == 1 ? 1 : (h->p.wall_model == 3 ? 6 : 3);
     h->mixed = h->p.precision == LSSPH_PRECISION_MIXED;
     h->pdl = pdl_enabled();
+    {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) h->high_priority = greatest;
+    }
+    {
+        const char* v = std::getenv("LSSPH_OVERLAP");   // 0: ghost launches run alone
+        h->overlap_allowed = !(v && std::strcmp(v, "0") == 0);
+    }
     h->G = h->p.lanes > 0 ? h->p.lanes : 4;
     h->Gg = h->p.lanes > 0 ? h->p.lanes : 4;
     h->ptype.assign(ptype, ptype + num_total);
@@ -488,6 +589,9 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     // ---- device memory ----
     auto cu = [&](cudaError_t e) { return e == cudaSuccess ? LSSPH_OK : fail(nullptr, LSSPH_E_CUDA, cudaGetErrorString(e)); };
     if ((rc = cu(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking))) != LSSPH_OK ||
+        (rc = cu(cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking))) != LSSPH_OK ||
+        (rc = cu(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming))) != LSSPH_OK ||
+        (rc = cu(cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming))) != LSSPH_OK ||
         (rc = cu(cudaEventCreate(&h->ev0))) != LSSPH_OK || (rc = cu(cudaEventCreate(&h->ev1))) != LSSPH_OK) {
         free_handle(h);
         return rc;
@@ -503,8 +607,25 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     std::vector<int32_t> vt_tile, vt_start, vt_vm;
     vm_chunks(h->grid, h->ntx, h->ntiles, &vt_tile, &vt_start, &vt_vm);
     h->nvt = (int)vt_tile.size();
+    // tiles whose halo holds no ghost particle (interior) and the others (wall)
+    std::vector<int32_t> t_int, t_wall;
+    for (int t = 0; t < h->ntiles; ++t) {
+        const int cx0 = (t % h->ntx) * TX - 1, cy0 = (t / h->ntx) * TY - 1;
+        bool interior = true;
+        for (int hy = 0; hy < HY && interior; ++hy)
+            for (int hx = 0; hx < HX && interior; ++hx) {
+                const int cx = cx0 + hx, cy = cy0 + hy;
+                if (cx < 0 || cx >= h->grid.nx || cy < 0 || cy >= h->grid.ny) { interior = false; break; }
+                const int c = cx + cy * h->grid.nx;
+                if (h->grid.gstart[c + 1] != h->grid.gstart[c]) interior = false;
+            }
+        (interior ? t_int : t_wall).push_back(t);
+    }
+    h->n_int = (int)t_int.size();
+    h->n_wall = (int)t_wall.size();
+    h->overlap = h->overlap_allowed && h->n_int > 0 && h->n_wall > 0;
     // one device block for every array of the solve (one cudaMalloc, one cudaFree)
-    const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt);
+    const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles);
     {
         const cudaError_t e = cudaMalloc(&h->block, block);
         if (e != cudaSuccess) {
@@ -514,7 +635,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         h->alloc_bytes = (int64_t)block;
         size_t off = 0;
         char* base = static_cast<char*>(h->block);
-        visit_solve_arrays(h, N, NI, NE, NC, h->grid.cap, h->nvt, [&](auto** p, size_t n) {
+        visit_solve_arrays(h, N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles, [&](auto** p, size_t n) {
             using T = std::remove_reference_t<decltype(**p)>;
             *p = reinterpret_cast<T*>(base + off);
             off += array_bytes(p, n);
@@ -572,6 +693,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     H2D(h->vt_tile, vt_tile.data(), sizeof(int32_t) * vt_tile.size());
     H2D(h->vt_start, vt_start.data(), sizeof(int32_t) * vt_start.size());
     H2D(h->vt_vm, vt_vm.data(), sizeof(int32_t) * NE);
+    H2D(h->tile_int, t_int.data(), sizeof(int32_t) * t_int.size());
+    H2D(h->tile_wall, t_wall.data(), sizeof(int32_t) * t_wall.size());
     if (ok && cudaMemsetAsync(h->sc, 0, sizeof(Scalars), h->stream) != cudaSuccess) ok = false;
     if (ok && cudaMemsetAsync(W.key, 0, sizeof(int32_t) * NI, h->stream) != cudaSuccess) ok = false;
     for (int b = 0; b < 2 && ok; ++b)
@@ -707,10 +830,12 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
             const int sb0 = h->sb, lb0 = h->lb;
             const int64_t c0 = h->launch_counter;
             CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            enq_step(h);
+            if (h->overlap) enq_step_overlap(h);
+            else enq_step(h);
             cudaGraph_t g = nullptr;
             CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
-            const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+            // per-node priorities: the overlapped step's critical path runs first
+            const cudaError_t e = cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
             h->graph_launches = (int)(h->launch_counter - c0);
@@ -780,7 +905,15 @@ int lssph_estimate_device_bytes(const lssph_params* pin, int64_t* bytes) {
     const int ntx = (grid.nx + TX - 1) / TX, nty = (grid.ny + TY - 1) / TY;
     std::vector<int32_t> vt_tile, vt_start, vt_vm;
     vm_chunks(grid, ntx, ntx * nty, &vt_tile, &vt_start, &vt_vm);
-    *bytes = solve_bytes(nt, ni, nt - ni, grid.ncell, grid.cap, (int)vt_tile.size());
+    *bytes = solve_bytes(nt, ni, nt - ni, grid.ncell, grid.cap, (int)vt_tile.size(), ntx * nty);
+    return LSSPH_OK;
+}
+
+int lssph_get_schedule(const lssph_handle* h, int32_t* tiles, int32_t* interior_tiles, int32_t* overlapped) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (tiles) *tiles = h->ntiles;
+    if (interior_tiles) *interior_tiles = h->n_int;
+    if (overlapped) *overlapped = h->overlap ? 1 : 0;
     return LSSPH_OK;
 }
 

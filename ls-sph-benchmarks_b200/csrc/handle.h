@@ -29,6 +29,14 @@ struct lssph_handle {
     std::vector<int32_t> ptype;
     lssph::Phys P{};
     cudaStream_t stream = nullptr;
+    cudaStream_t aux = nullptr;         // side stream of the overlapped time step
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    int* tile_int = nullptr;            // tiles whose halo holds no ghost particle
+    int* tile_wall = nullptr;           // the other tiles
+    int n_int = 0, n_wall = 0;
+    bool overlap_allowed = true;        // LSSPH_OVERLAP=0 turns the overlapped step off
+    bool overlap = false;               // ghost launches run beside interior tiles
+    int high_priority = 0;              // the device's highest launch priority (ghost + wall tiles)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     void* block = nullptr;              // the one device allocation all arrays live in
     int64_t alloc_bytes = 0;            // its size
@@ -67,19 +75,34 @@ namespace lssph {
 // scheduled while the previous kernel in the stream drains; it calls pdl_wait() before
 // touching that kernel's results).  Captured into CUDA graphs as programmatic edges.
 template <class... KArgs, class... Args>
-inline cudaError_t launch_kernel(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
-                                 cudaStream_t stream, Args&&... args) {
+inline cudaError_t launch_kernel_p(bool pdl, int priority, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                   cudaStream_t stream, Args&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = pdl ? attr : nullptr;
-    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchAttribute attr[2];
+    unsigned n = 0;
+    if (pdl) {
+        attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n].val.programmaticStreamSerializationAllowed = 1;
+        ++n;
+    }
+    if (priority != 0) {   // scheduling priority of the launch's CTAs (lower value: sooner)
+        attr[n].id = cudaLaunchAttributePriority;
+        attr[n].val.priority = priority;
+        ++n;
+    }
+    cfg.attrs = n ? attr : nullptr;
+    cfg.numAttrs = n;
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
+template <class... KArgs, class... Args>
+inline cudaError_t launch_kernel(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                 cudaStream_t stream, Args&&... args) {
+    return launch_kernel_p(pdl, 0, kern, grid, block, smem, stream, std::forward<Args>(args)...);
 }
 
 // LSSPH_PDL=0 turns programmatic dependent launches off (default on).

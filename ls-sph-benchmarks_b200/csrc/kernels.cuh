@@ -1312,8 +1312,9 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
 template <int NB, int G, bool TIGHT = false, bool MIXED = false>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
-            const int* __restrict__ glist, const Work W, const StageCfg S, Scalars* sc, int ntx) {
-    stage_body<NB, G, MIXED>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, blockIdx.x);
+            const int* __restrict__ glist, const Work W, const StageCfg S, Scalars* sc, int ntx,
+            const int* __restrict__ tiles) {   // tile of each CTA (NULL: CTA i runs tile i)
+    stage_body<NB, G, MIXED>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
 // =======================================================================================
@@ -1840,8 +1841,8 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
 template <int NB, int G, bool TIGHT = false, bool MIXED = false>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
-          const int* __restrict__ glist, const Work W, Scalars* sc, int ntx) {
-    pst_body<NB, G, MIXED>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, blockIdx.x);
+          const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
+    pst_body<NB, G, MIXED>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
 // =======================================================================================

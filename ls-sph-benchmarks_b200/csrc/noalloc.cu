@@ -229,9 +229,9 @@ extern "C" int lssph_rhs_noalloc(const lssph_params* pin, int32_t num_total, int
     const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY;
     const size_t sm = tile_smem_bytes(kCap, 4, p.target_problem == 4);
     if (p.target_problem == 4)
-        k_stage<5, 4><<<ntx * nty, PPB * 4, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx);
+        k_stage<5, 4><<<ntx * nty, PPB * 4, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx, nullptr);
     else
-        k_stage<4, 4><<<ntx * nty, PPB * 4, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx);
+        k_stage<4, 4><<<ntx * nty, PPB * 4, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(LSSPH_E_CUDA, std::string("lssph_rhs_noalloc: launch: ") + cudaGetErrorString(e));
     Scalars hs{};

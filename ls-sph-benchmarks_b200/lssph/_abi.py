@@ -163,6 +163,7 @@ _PROTOS = {
     "lssph_estimate_device_bytes": (C.c_int, [_P(Params), _P(C.c_int64)]),
     "lssph_set_step_budget": (C.c_int, [_H, C.c_int32]),
     "lssph_get_progress": (C.c_int, [_H, _i, _i]),
+    "lssph_get_schedule": (C.c_int, [_H, _i, _i, _i]),
     "lssph_get_tuning": (C.c_int, [_H, _i, _i, _P(C.c_double), _P(C.c_double)]),
     "lssph_step_profiled": (C.c_int, [_H, C.c_int32, _d, _P(C.c_int64)]),
     "lssph_batch_create": (C.c_int, [_P(C.c_void_p)]),

@@ -230,12 +230,16 @@ class Simulation:
         return n.value, ("running", "steady", "budget")[st.value]
 
     def tuning(self) -> dict:
-        """Kernel configuration picked for this solve (lanes, register budget, timings)."""
+        """Kernel configuration picked for this solve (lanes, register budget, timings, and
+        the tile schedule of the time step)."""
         lanes, tight = C.c_int32(), C.c_int32()
         lo, ti = C.c_double(), C.c_double()
         self._chk(self._lib.lssph_get_tuning(self._h, C.byref(lanes), C.byref(tight), C.byref(lo), C.byref(ti)))
+        nt, ni, ov = C.c_int32(), C.c_int32(), C.c_int32()
+        self._chk(self._lib.lssph_get_schedule(self._h, C.byref(nt), C.byref(ni), C.byref(ov)))
         return {"lanes": lanes.value, "register_budget": "tight" if tight.value else "loose",
-                "rhs_us_loose": lo.value, "rhs_us_tight": ti.value}
+                "rhs_us_loose": lo.value, "rhs_us_tight": ti.value, "tiles": nt.value,
+                "interior_tiles": ni.value, "ghost_overlap": bool(ov.value)}
 
     def last_step_stats(self) -> tuple[float, int]:
         ms = C.c_double()
