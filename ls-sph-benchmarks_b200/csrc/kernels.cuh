@@ -357,7 +357,8 @@ __device__ __forceinline__ void lu_permute(const int (&pv)[Q], double (&b)[Q]) {
 // FP64 matrix: x = x0 + LU \ (b - M x0).  M is read back from the packed upper triangle.
 template <int Q>
 __device__ __forceinline__ void lu_solve_refined(const double (&LU)[Q][Q], const double (&rpiv)[Q],
-                                                 const int (&pv)[Q], const double* Mu, double (&b)[Q]) {
+                                                 const int (&pv)[Q], const double (&Mu)[Q * (Q + 1) / 2],
+                                                 double (&b)[Q]) {
     double x[Q], r[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) x[k] = b[k];
@@ -629,11 +630,10 @@ __device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Ls
 }
 
 // ---- mixed-precision staging -------------------------------------------------------------
-// Positions as FP32 offsets from the FP64 origin of the particle's halo cell (cell width
-// cw = h_eff); fields as FP32 offsets from FP64 reference values (those of the first staged
-// particle); volumes in FP32.  The pair phase rebuilds x_j - x_i = ddx cw + (o_j - o_i) from
-// the cell delta (ddx, ddy) of the candidate's cell, so no FP32 value carries more than
-// the spread of one tile.  Hit lists are 16-bit: staged index (10 bits) and cell delta.
+// Positions as FP32 offsets from the FP64 origin of the tile's halo corner cell (at most
+// 4 cell widths, so an offset carries ~2e-7 h_eff of rounding); fields as FP32 offsets
+// from FP64 reference values (those of the first staged particle); volumes in FP32.
+// Pair offsets x_j - x_i are then plain FP32 differences.  Hit lists are 16-bit.
 struct SmemMx {
     double* sums;                                       // [PPB][row stride], as in SmemView
     float *ox, *oy, *u, *v, *rho, *pre, *vol, *tem;
@@ -679,9 +679,8 @@ __device__ __forceinline__ TileRef stage_fields_mx(const Phys& P, const Fld& F, 
         if (WITH_TEM) R.tem = __ldg(F.tem + j0);
     }
     const double cw = sqrt(P.h_eff_sq);
+    const double x0 = (double)cx0 * cw, y0 = (double)cy0 * cw;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int h = halo_cell_of(T, k);
-        const double x0 = (double)(cx0 + h % HX) * cw, y0 = (double)(cy0 + h / HX) * cw;
         const int j = S.idx[k];
         S.ox[k] = (float)(__ldg(F.x + j) - x0);
         S.oy[k] = (float)(__ldg(F.y + j) - y0);
@@ -696,52 +695,45 @@ __device__ __forceinline__ TileRef stage_fields_mx(const Phys& P, const Fld& F, 
     return R;
 }
 
-// Candidates of an own particle in halo cell hc with the code of their cell delta
-// (ddx + 1) + 3 (ddy + 1); the same visiting order as for_tile_candidates.
+
+// Visit the staged candidates of an own particle in halo cell hc: 3x3 cells in reference
+// order; lane `lane` of a G-lane group takes every G-th candidate of the concatenation.
+// The three cells of a halo row are staged next to each other, so each row is one
+// contiguous range of staged positions (in the reference's dx order).
 template <int G, class Fn>
-__device__ __forceinline__ void for_tile_candidates_code(const TileHdr& T, int hc, int lane, Fn&& f) {
+__device__ __forceinline__ void for_tile_candidates(const TileHdr& T, int hc, int lane, Fn&& f) {
     int base = 0;
 #pragma unroll 1
     for (int dy = -1; dy <= 1; ++dy) {
-        const int h0 = hc - 1 + dy * HX;
-        const int lo = T.off[h0], m1 = T.off[h0 + 1], m2 = T.off[h0 + 2], hi = T.off[h0 + 3];
-        const int row = 3 * (dy + 1);
+        const int lo = T.off[hc - 1 + dy * HX], hi = T.off[hc + 2 + dy * HX];
         int k = lo + ((G == 1) ? 0 : ((lane - base) & (G - 1)));
 #pragma unroll 4
-        for (; k < hi; k += G) f(k, row + (k >= m1 ? 1 : 0) + (k >= m2 ? 1 : 0));
+        for (; k < hi; k += G) f(k);
         base += hi - lo;
     }
 }
 
-// v[i] for i in 0..2 by selects (a dynamic index would put v in local memory).
-__device__ __forceinline__ float pick3(const float (&v)[3], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
-
 // Mixed-precision two-phase neighbour loop (see tile_pairs): FP32 cutoff test on the
-// rebuilt offsets, 16-bit hits, f(k, x_j - x_i, y_j - y_i) over the hits.  xs[d + 1] =
-// o_x,i - d cw (and ys for y) are the own particle's offsets seen from the three cell
-// columns (rows).  At the cutoff W and its gradient are zero, so a pair that the FP32
-// test classifies differently from FP64 contributes nothing either way.
+// staged offsets, 16-bit hits, f(k, x_j - x_i, y_j - y_i) over the hits.  At the cutoff
+// W and its gradient are zero, so a pair that the FP32 test classifies differently from
+// FP64 contributes nothing either way.
 template <int G, class Fn>
 __device__ __forceinline__ int tile_pairs_mx(const TileHdr& T, const SmemMx& S, bool active, int hc, int lane,
-                                             int skip, const float (&xs)[3], const float (&ys)[3], float heff2,
-                                             Fn&& f) {
+                                             int skip, float oxi, float oyi, float heff2, Fn&& f) {
     int nl = 0;
     const int stride = blockDim.x;
     unsigned short* list = S.nbr + threadIdx.x;
     if (active) {
-        for_tile_candidates_code<G>(T, hc, lane, [&](int k, int code) {
-            const float xji = S.ox[k] - pick3(xs, code % 3);
-            const float yji = S.oy[k] - pick3(ys, code / 3);
+        for_tile_candidates<G>(T, hc, lane, [&](int k) {
+            const float xji = S.ox[k] - oxi;
+            const float yji = S.oy[k] - oyi;
             if (k != skip && !(xji * xji + yji * yji > heff2)) {
-                list[nl * stride] = (unsigned short)(k | (code << 10));
+                list[nl * stride] = (unsigned short)k;
                 ++nl;
             }
         });
     }
-    auto body = [&](unsigned e) {
-        const int k = (int)(e & 1023u), code = (int)(e >> 10);
-        f(k, S.ox[k] - pick3(xs, code % 3), S.oy[k] - pick3(ys, code / 3));
-    };
+    auto body = [&](int k) { f(k, S.ox[k] - oxi, S.oy[k] - oyi); };
     if constexpr (G == 1) {
 #pragma unroll 2
         for (int t = 0; t < nl; ++t) body(list[t * stride]);
@@ -770,23 +762,6 @@ __device__ __forceinline__ int tile_pairs_mx(const TileHdr& T, const SmemMx& S, 
             body(S.nbr[(pidx - bo) * stride + lane0 + o]);
         }
         return total;
-    }
-}
-
-// Visit the staged candidates of an own particle in halo cell hc: 3x3 cells in reference
-// order; lane `lane` of a G-lane group takes every G-th candidate of the concatenation.
-// The three cells of a halo row are staged next to each other, so each row is one
-// contiguous range of staged positions (in the reference's dx order).
-template <int G, class Fn>
-__device__ __forceinline__ void for_tile_candidates(const TileHdr& T, int hc, int lane, Fn&& f) {
-    int base = 0;
-#pragma unroll 1
-    for (int dy = -1; dy <= 1; ++dy) {
-        const int lo = T.off[hc - 1 + dy * HX], hi = T.off[hc + 2 + dy * HX];
-        int k = lo + ((G == 1) ? 0 : ((lane - base) & (G - 1)));
-#pragma unroll 4
-        for (; k < hi; k += G) f(k);
-        base += hi - lo;
     }
 }
 
@@ -1101,35 +1076,7 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
             const int ki = SM.own_k[o];
             const int cnt = (int)sm[SR - 1];
             double d[NB][Q];
-            if constexpr (MIXED) {
-                // one right-hand side at a time, solutions written back over the b sums
-                if (cnt >= Q) {
-                    double A[Q][Q];
-#pragma unroll
-                    for (int r = 0; r < Q; ++r)
-#pragma unroll
-                        for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? sm[UT(r, c)] : sm[UT(c, r)];
-                    double rpiv[Q];
-                    int pv[Q];
-                    if (!lu_factor_p<Q>(A, rpiv, pv)) atomicOr(&sc->warn, WARN_SINGULAR);
-#pragma unroll 1
-                    for (int c = 0; c < NB; ++c) {
-                        double b[Q];
-#pragma unroll
-                        for (int k = 0; k < Q; ++k) b[k] = sm[15 + 5 * c + k];
-                        lu_solve_refined<Q>(A, rpiv, pv, sm, b);
-#pragma unroll
-                        for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = b[k] * (k < 2 ? P.ih1 : P.ih2A);
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 15; k < 15 + 5 * NB; ++k) sm[k] = 0.0;
-                }
-#pragma unroll
-                for (int c = 0; c < NB; ++c)
-#pragma unroll
-                    for (int k = 0; k < Q; ++k) d[c][k] = sm[15 + 5 * c + k];
-            } else {
+            {
                 double A[Q][Q];
                 double B[NB][Q];
 #pragma unroll
@@ -1178,6 +1125,9 @@ __device__ __forceinline__ void solve_row_refined(const Phys& P, double* row, in
         for (int r = 0; r < Q; ++r)
 #pragma unroll
             for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? row[UT(r, c)] : row[UT(c, r)];
+        double Mr[Q * (Q + 1) / 2];   // the matrix stays in registers for every refinement
+#pragma unroll
+        for (int k = 0; k < Q * (Q + 1) / 2; ++k) Mr[k] = row[k];
         double rpiv[Q];
         int pv[Q];
         if (!lu_factor_p<Q>(A, rpiv, pv)) atomicOr(&sc->warn, WARN_SINGULAR);
@@ -1186,7 +1136,7 @@ __device__ __forceinline__ void solve_row_refined(const Phys& P, double* row, in
             double b[Q];
 #pragma unroll
             for (int k = 0; k < Q; ++k) b[k] = row[15 + 5 * c + k];
-            lu_solve_refined<Q>(A, rpiv, pv, row, b);
+            lu_solve_refined<Q>(A, rpiv, pv, Mr, b);
 #pragma unroll
             for (int k = 0; k < Q; ++k) row[15 + 5 * c + k] = SCALE ? b[k] * (k < 2 ? P.ih1 : P.ih2A) : b[k];
         }
@@ -1219,7 +1169,6 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
     if (stop) return;
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
-    const float cw = (float)sqrt(P.h_eff_sq);
     const float heff2 = (float)P.h_eff_sq;
     const PairConst<float> C(P);
     for (int ob = 0; ob < n_own; ob += PPB) {
@@ -1230,8 +1179,6 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
             int ki = 0, hc = 0;
             if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
             const float oxi = SM.ox[ki], oyi = SM.oy[ki];
-            const float xs[3] = {oxi + cw, oxi, oxi - cw};
-            const float ys[3] = {oyi + cw, oyi, oyi - cw};
             const float my_u = SM.u[ki];
             float my_v = 0.f, my_rho = 0.f, my_pre = 0.f, my_tem = 0.f;
             if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
@@ -1244,7 +1191,7 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
             for (int c = 0; c < NB; ++c)
 #pragma unroll
                 for (int k = 0; k < Q; ++k) B[c][k] = 0.f;
-            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, xs, ys, heff2,
+            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2,
                                              [&](int k, float xji, float yji) {
                 const float r = sqrtf(xji * xji + yji * yji);
                 const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
@@ -1619,36 +1566,7 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
                 dy = ((0.2 * P.h) * dy) / rr;
             }
             double B[NB][Q];
-            if constexpr (MIXED) {
-                // one right-hand side at a time, solutions written back over the b sums
-                double* smw = SM.sums + threadIdx.x * SR;
-                if (cnt >= Q) {
-                    double A[Q][Q];
-#pragma unroll
-                    for (int r = 0; r < Q; ++r)
-#pragma unroll
-                        for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? smw[UT(r, c)] : smw[UT(c, r)];
-                    double rpiv[Q];
-                    int pv[Q];
-                    if (!lu_factor_p<Q>(A, rpiv, pv)) atomicOr(&sc->warn, WARN_SINGULAR);
-#pragma unroll 1
-                    for (int c = 0; c < NB; ++c) {
-                        double b[Q];
-#pragma unroll
-                        for (int k = 0; k < Q; ++k) b[k] = smw[15 + 5 * c + k];
-                        lu_solve_refined<Q>(A, rpiv, pv, smw, b);
-#pragma unroll
-                        for (int k = 0; k < Q; ++k) smw[15 + 5 * c + k] = b[k];
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 15; k < 15 + 5 * NB; ++k) smw[k] = 0.0;
-                }
-#pragma unroll
-                for (int c = 0; c < NB; ++c)
-#pragma unroll
-                    for (int k = 0; k < Q; ++k) B[c][k] = smw[15 + 5 * c + k];
-            } else {
+            {
                 double A[Q][Q];
 #pragma unroll
                 for (int r = 0; r < Q; ++r)
@@ -1721,7 +1639,6 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
     const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
     const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
     const int lane = threadIdx.x & (G - 1);
-    const float cw = (float)sqrt(P.h_eff_sq);
     const float heff2 = (float)P.h_eff_sq;
     const PairConst<float> C(P);
     for (int ob = 0; ob < n_own; ob += PPB) {
@@ -1732,8 +1649,6 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
             int ki = 0, hc = 0;
             if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
             const float oxi = SM.ox[ki], oyi = SM.oy[ki];
-            const float xs[3] = {oxi + cw, oxi, oxi - cw};
-            const float ys[3] = {oyi + cw, oyi, oyi - cw};
             const float my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
             float my_tem = 0.f;
             if constexpr (NB == 4) my_tem = SM.tem[ki];
@@ -1746,7 +1661,7 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
 #pragma unroll
                 for (int k = 0; k < Q; ++k) B[c][k] = 0.f;
             float sxy[2] = {0.f, 0.f};
-            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, xs, ys, heff2,
+            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2,
                                              [&](int k, float xji, float yji) {
                 const float r = sqrtf(xji * xji + yji * yji);
                 const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
