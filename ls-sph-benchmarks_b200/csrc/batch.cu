@@ -13,7 +13,9 @@
 // a group sits at state parity (descriptor's) xor (sbf_g & k) and list index
 // (descriptor's) + lba_g k (mod 3), and six graphs (k mod 6) cover every step.
 // Descriptors are rewritten whenever the membership changes or a member was advanced on
-// its own between batch calls.
+// its own between batch calls.  The step count lives in device memory: every batched
+// kernel derives its parities from it and a last one-thread launch advances it, so one
+// graph serves every step.
 
 #include <cuda_runtime.h>
 
@@ -37,6 +39,7 @@ struct BatchGroup {
     int nb = 4, nbg = 3, wq = 3, rk = 4, G = 4;
     bool p1 = false, pst_on = true, mixed = false;
     bool pdl = true;               // programmatic dependent launches between the group's kernels
+    const int* tstep = nullptr;    // the batch's device step counter
     int sbf = 1;                   // state-buffer flip per step (0/1)
     int lba = 2;                   // list advance per step (mod kLists)
     std::vector<int> members;      // indices into lssph_batch::members
@@ -61,7 +64,8 @@ struct lssph_batch {
     int t = 0;                           // steps since the descriptors were written, mod kPeriod
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
-    cudaGraphExec_t graph[kPeriod] = {};
+    cudaGraphExec_t graph = nullptr;     // one step of every member (parities from d_t)
+    int* d_t = nullptr;                  // device step counter, mod kPeriod
     int graph_launches = 0;
     SolveDesc* all_desc = nullptr;       // device, every member in member order (scalar gather)
     Scalars* d_sc = nullptr;             // device gather buffer: [0, n) before, [n, 2n) after a step call
@@ -124,7 +128,7 @@ void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool p
         constexpr bool MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
-            launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles}, S,
+            launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles, g.tstep, g.sbf, g.lba}, S,
                           ps, pl);
             ++*count;
         };
@@ -139,7 +143,7 @@ void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset
         constexpr int G = decltype(GG)::value;
         auto run = [&](auto kern) {
             if (prep) { optin(kern); return; }
-            launch_kernel(g.pdl, kern, g.nchunks, PPB * G, g.smem_ghost, g.stream, g.D, BatchMap{g.chunks}, ps, pl, zero_other,
+            launch_kernel(g.pdl, kern, g.nchunks, PPB * G, g.smem_ghost, g.stream, g.D, BatchMap{g.chunks, g.tstep, g.sbf, g.lba}, ps, pl, zero_other,
                           reset_umax);
             ++*count;
         };
@@ -161,7 +165,7 @@ void launch_pst(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
         constexpr bool MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
-            launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles}, ps,
+            launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles, g.tstep, g.sbf, g.lba}, ps,
                           pl);
             ++*count;
         };
@@ -236,8 +240,10 @@ SolveDesc make_desc(const lssph_handle* h) {
 }
 
 void release_groups(lssph_batch* b) {
-    for (auto& g : b->graph)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
     for (auto& g : b->groups) {
         cudaFree(g.D);
         cudaFree(g.tiles);
@@ -290,6 +296,7 @@ int rebuild(lssph_batch* b) {
             b->groups.push_back(g);
         }
         b->groups[it->second].members.push_back((int)i);
+        b->groups[it->second].tstep = b->d_t;
         b->base_sb[i] = b->members[i]->sb;
         b->base_lb[i] = b->members[i]->lb;
         b->sbf[i] = b->groups[it->second].sbf;
@@ -335,6 +342,7 @@ int rebuild(lssph_batch* b) {
         BATCH_TRY(b, cudaMallocHost(&b->h_sc, 2 * sizeof(Scalars) * n));
         b->sc_cap = n;
     }
+    BATCH_TRY(b, cudaMemsetAsync(b->d_t, 0, sizeof(int), b->stream));
     BATCH_TRY(b, cudaStreamSynchronize(b->stream));
     b->t = 0;
     b->dirty = false;
@@ -352,16 +360,18 @@ int gather_scalars(lssph_batch* b, int which) {
     return LSSPH_OK;
 }
 
-int capture(lssph_batch* b, int t, cudaGraphExec_t* out) {
+int capture(lssph_batch* b, cudaGraphExec_t* out) {
     BATCH_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaEventRecord(b->fork, b->stream);
     int count = 0;
     for (auto& g : b->groups) {
         cudaStreamWaitEvent(g.stream, b->fork, 0);
-        enq_group_step(g, g.sbf & t & 1, (g.lba * t) % kLists, false, &count);
+        enq_group_step(g, 0, 0, false, &count);
         cudaEventRecord(g.join, g.stream);
         cudaStreamWaitEvent(b->stream, g.join, 0);
     }
+    kb_advance<<<1, 1, 0, b->stream>>>(b->d_t);
+    ++count;
     cudaGraph_t graph = nullptr;
     BATCH_TRY(b, cudaStreamEndCapture(b->stream, &graph));
     const cudaError_t e = cudaGraphInstantiate(out, graph, 0);
@@ -392,7 +402,8 @@ int lssph_batch_create(lssph_batch** out) {
     lssph_batch* b = new lssph_batch();
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&b->d_t, sizeof(int)) != cudaSuccess) {
         lssph_batch_destroy(b);
         return bfail(nullptr, LSSPH_E_CUDA, "stream/event creation failed");
     }
@@ -407,6 +418,7 @@ void lssph_batch_destroy(lssph_batch* b) {
     release_groups(b);
     cudaFree(b->d_sc);
     cudaFreeHost(b->h_sc);
+    cudaFree(b->d_t);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->fork) cudaEventDestroy(b->fork);
@@ -467,8 +479,8 @@ int lssph_batch_launch(lssph_batch* b, int32_t nsteps) {
     }
     BATCH_TRY(b, cudaEventRecord(b->ev0, b->stream));
     for (int st = 0; st < nsteps; ++st) {
-        cudaGraphExec_t& ge = b->graph[b->t];
-        if (!ge && (rc = capture(b, b->t, &ge)) != LSSPH_OK) return rc;
+        if (!b->graph && (rc = capture(b, &b->graph)) != LSSPH_OK) return rc;
+        cudaGraphExec_t ge = b->graph;
         BATCH_TRY(b, cudaGraphLaunch(ge, b->stream));
         b->t = (b->t + 1) % kPeriod;
         for (size_t i = 0; i < n; ++i) {   // members follow the batch's parity

@@ -1783,7 +1783,17 @@ struct SolveDesc {
 
 struct BatchMap {
     const int2* cta;     // (solve, tile-or-chunk) per CTA
+    const int* tstep;    // steps since the descriptors were written, mod 2 kLists (device)
+    int sbf, lba;        // the group's state flip and list advance per step
 };
+
+// Buffer parity of a launch: the descriptor's, advanced by the steps taken since it was
+// written, plus the launch's offset (ds, dl) from the start of the step.
+__device__ __forceinline__ void batch_parity(const BatchMap& M, const SolveDesc& d, int ds, int dl, int& sb, int& lb) {
+    const int t = *M.tstep;
+    sb = d.sb ^ (M.sbf & t & 1) ^ ds;
+    lb = (d.lb + M.lba * t + dl) % kLists;
+}
 
 // Copy the CTA's solve descriptor to shared memory (one global round trip for all of it).
 __device__ __forceinline__ const SolveDesc& load_desc(const SolveDesc* D, int s, SolveDesc& sd) {
@@ -1801,7 +1811,8 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_stage(c
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);
-    const int sb = d.sb ^ ps, lb = (d.lb + pl) % kLists;
+    int sb, lb;
+    batch_parity(M, d, ps, pl, sb, lb);
     S.dt1 = d.dt1[S.stage - 1];
     S.dt2 = d.dt2[S.stage - 1];
     stage_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[next_list(lb)], d.gstart, d.glist, d.W, S, d.sc,
@@ -1814,7 +1825,8 @@ __global__ void __launch_bounds__(PPB * G) kb_ghost(const SolveDesc* __restrict_
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);
-    const int sb = d.sb ^ ps, lb = (d.lb + pl) % kLists;
+    int sb, lb;
+    batch_parity(M, d, ps, pl, sb, lb);
     ghost_body<NB, G, WQ>(d.P, d.F[sb], d.L[lb], d.gstart, d.glist, d.V, d.VT, d.ntx,
                           zero_other ? d.L[prev_list(lb)].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
 }
@@ -1824,7 +1836,8 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(con
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
     const SolveDesc& d = load_desc(D, m.x, sd);
-    const int sb = d.sb ^ ps, lb = (d.lb + pl) % kLists;
+    int sb, lb;
+    batch_parity(M, d, ps, pl, sb, lb);
     pst_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[next_list(lb)], d.gstart, d.glist, d.W, d.sc,
                            d.ntx, m.y);
 }
@@ -1878,6 +1891,10 @@ __device__ __forceinline__ void epilogue_body(double threshold, Scalars* sc) {
 }
 
 static __global__ void k_epilogue(const Phys P, Scalars* sc) { epilogue_body(P.threshold, sc); }
+
+// End of a batched step: advance the step counter the batched kernels read their buffer
+// parities from (one graph then serves every step).
+static __global__ void kb_advance(int* tstep) { *tstep = (*tstep + 1) % (2 * kLists); }
 
 // Problem-1 epilogue for every solve of a batch (one thread per solve).
 static __global__ void kb_epilogue(const SolveDesc* __restrict__ D, int nsolve) {

@@ -152,7 +152,8 @@ def test_one_launch_per_phase_for_many_members():
             bt.add(s)
         bt.step(2)
         _, launches = bt.last_step_stats()
-    assert launches == 2 * 10   # 16 solves, one RK4 + PST step's 10 kernels each step
+    # 16 solves, the 10 kernels of one RK4 + PST step plus the step-counter advance
+    assert launches == 2 * 11
     _same(sims[0], one, "member 0")
 
 
