@@ -160,6 +160,21 @@ Where all_tiles(const lssph_handle* h) { return Where{nullptr, h->ntiles, h->str
 // The mixed-precision kernels exist for 4 lanes per particle only.
 template <int NB, int GG, bool MX>
 void run_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
+    if (h->classical) {   // SPH_MODEL 1 / 2 (FP64 only)
+        if constexpr (!MX) {
+            if (h->preparing) {
+                smem_optin(k_stage_classical<NB, GG, false>);
+                smem_optin(k_stage_classical<NB, GG, true>);
+                return;
+            }
+            auto kern = h->tight ? k_stage_classical<NB, GG, true> : k_stage_classical<NB, GG, false>;
+            launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P,
+                            h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist,
+                            h->W, S, h->sc, h->ntx, w.tiles);
+            h->launch_counter++;
+        }
+        return;
+    }
     if (h->preparing) {
         smem_optin(k_stage<NB, GG, false, MX>);
         smem_optin(k_stage<NB, GG, true, MX>);
@@ -236,6 +251,21 @@ void launch_ghost(lssph_handle* h, int zero_list = -1, int reset_umax = 0) {
 
 template <int NB, int GG, bool MX>
 void run_pst(lssph_handle* h, const Where& w) {
+    if (h->classical) {   // first-order basis, q = 2 (shift_interpolate_mod.f90:43-44)
+        if constexpr (!MX) {
+            if (h->preparing) {
+                smem_optin(k_pst<NB, GG, false, false, 1>);
+                smem_optin(k_pst<NB, GG, true, false, 1>);
+                return;
+            }
+            auto kern = h->tight ? k_pst<NB, GG, true, false, 1> : k_pst<NB, GG, false, false, 1>;
+            launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P,
+                            h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist,
+                            h->W, h->sc, h->ntx, w.tiles);
+            h->launch_counter++;
+        }
+        return;
+    }
     if (h->preparing) {
         smem_optin(k_pst<NB, GG, false, MX>);
         smem_optin(k_pst<NB, GG, true, MX>);
@@ -502,8 +532,11 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (!pin || !ptype || !x || !y || !u || !v || !rho || !pre || !out) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
     *out = nullptr;
     if (check_param(pin, &msg) != LSSPH_OK) return fail(nullptr, LSSPH_E_BAD_PARAM, msg);
-    if (pin->sph_model != 3)
-        return fail(nullptr, LSSPH_E_UNSUPPORTED, "the GPU engine implements SPH_MODEL 3 (2nd-order LS-SPH)");
+    if (pin->sph_model < 1 || pin->sph_model > 3)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED,
+                    "the GPU engine implements SPH_MODEL 1, 2 (classical SPH) and 3 (2nd-order LS-SPH)");
+    if (pin->sph_model != 3 && pin->precision == LSSPH_PRECISION_MIXED)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs the LS-SPH model (SPH_MODEL 3) only");
     if (pin->precision != LSSPH_PRECISION_FP64 && pin->precision != LSSPH_PRECISION_MIXED)
         return fail(nullptr, LSSPH_E_BAD_PARAM, "precision must be LSSPH_PRECISION_FP64 or LSSPH_PRECISION_MIXED");
     if (pin->precision == LSSPH_PRECISION_MIXED && pin->lanes != 0 && pin->lanes != 4)
@@ -528,6 +561,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->nb_ghost = h->p1 ? 1 : (h->has_tem ? 4 : 3);
     h->wq = h->p.wall_model == 1 ? 1 : (h->p.wall_model == 3 ? 6 : 3);
     h->mixed = h->p.precision == LSSPH_PRECISION_MIXED;
+    h->classical = h->p.sph_model <= 2;
     h->pdl = pdl_enabled();
     {
         int least = 0, greatest = 0;
@@ -549,6 +583,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     const lssph_params& p = h->p;
     Phys& P = h->P;
     P.problem = p.target_problem; P.kt = p.kernel_type; P.rk = p.rk; P.wall_model = p.wall_model;
+    P.sph_model = p.sph_model;
     P.u_bc_top = p.u_bc_top; P.u_bc_bottom = p.u_bc_bottom; P.u_bc_left = p.u_bc_left; P.u_bc_right = p.u_bc_right;
     P.tem_bc_top = p.tem_bc_top; P.tem_bc_bottom = p.tem_bc_bottom; P.tem_bc_left = p.tem_bc_left;
     P.tem_bc_right = p.tem_bc_right;

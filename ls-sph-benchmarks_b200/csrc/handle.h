@@ -20,6 +20,7 @@ struct lssph_handle {
     int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
     int G = 4, Gg = 4;
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
+    bool classical = false;             // SPH_MODEL 1 / 2: kernel-gradient sums, q = 2 PST basis
     bool pdl = true;                    // programmatic dependent launches in the time step
     bool tuned = false;                 // register budget measured (first solo launch)
     bool tight = false;                 // register budget of stage/PST kernels (autotuned)

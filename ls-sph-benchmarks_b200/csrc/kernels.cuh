@@ -63,7 +63,7 @@ struct Phys {
     int u_bc_top, u_bc_bottom, u_bc_left, u_bc_right;
     int tem_bc_top, tem_bc_bottom, tem_bc_left, tem_bc_right;
     int nx, ny, ncell, cap;
-    int num_total, num_int, num_ext, pad;
+    int num_total, num_int, num_ext, sph_model;
     double u_top, tem_top, tem_bottom, tem_left, tem_right;
     double h, ih1, ih2A, ih2B, h_eff_sq, inv_h_eff, SP_mass, W_ave, wnorm, dt;
     double c_sq, rho_ref, vis_ref, delta, zeta_sq, xi_sq, alpha_ref, gravity, tem_ave;
@@ -818,10 +818,11 @@ __device__ __forceinline__ int tile_pairs(const TileHdr& T, const SmemView& S, b
 
 // Accumulate the LS type-A moment matrix (upper triangle) and b vectors of one pair
 // (LSSPH_A_mod.f90:136-190), df[c] = f_j - f_i.
-template <int NB, class R>
-__device__ __forceinline__ void accumulate_A(R (&Mu)[15], R (&B)[NB][5], R VW, const R (&a)[5], const R (&df)[NB]) {
+template <int NB, class R, int Q>
+__device__ __forceinline__ void accumulate_A(R (&Mu)[Q * (Q + 1) / 2], R (&B)[NB][Q], R VW, const R (&a)[Q],
+                                             const R (&df)[NB]) {
 #pragma unroll
-    for (int ii = 0; ii < 5; ++ii) {
+    for (int ii = 0; ii < Q; ++ii) {
         const R VWa = VW * a[ii];
 #pragma unroll
         for (int c = 0; c < NB; ++c) B[c][ii] = fma(VWa, df[c], B[c][ii]);
@@ -839,7 +840,16 @@ __device__ __forceinline__ void basis_A(R ih1, R ih2A, R x, R y, R (&a)[5]) {
     a[4] = (x * y) * ih2A;
 }
 
-__device__ __forceinline__ void basis_A(const Phys& P, double x, double y, double (&a)[5]) {
+// First-order basis [x/h, y/h] (order k = 1, q = 2: the PST interpolation of the classical
+// SPH models, shift_interpolate_mod.f90:43-54).
+template <class R>
+__device__ __forceinline__ void basis_A(R ih1, R, R x, R y, R (&a)[2]) {
+    a[0] = x * ih1;
+    a[1] = y * ih1;
+}
+
+template <int Q>
+__device__ __forceinline__ void basis_A(const Phys& P, double x, double y, double (&a)[Q]) {
     basis_A<double>(P.ih1, P.ih2A, x, y, a);
 }
 
@@ -875,15 +885,12 @@ __device__ __forceinline__ void group_reduce_to(const R (&v)[N], double (&out)[N
 // k_stage: LS-SPH type-A RHS (q = 5, SPH_MODEL 3) + RK stage update + cell scatter.
 // NB = number of b-vector columns: 1 (problem 1: u only), 4 (u,v,rho,p), 5 (+T).
 // =======================================================================================
-// Lane-0 tail of k_stage: RHS, stage update, scatter.  d[c][k] are the derivatives of
-// field c.  Returns this particle's value for the U_max / steady-state max reductions.
+// Right-hand sides of the governing equations from the LS derivatives (LSSPH_A_mod.f90:
+// 246-269); d[c][k] are the derivatives of field c (entries x, y, xx, yy, xy).
 template <int NB>
-__device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, const Lst& Ln,
-                                               const int* __restrict__ gstart, const Work& W, const StageCfg& S,
-                                               Scalars* sc, int i, double my_x, double my_y, double my_u,
-                                               double my_v, double my_rho, double my_tem, const double (&d)[NB][5]) {
-    // ---- RHS (LSSPH_A_mod.f90:246-269) ----
-    double Ru, Rv = 0.0, Rr = 0.0, Rt = 0.0;
+__device__ __forceinline__ void rhs_ls(const Phys& P, const Work& W, int i, double my_rho, double my_tem,
+                                       const double (&d)[NB][5], double& Ru, double& Rv, double& Rr, double& Rt) {
+    Rv = 0.0; Rr = 0.0; Rt = 0.0;
     if constexpr (NB == 1) {
         Ru = (d[0][2] + d[0][3]) + W.src[i];
     } else {
@@ -900,6 +907,16 @@ __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, co
             Rt = P.thermal_dif * (d[NB - 1][2] + d[NB - 1][3]);
         }
     }
+}
+
+// Tail of a stage: keep the RHS, RK stage update, EOS, scatter into the next cell list.
+// Returns this particle's value for the U_max / steady-state max reductions.
+template <int NB>
+__device__ __forceinline__ double stage_advance(const Phys& P, const Fld& nxt, const Lst& Ln,
+                                                const int* __restrict__ gstart, const Work& W, const StageCfg& S,
+                                                Scalars* sc, int i, double my_x, double my_y, double my_u,
+                                                double my_v, double my_rho, double my_tem, double Ru, double Rv,
+                                                double Rr, double Rt) {
     if (S.write_rhs) {
         W.rhs_u[i] = Ru;
         if constexpr (NB >= 4) { W.rhs_v[i] = Rv; W.rhs_rho[i] = Rr; }
@@ -989,6 +1006,17 @@ __device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, co
         W.f_prev[i] = un;
     }
     return red;
+}
+
+// LS tail of k_stage: RHS from the derivatives, then the stage update.
+template <int NB>
+__device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, const Lst& Ln,
+                                               const int* __restrict__ gstart, const Work& W, const StageCfg& S,
+                                               Scalars* sc, int i, double my_x, double my_y, double my_u,
+                                               double my_v, double my_rho, double my_tem, const double (&d)[NB][5]) {
+    double Ru, Rv, Rr, Rt;
+    rhs_ls<NB>(P, W, i, my_rho, my_tem, d, Ru, Rv, Rr, Rt);
+    return stage_advance<NB>(P, nxt, Ln, gstart, W, S, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem, Ru, Rv, Rr, Rt);
 }
 
 // One tile of one solve (the CTA's work in both the single-solve and the batched kernel).
@@ -1248,6 +1276,128 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
     }
 }
 
+// =======================================================================================
+// Classical SPH (classical_SPH_mod.f90:26-169): SPH_MODEL 1 (sum model for the pressure
+// gradient) and 2 (difference model).  Kernel-gradient sums replace the LS solve:
+//   du_dx = sum gx (u_j - u_i), dv_dy = sum gy (v_j - v_i), dp = sum g (p_j +/- p_i),
+//   L f   = sum 2 V_j dW/r (f_i - f_j)  for f = u, v, rho (, T),
+// with x_ij = x_i - x_j, g = dW x_ij / r V_j.  Same tile staging and two-phase pair loop as
+// the LS kernel; the reduced sums go to the stage update directly.
+// =======================================================================================
+template <int NB>
+__device__ __forceinline__ void rhs_classical(const Phys& P, const Work& W, int i, double my_rho, double my_tem,
+                                              const double* s, double& Ru, double& Rv, double& Rr, double& Rt) {
+    // s: du_dx, dv_dy, dp_dx, dp_dy, Lu, Lv, Lrho (, LT); problem 1: Lu only
+    Rv = 0.0; Rr = 0.0; Rt = 0.0;
+    if constexpr (NB == 1) {
+        Ru = s[0] + W.src[i];
+    } else {
+        Rr = -(my_rho * (s[0] + s[1])) + P.delta * s[6];
+        Ru = -(s[2] / my_rho) + (P.vis_ref / my_rho) * s[4];
+        Rv = -(s[3] / my_rho) + (P.vis_ref / my_rho) * s[5];
+        Rr = Rr / P.zeta_sq;
+        if constexpr (NB == 5) {
+            Rv = Rv + ((P.alpha_ref * (my_tem - P.tem_ave)) * P.gravity);
+            Ru = Ru / P.xi_sq;
+            Rv = Rv / P.xi_sq;
+            Rt = P.thermal_dif * s[7];
+        }
+    }
+}
+
+template <int NB, int G>
+__device__ __forceinline__ void stage_body_classical(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
+                                                     const Lst& Ln, const int* __restrict__ gstart,
+                                                     const int* __restrict__ glist, const Work& W, const StageCfg& S,
+                                                     Scalars* sc, int ntx, int tile) {
+    pdl_wait();
+    const bool stop = halted(sc);
+    constexpr int NS = (NB == 1) ? 1 : (NB == 5 ? 8 : 7);
+    constexpr int SR = sums_stride(NS);
+    static_assert(SR <= SUMS_MAX, "reduced sums overflow");
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemView SM = smem_view<NB == 5>(smem_raw, P.cap);
+    const int tx = tile % ntx, ty = tile / ntx;
+    stage_halo<false, NB == 5>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    pdl_release();
+    if (stop) return;
+    const int n_own = T.own_off[OC];
+    const int lane = threadIdx.x & (G - 1);
+    const bool sum_model = P.sph_model == 1;
+    for (int ob = 0; ob < n_own; ob += PPB) {
+        {
+            const int slot = (int)threadIdx.x / G;
+            const int o = ob + slot;
+            const bool active = o < n_own;
+            int ki = 0, hc = 0;
+            if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+            const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
+            double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
+            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
+            if constexpr (NB == 5) my_tem = SM.tem[ki];
+            double acc[NS];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) acc[k] = 0.0;
+            tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+                const double x_ij = my_x - SM.x[k], y_ij = my_y - SM.y[k];
+                const double r = sqrt(x_ij * x_ij + y_ij * y_ij);
+                const double dW = dev_dW<double>(P.kt, r, P.ih1, P.m3h, P.m5h, P.wnorm);
+                const double Vj = SM.vol[k];
+                const double L = ((2.0 * Vj) * dW) / r;
+                if constexpr (NB == 1) {
+                    acc[0] = fma(L, my_u - SM.u[k], acc[0]);
+                } else {
+                    const double gx = ((dW * x_ij) / r) * Vj, gy = ((dW * y_ij) / r) * Vj;
+                    acc[0] = fma(gx, SM.u[k] - my_u, acc[0]);
+                    acc[1] = fma(gy, SM.v[k] - my_v, acc[1]);
+                    const double pj = SM.pre[k];
+                    const double dp = sum_model ? pj + my_pre : pj - my_pre;
+                    acc[2] = fma(gx, dp, acc[2]);
+                    acc[3] = fma(gy, dp, acc[3]);
+                    acc[4] = fma(L, my_u - SM.u[k], acc[4]);
+                    acc[5] = fma(L, my_v - SM.v[k], acc[5]);
+                    if constexpr (NB == 5) acc[7] = fma(L, my_tem - SM.tem[k], acc[7]);
+                    acc[6] = fma(L, my_rho - SM.rho[k], acc[6]);
+                }
+            });
+            group_reduce<G>(acc);
+            if (active && lane == 0) {
+                double* sm = SM.sums + slot * SR;
+#pragma unroll
+                for (int k = 0; k < NS; ++k) sm[k] = acc[k];
+            }
+        }
+        __syncthreads();
+        double red = 0.0;
+        const int o = ob + (int)threadIdx.x;
+        if ((int)threadIdx.x < PPB && o < n_own) {
+            const double* sm = SM.sums + threadIdx.x * SR;
+            const int ki = SM.own_k[o];
+            double my_v = 0, my_rho = 0, my_tem = 0;
+            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
+            if constexpr (NB == 5) my_tem = SM.tem[ki];
+            const int i = SM.idx[ki];
+            double Ru, Rv, Rr, Rt;
+            rhs_classical<NB>(P, W, i, my_rho, my_tem, sm, Ru, Rv, Rr, Rt);
+            red = stage_advance<NB>(P, nxt, Ln, gstart, W, S, sc, i, SM.x[ki], SM.y[ki], SM.u[ki], my_v, my_rho,
+                                    my_tem, Ru, Rv, Rr, Rt);
+        }
+        if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
+            warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
+        __syncthreads();
+    }
+}
+
+template <int NB, int G, bool TIGHT = false>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
+    k_stage_classical(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln,
+                      const int* __restrict__ gstart, const int* __restrict__ glist, const Work W, const StageCfg S,
+                      Scalars* sc, int ntx, const int* __restrict__ tiles) {
+    stage_body_classical<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx,
+                                tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
+}
+
 template <int NB, int G, bool MIXED>
 __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                            const int* __restrict__ gstart, const int* __restrict__ glist,
@@ -1469,14 +1619,16 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
 // k_pst: particle shifting (q = 5) + copy-back + EOS + cell scatter.
 // NB = 3 (u,v,rho) or 4 (+T).  umax2 holds max(u^2+v^2) of the state being shifted.
 // =======================================================================================
-template <int NB, int G, bool MIXED>
+// K: order of the Taylor basis (2: q = 5 for SPH_MODEL 3; 1: q = 2 for the classical models).
+template <int NB, int G, bool MIXED, int K = 2>
 __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                          const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
                                          Scalars* sc, int ntx, int tile) {
     pdl_wait();
     const bool stop = halted(sc);   // consumed after staging, so its load overlaps the staging loads
-    constexpr int Q = 5;
-    constexpr int SR = sums_stride(15 + 5 * NB + 3);
+    constexpr int Q = (K == 1) ? 2 : 5;
+    constexpr int QU = Q * (Q + 1) / 2;
+    constexpr int SR = sums_stride(QU + Q * NB + 3);
     static_assert(SR <= SUMS_MAX, "reduced sums overflow");
     __shared__ TileHdr T;
     extern __shared__ double smem_raw[];
@@ -1501,10 +1653,10 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
             if constexpr (NB == 4) my_tem = SM.tem[ki];
             using R = typename std::conditional<MIXED, float, double>::type;
             const PairConst<R> C(P);
-            R Mu[15];
+            R Mu[QU];
             R B[NB][Q];
 #pragma unroll
-            for (int k = 0; k < 15; ++k) Mu[k] = R(0);
+            for (int k = 0; k < QU; ++k) Mu[k] = R(0);
 #pragma unroll
             for (int c = 0; c < NB; ++c)
 #pragma unroll
@@ -1534,7 +1686,7 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
                 if constexpr (NB == 4) df[3] = R(SM.tem[k] - my_tem);
                 accumulate_A<NB, R>(Mu, B, VW, a, df);
             });
-            double Md[15], Bd[NB][Q], sd[2];
+            double Md[QU], Bd[NB][Q], sd[2];
             group_reduce_to<G>(Mu, Md);
 #pragma unroll
             for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
@@ -1542,11 +1694,11 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
-                for (int k = 0; k < 15; ++k) sm[k] = Md[k];
+                for (int k = 0; k < QU; ++k) sm[k] = Md[k];
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) sm[15 + 5 * c + k] = Bd[c][k];
+                    for (int k = 0; k < Q; ++k) sm[QU + Q * c + k] = Bd[c][k];
                 sm[SR - 3] = sd[0];
                 sm[SR - 2] = sd[1];
                 sm[SR - 1] = (double)cnt;
@@ -1575,7 +1727,7 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) B[c][k] = sm[15 + 5 * c + k];
+                    for (int k = 0; k < Q; ++k) B[c][k] = sm[QU + Q * c + k];
                 if (cnt >= Q) {
                     if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
                 } else {
@@ -1745,19 +1897,20 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
     }
 }
 
-template <int NB, int G, bool MIXED>
+template <int NB, int G, bool MIXED, int K = 2>
 __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                          const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
                                          Scalars* sc, int ntx, int tile) {
+    static_assert(!(MIXED && K != 2), "mixed precision runs the q = 5 basis only");
     if constexpr (MIXED) pst_body_mx<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
-    else pst_body_fp64<NB, G, false>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
+    else pst_body_fp64<NB, G, false, K>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
 }
 
-template <int NB, int G, bool TIGHT = false, bool MIXED = false>
+template <int NB, int G, bool TIGHT = false, bool MIXED = false, int K = 2>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
           const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
-    pst_body<NB, G, MIXED>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
+    pst_body<NB, G, MIXED, K>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
 // =======================================================================================

@@ -75,6 +75,8 @@ class ServerStats:
     host_create_s: float = 0.0
     wait_s: float = 0.0
     host_retire_s: float = 0.0
+    max_queue: int = 0               # most requests waiting for admission at one scheduling point
+    mean_queue: float = 0.0          # waiting requests averaged over scheduling points
     latencies_s: list = field(default_factory=list)
 
 
@@ -103,6 +105,7 @@ class Server:
         self.wait_s = 0.0            # waiting for batch calls after the set-up work
         self.host_retire_s = 0.0     # downloading results, freeing solves
         self.batch_calls = 0
+        self.queue_samples: list[int] = []
         self.peak_active = 0
         self.particle_steps = 0
 
@@ -209,6 +212,7 @@ class Server:
             if not self.active and pending and not any(r.arrival <= self.now() for r in self.waiting):
                 time.sleep(max(0.0, min(pending[0].arrival - self.now(), 0.05)))
                 continue
+            self.queue_samples.append(len(self.waiting))
             self.step_once()
         return self.stats()
 
@@ -222,6 +226,8 @@ class Server:
                            particle_updates_per_s=self.particle_steps / span if span > 0 else math.nan,
                            device_ms=self.device_ms, max_active=self.peak_active, batch_calls=self.batch_calls,
                            host_create_s=self.host_create_s, wait_s=self.wait_s, host_retire_s=self.host_retire_s,
+                           max_queue=max(self.queue_samples, default=0),
+                           mean_queue=float(np.mean(self.queue_samples)) if self.queue_samples else 0.0,
                            latencies_s=lat)
 
     def close(self) -> None:

@@ -1,0 +1,123 @@
+"""Operator variants on the GPU against the oracle (needs a B200).
+
+Covers the options beside the default LS-SPH q = 5 / Wendland C2 / LS-B q = 3 path:
+  * SPH_MODEL 1 and 2: classical SPH (classical_SPH_mod.f90:26-169), with the q = 2 PST
+    interpolation (shift_interpolate_mod.f90:43-44);
+  * KERNEL_TYPE 1, 2, 4, 5: cubic spline, quintic spline (h_eff = 3h), Wendland C4, C6
+    (kernel_functions_mod.f90:26-146);
+  * WALL_MODEL 1 and 3: CSPH ghost interpolation and LS-B with q = 6
+    (interpolate_CSPH_mod.f90, interpolate_LSSPH_B_mod.f90).
+
+Tolerances as in the default-path parity tests: lanes = 1 bit-identical to the oracle;
+lanes = 4 within a relative 1e-12 of the field scale for one RHS evaluation and relative
+L2 1e-10 after whole steps.
+"""
+import numpy as np
+import pytest
+
+import lssph
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("x", "y", "u", "v", "rho", "pre")
+
+
+def _pair(p, lanes, amp=0.1, seed=0):
+    q = lssph.make_params(p, lanes=lanes)
+    st, ni = lssph.setup_particles(q)
+    rng = np.random.default_rng(seed)
+    if q.target_problem != 1:
+        st.x[:ni] += amp * q.dx * (2 * rng.random(ni) - 1)
+        st.y[:ni] += amp * q.dx * (2 * rng.random(ni) - 1)
+    sim = lssph.Simulation(q, st, ni)
+    sim.ghost()
+    orc = O.Oracle(q, st, ni, ghost=True)
+    return sim, orc
+
+
+def _rel_l2(a, b):
+    d = np.linalg.norm(a - b)
+    s = np.linalg.norm(b)
+    return d / s if s > 0 else d
+
+
+BASE = {
+    "diffusion": lambda **kw: lssph.diffusion_params(num=40, seed=1, **kw),
+    "taylor_green": lambda **kw: lssph.taylor_green_params(num=48, **kw),
+    "cavity": lambda **kw: lssph.cavity_params(num=40, **kw),
+    "boussinesq": lambda **kw: lssph.boussinesq_params(num=40, ra=1e5, **kw),
+}
+
+VARIANTS = (
+    [(case, {"SPH_MODEL": m}) for case in BASE for m in (1, 2)]
+    + [(case, {"KERNEL_TYPE": kt}) for case in ("taylor_green", "cavity") for kt in (1, 2, 4, 5)]
+    + [("diffusion", {"KERNEL_TYPE": 2})]
+    + [(case, {"WALL_MODEL": wm}) for case in ("cavity", "boussinesq", "diffusion") for wm in (1, 3)]
+    + [("cavity", {"SPH_MODEL": 1, "KERNEL_TYPE": 1, "WALL_MODEL": 1})]
+)
+
+
+def _ids(v):
+    case, kw = v
+    return case + "-" + "-".join(f"{k.lower()}{x}" for k, x in kw.items())
+
+
+def _rhs_keys(p):
+    if p.target_problem == 1:
+        return ("u",)
+    return ("u", "v", "rho") + (("tem",) if p.target_problem == 4 else ())
+
+
+@pytest.mark.parametrize("variant", VARIANTS, ids=_ids)
+def test_variant_single_rhs(variant):
+    case, kw = variant
+    p = BASE[case](**kw)
+    for lanes in (1, 4):
+        sim, orc = _pair(p, lanes=lanes, amp=0.2, seed=4)
+        sim.calculate_rhs()
+        orc.calculate_rhs()
+        rg, ro = sim.rhs(), orc.rhs()
+        for k in _rhs_keys(p):
+            if lanes == 1:
+                assert np.array_equal(rg[k], ro[k]), (k, lanes)
+            else:
+                scale = max(np.abs(ro[k]).max(), 1e-30)
+                assert np.abs(rg[k] - ro[k]).max() <= 1e-12 * scale, (k, lanes)
+        sim.close()
+
+
+@pytest.mark.parametrize("variant", VARIANTS, ids=_ids)
+def test_variant_steps_bit_exact_with_one_lane(variant):
+    case, kw = variant
+    p = BASE[case](**kw)
+    nsteps = 20 if p.target_problem == 1 else 5
+    sim, orc = _pair(p, lanes=1, amp=0.1, seed=5)
+    sim.step(nsteps)
+    orc.run(nsteps)
+    g, o = sim.download(), orc.get()
+    for k in FIELDS + (("tem",) if p.target_problem == 4 else ()):
+        assert np.array_equal(getattr(g, k), o[k]), k
+    sim.close()
+
+
+@pytest.mark.parametrize("variant", VARIANTS, ids=_ids)
+def test_variant_steps_rel_l2(variant):
+    case, kw = variant
+    p = BASE[case](**kw)
+    nsteps = 100 if p.target_problem == 1 else 30
+    sim, orc = _pair(p, lanes=4, amp=0.05, seed=6)
+    sim.step(nsteps)
+    orc.run(nsteps)
+    g, o = sim.download(), orc.get()
+    keys = ("u",) if p.target_problem == 1 else ("u", "v", "pre") + (("tem",) if p.target_problem == 4 else ())
+    for k in keys:
+        assert _rel_l2(getattr(g, k), o[k]) <= 1e-10, k
+    sim.close()
+
+
+def test_classical_rejects_mixed_precision():
+    p = lssph.make_params(lssph.taylor_green_params(num=32, SPH_MODEL=1), precision=lssph.PRECISION_MIXED)
+    st, ni = lssph.setup_particles(p)
+    with pytest.raises(lssph.LssphError):
+        lssph.Simulation(p, st, ni)
