@@ -299,6 +299,43 @@ def bench_mixed(steps: int = 100, acc_steps: int = 500) -> dict:
     return out
 
 
+def bench_variants(steps: int = 50, cpu_seconds: float = 2.0) -> dict:
+    """The other operator variants (SPH_MODEL 1/2 classical SPH, 4/5/6 higher-order LS) on
+    the headline Taylor-Green 128^2 RK4 + PST workload: device particle-updates/s, and
+    the oracle on all host cores over a short sample of the same solve."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    import lssph
+    cores = O.set_threads(os.cpu_count() or 1)
+    out = {"workload": "taylor_green_re100_128x128_rk4_pst_fp64", "steps": steps, "models": {}}
+    for name, kw in (("classical_sum", {"SPH_MODEL": 1}), ("classical_difference", {"SPH_MODEL": 2}),
+                     ("ls_q5", {"SPH_MODEL": 3}), ("ls_q9", {"SPH_MODEL": 4}), ("ls_q14", {"SPH_MODEL": 5}),
+                     ("ls_q20_quintic", {"SPH_MODEL": 6, "KERNEL_TYPE": 2})):
+        p = lssph.taylor_green_params(num=128, **kw)
+        sim = lssph.Simulation.new(p)
+        sim.step(5)
+        sim.step(steps)
+        ms, _ = sim.last_step_stats()
+        row = {"value": sim.num_int * steps / (ms * 1e-3), "us_per_step": 1e3 * ms / steps}
+        sim.close()
+        orc = O.Oracle(p)
+        orc.run(1)
+        n, t0 = 0, time.perf_counter()
+        while n < 200:
+            orc.run(1)
+            n += 1
+            if time.perf_counter() - t0 >= cpu_seconds:
+                break
+        row["cpu_value"] = orc.num_int * n / (time.perf_counter() - t0)
+        row["cpu_steps"] = n
+        row["speedup_vs_cpu"] = row["value"] / row["cpu_value"]
+        out["models"][name] = row
+    out["unit"] = UNIT
+    out["cpu_cores"] = cores
+    return out
+
+
 def batched_mix(seed: int = 4, n: int = 64, precision: int = 0):
     """64 solves: half diffusion, half Taylor-Green; lattice side uniform over
     {32,48,64,96,128,192,256}; Re log-uniform in [50, 1000]; jitter +-0.05 dx."""
@@ -528,6 +565,7 @@ def run_engine(args) -> int:
         extras["mixed"] = bench_mixed()
         extras["batched"] = bench_batched()
         extras["serving"] = bench_serving()
+        extras["variants"] = bench_variants()
 
     if dist:
         dist.barrier()

@@ -16,8 +16,8 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "liblssph.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 
-SOURCES = ["host.cpp", "engine.cu", "batch.cu", "noalloc.cu"]
-HEADERS = ["engine.h", "handle.h", "kernels.cuh"]
+SOURCES = ["host.cpp", "engine.cu", "batch.cu", "noalloc.cu", "highorder.cu"]
+HEADERS = ["engine.h", "handle.h", "kernels.cuh", "kernels_hi.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -432,7 +432,8 @@ int lssph_batch_add(lssph_batch* b, lssph_handle* h) {
     if (!b || !h) return bfail(b, LSSPH_E_BAD_PARAM, "null argument");
     if (h->batch) return bfail(b, LSSPH_E_BAD_PARAM, "the handle is already a member of a batch");
     if (b->in_flight) return bfail(b, LSSPH_E_BAD_PARAM, "a batch step call is in flight");
-    if (h->classical) return bfail(b, LSSPH_E_UNSUPPORTED, "batched solves run the LS-SPH model (SPH_MODEL 3) only");
+    if (h->p.sph_model != 3)
+        return bfail(b, LSSPH_E_UNSUPPORTED, "batched solves run the 2nd-order LS-SPH model (SPH_MODEL 3) only");
     b->members.push_back(h);
     h->batch = b;
     b->dirty = true;

@@ -190,6 +190,7 @@ void run_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
 template <int NB>
 void launch_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_STAGE);
+    if (h->order >= 3) { launch_stage_hi(h, S, w.tiles, w.count, w.stream, w.pdl, w.priority); return; }
     if (h->mixed) { run_stage<NB, 4, true>(h, S, w); return; }
     switch (h->G) {
         case 1: run_stage<NB, 1, false>(h, S, w); break;
@@ -281,6 +282,7 @@ void run_pst(lssph_handle* h, const Where& w) {
 template <int NB>
 void launch_pst_t(lssph_handle* h, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_PST);
+    if (h->order >= 3) { launch_pst_hi(h, w.tiles, w.count, w.stream, w.pdl, w.priority); return; }
     if (h->mixed) { run_pst<NB, 4, true>(h, w); return; }
     switch (h->G) {
         case 1: run_pst<NB, 1, false>(h, w); break;
@@ -532,9 +534,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (!pin || !ptype || !x || !y || !u || !v || !rho || !pre || !out) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
     *out = nullptr;
     if (check_param(pin, &msg) != LSSPH_OK) return fail(nullptr, LSSPH_E_BAD_PARAM, msg);
-    if (pin->sph_model < 1 || pin->sph_model > 3)
-        return fail(nullptr, LSSPH_E_UNSUPPORTED,
-                    "the GPU engine implements SPH_MODEL 1, 2 (classical SPH) and 3 (2nd-order LS-SPH)");
+    if (pin->sph_model < 1 || pin->sph_model > 6)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED, "SPH_MODEL must be between 1 and 6");
     if (pin->sph_model != 3 && pin->precision == LSSPH_PRECISION_MIXED)
         return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs the LS-SPH model (SPH_MODEL 3) only");
     if (pin->precision != LSSPH_PRECISION_FP64 && pin->precision != LSSPH_PRECISION_MIXED)
@@ -562,6 +563,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->wq = h->p.wall_model == 1 ? 1 : (h->p.wall_model == 3 ? 6 : 3);
     h->mixed = h->p.precision == LSSPH_PRECISION_MIXED;
     h->classical = h->p.sph_model <= 2;
+    h->order = h->p.sph_model >= 4 ? h->p.sph_model - 1 : 2;   // LSSPH_A_mod.f90:46-56
     h->pdl = pdl_enabled();
     {
         int least = 0, greatest = 0;

@@ -21,6 +21,7 @@ struct lssph_handle {
     int G = 4, Gg = 4;
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
     bool classical = false;             // SPH_MODEL 1 / 2: kernel-gradient sums, q = 2 PST basis
+    int order = 2;                      // Taylor order k of the LS basis (SPH_MODEL 3: 2; 4 / 5 / 6: 3 / 4 / 5)
     bool pdl = true;                    // programmatic dependent launches in the time step
     bool tuned = false;                 // register budget measured (first solo launch)
     bool tight = false;                 // register budget of stage/PST kernels (autotuned)
@@ -111,4 +112,11 @@ bool pdl_enabled();
 
 // Drop a handle that is being destroyed from the batch that holds it (batch.cu).
 void batch_forget(lssph_batch* b, lssph_handle* h);
+
+// Higher-order LS stage and PST launches, SPH_MODEL 4 / 5 / 6 (highorder.cu).  tiles:
+// tile of each CTA (NULL: CTA i runs tile i); while h->preparing they only set the
+// kernels' shared-memory attributes.
+void launch_stage_hi(lssph_handle* h, const StageCfg& S, const int* tiles, int count, cudaStream_t stream, bool pdl,
+                     int priority);
+void launch_pst_hi(lssph_handle* h, const int* tiles, int count, cudaStream_t stream, bool pdl, int priority);
 }  // namespace lssph

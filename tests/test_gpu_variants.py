@@ -116,6 +116,83 @@ def test_variant_steps_rel_l2(variant):
     sim.close()
 
 
+# Higher-order LS (SPH_MODEL 4 / 5 / 6; q = 9 / 14 / 20).  Every accumulator entry is the
+# oracle's fma chain over the hits in reference order and the GEPP runs the oracle's
+# operations row-parallel, so the stage and PST kernels are bit-identical to the oracle
+# whatever the lane setting; with lanes = 4 only the ghost values (LS-B, lane-split sums)
+# differ in the last bits, so those runs are checked to tolerance.  q = 20 needs more than
+# the ~20 neighbours of h = 1.2 dx with Wendland C2 to stay stable (the oracle blows up
+# there too), so model 6 runs with the quintic spline (h_eff = 3h, ~36 neighbours); one
+# single-RHS case keeps the marginal default, bit-exact only (its conditioning amplifies
+# last-bit ghost differences).
+HI_VARIANTS = (
+    [(case, {"SPH_MODEL": m}) for case in BASE for m in (4, 5)]
+    + [(case, {"SPH_MODEL": 6, "KERNEL_TYPE": 2}) for case in BASE]
+    + [("cavity", {"SPH_MODEL": 4, "WALL_MODEL": 3}), ("taylor_green", {"SPH_MODEL": 5, "KERNEL_TYPE": 4})]
+)
+
+
+@pytest.mark.parametrize("variant", HI_VARIANTS + [("cavity", {"SPH_MODEL": 6})], ids=_ids)
+def test_high_order_single_rhs(variant):
+    case, kw = variant
+    p = BASE[case](**kw)
+    marginal = kw.get("SPH_MODEL") == 6 and kw.get("KERNEL_TYPE", 3) != 2
+    for lanes in ((1,) if marginal else (1, 4)):
+        sim, orc = _pair(p, lanes=lanes, amp=0.2, seed=7)
+        sim.calculate_rhs()
+        orc.calculate_rhs()
+        rg, ro = sim.rhs(), orc.rhs()
+        for k in _rhs_keys(p):
+            if lanes == 1:
+                assert np.array_equal(rg[k], ro[k]), (k, lanes)
+            else:
+                # q = 9 / 14 systems on ~20 neighbours are less well conditioned than
+                # q = 5: last-bit ghost differences come out up to ~1e-11 of the scale
+                scale = max(np.abs(ro[k]).max(), 1e-30)
+                assert np.abs(rg[k] - ro[k]).max() <= 1e-10 * scale, (k, lanes)
+        sim.close()
+
+
+@pytest.mark.parametrize("variant", HI_VARIANTS, ids=_ids)
+def test_high_order_steps_bit_exact_with_one_lane(variant):
+    case, kw = variant
+    p = BASE[case](**kw)
+    nsteps = 20 if p.target_problem == 1 else 8
+    sim, orc = _pair(p, lanes=1, amp=0.1, seed=8)
+    sim.step(nsteps)
+    orc.run(nsteps)
+    g, o = sim.download(), orc.get()
+    for k in FIELDS + (("tem",) if p.target_problem == 4 else ()):
+        assert np.array_equal(getattr(g, k), o[k]), k
+    sim.close()
+
+
+@pytest.mark.parametrize("variant", HI_VARIANTS, ids=_ids)
+def test_high_order_steps_rel_l2(variant):
+    case, kw = variant
+    p = BASE[case](**kw)
+    nsteps = 100 if p.target_problem == 1 else 30
+    sim, orc = _pair(p, lanes=4, amp=0.05, seed=9)
+    sim.step(nsteps)
+    orc.run(nsteps)
+    g, o = sim.download(), orc.get()
+    keys = ("u",) if p.target_problem == 1 else ("u", "v", "pre") + (("tem",) if p.target_problem == 4 else ())
+    for k in keys:
+        assert _rel_l2(getattr(g, k), o[k]) <= 1e-10, k
+    sim.close()
+
+
+def test_high_order_rejects_batching():
+    p = lssph.taylor_green_params(num=32, SPH_MODEL=4)
+    st, ni = lssph.setup_particles(p)
+    sim = lssph.Simulation(p, st, ni)
+    b = lssph.Batch()
+    with pytest.raises(lssph.LssphError):
+        b.add(sim)
+    b.close()
+    sim.close()
+
+
 def test_classical_rejects_mixed_precision():
     p = lssph.make_params(lssph.taylor_green_params(num=32, SPH_MODEL=1), precision=lssph.PRECISION_MIXED)
     st, ni = lssph.setup_particles(p)
