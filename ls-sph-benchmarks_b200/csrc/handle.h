@@ -22,6 +22,7 @@ struct lssph_handle {
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
     bool classical = false;             // SPH_MODEL 1 / 2: kernel-gradient sums, q = 2 PST basis
     int order = 2;                      // Taylor order k of the LS basis (SPH_MODEL 3: 2; 4 / 5 / 6: 3 / 4 / 5)
+    bool hi_thread = false;             // order >= 3: thread per particle (else warp per particle)
     bool pdl = true;                    // programmatic dependent launches in the time step
     bool tuned = false;                 // register budget measured (first solo launch)
     bool tight = false;                 // register budget of stage/PST kernels (autotuned)

@@ -19,6 +19,19 @@ void hi_optin(Kern kern, bool tem) {
 template <int K, int NB>
 void stage_hi(lssph_handle* h, const StageCfg& S, const int* tiles, int count, cudaStream_t stream, bool pdl,
               int priority) {
+    if (h->hi_thread) {
+        using St = TppShape<K, NB, false>;
+        auto kt = k_stage_tpp<K, NB>;
+        if (h->preparing) {
+            cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tpp_smem_bytes<St>(64, NB == 5));
+            return;
+        }
+        launch_kernel_p(pdl, priority, kt, count, St::NT, tpp_smem_bytes<St>(h->P.cap, NB == 5), stream, h->P,
+                        h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W,
+                        S, h->sc, h->ntx, tiles);
+        h->launch_counter++;
+        return;
+    }
     using Sh = HiShape<K, NB, false>;
     auto kern = k_stage_hi<K, NB>;
     if (h->preparing) { hi_optin<Sh>(kern, NB == 5); return; }
@@ -30,6 +43,19 @@ void stage_hi(lssph_handle* h, const StageCfg& S, const int* tiles, int count, c
 
 template <int K, int NB>
 void pst_hi(lssph_handle* h, const int* tiles, int count, cudaStream_t stream, bool pdl, int priority) {
+    if (h->hi_thread) {
+        using St = TppShape<K, NB, true>;
+        auto kt = k_pst_tpp<K, NB>;
+        if (h->preparing) {
+            cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tpp_smem_bytes<St>(64, NB == 4));
+            return;
+        }
+        launch_kernel_p(pdl, priority, kt, count, St::NT, tpp_smem_bytes<St>(h->P.cap, NB == 4), stream, h->P,
+                        h->F[h->sb], h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W,
+                        h->sc, h->ntx, tiles);
+        h->launch_counter++;
+        return;
+    }
     using Sh = HiShape<K, NB, true>;
     auto kern = k_pst_hi<K, NB>;
     if (h->preparing) { hi_optin<Sh>(kern, NB == 4); return; }

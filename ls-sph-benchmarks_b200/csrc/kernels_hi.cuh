@@ -182,7 +182,7 @@ __device__ __forceinline__ void hi_accumulate(const int* hits, int n, double* wa
         const int m = min(S::CH, n - c0);
         if (lane < m) pair(lane, hits[c0 + lane], U + lane * S::US, V + lane * S::VS);
         __syncwarp();
-#pragma unroll 1
+#pragma unroll 4
         for (int h = 0; h < m; ++h) {
             const double* u = U + h * S::US;
             const double* v = V + h * S::VS;
@@ -243,21 +243,22 @@ __device__ __forceinline__ bool hi_solve(double* wa, const int (&eu)[S::PER], co
         }
         const int p = (isnan(akk) || !(av > akk)) ? k : ai;
         const double apk = __shfl_sync(0xffffffffu, A[k], p);
+        if (apk != 0.0 && p != k) {   // swap rows k and p (all columns and right-hand sides)
+            const int src = lane == k ? p : (lane == p ? k : lane);
+#pragma unroll
+            for (int j = 0; j < Q; ++j) A[j] = __shfl_sync(0xffffffffu, A[j], src);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) B[c] = __shfl_sync(0xffffffffu, B[c], src);
+        }
+        // after the interchange the diagonal is apk; the oracle's scaling reciprocal and
+        // its stored reciprocal pivot are both 1 / A(k,k), one division serves both
+        const double rk = 1.0 / apk;
         if (apk != 0.0) {
-            if (p != k) {   // swap rows k and p (all columns and right-hand sides)
-                const int src = lane == k ? p : (lane == p ? k : lane);
-#pragma unroll
-                for (int j = 0; j < Q; ++j) A[j] = __shfl_sync(0xffffffffu, A[j], src);
-#pragma unroll
-                for (int c = 0; c < NB; ++c) B[c] = __shfl_sync(0xffffffffu, B[c], src);
-            }
-            const double rp = 1.0 / __shfl_sync(0xffffffffu, A[k], k);
-            if (lane > k) A[k] = A[k] * rp;
+            if (lane > k) A[k] = A[k] * rk;
         } else {
             ok = false;
         }
-        const double dkk = __shfl_sync(0xffffffffu, A[k], k);
-        if (lane == k) rpiv = 1.0 / dkk;
+        if (lane == k) rpiv = rk;
         // right-looking update of the trailing block: A(i,j) -= A(i,k) A(k,j)
 #pragma unroll
         for (int j = k + 1; j < Q; ++j) {
@@ -265,16 +266,20 @@ __device__ __forceinline__ bool hi_solve(double* wa, const int (&eu)[S::PER], co
             if (lane > k) A[j] = fma(-A[k], akj, A[j]);
         }
     }
-    // forward substitution (unit lower), then back substitution, per right-hand side
+    // forward substitution (unit lower), then back substitution; each right-hand side
+    // gets the oracle's sequence, the NB independent sequences are interleaved
 #pragma unroll
-    for (int c = 0; c < NB; ++c) {
+    for (int k = 0; k < Q; ++k) {
 #pragma unroll
-        for (int k = 0; k < Q; ++k) {
+        for (int c = 0; c < NB; ++c) {
             const double bk = __shfl_sync(0xffffffffu, B[c], k);
             if (lane > k) B[c] = fma(-bk, A[k], B[c]);
         }
+    }
 #pragma unroll
-        for (int k = Q - 1; k >= 0; --k) {
+    for (int k = Q - 1; k >= 0; --k) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
             if (lane == k) B[c] = B[c] * rpiv;
             const double bk = __shfl_sync(0xffffffffu, B[c], k);
             if (lane < k) B[c] = fma(-bk, A[k], B[c]);
@@ -498,6 +503,366 @@ __global__ void __launch_bounds__(32 * HI_WARPS)
     k_pst_hi(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
              const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
     pst_body_hi<K, NB>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
+}
+
+
+// =======================================================================================
+// Thread-per-particle variant.  Each thread owns one particle and a private slot of shared
+// memory holding its moment matrix, right-hand sides and reciprocal pivots (element e of
+// thread t at slot[e * NT + t], so a warp's accesses to one element are conflict-free).
+// The thread runs the oracle's loops verbatim -- accumulation over its hits in reference
+// order, symmetric fill, GEPP, substitutions -- so results are again bit-identical, and a
+// warp advances 32 particles per instruction instead of one.  Hits are found in chunks of
+// HCH per thread (16-bit staged indices), so a particle with many neighbours resumes its
+// candidate scan where the previous chunk stopped.
+// =======================================================================================
+template <int K, int NBV, bool SHIFT>
+struct TppShape {
+    static constexpr int Q = q_of_order(K);
+    static constexpr int NB = NBV;
+    static constexpr int NT = (Q <= 9) ? 64 : 32;      // threads (particles in flight) per CTA
+    static constexpr int SLOT = Q * Q + Q * NBV + Q;   // A (row-major), B (column-major), 1/pivots
+    static constexpr int HCH = 32;                     // hits per chunk
+    static constexpr int EA = 0, EB = Q * Q, ER = Q * Q + Q * NBV;
+};
+
+template <class S>
+__host__ __device__ inline size_t tpp_smem_bytes(int cap, bool tem) {
+    const size_t maxp = (size_t)HC * cap, maxo = (size_t)OC * cap;
+    const size_t hl = (size_t)S::NT * S::HCH * 2;
+    const size_t scratch = maxp * sizeof(int) > hl ? maxp * sizeof(int) : hl;
+    return (size_t)S::NT * S::SLOT * sizeof(double) + maxp * ((tem ? 8 : 7) * sizeof(double) + sizeof(int)) +
+           2 * maxo * sizeof(int) + scratch;
+}
+
+template <class S, bool TEM>
+__device__ __forceinline__ SmemView tpp_smem_view(void* raw, int cap, double*& slots) {
+    SmemView V;
+    const int maxp = HC * cap, maxo = OC * cap;
+    double* d = static_cast<double*>(raw);
+    slots = d;
+    d += S::NT * S::SLOT;
+    V.sums = nullptr;
+    V.x = d; V.y = d + maxp; V.u = d + 2 * maxp; V.v = d + 3 * maxp; V.rho = d + 4 * maxp;
+    V.pre = d + 5 * maxp; V.vol = d + 6 * maxp; V.tem = TEM ? d + 7 * maxp : nullptr;
+    int* q = reinterpret_cast<int*>(d + (TEM ? 8 : 7) * maxp);
+    V.idx = q; V.own_k = q + maxp; V.own_hc = q + maxp + maxo;
+    V.nbr = q + maxp + 2 * maxo;   // staging scratch, then the per-thread hit chunks
+    return V;
+}
+
+// Visit this thread's hits (reference order) in chunks; f(k) per hit.  Returns the count.
+template <class S, class F>
+__device__ __forceinline__ int tpp_pairs(const TileHdr& T, const SmemView& SM, int hc, int self, double mx, double my,
+                                         double h_eff_sq, F&& f) {
+    unsigned short* hl = reinterpret_cast<unsigned short*>(SM.nbr) + threadIdx.x;
+    int row = 0, k = T.off[hc - 1 - HX], total = 0;
+    bool more = true;
+    while (more) {
+        int nh = 0;
+        while (row < 3 && nh < S::HCH) {
+            const int hi = T.off[hc + 2 + (row - 1) * HX];
+            for (; k < hi && nh < S::HCH; ++k) {
+                const double xji = SM.x[k] - mx;
+                const double yji = SM.y[k] - my;
+                if (k != self && !(xji * xji + yji * yji > h_eff_sq)) hl[(nh++) * S::NT] = (unsigned short)k;
+            }
+            if (k >= hi) {
+                ++row;
+                if (row < 3) k = T.off[hc - 1 + (row - 1) * HX];
+            }
+        }
+        more = row < 3;
+#pragma unroll 1
+        for (int t = 0; t < nh; ++t) f((int)hl[t * S::NT]);
+        total += nh;
+    }
+    return total;
+}
+
+#define TA(r, c) sl[(S::EA + (r) * S::Q + (c)) * S::NT]
+#define TB(r, c) sl[(S::EB + (c) * S::Q + (r)) * S::NT]
+#define TR(k) sl[(S::ER + (k)) * S::NT]
+
+// The oracle's GEPP + substitutions on one thread's slot (sl[e * NT] = element e).
+// Returns false on a zero pivot.
+template <class S>
+__device__ __forceinline__ bool tpp_solve(double* sl) {
+    constexpr int Q = S::Q, NB = S::NB;
+    // elimination steps are unrolled for q = 9 only: unrolled q = 14 / 20 code would not
+    // fit the instruction cache
+    constexpr int UK = Q <= 9 ? Q : 1;
+    bool ok = true;
+#pragma unroll UK
+    for (int k = 0; k < Q; ++k) {
+        int p = k;
+        double amax = fabs(TA(k, k));
+#pragma unroll
+        for (int i = k + 1; i < Q; ++i) {
+            const double a = fabs(TA(i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        const double apk = TA(p, k);
+        if (apk != 0.0 && p != k) {
+#pragma unroll
+            for (int c = 0; c < Q; ++c) { const double t = TA(k, c); TA(k, c) = TA(p, c); TA(p, c) = t; }
+#pragma unroll
+            for (int c = 0; c < NB; ++c) { const double t = TB(k, c); TB(k, c) = TB(p, c); TB(p, c) = t; }
+        }
+        // the scaling reciprocal and the stored reciprocal pivot are both 1 / A(k,k)
+        const double rk = 1.0 / apk;
+        if (apk != 0.0) {
+#pragma unroll
+            for (int i = k + 1; i < Q; ++i) TA(i, k) = TA(i, k) * rk;
+        } else {
+            ok = false;
+        }
+        TR(k) = rk;
+#pragma unroll
+        for (int j = k + 1; j < Q; ++j) {
+            const double akj = TA(k, j);
+#pragma unroll
+            for (int i = k + 1; i < Q; ++i) TA(i, j) = fma(-TA(i, k), akj, TA(i, j));
+        }
+    }
+#pragma unroll UK
+    for (int k = 0; k < Q; ++k) {
+        double bk[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) bk[c] = TB(k, c);
+#pragma unroll
+        for (int i = k + 1; i < Q; ++i) {
+            const double aik = TA(i, k);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) TB(i, c) = fma(-bk[c], aik, TB(i, c));
+        }
+    }
+#pragma unroll UK
+    for (int k = Q - 1; k >= 0; --k) {
+        const double rp = TR(k);
+        double bk[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) { bk[c] = TB(k, c) * rp; TB(k, c) = bk[c]; }
+#pragma unroll
+        for (int i = 0; i < k; ++i) {
+            const double aik = TA(i, k);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) TB(i, c) = fma(-bk[c], aik, TB(i, c));
+        }
+    }
+    return ok;
+}
+
+// Zero A and B of a slot.
+template <class S>
+__device__ __forceinline__ void tpp_clear(double* sl) {
+#pragma unroll
+    for (int e = 0; e < S::ER; ++e) sl[e * S::NT] = 0.0;
+}
+
+// Lower triangle of A from its upper triangle (LSSPH_A_mod.f90:203-205).
+template <class S>
+__device__ __forceinline__ void tpp_symmetrize(double* sl) {
+#pragma unroll
+    for (int i = 1; i < S::Q; ++i)
+#pragma unroll
+        for (int j = 0; j < i; ++j) TA(i, j) = TA(j, i);
+}
+
+// One hit's contribution (LSSPH_A_mod.f90:174-188 / shift_interpolate_mod.f90:188-201):
+// b(i, c) += V W a_i df_c, M(j, i) += V W a_i a_j for j <= i.
+template <class S>
+__device__ __forceinline__ void tpp_accumulate(double* sl, double VW, const double (&a)[S::Q], const double (&df)[S::NB]) {
+#pragma unroll
+    for (int i = 0; i < S::Q; ++i) {
+        const double VWa = VW * a[i];
+#pragma unroll
+        for (int c = 0; c < S::NB; ++c) TB(i, c) = fma(VWa, df[c], TB(i, c));
+#pragma unroll
+        for (int j = 0; j <= i; ++j) TA(j, i) = fma(VWa, a[j], TA(j, i));
+    }
+}
+
+template <int K, int NB>
+__device__ __forceinline__ void stage_body_tpp(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
+                                               const Lst& Ln, const int* __restrict__ gstart,
+                                               const int* __restrict__ glist, const Work& W, const StageCfg& Sc,
+                                               Scalars* sc, int ntx, int tile) {
+    using S = TppShape<K, NB, false>;
+    constexpr int Q = S::Q;
+    pdl_wait();
+    const bool stop = halted(sc);
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    double* slots;
+    const SmemView SM = tpp_smem_view<S, NB == 5>(smem_raw, P.cap, slots);
+    const int tx = tile % ntx, ty = tile / ntx;
+    stage_halo<false, NB == 5>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    pdl_release();
+    if (stop) return;
+    const int n_own = T.own_off[OC];
+    double* sl = slots + threadIdx.x;
+    double ih[5];
+    inv_h_powers(P, ih);
+    double red = 0.0;
+#pragma unroll 1
+    for (int o = threadIdx.x; o < n_own; o += S::NT) {
+        const int ki = SM.own_k[o], hc = SM.own_hc[o];
+        const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
+        double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
+        if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
+        if constexpr (NB == 5) my_tem = SM.tem[ki];
+        tpp_clear<S>(sl);
+        const int n = tpp_pairs<S>(T, SM, hc, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+            const double xji = SM.x[k] - my_x, yji = SM.y[k] - my_y;
+            const double r = sqrt(xji * xji + yji * yji);
+            const double Wv = dev_W<double>(P.kt, r, P.ih1, P.wnorm);
+            const double VW = SM.vol[k] * Wv;
+            double a[Q];
+            basis_hi<K>(xji, yji, ih, a);
+            double df[NB];
+            df[0] = SM.u[k] - my_u;
+            if constexpr (NB >= 4) {
+                df[1] = SM.v[k] - my_v;
+                df[2] = SM.rho[k] - my_rho;
+                df[3] = SM.pre[k] - my_pre;
+            }
+            if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
+            tpp_accumulate<S>(sl, VW, a, df);
+        });
+        double d[NB][5];
+        if (n >= Q) {
+            tpp_symmetrize<S>(sl);
+            if (!tpp_solve<S>(sl)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+#pragma unroll
+                for (int m = 0; m < 5; ++m) d[c][m] = TB(m, c) * (m < 2 ? ih[0] : ih[1]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+#pragma unroll
+                for (int m = 0; m < 5; ++m) d[c][m] = 0.0;
+        }
+        const int i = SM.idx[ki];
+        double Ru, Rv, Rr, Rt;
+        rhs_ls<NB>(P, W, i, my_rho, my_tem, d, Ru, Rv, Rr, Rt);
+        red = fmax(red, stage_advance<NB>(P, nxt, Ln, gstart, W, Sc, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem,
+                                          Ru, Rv, Rr, Rt));
+    }
+    if (Sc.mode == MODE_STAGE && Sc.last && (Sc.do_umax || Sc.do_steady))
+        warp_max_atomic(Sc.do_umax ? &sc->umax2 : &sc->dfmax, red);
+}
+
+template <int K, int NB>
+__global__ void __launch_bounds__(TppShape<K, NB, false>::NT)
+    k_stage_tpp(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
+                const int* __restrict__ glist, const Work W, const StageCfg S, Scalars* sc, int ntx,
+                const int* __restrict__ tiles) {
+    stage_body_tpp<K, NB>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
+}
+
+template <int K, int NB>
+__device__ __forceinline__ void pst_body_tpp(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
+                                             const Lst& Ln, const int* __restrict__ gstart,
+                                             const int* __restrict__ glist, const Work& W, Scalars* sc, int ntx,
+                                             int tile) {
+    using S = TppShape<K, NB, true>;
+    constexpr int Q = S::Q;
+    pdl_wait();
+    const bool stop = halted(sc);
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    double* slots;
+    const SmemView SM = tpp_smem_view<S, NB == 4>(smem_raw, P.cap, slots);
+    const int tx = tile % ntx, ty = tile / ntx;
+    stage_halo<false, NB == 4>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    pdl_release();
+    if (stop) return;
+    const int n_own = T.own_off[OC];
+    const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
+    const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
+    double* sl = slots + threadIdx.x;
+    double ih[5];
+    inv_h_powers(P, ih);
+#pragma unroll 1
+    for (int o = threadIdx.x; o < n_own; o += S::NT) {
+        const int ki = SM.own_k[o], hc = SM.own_hc[o];
+        const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
+        double my_tem = 0.0;
+        if constexpr (NB == 4) my_tem = SM.tem[ki];
+        tpp_clear<S>(sl);
+        double sx = 0.0, sy = 0.0;
+        const int n = tpp_pairs<S>(T, SM, hc, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+            const double xji = SM.x[k] - my_x, yji = SM.y[k] - my_y;
+            const double r = sqrt(xji * xji + yji * yji);
+            const double Wv = dev_W<double>(P.kt, r, P.ih1, P.wnorm);
+            const double dWdr = dev_dW<double>(P.kt, r, P.ih1, P.m3h, P.m5h, P.wnorm);
+            const double Vj = SM.vol[k];
+            const double VW = Vj * Wv;
+            const double rinv = 1.0 / r;
+            const double gx = ((dWdr * (-xji)) * rinv) * Vj;
+            const double gy = ((dWdr * (-yji)) * rinv) * Vj;
+            const double t = Wv * P.iWave, t2 = t * t, t4 = t2 * t2;
+            const double fac = 1.0 + 0.2 * t4;
+            sx = fma(fac, gx, sx);
+            sy = fma(fac, gy, sy);
+            double a[Q];
+            basis_hi<K>(xji, yji, ih, a);
+            double df[NB];
+            df[0] = SM.u[k] - my_u;
+            df[1] = SM.v[k] - my_v;
+            df[2] = SM.rho[k] - my_rho;
+            if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
+            tpp_accumulate<S>(sl, VW, a, df);
+        });
+        // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
+        double dx = -coe * sx, dy = -coe * sy;
+        const double rr = sqrt(dx * dx + dy * dy);
+        if (rr > 0.2 * P.h) {
+            dx = ((0.2 * P.h) * dx) / rr;
+            dy = ((0.2 * P.h) * dy) / rr;
+        }
+        double accf[NB];
+        if (n >= Q) {
+            tpp_symmetrize<S>(sl);
+            if (!tpp_solve<S>(sl)) atomicOr(&sc->warn, WARN_SINGULAR);
+            double a[Q];
+            basis_hi<K>(dx, dy, ih, a);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                double s = 0.0;
+#pragma unroll
+                for (int i = 0; i < Q; ++i) s = fma(a[i], TB(i, c), s);
+                accf[c] = s;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < NB; ++c) accf[c] = 0.0;
+        }
+        const int i = SM.idx[ki];
+        const double xn = my_x + dx, yn = my_y + dy;
+        const double un = my_u + accf[0], vn = my_v + accf[1], rn = my_rho + accf[2];
+        nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
+        nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
+        nxt.vol[i] = P.SP_mass / rn;
+        bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
+        if constexpr (NB == 4) { const double tn = my_tem + accf[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
+        if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
+        const int nk = cell_key_mul(P, xn, yn, sc);
+        if (nk >= 0) W.key[i] = nk;
+        scatter_to_cell(P, Ln, gstart, nk, i, sc);
+    }
+}
+#undef TA
+#undef TB
+#undef TR
+
+template <int K, int NB>
+__global__ void __launch_bounds__(TppShape<K, NB, true>::NT)
+    k_pst_tpp(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
+              const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
+    pst_body_tpp<K, NB>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
 }  // namespace lssph
