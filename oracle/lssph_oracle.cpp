@@ -704,6 +704,88 @@ int lssph_b_point(const lssph_params& p, int q, int nb, double my_x, double my_y
     return num_neighbors;
 }
 
+// ---------------------------------------------------------------------------------
+// Post-processing LS type-B interpolation (analysis/common/lssph_b.py:21-143): value and
+// first derivatives of one field at arbitrary points from every particle within h_eff.
+// ---------------------------------------------------------------------------------
+// Basis size of the post-processing interpolation (lssph_b.py:45-55).
+int lsb_post_q(int sph_model, int target_problem) {
+    const bool t4 = target_problem == 4;
+    if (sph_model <= 3) return t4 ? 6 : 3;
+    if (sph_model == 4) return t4 ? 10 : 6;
+    if (sph_model == 5) return t4 ? 15 : 10;
+    return t4 ? 21 : 15;
+}
+
+// Its basis columns on normalised offsets (lssph_b.py:83-125; the q = 6 / 10 orders differ
+// from the q = 15 / 21 ones, as in the reference).
+void lsb_post_basis(int q, double X, double Y, double* a) {
+    a[0] = 1.0;
+    a[1] = X;
+    a[2] = Y;
+    if (q == 3) return;
+    const double X2 = X * X, Y2 = Y * Y;
+    if (q == 6 || q == 10) {
+        a[3] = 0.5 * X2;
+        a[4] = X * Y;
+        a[5] = 0.5 * Y2;
+        if (q == 10) {
+            a[6] = (1.0 / 6.0) * (X2 * X);
+            a[7] = (0.5 * X2) * Y;
+            a[8] = (0.5 * X) * Y2;
+            a[9] = (1.0 / 6.0) * (Y2 * Y);
+        }
+        return;
+    }
+    const double X3 = X2 * X, Y3 = Y2 * Y, X4 = X2 * X2, Y4 = Y2 * Y2;
+    a[3] = 0.5 * X2;
+    a[4] = 0.5 * Y2;
+    a[5] = X * Y;
+    a[6] = (1.0 / 6.0) * X3;
+    a[7] = (1.0 / 6.0) * Y3;
+    a[8] = (0.5 * X2) * Y;
+    a[9] = (0.5 * Y2) * X;
+    a[10] = (1.0 / 24.0) * X4;
+    a[11] = (1.0 / 24.0) * Y4;
+    a[12] = ((1.0 / 6.0) * X3) * Y;
+    a[13] = ((1.0 / 6.0) * Y3) * X;
+    a[14] = (0.25 * X2) * Y2;
+    if (q == 15) return;
+    a[15] = (1.0 / 120.0) * (X4 * X);
+    a[16] = (1.0 / 120.0) * (Y4 * Y);
+    a[17] = ((1.0 / 24.0) * X4) * Y;
+    a[18] = ((1.0 / 24.0) * Y4) * X;
+    a[19] = ((1.0 / 12.0) * X3) * Y2;
+    a[20] = ((1.0 / 12.0) * Y3) * X2;
+}
+
+// One target: neighbours in ascending particle index (the reference's sorted ball query),
+// normal equations M = A^T W A, b = A^T W f with W = diag(W_ij V_j), GEPP.  NaN when fewer
+// than q neighbours or a zero pivot (numpy's LinAlgError).  out = d0, d1 / h, d2 / h.
+void lsb_post_point(const lssph_params& p, int q, double tx, double ty, const std::vector<int>& nbrs,
+                    const double* X, const double* Y, const double* val, const double* rho, double* out) {
+    const double h = p.h;
+    if ((int)nbrs.size() < q) { out[0] = out[1] = out[2] = NAN; return; }
+    double M[441] = {0}, b[21] = {0}, a[21];
+    for (int j : nbrs) {
+        const double dx = X[j] - tx, dy = Y[j] - ty;
+        const double r = std::sqrt(dx * dx + dy * dy);
+        const double w = cal_W(p.kernel_type, r, h) * (p.SP_mass / rho[j]);
+        lsb_post_basis(q, dx / h, dy / h, a);
+        for (int i = 0; i < q; ++i) {
+            const double wa = w * a[i];
+            b[i] = std::fma(wa, val[j], b[i]);
+            for (int k = 0; k <= i; ++k) M[k + i * q] = std::fma(wa, a[k], M[k + i * q]);
+        }
+    }
+    for (int i = 0; i < q - 1; ++i)
+        for (int k = i + 1; k < q; ++k) M[k + i * q] = M[i + k * q];
+    if (gepp_solve(q, 1, M, b) != 0) { out[0] = out[1] = out[2] = NAN; return; }
+    out[0] = b[0];
+    out[1] = b[1] / h;
+    out[2] = b[2] / h;
+}
+
 // interpolate_LSSPH_B_mod.f90:24-178 (WALL_MODEL 2: q=3, 3: q=6)
 void interpolate_LSSPH_B(orc_state* s, int me) {
     const lssph_params& p = s->p;
@@ -1199,6 +1281,48 @@ int orc_lssph_b(const lssph_params* p, int q, int n_src, const double* xs, const
         out[t] = o[0];
     }
     return short_count;
+}
+
+// analysis/common/lssph_b.py:21-143 over n_src particles at n_tgt points; out[3 * t + k].
+// The ball query bins the particles into cells of h_eff and sorts each target's hits by
+// index, which gives the same neighbour list as the reference's KD-tree query.
+int orc_lsb_post(const lssph_params* p, int n_src, const double* xs, const double* ys, const double* val,
+                 const double* rho, int n_tgt, const double* xt, const double* yt, double* out) {
+    const int q = lsb_post_q(p->sph_model, p->target_problem);
+    if (n_src <= 0) {
+        for (int t = 0; t < 3 * n_tgt; ++t) out[t] = NAN;
+        return q;
+    }
+    const double he = p->h_eff, he2 = he * he;
+    double x0 = xs[0], y0 = ys[0], x1 = xs[0], y1 = ys[0];
+    for (int j = 1; j < n_src; ++j) {
+        x0 = std::min(x0, xs[j]); x1 = std::max(x1, xs[j]);
+        y0 = std::min(y0, ys[j]); y1 = std::max(y1, ys[j]);
+    }
+    const int ncx = (int)std::floor((x1 - x0) / he) + 1, ncy = (int)std::floor((y1 - y0) / he) + 1;
+    std::vector<std::vector<int>> cells((size_t)ncx * ncy);
+    for (int j = 0; j < n_src; ++j) {
+        const int cx = std::min(ncx - 1, (int)std::floor((xs[j] - x0) / he));
+        const int cy = std::min(ncy - 1, (int)std::floor((ys[j] - y0) / he));
+        cells[(size_t)cy * ncx + cx].push_back(j);
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int t = 0; t < n_tgt; ++t) {
+        std::vector<int> nb;
+        const double fx = std::floor((xt[t] - x0) / he), fy = std::floor((yt[t] - y0) / he);
+        if (fx >= -1.0 && fx <= ncx && fy >= -1.0 && fy <= ncy) {
+            const int cx = (int)fx, cy = (int)fy;
+            for (int yy = std::max(cy - 1, 0); yy <= std::min(cy + 1, ncy - 1); ++yy)
+                for (int xx = std::max(cx - 1, 0); xx <= std::min(cx + 1, ncx - 1); ++xx)
+                    for (int j : cells[(size_t)yy * ncx + xx]) {
+                        const double dx = xs[j] - xt[t], dy = ys[j] - yt[t];
+                        if (dx * dx + dy * dy <= he2) nb.push_back(j);
+                    }
+        }
+        std::sort(nb.begin(), nb.end());
+        lsb_post_point(*p, q, xt[t], yt[t], nb, xs, ys, val, rho, out + 3 * t);
+    }
+    return q;
 }
 
 int orc_calculate_rhs(orc_state* s) { calculate_RHS(s); return s->error; }

@@ -48,6 +48,7 @@ _PROTOS = {
     "orc_run": (C.c_int, [_S, C.c_int, _i]),
     "orc_neighbors_csr": (C.c_int64, [_S, C.c_int, _i, _i, C.c_int64]),
     "orc_lssph_b": (C.c_int, [C.POINTER(Params), C.c_int, C.c_int, _d, _d, _d, _d, C.c_int, _d, _d, _d]),
+    "orc_lsb_post": (C.c_int, [C.POINTER(Params), C.c_int, _d, _d, _d, _d, C.c_int, _d, _d, _d]),
 }
 
 _lib = None
@@ -111,6 +112,16 @@ def lssph_b(p: Params, q: int, xs, ys, rho, val, xt, yt) -> np.ndarray:
     out = np.zeros(xt.shape[0])
     load().orc_lssph_b(C.byref(p), q, xs.shape[0], _dp(xs), _dp(ys), _dp(rho), _dp(val), xt.shape[0], _dp(xt),
                        _dp(yt), _dp(out))
+    return out
+
+
+def lsb_post(p: Params, xt, yt, xs, ys, val, rho) -> np.ndarray:
+    """analysis/common/lssph_b.py main(): (n_targets, 3) = value, d/dx, d/dy (NaN where
+    fewer than q particles lie within h_eff or the system is singular)."""
+    xs, ys, val, rho, xt, yt = (np.ascontiguousarray(a, dtype=np.float64) for a in (xs, ys, val, rho, xt, yt))
+    out = np.zeros((xt.shape[0], 3))
+    load().orc_lsb_post(C.byref(p), xs.shape[0], _dp(xs), _dp(ys), _dp(val), _dp(rho), xt.shape[0], _dp(xt),
+                        _dp(yt), out.ctypes.data_as(_d))
     return out
 
 

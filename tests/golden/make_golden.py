@@ -13,6 +13,10 @@ The fixtures it writes are committed; the tests read only the .npz files.
                 points over a seeded jittered particle cloud, from lssph_b.main
                 (analysis/common/lssph_b.py:21-143), the interpolation the reference
                 uses for its virtual markers (interpolate_LSSPH_B_mod.f90)
+  lssph_b_post.npz  the full post-processing output of lssph_b.main (value, d/dx, d/dy)
+                for every basis size it supports (q = 3, 6, 10, 15, 21: SPH_MODEL x
+                TARGET_PROBLEM), several kernels, over a jittered cloud, with targets
+                inside, on the edge of and outside the cloud
 """
 import os
 import sys
@@ -54,7 +58,32 @@ def main(ref_root: str) -> None:
         out[f"q{q}"] = res[:, 0]
     np.savez(os.path.join(HERE, "lssph_b.npz"), xs=xs, ys=ys, rho=rho, val=val, xt=xt, yt=yt, dx=np.array(dx),
              q3=out["q3"], q6=out["q6"])
-    print("wrote", os.path.join(HERE, "kernels.npz"), os.path.join(HERE, "lssph_b.npz"))
+    # ---- post-processing LS type B, every basis size -------------------------------------
+    rng = np.random.default_rng(20261204)
+    n = 20
+    gx, gy = np.meshgrid((np.arange(n) + 0.5) * dx, (np.arange(n) + 0.5) * dx)
+    xs = gx.ravel() + 0.2 * dx * (2 * rng.random(n * n) - 1)
+    ys = gy.ravel() + 0.2 * dx * (2 * rng.random(n * n) - 1)
+    rho = 1.0 + 0.02 * np.sin(3.0 * xs) * np.cos(2.0 * ys)
+    val = np.sin(2.0 * np.pi * xs) * np.cos(np.pi * ys) + 0.3 * xs * ys
+    L = n * dx
+    xt = np.concatenate([0.1 * L + 0.8 * L * rng.random(24), [0.0, L, 0.5 * L, -0.2 * L, 0.5 * L],
+                         np.linspace(0.0, L, 8)])
+    yt = np.concatenate([0.1 * L + 0.8 * L * rng.random(24), [0.5 * L, 0.5 * L, 0.0, 0.5 * L, 1.3 * L],
+                         np.full(8, 0.5 * L)])
+    cases = []
+    # (target_problem, sph_model, kernel_type, h / dx, h_eff / h)
+    for tp, sm, kt, ch, he in ((2, 3, 3, 1.2, 2.0), (4, 3, 3, 1.2, 2.0), (2, 4, 1, 1.5, 2.0), (4, 4, 4, 1.5, 2.0),
+                               (2, 5, 5, 2.0, 2.0), (4, 5, 2, 1.2, 3.0), (2, 6, 2, 1.4, 3.0), (4, 6, 3, 2.2, 2.0)):
+        h = ch * dx
+        param = SimpleNamespace(h_eff=he * h, h=h, target_problem=tp, kernel_type=kt, sph_model=sm,
+                                SP_mass=1.0 * dx * dx)
+        cases.append([tp, sm, kt, h, he * h])
+        out[f"case{len(cases) - 1}"] = lssph_b.main(param, xt, yt, xs, ys, val, rho)
+    np.savez(os.path.join(HERE, "lssph_b_post.npz"), xs=xs, ys=ys, rho=rho, val=val, xt=xt, yt=yt,
+             dx=np.array(dx), cases=np.array(cases), **{k: v for k, v in out.items() if k.startswith("case")})
+    print("wrote", os.path.join(HERE, "kernels.npz"), os.path.join(HERE, "lssph_b.npz"),
+          os.path.join(HERE, "lssph_b_post.npz"))
 
 
 if __name__ == "__main__":
