@@ -357,6 +357,63 @@ def bench_variants(steps: int = 50, cpu_seconds: float = 2.0) -> dict:
     return out
 
 
+def bench_postproc(reps: int = 5) -> dict:
+    """Post-processing LS type-B interpolation (analysis/common/lssph_b.py): points/s through
+    the C ABI with host arrays (lsb_interpolate, what the analysis scripts would call on a
+    .dat snapshot) and from the device-resident state (Simulation.interpolate), against the
+    oracle's restatement on all host cores."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    import lssph
+    cores = O.set_threads(os.cpu_count() or 1)
+    out = {"unit": "points/s", "cpu_cores": cores, "cases": {}}
+    for name, p, field, grid in (
+            ("cavity_256_centre_profiles_q3", lssph.cavity_params(num=256), "u", False),
+            ("cavity_256_full_field_q3", lssph.cavity_params(num=256), "u", True),
+            ("boussinesq_128_wall_gradients_q6", lssph.boussinesq_params(num=128), "tem", False),
+            ("boussinesq_96_q21_quintic", lssph.boussinesq_params(num=96, SPH_MODEL=6, KERNEL_TYPE=2), "tem", False)):
+        sim = lssph.Simulation.new(p)
+        sim.step(5)
+        st = sim.download()
+        L, n = p.len_x, p.num_x
+        s = np.linspace(0.0, L, n)
+        if grid:
+            gx, gy = np.meshgrid((np.arange(n) + 0.5) * (L / n), (np.arange(n) + 0.5) * (L / n))
+            tx, ty = gx.ravel(), gy.ravel()
+        elif field == "tem":
+            tx, ty = np.concatenate([s, s]), np.concatenate([np.zeros(n), np.full(n, L)])
+        else:
+            tx, ty = np.concatenate([np.full(n, 0.5 * L), s]), np.concatenate([s, np.full(n, 0.5 * L)])
+        xs, ys, val = st.x - p.WL_thick, st.y - p.WL_thick, getattr(st, field)
+        lssph.lsb_interpolate(p, tx, ty, xs, ys, val, st.rho)
+        t = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            res = lssph.lsb_interpolate(p, tx, ty, xs, ys, val, st.rho)
+            t.append(time.perf_counter() - t0)
+        td = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            sim.interpolate(field, tx, ty)
+            td.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        ref = O.lsb_post(p, tx, ty, xs, ys, val, st.rho)
+        tc = time.perf_counter() - t0
+        ok = ~np.isnan(ref[:, 0])
+        rel = float((np.abs(res[ok] - ref[ok]).max(axis=0) / np.abs(ref[ok]).max(axis=0)).max()) if ok.any() else 0.0
+        out["cases"][name] = {"points": int(tx.shape[0]), "particles": int(xs.shape[0]),
+                              "gpu_host_arrays_points_per_s": tx.shape[0] / float(np.median(t)),
+                              "gpu_device_state_points_per_s": tx.shape[0] / float(np.median(td)),
+                              "cpu_points_per_s": tx.shape[0] / tc,
+                              "speedup_host_arrays_vs_cpu": tc / float(np.median(t)),
+                              "max_rel_diff_vs_oracle": rel}
+        sim.close()
+    return out
+
+
 def batched_mix(seed: int = 4, n: int = 64, precision: int = 0):
     """64 solves: half diffusion, half Taylor-Green; lattice side uniform over
     {32,48,64,96,128,192,256}; Re log-uniform in [50, 1000]; jitter +-0.05 dx."""
@@ -587,6 +644,7 @@ def run_engine(args) -> int:
         extras["batched"] = bench_batched()
         extras["serving"] = bench_serving()
         extras["variants"] = bench_variants()
+        extras["postproc"] = bench_postproc()
 
     if dist:
         dist.barrier()

@@ -262,6 +262,30 @@ int  lssph_batch_wait(lssph_batch* b, int32_t* status, int32_t* steady, int32_t*
 /* Device time and kernel launches of the last lssph_batch_step (all members). */
 int  lssph_batch_last_step_stats(const lssph_batch* b, double* device_ms, int64_t* kernel_launches);
 
+/* ---- post-processing interpolation (analysis/common/lssph_b.py:21-143) ---------------- */
+/* LS-SPH type-B interpolation of one particle field at arbitrary points, the reference's
+   analysis step `lssph_b.main(param, target_x, target_y, x_j, y_j, val_j, rho_j)`: for each
+   point the value and the derivatives d/dx, d/dy from every particle within h_eff
+   (normal equations with weights W_ij m / rho_j, basis size q = 3 / 6 / 10 / 15 / 21 from
+   SPH_MODEL and TARGET_PROBLEM as in lssph_b.py:45-55).  out receives 3 doubles per point
+   (value, d/dx, d/dy); a point with fewer than q particles in range, or a singular system,
+   gets NaN, as in the reference.  Uses p->h, h_eff, kernel_type, sph_model,
+   target_problem and SP_mass.  Host arrays in and out; the work runs on the GPU. */
+int lssph_lsb_interpolate(const lssph_params* p, int32_t n, const double* x, const double* y,
+                          const double* val, const double* rho, int32_t n_targets,
+                          const double* tx, const double* ty, double* out);
+/* The same on a solve's current device state (all num_total particles, ghosts included,
+   as the analysis scripts read them from a .dat file).  Points are in the physical frame
+   of the analysis scripts: particle positions minus WL_thick, so [0, LEN_X] x [0, LEN_Y]
+   is the fluid box. */
+#define LSSPH_FIELD_U   0
+#define LSSPH_FIELD_V   1
+#define LSSPH_FIELD_RHO 2
+#define LSSPH_FIELD_PRE 3
+#define LSSPH_FIELD_TEM 4
+int lssph_interpolate(lssph_handle* h, int32_t field, int32_t n_targets, const double* tx,
+                      const double* ty, double* out);
+
 /* ---- allocation-free RHS (no counterpart in the reference) ---------------------------- */
 /* One calculate_RHS pass (LS-SPH type A, problems 2-4, FP64) over a particle state that
    already lives in caller-owned device memory, writing the RHS arrays to caller-owned

@@ -6,11 +6,12 @@ from .params import (boussinesq_params, cavity_params, check_param, default_para
 from .simulation import Simulation, State, estimate_device_bytes, read_data, setup_particles
 from .batch import Batch
 from .serving import Request, Server, ServerStats, device_memory
+from .postproc import lsb_interpolate
 
 __all__ = [
     "LIB_PATH", "PRECISION_FP64", "PRECISION_MIXED", "LssphError", "Params", "exported_names", "load",
     "boussinesq_params", "cavity_params", "check_param", "default_params", "diffusion_params",
     "from_config", "init_param", "make_params", "taylor_green_params", "write_config_h",
     "Simulation", "State", "estimate_device_bytes", "read_data", "setup_particles", "Batch",
-    "Request", "Server", "ServerStats", "device_memory",
+    "Request", "Server", "ServerStats", "device_memory", "lsb_interpolate",
 ]

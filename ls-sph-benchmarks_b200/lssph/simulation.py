@@ -213,6 +213,21 @@ class Simulation:
         self._chk(self._lib.lssph_step_profiled(self._h, int(nsteps), ms, nl))
         return {k: (ms[i], nl[i]) for i, k in enumerate(_abi.KIND_NAMES)}
 
+    def interpolate(self, field: str, target_x, target_y) -> np.ndarray:
+        """LS type-B value, d/dx, d/dy of ``field`` ("u", "v", "rho", "pre", "tem") at points
+        of the analysis frame (positions minus WL_thick), from the current device state:
+        the reference's lssph_b.main over a .dat snapshot, without the download."""
+        from .postproc import FIELDS
+        tx = np.ascontiguousarray(target_x, dtype=np.float64).ravel()
+        ty = np.ascontiguousarray(target_y, dtype=np.float64).ravel()
+        if tx.shape != ty.shape:
+            raise ValueError("target_x and target_y must have the same length")
+        out = np.empty((tx.shape[0], 3))
+        dp = C.POINTER(C.c_double)
+        self._chk(self._lib.lssph_interpolate(self._h, FIELDS[field], tx.shape[0], tx.ctypes.data_as(dp),
+                                              ty.ctypes.data_as(dp), out.ctypes.data_as(dp)))
+        return out
+
     def device_bytes(self) -> int:
         """Device memory this solve holds (requested bytes)."""
         n = C.c_int64()
