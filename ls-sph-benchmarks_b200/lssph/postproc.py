@@ -17,10 +17,26 @@ def _d(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def lsb_interpolate(param: Params, target_x, target_y, x_j, y_j, val_j, rho_j) -> np.ndarray:
+_USED = ("h", "h_eff", "kernel_type", "sph_model", "target_problem", "SP_mass")
+
+
+def _as_params(param) -> Params:
+    """A Params as is; any other object (the analysis scripts' SimpleNamespace from
+    read_utils) by the attributes the interpolation reads."""
+    if isinstance(param, Params):
+        return param
+    p = Params()
+    for name in _USED:
+        setattr(p, name, getattr(param, name))
+    return p
+
+
+def lsb_interpolate(param, target_x, target_y, x_j, y_j, val_j, rho_j) -> np.ndarray:
     """Same arguments and result as the reference's ``lssph_b.main``: an (n_targets, 3) array
     of value, d/dx, d/dy, NaN where fewer than q particles lie within h_eff or the system is
-    singular.  ``param`` needs h, h_eff, kernel_type, sph_model, target_problem, SP_mass."""
+    singular.  ``param`` is a Params or any object with h, h_eff, kernel_type, sph_model,
+    target_problem and SP_mass."""
+    param = _as_params(param)
     tx, ty, xs, ys, val, rho = (np.ascontiguousarray(a, dtype=np.float64).ravel()
                                 for a in (target_x, target_y, x_j, y_j, val_j, rho_j))
     if tx.shape != ty.shape or not (xs.shape == ys.shape == val.shape == rho.shape):

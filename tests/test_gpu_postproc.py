@@ -93,6 +93,18 @@ def test_solver_state_matches_oracle(case):
     sim.close()
 
 
+def test_accepts_the_analysis_namespace(golden_dir):
+    # the analysis scripts pass a SimpleNamespace, not a Params
+    from types import SimpleNamespace
+    g = np.load(f"{golden_dir}/lssph_b_post.npz")
+    tp, sm, kt, h, he = g["cases"][1]
+    ns = SimpleNamespace(h=float(h), h_eff=float(he), kernel_type=int(kt), sph_model=int(sm),
+                         target_problem=int(tp), SP_mass=0.02 ** 2)
+    a = lssph.lsb_interpolate(ns, g["xt"], g["yt"], g["xs"], g["ys"], g["val"], g["rho"])
+    b = lssph.lsb_interpolate(post_params(g["cases"][1]), g["xt"], g["yt"], g["xs"], g["ys"], g["val"], g["rho"])
+    assert np.array_equal(a, b, equal_nan=True)
+
+
 def test_empty_inputs():
     p = lssph.taylor_green_params(num=32)
     out = lssph.lsb_interpolate(p, [0.1, 0.2], [0.1, 0.2], [], [], [], [])
