@@ -414,6 +414,39 @@ def bench_postproc(reps: int = 5) -> dict:
     return out
 
 
+def bench_snapshots(steps: int = 200, every: int = 10) -> dict:
+    """Taylor-Green 256^2 RK4 + PST with a data/<step>.dat snapshot every `every` steps:
+    wall time per step without snapshots, with lssph_write_data (download + write, the
+    reference's synchronous write_data) and with lssph_write_data_async."""
+    import shutil
+    import tempfile
+
+    import lssph
+    p = lssph.taylor_green_params(num=256)
+    out = {"workload": f"taylor_green_256x256_rk4_pst_fp64, snapshot every {every} steps", "steps": steps}
+    root = tempfile.mkdtemp(prefix="lssph_snap_")
+    try:
+        for mode in ("none", "sync", "async"):
+            sim = lssph.Simulation.new(p)
+            sim.step(5)
+            t0 = time.perf_counter()
+            for k in range(0, steps, every):
+                sim.step(every)
+                if mode == "sync":
+                    sim.write_data(root, k + every)
+                elif mode == "async":
+                    sim.write_data_async(root, k + every)
+            sim.snapshot_wait()
+            out[f"{mode}_ms_per_step"] = 1e3 * (time.perf_counter() - t0) / steps
+            sim.close()
+        out["snapshot_bytes"] = os.path.getsize(os.path.join(root, p.save_name.decode(), "data", f"{steps}.dat"))
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+    out["async_overhead_vs_none"] = out["async_ms_per_step"] / out["none_ms_per_step"] - 1.0
+    out["sync_overhead_vs_none"] = out["sync_ms_per_step"] / out["none_ms_per_step"] - 1.0
+    return out
+
+
 def batched_mix(seed: int = 4, n: int = 64, precision: int = 0):
     """64 solves: half diffusion, half Taylor-Green; lattice side uniform over
     {32,48,64,96,128,192,256}; Re log-uniform in [50, 1000]; jitter +-0.05 dx."""
@@ -645,6 +678,7 @@ def run_engine(args) -> int:
         extras["serving"] = bench_serving()
         extras["variants"] = bench_variants()
         extras["postproc"] = bench_postproc()
+        extras["snapshots"] = bench_snapshots()
 
     if dist:
         dist.barrier()

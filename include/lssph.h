@@ -194,6 +194,15 @@ int lssph_write_param(lssph_handle* h, const char* results_root, const char* con
 /* parameters.csv alone (write_param_mod.f90:58-128), host only. */
 int lssph_write_parameters(const lssph_params* p, int32_t num_total, int32_t num_int,
                            const char* path);
+/* write_data without stopping the time loop (no counterpart in the reference, which writes
+   synchronously): captures the current state with device-to-device copies on the handle's
+   stream and returns; a copy to pinned host memory and the file write run in the
+   background while later lssph_step calls proceed.  The file is the one lssph_write_data
+   writes for the same state, byte for byte.  A write error is returned by the next call or
+   by lssph_snapshot_wait, which waits for every pending snapshot of the handle;
+   lssph_destroy waits as well. */
+int lssph_write_data_async(lssph_handle* h, const char* results_root, int32_t step);
+int lssph_snapshot_wait(lssph_handle* h);
 /* Restart reader (restart_mod.f90:22-53): fills caller buffers of length num_total. */
 int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32_t* ptype,
                     double* x, double* y, double* u, double* v, double* rho, double* pre,

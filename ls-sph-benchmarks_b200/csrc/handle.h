@@ -11,6 +11,10 @@
 #include "engine.h"
 #include "kernels.cuh"
 
+namespace lssph {
+struct SnapState;   // asynchronous snapshots (snapshot.cu)
+}
+
 struct lssph_handle {
 
     lssph_params p{};
@@ -70,6 +74,7 @@ struct lssph_handle {
     std::vector<int> prof_kinds;
     size_t prof_next = 0;
     lssph_batch* batch = nullptr;   // the batch this solve is a member of, if any
+    lssph::SnapState* snap = nullptr;   // snapshot slots and side stream, set up on first use
     std::string err;
 };
 
@@ -113,6 +118,9 @@ bool pdl_enabled();
 
 // Drop a handle that is being destroyed from the batch that holds it (batch.cu).
 void batch_forget(lssph_batch* b, lssph_handle* h);
+
+// Finish and free a handle's asynchronous snapshots (snapshot.cu).
+void snapshot_release(lssph_handle* h);
 
 // Higher-order LS stage and PST launches, SPH_MODEL 4 / 5 / 6 (highorder.cu).  tiles:
 // tile of each CTA (NULL: CTA i runs tile i); while h->preparing they only set the

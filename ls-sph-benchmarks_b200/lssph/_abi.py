@@ -176,6 +176,8 @@ _PROTOS = {
     "lssph_batch_launch": (C.c_int, [_H, C.c_int32]),
     "lssph_batch_wait": (C.c_int, [_H, _i, _i, _i]),
     "lssph_batch_last_step_stats": (C.c_int, [_H, _P(C.c_double), _P(C.c_int64)]),
+    "lssph_write_data_async": (C.c_int, [_H, C.c_char_p, C.c_int32]),
+    "lssph_snapshot_wait": (C.c_int, [_H]),
     "lssph_lsb_interpolate": (C.c_int, [_P(Params), C.c_int32, _d, _d, _d, _d, C.c_int32, _d, _d, _d]),
     "lssph_interpolate": (C.c_int, [_H, C.c_int32, C.c_int32, _d, _d, _d]),
     # device pointers (caller-owned device memory), stream handle

@@ -270,6 +270,15 @@ class Simulation:
     def write_data(self, results_root: str, step: int) -> None:
         self._chk(self._lib.lssph_write_data(self._h, results_root.encode(), int(step)))
 
+    def write_data_async(self, results_root: str, step: int) -> None:
+        """write_data that returns at once: the state is captured on the device and the file
+        is written in the background while stepping continues (snapshot_wait to finish)."""
+        self._chk(self._lib.lssph_write_data_async(self._h, results_root.encode(), int(step)))
+
+    def snapshot_wait(self) -> None:
+        """Wait for every pending write_data_async file of this solve."""
+        self._chk(self._lib.lssph_snapshot_wait(self._h))
+
 
 def setup_counts(params: Params) -> tuple[int, int]:
     """(num_total, num_int) of the closed box described by params."""
