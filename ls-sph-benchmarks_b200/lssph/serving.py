@@ -13,6 +13,13 @@ batch calls it
     final state, frees the device memory and records the time to solution.
 Each result is bit-identical to running the same request alone (the batched kernels run
 the solo arithmetic per member); the serving test checks this.
+
+Pre-emption: a request with a higher ``priority`` that has arrived but finds no slot or
+memory suspends active members of lower priority (newest first) until it fits.  A
+suspended member's state is downloaded (the checkpoint), its device memory freed, and it
+waits again; when re-admitted it resumes from that state with its remaining step budget.
+A solve restarted from its state continues bit for bit, so a pre-empted request still ends
+with exactly its solo result.
 """
 from __future__ import annotations
 
@@ -47,6 +54,7 @@ class Request:
     arrival: float = 0.0                 # seconds on the server clock
     tag: str = ""
     init: Callable[[], State] | None = None   # builds the initial state (default: fresh start)
+    priority: int = 0                    # higher pre-empts lower when slots or memory run out
     # filled in by the server
     footprint: int = 0
     admitted: float | None = None
@@ -55,6 +63,8 @@ class Request:
     status: int = 0
     stopped: str = ""                    # "budget" | "steady" | "error"
     result: State | None = None
+    preemptions: int = 0
+    resume: State | None = None          # checkpoint of a suspended request
 
     @property
     def latency(self) -> float | None:
@@ -77,6 +87,7 @@ class ServerStats:
     host_retire_s: float = 0.0
     max_queue: int = 0               # most requests waiting for admission at one scheduling point
     mean_queue: float = 0.0          # waiting requests averaged over scheduling points
+    preemptions: int = 0             # active solves suspended for higher-priority requests
     latencies_s: list = field(default_factory=list)
 
 
@@ -84,7 +95,7 @@ class Server:
     """Continuous-batching request loop (single thread, one device)."""
 
     def __init__(self, hbm_budget: int | None = None, max_active: int = 64, chunk_steps: int = 50,
-                 keep_results: bool = True, clock=time.perf_counter):
+                 keep_results: bool = True, clock=time.perf_counter, preempt: bool = True):
         if hbm_budget is None:
             free, _ = device_memory()
             hbm_budget = int(0.8 * free)
@@ -92,6 +103,8 @@ class Server:
         self.max_active = int(max_active)
         self.chunk_steps = int(chunk_steps)
         self.keep_results = keep_results
+        self.preempt = preempt
+        self.preemptions = 0
         self.clock = clock
         self.batch = Batch()
         self.waiting: deque[Request] = deque()
@@ -137,15 +150,61 @@ class Server:
             else:
                 keep.append(req)
         self.waiting = keep
+        if self.preempt:
+            picked += self._preempt_for(now, len(picked))
         return picked
 
+    def _preempt_for(self, now: float, n_picked: int) -> list[Request]:
+        """Admit arrived waiting requests that outrank active members by suspending those
+        members (lowest priority first, newest first among equals)."""
+        picked: list[Request] = []
+        for req in sorted((r for r in self.waiting if r.arrival <= now), key=lambda r: -r.priority):
+            victims = sorted((i for i, (a, _) in enumerate(self.active) if a.priority < req.priority),
+                             key=lambda i: (self.active[i][0].priority, -(self.active[i][0].admitted or 0.0)))
+            free_slots = self.max_active - len(self.active) - n_picked - len(picked)
+            free_mem = self.hbm_budget - self.used
+            chosen = []
+            for i in victims:
+                if free_slots >= 1 and free_mem >= req.footprint:
+                    break
+                chosen.append(i)
+                free_slots += 1
+                free_mem += self.active[i][0].footprint
+            if free_slots < 1 or free_mem < req.footprint:
+                continue
+            for i in sorted(chosen, reverse=True):
+                self.suspend(i)
+            self.waiting = deque(r for r in self.waiting if r is not req)
+            self.used += req.footprint
+            self.peak_used = max(self.peak_used, self.used)
+            req.admitted = self.now()
+            picked.append(req)
+        return picked
+
+    def suspend(self, i: int) -> Request:
+        """Checkpoint active member i to host memory, free its device memory and put it back
+        at the head of the queue; it resumes from the checkpoint when re-admitted."""
+        req, sim = self.active.pop(i)
+        req.resume = sim.download()
+        self.batch.remove(sim)
+        sim.close()
+        self.used -= req.footprint
+        req.preemptions += 1
+        self.preemptions += 1
+        self.waiting.appendleft(req)
+        return req
+
     def _create(self, req: Request) -> Simulation:
-        if req.init is None:
+        ni = setup_counts(req.params)[1]
+        if req.resume is not None:               # restart from the checkpoint, no extra ghost pass
+            sim = Simulation(req.params, req.resume, ni)
+            req.resume = None
+        elif req.init is None:
             sim = Simulation.new(req.params)
         else:
-            sim = Simulation(req.params, req.init(), setup_counts(req.params)[1])
+            sim = Simulation(req.params, req.init(), ni)
             sim.ghost()
-        sim.set_step_budget(req.nsteps)
+        sim.set_step_budget(req.nsteps - req.steps_done)
         return sim
 
     # ---- one batch call ---------------------------------------------------------------
@@ -228,6 +287,7 @@ class Server:
                            host_create_s=self.host_create_s, wait_s=self.wait_s, host_retire_s=self.host_retire_s,
                            max_queue=max(self.queue_samples, default=0),
                            mean_queue=float(np.mean(self.queue_samples)) if self.queue_samples else 0.0,
+                           preemptions=self.preemptions,
                            latencies_s=lat)
 
     def close(self) -> None:

@@ -74,3 +74,31 @@ def test_realtime_arrivals_report_latency():
     assert 0 < stats.p50_s <= stats.p99_s
     assert stats.solves_per_s > 0 and stats.particle_updates_per_s > 0
     srv.close()
+
+
+def test_preempted_requests_end_with_their_solo_result():
+    # two long low-priority solves hold both slots; an urgent request arrives later and
+    # suspends one of them (checkpoint to host), which later resumes from that checkpoint
+    low = [Request(rid=0, params=lssph.taylor_green_params(num=48), nsteps=1500, arrival=0.0),
+           Request(rid=1, params=lssph.cavity_params(num=48), nsteps=1500, arrival=0.0)]
+    urgent = Request(rid=2, params=lssph.boussinesq_params(num=40), nsteps=60, arrival=0.03, priority=5)
+    srv = Server(max_active=2, chunk_steps=20)
+    stats = srv.run(low + [urgent], realtime=True)
+    assert stats.completed == 3 and stats.preemptions >= 1
+    assert any(r.preemptions > 0 for r in srv.done if r.rid != 2)
+    done = {r.rid: r for r in srv.done}
+    assert done[2].finished < max(done[0].finished, done[1].finished)
+    for r in srv.done:
+        assert r.stopped == "budget" and r.steps_done == r.nsteps and r.status == 0
+        ref = _solo(r)
+        for k in _fields(r.params):
+            assert np.array_equal(getattr(r.result, k), getattr(ref, k)), (r.rid, k)
+    srv.close()
+
+
+def test_no_preemption_among_equal_priorities():
+    reqs = _requests()
+    srv = Server(max_active=2, chunk_steps=5, keep_results=False)
+    stats = srv.run(reqs, realtime=False)
+    assert stats.completed == len(reqs) and stats.preemptions == 0
+    srv.close()
