@@ -117,6 +117,29 @@ module lssph_cuda_mod
             integer(c_int32_t), value :: step
         end function
 
+        ! write_data that returns at once (device-side capture, background file write)
+        integer(c_int) function lssph_write_data_async(h, results_root, step) bind(c, name="lssph_write_data_async")
+            import :: c_int, c_int32_t, c_char, c_ptr
+            type(c_ptr), value :: h
+            character(kind=c_char), intent(in) :: results_root(*)
+            integer(c_int32_t), value :: step
+        end function
+
+        integer(c_int) function lssph_snapshot_wait(h) bind(c, name="lssph_snapshot_wait")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function
+
+        ! analysis/common/lssph_b.py main(): value, d/dx, d/dy at n_targets points
+        integer(c_int) function lssph_lsb_interpolate(p, n, x, y, val, rho, n_targets, tx, ty, out) &
+                bind(c, name="lssph_lsb_interpolate")
+            import :: c_int, c_int32_t, c_double, lssph_params
+            type(lssph_params), intent(in) :: p
+            integer(c_int32_t), value :: n, n_targets
+            real(c_double), intent(in) :: x(*), y(*), val(*), rho(*), tx(*), ty(*)
+            real(c_double), intent(out) :: out(*)
+        end function
+
         integer(c_int) function lssph_read_data(path, num_total, with_tem, ptype, x, y, u, v, rho, pre, tem) &
                 bind(c, name="lssph_read_data")
             import :: c_int, c_int32_t, c_char, c_double

@@ -77,9 +77,15 @@ program main_gpu
             exit
         endif
         step = step + chunk
-        if (mod(step - 1, p%write_step) == 0) rc = lssph_write_data(h, "results" // c_null_char, step - 1)
+        ! the snapshot is written in the background while the next chunk steps
+        if (mod(step - 1, p%write_step) == 0) rc = lssph_write_data_async(h, "results" // c_null_char, step - 1)
+        if (rc /= LSSPH_OK) then
+            write(*,*) "Fatal Error while writing data: ", lssph_last_error_f()
+            error stop
+        endif
     enddo
 
+    rc = lssph_snapshot_wait(h)
     call lssph_destroy(h)
 
 contains
