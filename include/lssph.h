@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define LSSPH_ABI_VERSION 1
+#define LSSPH_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------------------- */
 #define LSSPH_OK                 0
@@ -88,6 +88,10 @@ typedef struct lssph_params {
                              1 = reference summation order (bit-exact vs the oracle) */
     uint64_t seed;        /* POS_PERT jitter seed (the reference seeds from the clock,
                              impose_initial_conditions_mod.f90:43-51) */
+    int32_t  periodic;    /* 1: periodic square [0, LEN_X)^2 without walls (problems 1, 2);
+                             problem 1 then decays u = sin(2 pi x) sin(2 pi y) without the
+                             source term.  0: the reference's closed box */
+    int32_t  pad2_;
 } lssph_params;
 
 typedef struct lssph_handle lssph_handle;

@@ -241,6 +241,15 @@ void launch_ghost_nb(lssph_handle* h, int zero_list, int reset_umax, cudaStream_
 
 void launch_ghost_on(lssph_handle* h, int zero_list, int reset_umax, cudaStream_t stream, bool pdl,
                      int priority = 0) {
+    if (h->num_ext == 0) {   // periodic domain: no ghosts, only the bookkeeping of the launch
+        ProfScope prof(h, LSSPH_KIND_GHOST);
+        if (h->preparing) return;
+        const int nb = std::max(1, std::min(148, (h->grid.ncell + 255) / 256));
+        int* zc = zero_list >= 0 ? h->L[zero_list].cnt : nullptr;
+        launch_kernel_p(pdl, priority, k_housekeep, nb, 256, 0, stream, h->P, zc, reset_umax, h->sc);
+        h->launch_counter++;
+        return;
+    }
     if (h->nb_ghost == 1) launch_ghost_nb<1>(h, zero_list, reset_umax, stream, pdl, priority);
     else if (h->nb_ghost == 4) launch_ghost_nb<4>(h, zero_list, reset_umax, stream, pdl, priority);
     else launch_ghost_nb<3>(h, zero_list, reset_umax, stream, pdl, priority);
@@ -544,7 +553,12 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (pin->precision == LSSPH_PRECISION_MIXED && pin->lanes != 0 && pin->lanes != 4)
         return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs with 4 lanes per particle (lanes = 0 or 4)");
     if (pin->target_problem == 4 && !tem) return fail(nullptr, LSSPH_E_BAD_PARAM, "tem required for problem 4");
-    if (num_int <= 0 || num_total <= num_int) return fail(nullptr, LSSPH_E_BAD_PARAM, "bad particle counts");
+    if (num_int <= 0 || num_total < num_int || (num_total == num_int && !pin->periodic))
+        return fail(nullptr, LSSPH_E_BAD_PARAM, "bad particle counts");
+    if (pin->periodic && num_total != num_int)
+        return fail(nullptr, LSSPH_E_BAD_PARAM, "a periodic domain has no ghost particles (num_total == num_int)");
+    if (pin->periodic && pin->precision == LSSPH_PRECISION_MIXED)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs the closed box only");
     for (int i = 0; i < num_total; ++i) {
         if ((i < num_int) != (ptype[i] == 0))
             return fail(nullptr, LSSPH_E_BAD_PARAM, "ptype must be 0 for the first num_int particles and 1..8 after");
@@ -596,6 +610,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     Phys& P = h->P;
     P.problem = p.target_problem; P.kt = p.kernel_type; P.rk = p.rk; P.wall_model = p.wall_model;
     P.sph_model = p.sph_model;
+    P.periodic = p.periodic;
+    P.Lx = p.len_x;
     P.u_bc_top = p.u_bc_top; P.u_bc_bottom = p.u_bc_bottom; P.u_bc_left = p.u_bc_left; P.u_bc_right = p.u_bc_right;
     P.tem_bc_top = p.tem_bc_top; P.tem_bc_bottom = p.tem_bc_bottom; P.tem_bc_left = p.tem_bc_left;
     P.tem_bc_right = p.tem_bc_right;
@@ -608,7 +624,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     P.ih2A = P.ih1 / p.h;          // inv_h(2) = inv_h(1)/h  (LSSPH_A_mod.f90:90-93)
     P.ih2B = P.ih1 * P.ih1;        // inv_h2 = inv_h*inv_h  (interpolate_LSSPH_B_mod.f90:151-152)
     P.h_eff_sq = p.h_eff * p.h_eff;
-    P.inv_h_eff = 1.0 / p.h_eff;
+    P.inv_h_eff = p.periodic ? h->grid.inv_cw : 1.0 / p.h_eff;   // cell keys
     P.SP_mass = p.SP_mass;
     P.W_ave = p.W_ave;
     P.wnorm = kernel_norm(p.kernel_type, p.h);
@@ -670,7 +686,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     }
     h->n_int = (int)t_int.size();
     h->n_wall = (int)t_wall.size();
-    h->overlap = h->overlap_allowed && h->n_int > 0 && h->n_wall > 0;
+    h->overlap = h->overlap_allowed && h->n_int > 0 && h->n_wall > 0 && !p.periodic;
     // one device block for every array of the solve (one cudaMalloc, one cudaFree)
     const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles);
     {
@@ -695,7 +711,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     // ---- host-side constant arrays ----
     std::vector<double> src(NI, 0.0), K(NE, 0.0), zeros(std::max(NI, NE), 0.0), ones(NI, 1.0);
     std::vector<int32_t> mode(NE, XM_NEG);
-    if (h->p1) {
+    if (h->p1 && !p.periodic) {   // the periodic problem 1 is source-free (src stays 0.0)
         for (size_t i = 0; i < NI; ++i)   // LSSPH_A_mod.f90:247-248 (positions never move in problem 1)
             src[i] = ((2.0 * (kPi * kPi)) * std::sin(kPi * (x[i] - p.WL_thick))) * std::cos(kPi * (y[i] - p.WL_thick));
         for (size_t me = 0; me < NE; ++me) {   // extrapolate_diff_test_mod.f90:40-103

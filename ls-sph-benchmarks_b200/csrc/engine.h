@@ -39,6 +39,7 @@ struct CellGrid {
     int nx = 0, ny = 0, ncell = 0;
     int capacity = 0;   // max particles per cell at init (all particles, division keys)
     int cap = 0;        // slot capacity per cell on the device (>= 2 * capacity)
+    double inv_cw = 0.0;   // periodic domain: 1 / cell width (cells L / n >= h_eff, n even)
     std::vector<int32_t> ghost_key;    // [num_ext] 0-based cell of each ghost (division)
     std::vector<int32_t> vm_key;       // [num_ext] 0-based cell of each virtual marker
     std::vector<int32_t> gstart;       // [ncell+1] CSR of ghosts per cell

@@ -125,6 +125,7 @@ void init_param(lssph_params* p) {
     p->h_eff = (p->kernel_type == 2) ? 3.0 * p->h : 2.0 * p->h;
     p->W_ave = kernel_W_host(p->kernel_type, p->dx, p->h);
     p->num_WL = (int32_t)std::ceil(p->h_eff / p->dx);
+    if (p->periodic) p->num_WL = 0;   // no wall layers in a periodic domain
     p->WL_thick = (double)p->num_WL * p->dx;
     if (p->target_problem == 4) {
         p->delta_tem = p->tem_bottom - p->tem_top;
@@ -198,6 +199,15 @@ int check_param(const lssph_params* p, std::string* msg) {
         return fail("precision must be LSSPH_PRECISION_FP64 or LSSPH_PRECISION_MIXED.");
     if (!(p->lanes == 0 || p->lanes == 1 || p->lanes == 2 || p->lanes == 4 || p->lanes == 8))
         return fail("lanes must be 0 (auto), 1, 2, 4 or 8.");
+    if (p->periodic != 0 && p->periodic != 1) return fail("periodic must be 0 or 1.");
+    if (p->periodic) {
+        if (p->target_problem != 1 && p->target_problem != 2)
+            return fail("A periodic domain is available for problems 1 and 2 (no walls).");
+        if (p->len_x != p->len_y || p->num_x != p->num_y)
+            return fail("A periodic domain must be square (LEN_X == LEN_Y, NUM_X == NUM_Y).");
+        if (p->h_eff > 0.0 && p->len_x < 4.0 * p->h_eff)
+            return fail("A periodic domain needs LEN_X >= 4 h_eff.");
+    }
     return LSSPH_OK;
 }
 
@@ -275,7 +285,7 @@ int parse_config(const char* path, lssph_params* p, std::string* msg) {
         {"NUM_X", &p->num_x}, {"NUM_Y", &p->num_y}, {"RK", &p->rk}, {"START_STEP", &p->start_step},
         {"END_STEP", &p->end_step}, {"WRITE_STEP", &p->write_step}, {"TG_A", &p->tg_a},
         {"TG_B", &p->tg_b}, {"KERNEL_TYPE", &p->kernel_type}, {"SPH_MODEL", &p->sph_model},
-        {"WALL_MODEL", &p->wall_model}};
+        {"WALL_MODEL", &p->wall_model}, {"PERIODIC", &p->periodic}};
     const DblField dbls[] = {
         {"U_TOP", &p->u_top}, {"TEM_TOP", &p->tem_top}, {"TEM_BOTTOM", &p->tem_bottom},
         {"TEM_LEFT", &p->tem_left}, {"TEM_RIGHT", &p->tem_right}, {"LEN_X", &p->len_x},
@@ -400,6 +410,10 @@ int setup_particles(const lssph_params* p, int num_total, int32_t* ptype, double
             r = rng.uniform();
             y[i] = y[i] + (p->pos_pert * p->dx) * (2.0 * r - 1.0);
         }
+        if (p->periodic) {   // free decay of sin(2 pi x) sin(2 pi y), rate 8 pi^2
+            for (int i = 0; i < ni; ++i)
+                u[i] = std::sin(((2.0 * kPi) * x[i]) / p->len_x) * std::sin(((2.0 * kPi) * y[i]) / p->len_y);
+        }
     } else if (p->target_problem == 2) {
         const double a = (double)p->tg_a, b = (double)p->tg_b, Lx = p->len_x, Ly = p->len_y;
         const double ratio = (a * Ly) / (b * Lx);
@@ -462,8 +476,23 @@ int build_cell_grid(const lssph_params* p, int num_total, int num_int, const dou
     g->ncell = g->nx * g->ny;
     const int ne = num_total - num_int;
     std::vector<int> count(g->ncell, 0);
+    if (p->periodic) {   // an even number of cells of width L / n >= h_eff per side
+        const int n = 2 * (int)std::floor(p->len_x / (2.0 * p->h_eff));
+        if (n < 4) {
+            if (msg) *msg = "a periodic domain needs at least 4 cells of h_eff per side";
+            return LSSPH_E_BAD_PARAM;
+        }
+        g->nx = g->ny = n;
+        g->ncell = n * n;
+        g->inv_cw = 1.0 / (p->len_x / (double)n);
+    }
     auto key_div = [&](double px, double py, int* key) {
-        const double cxd = std::ceil(px / p->h_eff), cyd = std::ceil(py / p->h_eff);
+        double cxd = std::ceil(px / p->h_eff), cyd = std::ceil(py / p->h_eff);
+        if (p->periodic) {   // positions in (0, L], rounding at the ends clamped
+            if (!(px > 0.0 && px <= p->len_x && py > 0.0 && py <= p->len_y)) return false;
+            cxd = std::min(std::max(std::ceil(px * g->inv_cw), 1.0), (double)g->nx);
+            cyd = std::min(std::max(std::ceil(py * g->inv_cw), 1.0), (double)g->ny);
+        }
         if (!(cxd >= 1.0 && cxd <= g->nx && cyd >= 1.0 && cyd <= g->ny)) return false;
         *key = ((int)cxd - 1) + ((int)cyd - 1) * g->nx;
         return true;

@@ -64,13 +64,18 @@ struct Phys {
     int tem_bc_top, tem_bc_bottom, tem_bc_left, tem_bc_right;
     int nx, ny, ncell, cap;
     int num_total, num_int, num_ext, sph_model;
+    int periodic, pad_;   // periodic: square domain (0, Lx]^2, cells wrap, no ghosts
     double u_top, tem_top, tem_bottom, tem_left, tem_right;
     double h, ih1, ih2A, ih2B, h_eff_sq, inv_h_eff, SP_mass, W_ave, wnorm, dt;
     double c_sq, rho_ref, vis_ref, delta, zeta_sq, xi_sq, alpha_ref, gravity, tem_ave;
     double thermal_dif, PST_c, threshold, hydro_coef_top, hydro_coef_bottom;
     // reciprocals of loop-invariant divisors (1/W_ave, 1/zeta^2, 1/xi^2, -3/h, -5/h)
     double iWave, izeta2, ixi2, m3h, m5h;
+    double Lx;   // periodic domain side
 };
+
+// Periodic position wrap into (0, L] (the oracle's wrap_pos).
+__device__ __forceinline__ double wrap_pos(double x, double L) { return x <= 0.0 ? x + L : (x > L ? x - L : x); }
 
 struct Fld {   // SoA particle state over num_total
     double *x, *y, *u, *v, *rho, *pre, *tem, *vol;
@@ -407,26 +412,41 @@ __device__ __forceinline__ int group_sum_i(int v) {
 template <bool FLUID_ONLY, class F>
 __device__ __forceinline__ void for_candidates(const Phys& P, const Lst& L, const int* gstart, const int* glist,
                                                int key, F&& f) {
+    // f(j, sx, sy): sx, sy = position shift of j's cell (-+Lx across a periodic boundary)
     const int cx = key % P.nx, cy = key / P.nx;
     for (int dy = -1; dy <= 1; ++dy) {
-        const int yy = cy + dy;
+        int yy = cy + dy;
+        double sy = 0.0;
+        if (P.periodic) {
+            if (yy < 0) { yy += P.ny; sy = -P.Lx; }
+            else if (yy >= P.ny) { yy -= P.ny; sy = P.Lx; }
+        }
         if (yy < 0 || yy >= P.ny) continue;
         for (int dx = -1; dx <= 1; ++dx) {
-            const int xx = cx + dx;
+            int xx = cx + dx;
+            double sx = 0.0;
+            if (P.periodic) {
+                if (xx < 0) { xx += P.nx; sx = -P.Lx; }
+                else if (xx >= P.nx) { xx -= P.nx; sx = P.Lx; }
+            }
             if (xx < 0 || xx >= P.nx) continue;
             const int c = xx + yy * P.nx;
             const int ng = gstart[c + 1] - gstart[c];
             const int nf = min(L.cnt[c], P.cap - ng);
-            for (int t = 0; t < nf; ++t) f(L.slots[(size_t)c * P.cap + t]);
+            for (int t = 0; t < nf; ++t) f(L.slots[(size_t)c * P.cap + t], sx, sy);
             if (!FLUID_ONLY)
-                for (int t = 0; t < ng; ++t) f(glist[gstart[c] + t]);
+                for (int t = 0; t < ng; ++t) f(glist[gstart[c] + t], sx, sy);
         }
     }
 }
 
 // Cell key of an interior particle, update_cell_mod.f90:53-55 (multiplication form).
 __device__ __forceinline__ int cell_key_mul(const Phys& P, double x, double y, Scalars* sc) {
-    const double cxd = ceil(x * P.inv_h_eff), cyd = ceil(y * P.inv_h_eff);
+    double cxd = ceil(x * P.inv_h_eff), cyd = ceil(y * P.inv_h_eff);
+    if (P.periodic) {   // wrapped positions lie in (0, Lx]: clamp the rounding at the ends
+        if (x > 0.0 && x <= P.Lx) cxd = fmin(fmax(cxd, 1.0), (double)P.nx);
+        if (y > 0.0 && y <= P.Lx) cyd = fmin(fmax(cyd, 1.0), (double)P.ny);
+    }
     if (!(cxd >= 1.0 && cxd <= (double)P.nx && cyd >= 1.0 && cyd <= (double)P.ny)) {
         atomicOr(&sc->err, ERR_OUT_OF_DOMAIN);
         return -1;
@@ -477,6 +497,7 @@ struct TileHdr {
     int own_off[OC + 1];
     int cell[HC];       // global cell of each halo cell (-1 outside the grid)
     int g0[HC];         // start of its ghost list
+    double sx[HC], sy[HC];   // position shift of each halo cell (-+Lx across a periodic boundary)
 };
 
 // Halo cell holding staged position k (cells in staging order; empty cells skipped).
@@ -549,7 +570,16 @@ __device__ __forceinline__ void stage_lists(const Phys& P, const Lst& L, const i
     const int tid = threadIdx.x;
     int c = -1, g0 = 0;
     if (tid < HC) {
-        const int cx = cx0 + tid % HX, cy = cy0 + tid / HX;
+        int cx = cx0 + tid % HX, cy = cy0 + tid / HX;
+        double sx = 0.0, sy = 0.0;
+        if (P.periodic) {   // halo cells past an edge wrap; the even cell count keeps own cells inside
+            if (cx < 0) { cx += P.nx; sx = -P.Lx; }
+            else if (cx >= P.nx) { cx -= P.nx; sx = P.Lx; }
+            if (cy < 0) { cy += P.ny; sy = -P.Lx; }
+            else if (cy >= P.ny) { cy -= P.ny; sy = P.Lx; }
+        }
+        T.sx[tid] = sx;
+        T.sy[tid] = sy;
         int nf = 0, ng = 0;
         if (cx >= 0 && cx < P.nx && cy >= 0 && cy < P.ny) {
             c = cx + cy * P.nx;
@@ -617,8 +647,14 @@ __device__ __forceinline__ void stage_halo(const Phys& P, const Fld& F, const Ls
     const int n = T.off[HC];
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int j = S.idx[k];
-        S.x[k] = __ldg(F.x + j);
-        S.y[k] = __ldg(F.y + j);
+        double xj = __ldg(F.x + j), yj = __ldg(F.y + j);
+        if (P.periodic) {   // x_j + shift, so that staged x_j - x_i is the periodic offset
+            const int h = halo_cell_of(T, k);
+            xj = xj + T.sx[h];
+            yj = yj + T.sy[h];
+        }
+        S.x[k] = xj;
+        S.y[k] = yj;
         S.u[k] = __ldg(F.u + j);
         S.v[k] = __ldg(F.v + j);
         S.rho[k] = __ldg(F.rho + j);
@@ -982,6 +1018,9 @@ __device__ __forceinline__ double stage_advance(const Phys& P, const Fld& nxt, c
             if constexpr (!p1) { vn = va; xn = xa; yn = ya; rn = ra; }
             if constexpr (NB == 5) tn = ta;
         }
+    }
+    if constexpr (!p1) {
+        if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
     }
     nxt.u[i] = un;
     bool finite = isfinite(un);
@@ -1750,7 +1789,8 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
             }
             const int i = SM.idx[ki];
             const double my_x = SM.x[ki], my_y = SM.y[ki];
-            const double xn = my_x + dx, yn = my_y + dy;
+            double xn = my_x + dx, yn = my_y + dy;
+            if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
             const double un = SM.u[ki] + acc[0], vn = SM.v[ki] + acc[1], rn = SM.rho[ki] + acc[2];
             nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
             nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
@@ -1999,6 +2039,19 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(con
 // Small kernels (static: this header is compiled into more than one translation unit)
 // =======================================================================================
 // Scatter the interior particles of the current positions (standalone update_cell).
+// A periodic domain has no ghost particles.  In place of the ghost launch this kernel does
+// that launch's other duties in the step: clear the scatter counters of the cell list the
+// preceding stage consumed, reset the U_max slot after PST, and count the step.
+static __global__ void k_housekeep(const Phys P, int* zero_cnt, int reset_umax, Scalars* sc) {
+    pdl_wait();
+    const bool stop = halted(sc);
+    if (zero_cnt && !stop)
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < P.ncell; c += gridDim.x * blockDim.x) zero_cnt[c] = 0;
+    if (reset_umax && blockIdx.x == 0 && threadIdx.x == 0) sc->umax2 = 0ull;
+    pdl_release();
+    if (reset_umax) end_of_step(sc, gridDim.x);
+}
+
 static __global__ void k_scatter(const Phys P, const Fld F, const Lst Ln, const int* __restrict__ gstart, int* key,
                           Scalars* sc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2077,9 +2130,9 @@ static __global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const
     const double my = which == 0 ? F.y[i] : V.y[i];
     const int k = which == 0 ? key[i] : V.key[i];
     int c = 0;
-    auto f = [&](int j) {
+    auto f = [&](int j, double sx, double sy) {
         if (which == 0 && j == i) return;
-        const double xj = F.x[j] - mx, yj = F.y[j] - my;
+        const double xj = (F.x[j] + sx) - mx, yj = (F.y[j] + sy) - my;
         if (xj * xj + yj * yj > P.h_eff_sq) return;
         if (c < stride) out[(size_t)i * stride + c] = j;
         ++c;

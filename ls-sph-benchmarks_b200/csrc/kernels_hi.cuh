@@ -483,7 +483,8 @@ __device__ __forceinline__ void pst_body_hi(const Phys& P, const Fld& cur, const
         __syncwarp();
         if (lane == 0) {
             const int i = SM.idx[ki];
-            const double xn = my_x + dx, yn = my_y + dy;
+            double xn = my_x + dx, yn = my_y + dy;
+            if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
             const double un = my_u + accf[0], vn = my_v + accf[1], rn = my_rho + accf[2];
             nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
             nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
@@ -841,7 +842,8 @@ __device__ __forceinline__ void pst_body_tpp(const Phys& P, const Fld& cur, cons
             for (int c = 0; c < NB; ++c) accf[c] = 0.0;
         }
         const int i = SM.idx[ki];
-        const double xn = my_x + dx, yn = my_y + dy;
+        double xn = my_x + dx, yn = my_y + dy;
+        if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
         const double un = my_u + accf[0], vn = my_v + accf[1], rn = my_rho + accf[2];
         nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
         nxt.pre[i] = P.c_sq * (rn - P.rho_ref);

@@ -46,6 +46,7 @@ module lssph_cuda_mod
         integer(c_int32_t) :: precision
         integer(c_int32_t) :: lanes
         integer(c_int64_t) :: seed
+        integer(c_int32_t) :: periodic, pad2_
     end type lssph_params
 
     interface

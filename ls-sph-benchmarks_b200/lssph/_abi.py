@@ -81,6 +81,8 @@ class Params(C.Structure):
         ("precision", C.c_int32),
         ("lanes", C.c_int32),
         ("seed", C.c_uint64),
+        ("periodic", C.c_int32),
+        ("pad2_", C.c_int32),
     ]
 
     # user-facing names of config.h macros -> fields
@@ -100,6 +102,7 @@ class Params(C.Structure):
         "GRAVITY": "gravity", "POS_PERT": "pos_pert", "TG_A": "tg_a", "TG_B": "tg_b",
         "COE_H": "coe_h", "PST_C": "PST_c", "COE_DELTA_SPH": "coe_delta_sph",
         "KERNEL_TYPE": "kernel_type", "SPH_MODEL": "sph_model", "WALL_MODEL": "wall_model",
+        "PERIODIC": "periodic",
     }
 
     def copy(self) -> "Params":

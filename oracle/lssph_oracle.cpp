@@ -263,6 +263,9 @@ struct orc_state {
     std::vector<double> vm_x, vm_y, vm_u, vm_v, vm_pre, vm_tem, vm_nx, vm_ny;
     int idx_x_max = 0, idx_y_max = 0, idx_max = 0, capacity = 0, list_cap = 0;
     std::vector<int> idx_SP, num_SP, num_WL, neighbors, list, list_WL, idx_VM;
+    // periodic domain: cell width, and the position shift (+-L or 0) of each neighbour cell
+    double inv_cw = 0.0;
+    std::vector<double> nshift_x, nshift_y;
     int error = 0;
 };
 
@@ -282,6 +285,7 @@ void init_param(lssph_params* p) {
     p->h_eff = (p->kernel_type == 2) ? 3.0 * p->h : 2.0 * p->h;
     p->W_ave = cal_W(p->kernel_type, p->dx, p->h);
     p->num_WL = (int)std::ceil(p->h_eff / p->dx);
+    if (p->periodic) p->num_WL = 0;   // periodic extension: no wall layers
     p->WL_thick = (double)p->num_WL * p->dx;
     if (p->target_problem == 4) {
         p->delta_tem = p->tem_bottom - p->tem_top;
@@ -362,6 +366,10 @@ void impose_ic(orc_state* s) {
             r = rng.uniform();
             s->y[i] = s->y[i] + (p.pos_pert * p.dx) * (2.0 * r - 1.0);
         }
+        if (p.periodic) {   // periodic extension: free decay of sin(2 pi x) sin(2 pi y)
+            for (int i = 0; i < n; ++i)
+                s->u[i] = std::sin(((2.0 * PI) * s->x[i]) / p.len_x) * std::sin(((2.0 * PI) * s->y[i]) / p.len_y);
+        }
     } else if (p.target_problem == 2) {  // :68-96
         const double a = (double)p.tg_a, b = (double)p.tg_b, Lx = p.len_x, Ly = p.len_y;
         const double ratio = (a * Ly) / (b * Lx);
@@ -432,12 +440,28 @@ void init_virtual_markers(orc_state* s) {
     }
 }
 
-// init_cell_mod.f90:23-184
+// Cell of a position in a periodic square: an even number of cells of width L / n >= h_eff,
+// x in (0, L] -> ceil(x / width), clamped against rounding at x = L.
+int periodic_cell(const orc_state* s, double x) {
+    int c = (int)std::ceil(x * s->inv_cw);
+    return c < 1 ? 1 : (c > s->idx_x_max ? s->idx_x_max : c);
+}
+
+// Periodic position wrap into (0, L].
+inline double wrap_pos(double x, double L) { return x <= 0.0 ? x + L : (x > L ? x - L : x); }
+
+// init_cell_mod.f90:23-184 (+ the periodic extension)
 void init_cell(orc_state* s) {
     const lssph_params& p = s->p;
     const double xm = p.len_x + 2.0 * p.WL_thick, ym = p.len_y + 2.0 * p.WL_thick;
     s->idx_x_max = (int)std::ceil(xm / p.h_eff);
     s->idx_y_max = (int)std::ceil(ym / p.h_eff);
+    if (p.periodic) {
+        const int n = 2 * (int)std::floor(p.len_x / (2.0 * p.h_eff));
+        s->idx_x_max = n;
+        s->idx_y_max = n;
+        s->inv_cw = 1.0 / (p.len_x / (double)n);
+    }
     s->idx_max = s->idx_x_max * s->idx_y_max;
     const int nc = s->idx_max;
     s->idx_SP.assign(s->num_total, 0);
@@ -446,7 +470,8 @@ void init_cell(orc_state* s) {
     s->idx_VM.assign(s->num_ext, 0);
     s->neighbors.assign(9 * (nc + 1), 0);
     for (int me = 0; me < s->num_total; ++me) {
-        const int cx = (int)std::ceil(s->x[me] / p.h_eff), cy = (int)std::ceil(s->y[me] / p.h_eff);
+        int cx = (int)std::ceil(s->x[me] / p.h_eff), cy = (int)std::ceil(s->y[me] / p.h_eff);
+        if (p.periodic) { cx = periodic_cell(s, s->x[me]); cy = periodic_cell(s, s->y[me]); }
         int c = cx + (cy - 1) * s->idx_x_max;
         if (cx < 1 || cx > s->idx_x_max || cy < 1 || cy > s->idx_y_max) {
             set_err(s, LSSPH_E_OUT_OF_DOMAIN, "init_cell: particle outside the cell grid");
@@ -464,12 +489,20 @@ void init_cell(orc_state* s) {
         s->num_WL[c] += 1;
         s->list_WL[(size_t)c * s->list_cap + (s->num_WL[c] - 1)] = me;
     }
+    s->nshift_x.assign(9 * (nc + 1), 0.0);
+    s->nshift_y.assign(9 * (nc + 1), 0.0);
     for (int c = 1; c <= nc; ++c) {
         const int cx = (c - 1) % s->idx_x_max + 1, cy = (c - 1) / s->idx_x_max + 1;
         int k = 0;
         for (int dy = -1; dy <= 1; ++dy)
             for (int dx = -1; dx <= 1; ++dx) {
-                const int yx = cx + dx, yy = cy + dy;
+                int yx = cx + dx, yy = cy + dy;
+                if (p.periodic) {   // wrap; the neighbour's positions appear shifted by -+L
+                    if (yx < 1) { yx += s->idx_x_max; s->nshift_x[9 * c + k] = -p.len_x; }
+                    if (yx > s->idx_x_max) { yx -= s->idx_x_max; s->nshift_x[9 * c + k] = p.len_x; }
+                    if (yy < 1) { yy += s->idx_y_max; s->nshift_y[9 * c + k] = -p.len_y; }
+                    if (yy > s->idx_y_max) { yy -= s->idx_y_max; s->nshift_y[9 * c + k] = p.len_y; }
+                }
                 s->neighbors[9 * c + k] = (yx < 1 || yx > s->idx_x_max || yy < 1 || yy > s->idx_y_max)
                                               ? 0 : yx + (yy - 1) * s->idx_x_max;
                 ++k;
@@ -487,7 +520,8 @@ void update_cell(orc_state* s) {
     const int nc = s->idx_max;
     for (int c = 1; c <= nc; ++c) s->num_SP[c] = 0;
     for (int me = 0; me < s->num_int; ++me) {
-        const int cx = (int)std::ceil(s->x[me] * inv_h_eff), cy = (int)std::ceil(s->y[me] * inv_h_eff);
+        int cx = (int)std::ceil(s->x[me] * inv_h_eff), cy = (int)std::ceil(s->y[me] * inv_h_eff);
+        if (s->p.periodic) { cx = periodic_cell(s, s->x[me]); cy = periodic_cell(s, s->y[me]); }
         int c = cx + (cy - 1) * s->idx_x_max;
         if (cx < 1 || cx > s->idx_x_max || cy < 1 || cy > s->idx_y_max) {
             set_err(s, LSSPH_E_OUT_OF_DOMAIN, "update_cell: particle outside the cell grid");
@@ -510,7 +544,9 @@ void update_cell(orc_state* s) {
     }
 }
 
-// Iterate the candidate list of cell `my_cell` in reference order (9 cells, list order).
+// Iterate the candidate list of cell `my_cell` in reference order (9 cells, list order):
+// f(you, sx, sy) with the position shift of you's cell (0 in the closed box; -+L across a
+// periodic boundary), so that x_j + sx - x_i is the pair offset.
 template <class F>
 inline void for_candidates(const orc_state* s, int my_cell, F&& f) {
     for (int k = 0; k < 9; ++k) {
@@ -518,8 +554,16 @@ inline void for_candidates(const orc_state* s, int my_cell, F&& f) {
         if (c == 0) continue;
         const int n = s->num_SP[c];
         const int* L = &s->list[(size_t)c * s->list_cap];
-        for (int t = 0; t < n; ++t) f(L[t]);
+        const double sx = s->nshift_x[9 * my_cell + k], sy = s->nshift_y[9 * my_cell + k];
+        for (int t = 0; t < n; ++t) f(L[t], sx, sy);
     }
+}
+
+// Problem 1 source 2 pi^2 sin(pi (x - WL)) cos(pi (y - WL)) (LSSPH_A_mod.f90:247); the
+// periodic extension is source-free (0.0, added all the same).
+inline double p1_source(const lssph_params& p, double x, double y) {
+    if (p.periodic) return 0.0;
+    return ((2.0 * (PI * PI)) * std::sin(PI * (x - p.WL_thick))) * std::cos(PI * (y - p.WL_thick));
 }
 
 // LSSPH_A_mod.f90:26-271
@@ -538,9 +582,9 @@ void LSSPH_A(orc_state* s, int me) {
     int num_neighbors = 0;
     const int qq = (k == 2) ? 5 : (k == 3) ? 9 : (k == 4) ? 14 : 20;
     q = qq;
-    for_candidates(s, s->idx_SP[me], [&](int you) {
+    for_candidates(s, s->idx_SP[me], [&](int you, double sx, double sy) {
         if (me == you) return;
-        const double x_ji = s->x[you] - my_x, y_ji = s->y[you] - my_y;
+        const double x_ji = (s->x[you] + sx) - my_x, y_ji = (s->y[you] + sy) - my_y;
         const double r2 = x_ji * x_ji + y_ji * y_ji;
         if (r2 > h_eff_sq) return;
         const double r = std::sqrt(r2);
@@ -578,8 +622,7 @@ void LSSPH_A(orc_state* s, int me) {
     const double* dpre = d[3];
     const double* dtem = d[4];
     if (p.target_problem == 1) {
-        s->RHS_u[me] = (du[2] + du[3]) + ((2.0 * (PI * PI)) * std::sin(PI * (my_x - p.WL_thick))) *
-                                             std::cos(PI * (my_y - p.WL_thick));
+        s->RHS_u[me] = (du[2] + du[3]) + p1_source(p, my_x, my_y);
     } else {
         const double delta = ((p.coe_delta_sph * p.sound_speed) * h) * p.zeta_RSST;
         const double irho = 1.0 / my_rho;
@@ -605,9 +648,9 @@ void classical_SPH(orc_state* s, int me) {
     const double my_x = s->x[me], my_y = s->y[me], my_u = s->u[me], my_v = s->v[me];
     const double my_rho = s->rho[me], my_pre = s->pre[me], my_tem = s->has_tem ? s->tem[me] : 0.0;
     double du_dx = 0, dv_dy = 0, dp_dx = 0, dp_dy = 0, Lu = 0, Lv = 0, Lt = 0, Lr = 0;
-    for_candidates(s, s->idx_SP[me], [&](int you) {
+    for_candidates(s, s->idx_SP[me], [&](int you, double sx, double sy) {
         if (me == you) return;
-        const double x_ij = my_x - s->x[you], y_ij = my_y - s->y[you];
+        const double x_ij = my_x - (s->x[you] + sx), y_ij = my_y - (s->y[you] + sy);
         const double r2 = x_ij * x_ij + y_ij * y_ij;
         if (r2 > h_eff_sq) return;
         const double r = std::sqrt(r2);
@@ -630,7 +673,7 @@ void classical_SPH(orc_state* s, int me) {
         Lr = std::fma(L, my_rho - s->rho[you], Lr);
     });
     if (p.target_problem == 1) {
-        s->RHS_u[me] = Lu + ((2.0 * (PI * PI)) * std::sin(PI * (my_x - p.WL_thick))) * std::cos(PI * (my_y - p.WL_thick));
+        s->RHS_u[me] = Lu + p1_source(p, my_x, my_y);
     } else {
         const double delta = ((p.coe_delta_sph * p.sound_speed) * h) * p.zeta_RSST;
         double Rr = -(my_rho * (du_dx + dv_dy)) + delta * Lr;
@@ -795,7 +838,7 @@ void interpolate_LSSPH_B(orc_state* s, int me) {
     int info = 0;
     lssph_b_point(p, q, nb, s->vm_x[me], s->vm_y[me],
                   [&](auto&& f) {
-                      for_candidates(s, s->idx_VM[me], [&](int you) {
+                      for_candidates(s, s->idx_VM[me], [&](int you, double, double) {
                           if (s->ptype[you] == 0) f(you);
                       });
                   },
@@ -816,7 +859,7 @@ void interpolate_CSPH(orc_state* s, int me) {
     const double my_x = s->vm_x[me], my_y = s->vm_y[me];
     double u = 0, v = 0, pre = 0, tem = 0, sw = 0;
     int num_neighbors = 0;
-    for_candidates(s, s->idx_VM[me], [&](int you) {
+    for_candidates(s, s->idx_VM[me], [&](int you, double, double) {
         if (s->ptype[you] != 0) return;
         const double x_ij = my_x - s->x[you], y_ij = my_y - s->y[you];
         const double r2 = x_ij * x_ij + y_ij * y_ij;
@@ -948,6 +991,7 @@ void RK2(orc_state* s) {
             if (!P1) {
                 s->x[me] = s->x_old[me] + s->u[me] * dt_eff;
                 s->y[me] = s->y_old[me] + s->v[me] * dt_eff;
+                if (p.periodic) { s->x[me] = wrap_pos(s->x[me], p.len_x); s->y[me] = wrap_pos(s->y[me], p.len_y); }
                 s->v[me] = s->v_old[me] + s->RHS_v[me] * dt_eff;
                 s->rho[me] = s->rho_old[me] + s->RHS_rho[me] * dt_eff;
             }
@@ -996,6 +1040,7 @@ void RK4(orc_state* s) {
                 if (!P1) {
                     s->x[me] = s->x_old[me] + s->u[me] * dt_2;
                     s->y[me] = s->y_old[me] + s->v[me] * dt_2;
+                    if (p.periodic) { s->x[me] = wrap_pos(s->x[me], p.len_x); s->y[me] = wrap_pos(s->y[me], p.len_y); }
                     s->v[me] = s->v_old[me] + s->RHS_v[me] * dt_2;
                     s->rho[me] = s->rho_old[me] + s->RHS_rho[me] * dt_2;
                 }
@@ -1006,6 +1051,7 @@ void RK4(orc_state* s) {
                 if (!P1) {
                     s->v[me] = s->v_new[me]; s->x[me] = s->x_new[me]; s->y[me] = s->y_new[me];
                     s->rho[me] = s->rho_new[me];
+                    if (p.periodic) { s->x[me] = wrap_pos(s->x[me], p.len_x); s->y[me] = wrap_pos(s->y[me], p.len_y); }
                 }
                 if (s->has_tem) s->tem[me] = s->tem_new[me];
             }
@@ -1031,9 +1077,9 @@ void shift_interpolate(orc_state* s, int me, double coe_PST) {
     double M[400] = {0}, b[80] = {0}, a[20] = {0};
     double dx = 0.0, dy = 0.0;
     int num_neighbors = 0;
-    for_candidates(s, s->idx_SP[me], [&](int you) {
+    for_candidates(s, s->idx_SP[me], [&](int you, double sx, double sy) {
         if (me == you) return;
-        const double x_ji = s->x[you] - my_x, y_ji = s->y[you] - my_y;
+        const double x_ji = (s->x[you] + sx) - my_x, y_ji = (s->y[you] + sy) - my_y;
         const double r2 = x_ji * x_ji + y_ji * y_ji;
         if (r2 > h_eff_sq) return;
         const double r = std::sqrt(r2);
@@ -1105,6 +1151,7 @@ void PST(orc_state* s) {
     for (int me = 0; me < n; ++me) {
         s->x[me] = s->x_old[me]; s->y[me] = s->y_old[me]; s->u[me] = s->u_old[me];
         s->v[me] = s->v_old[me]; s->rho[me] = s->rho_old[me];
+        if (p.periodic) { s->x[me] = wrap_pos(s->x[me], p.len_x); s->y[me] = wrap_pos(s->y[me], p.len_y); }
         if (s->has_tem) s->tem[me] = s->tem_old[me];
         s->pre[me] = c_sq * (s->rho[me] - rho_ref);
     }
@@ -1352,10 +1399,10 @@ int64_t orc_neighbors_csr(const orc_state* s, int which, int32_t* offsets, int32
         const double mx = which == 0 ? s->x[me] : s->vm_x[me];
         const double my = which == 0 ? s->y[me] : s->vm_y[me];
         const int cell = which == 0 ? s->idx_SP[me] : s->idx_VM[me];
-        for_candidates(s, cell, [&](int you) {
+        for_candidates(s, cell, [&](int you, double sx, double sy) {
             if (which == 0 && you == me) return;
             if (which == 1 && s->ptype[you] != 0) return;
-            const double xj = s->x[you] - mx, yj = s->y[you] - my;
+            const double xj = (s->x[you] + sx) - mx, yj = (s->y[you] + sy) - my;
             if (xj * xj + yj * yj > h_eff_sq) return;
             tmp.push_back(you);
         });

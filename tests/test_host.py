@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) == set(_abi.exported_names())
-    assert lib.lssph_abi_version() == 1
+    assert lib.lssph_abi_version() == 2
     assert lib.lssph_params_sizeof() == C.sizeof(lssph.Params)
 
 

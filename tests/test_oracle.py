@@ -179,3 +179,37 @@ def test_taylor_green_decays_at_the_analytic_rate():
     sigma = p.kinematic_vis * 2 * (2 * np.pi) ** 2
     expect = np.exp(-2 * sigma * n * p.dt)
     assert e / e0 == pytest.approx(expect, rel=2e-2)
+
+
+# Periodic-domain extension (no counterpart in the reference, so not reference-pinned):
+# pinned to the analytic solutions instead.
+def test_periodic_diffusion_decays_at_the_analytic_rate():
+    # u = sin(2 pi x) sin(2 pi y) exp(-8 pi^2 t) with nu = 1, on the jittered lattice
+    errs = []
+    for num in (32, 64):
+        p = lssph.diffusion_params(num=num, seed=3, PERIODIC=1)
+        orc = O.Oracle(p)
+        n = 100
+        orc.run(n)
+        o, ni = orc.get(), orc.num_int
+        assert orc.num_total == ni == num * num          # no ghost particles
+        ex = np.sin(2 * np.pi * o["x"][:ni]) * np.sin(2 * np.pi * o["y"][:ni]) * np.exp(-8 * np.pi ** 2 * n * p.dt)
+        errs.append(np.linalg.norm(o["u"][:ni] - ex) / np.linalg.norm(ex))
+    assert errs[1] < 5e-3 and errs[1] < errs[0] / 3      # converges with resolution
+
+
+def test_periodic_taylor_green_decays_at_the_analytic_rate():
+    p = lssph.taylor_green_params(num=64, PERIODIC=1)
+    orc = O.Oracle(p)
+    n = 200
+    orc.run(n)
+    o = orc.get()
+    amp = np.sqrt(np.mean(o["u"] ** 2 + o["v"] ** 2) / 0.5)
+    exact = np.exp(-8 * np.pi ** 2 * p.kinematic_vis * n * p.dt)
+    assert abs(amp - exact) < 2e-3
+    assert (o["x"] > 0).all() and (o["x"] <= p.len_x).all() and (o["y"] > 0).all() and (o["y"] <= p.len_y).all()
+
+
+def test_periodic_rejects_wall_problems():
+    with pytest.raises(lssph.LssphError):
+        lssph.cavity_params(num=32, PERIODIC=1)
