@@ -31,18 +31,23 @@ sys.path.insert(0, os.path.join(ROOT, "ls-sph-benchmarks_b200"))
 
 METRIC = "particle-updates/s per RK step"
 UNIT = "particle-updates/s"
-WORKLOAD = "taylor_green_re100_128x128_rk4_pst_fp64"
+WORKLOAD = "taylor_green_re100_128x128_periodic_rk4_pst_fp64"
 
 
-def _params(lanes: int = 0):
+def _params(lanes: int = 0, periodic: bool = True):
+    """Taylor-Green, Re = 100, 128^2, RK4 + PST, CFL 0.1.  periodic: the benchmark's periodic
+    unit square (its u = -cos 2pi x sin 2pi y is the reference's sin 2pi x cos 2pi y moved by
+    a quarter period, the same flow); else the reference's free-slip closed box."""
     import lssph
-    return lssph.taylor_green_params(num=128, re=100.0, coe_cfl=0.1, tg=2, lanes=lanes)
+    return lssph.taylor_green_params(num=128, re=100.0, coe_cfl=0.1, tg=2, lanes=lanes,
+                                     PERIODIC=1 if periodic else 0)
 
 
 def _config(p, extra=None):
     cfg = {"workload": WORKLOAD, "problem": "taylor_green", "num_x": p.num_x, "num_y": p.num_y,
            "num_int": None, "num_total": None, "rk": p.rk, "pst": True, "re": 1.0 / p.vis_ref,
-           "dt": p.dt, "precision": "fp64", "l2": "flushed between timed steps (256 MB write)"}
+           "dt": p.dt, "precision": "fp64", "domain": "periodic unit square" if p.periodic else "closed box",
+           "l2": "flushed between timed steps (256 MB write)"}
     if extra:
         cfg.update(extra)
     return cfg
@@ -163,7 +168,7 @@ def _dist():
 
 def _profile_traffic():
     """DRAM bytes per k_stage launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "k_stage_taylor_green_128.txt")
+    path = os.path.join(ROOT, "profiles", "k_stage_taylor_green_128_periodic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -317,6 +322,23 @@ def bench_mixed(steps: int = 100, acc_steps: int = 500) -> dict:
     out["rel_l2_vs_fp64"] = {k: float(np.linalg.norm(getattr(gmx, k)[:ni] - getattr(g64, k)[:ni]) /
                                       np.linalg.norm(getattr(g64, k)[:ni])) for k in ("x", "y", "u", "v", "rho", "pre")}
     out["rel_l2_after_steps"] = acc_steps
+    return out
+
+
+def bench_closed_box(steps: int = 300) -> dict:
+    """The same Taylor-Green 128^2 workload in the reference's own free-slip closed box
+    (wall ghosts and the overlapped ghost schedule): device particle-updates/s over
+    `steps` steps of one lssph_step call (5 MB working set, L2-resident either way)."""
+    import lssph
+    p = _params(periodic=False)
+    sim = lssph.Simulation.new(p)
+    sim.step(5)
+    sim.step(steps)
+    ms, nl = sim.last_step_stats()
+    out = {"workload": "taylor_green_re100_128x128_closed_box_rk4_pst_fp64", "steps": steps,
+           "value": sim.num_int * steps / (ms * 1e-3), "unit": UNIT, "us_per_step": 1e3 * ms / steps,
+           "num_int": sim.num_int, "num_total": sim.num_total, "schedule": sim.tuning()}
+    sim.close()
     return out
 
 
@@ -619,6 +641,16 @@ def run_engine(args) -> int:
         dist.barrier()
     value = ws * ni * args.steps / (dev_ms * 1e-3)
 
+    # velocity error against the analytic decay exp(-8 pi^2 nu t) after the timed steps
+    cur = sim.download()
+    t_now = (args.warmup + args.steps) * p.dt
+    dec = np.exp(-8.0 * np.pi ** 2 * p.kinematic_vis * t_now)
+    xs, ys = cur.x[:ni] - p.WL_thick, cur.y[:ni] - p.WL_thick
+    ue = np.sin(2 * np.pi * xs) * np.cos(2 * np.pi * ys) * dec
+    ve = -np.cos(2 * np.pi * xs) * np.sin(2 * np.pi * ys) * dec
+    l2_analytic = float(np.sqrt((np.sum((cur.u[:ni] - ue) ** 2) + np.sum((cur.v[:ni] - ve) ** 2)) /
+                                (np.sum(ue ** 2) + np.sum(ve ** 2))))
+
     # ---- per-kernel device times (same launch sequence, un-graphed, events per launch) ----
     prof_steps = max(5, min(50, args.steps))
     prof = sim.step_profiled(prof_steps)
@@ -673,6 +705,7 @@ def run_engine(args) -> int:
         cpu = cpu_baseline()
     extras = {}
     if rank == 0 and ws == 1 and not args.no_extras:
+        extras["closed_box"] = bench_closed_box()
         extras["mixed"] = bench_mixed()
         extras["batched"] = bench_batched()
         extras["serving"] = bench_serving()
@@ -693,6 +726,8 @@ def run_engine(args) -> int:
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "particle_stages_per_s": value * p.rk,
+            "velocity_rel_l2_vs_analytic": {"value": l2_analytic, "t": t_now,
+                                            "steps": args.warmup + args.steps},
             "clocks": clocks.summary(), **extras}
     print(json.dumps(line), flush=True)
     return 0
