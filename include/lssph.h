@@ -213,9 +213,10 @@ int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32
                     double* tem);
 
 /* Kernel configuration the handle runs (no counterpart in the reference): lanes per
-   particle, and whether the stage/PST kernels use the tight register budget (1) or the
-   loose one (0), with the RHS-pass time of each measured when the handle was created.
-   The budget is picked by that measurement; it never changes a result. */
+   particle, and the register budget of the stage/PST kernels: 0 loose, 1 tight (four CTAs
+   per SM), 2 five CTAs per SM (FP64 q = 5 only), with the RHS-pass time of the loose and
+   tight budgets measured when the handle was created.  The budget is picked by that
+   measurement; it never changes a result. */
 int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
                      double* rhs_us_tight);
 

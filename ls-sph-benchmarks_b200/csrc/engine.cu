@@ -176,11 +176,15 @@ void run_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
         return;
     }
     if (h->preparing) {
-        smem_optin(k_stage<NB, GG, false, MX>);
-        smem_optin(k_stage<NB, GG, true, MX>);
+        smem_optin(k_stage<NB, GG, 0, MX>);
+        smem_optin(k_stage<NB, GG, 1, MX>);
+        if constexpr (!MX) smem_optin(k_stage<NB, GG, 2, MX>);
         return;
     }
-    auto kern = h->tight ? k_stage<NB, GG, true, MX> : k_stage<NB, GG, false, MX>;
+    auto kern = h->tight ? k_stage<NB, GG, 1, MX> : k_stage<NB, GG, 0, MX>;
+    if constexpr (!MX) {
+        if (h->budget == 2) kern = k_stage<NB, GG, 2, MX>;
+    }
     launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P, h->F[h->sb],
                     h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, S, h->sc, h->ntx,
                     w.tiles);
@@ -277,11 +281,15 @@ void run_pst(lssph_handle* h, const Where& w) {
         return;
     }
     if (h->preparing) {
-        smem_optin(k_pst<NB, GG, false, MX>);
-        smem_optin(k_pst<NB, GG, true, MX>);
+        smem_optin(k_pst<NB, GG, 0, MX>);
+        smem_optin(k_pst<NB, GG, 1, MX>);
+        if constexpr (!MX) smem_optin(k_pst<NB, GG, 2, MX>);
         return;
     }
-    auto kern = h->tight ? k_pst<NB, GG, true, MX> : k_pst<NB, GG, false, MX>;
+    auto kern = h->tight ? k_pst<NB, GG, 1, MX> : k_pst<NB, GG, 0, MX>;
+    if constexpr (!MX) {
+        if (h->budget == 2) kern = k_pst<NB, GG, 2, MX>;
+    }
     launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P, h->F[h->sb],
                     h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, h->sc, h->ntx,
                     w.tiles);
@@ -439,13 +447,19 @@ int autotune(lssph_handle* h) {
     S.stage = 1;
     S.write_rhs = 1;
     const int64_t c0 = h->launch_counter;
-    const char* force = std::getenv("LSSPH_REGISTER_BUDGET");   // "loose" / "tight": skip the timing
-    if (force && (std::strcmp(force, "loose") == 0 || std::strcmp(force, "tight") == 0)) {
-        h->tight = std::strcmp(force, "tight") == 0;
+    // level 2 (five CTAs per SM) exists for the FP64 q = 5 stage and PST kernels
+    const int levels = (!h->mixed && !h->classical && h->order == 2) ? 3 : 2;
+    // LSSPH_REGISTER_BUDGET = loose / tight / five: skip the timing
+    const char* force = std::getenv("LSSPH_REGISTER_BUDGET");
+    if (force && (std::strcmp(force, "loose") == 0 || std::strcmp(force, "tight") == 0 ||
+                  std::strcmp(force, "five") == 0)) {
+        h->budget = std::strcmp(force, "loose") == 0 ? 0 : (std::strcmp(force, "tight") == 0 ? 1 : levels - 1);
+        h->tight = h->budget >= 1;
         return LSSPH_OK;
     }
-    for (int t = 0; t < 2; ++t) {
-        h->tight = t == 1;
+    for (int t = 0; t < levels; ++t) {
+        h->tight = t >= 1;
+        h->budget = t;
         launch_stage_any(h, S);   // warm-up (instruction cache, L2)
         CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
         for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
@@ -458,7 +472,12 @@ int autotune(lssph_handle* h) {
     // In the overlapped step the interior tiles share the SMs with the ghost launch: four
     // CTAs per SM (the tight budget) leave room for it where three do not, which an RHS
     // pass alone does not show, so the overlapped step always takes the tight budget.
-    h->tight = h->overlap ? true : (h->tune_us[1] < h->tune_us[0]);
+    int best = 0;
+    for (int t = 1; t < levels; ++t)
+        if (h->tune_us[t] < h->tune_us[best]) best = t;
+    if (h->overlap) best = 1;
+    h->budget = best;
+    h->tight = best >= 1;
     h->launch_counter = c0;
     return sync_check(h);
 }
@@ -1169,7 +1188,7 @@ int lssph_get_tuning(const lssph_handle* hc, int32_t* lanes, int32_t* tight, dou
     lssph_handle* h = const_cast<lssph_handle*>(hc);   // the measurement is a cache
     if (const int rc = ensure_tuned(h)) return rc;
     if (lanes) *lanes = h->G;
-    if (tight) *tight = h->tight ? 1 : 0;
+    if (tight) *tight = h->budget;
     if (rhs_us_loose) *rhs_us_loose = h->tune_us[0];
     if (rhs_us_tight) *rhs_us_tight = h->tune_us[1];
     return LSSPH_OK;

@@ -29,8 +29,9 @@ struct lssph_handle {
     bool hi_thread = false;             // order >= 3: thread per particle (else warp per particle)
     bool pdl = true;                    // programmatic dependent launches in the time step
     bool tuned = false;                 // register budget measured (first solo launch)
-    bool tight = false;                 // register budget of stage/PST kernels (autotuned)
-    double tune_us[2] = {0.0, 0.0};     // RHS pass time with the loose / tight budget
+    bool tight = false;                 // register budget of stage/PST kernels (autotuned): 4 CTAs/SM or more
+    int budget = 0;                     // 0 loose, 1 tight (4 CTAs/SM), 2 five CTAs/SM (FP64 q = 5 solo)
+    double tune_us[3] = {0.0, 0.0, 0.0};   // RHS pass time per budget level
     lssph::CellGrid grid;
     lssph::VirtualMarkers vm;
     std::vector<int32_t> ptype;

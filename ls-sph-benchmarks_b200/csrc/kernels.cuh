@@ -485,8 +485,11 @@ constexpr int PPB = LSSPH_PPB;              // particles per pass: a CTA has PPB
 // registers per thread, 3 CTAs of 128 threads per SM).  Tight: at most 128 registers, so
 // that 512 threads fit per SM, for a few spilled values.  Both compute identical results;
 // which is faster depends on how many tiles a launch has, and each handle times both.
-__host__ __device__ constexpr int tile_min_blocks(int G, bool tight) {
-    return (tight && PPB * G <= 512) ? 512 / (PPB * G) : 1;
+// Level 2 (FP64 single solves only): at most 102 registers, 640 threads per SM, so that a
+// launch of up to 5 CTAs per SM fits one wave.
+__host__ __device__ constexpr int tile_min_blocks(int G, int tight) {
+    return tight == 2 ? (PPB * G <= 640 ? 640 / (PPB * G) : 1)
+                      : ((tight && PPB * G <= 512) ? 512 / (PPB * G) : 1);
 }
 static_assert(HC <= 32 && OC <= 32, "tile scans run in one warp");
 
@@ -514,7 +517,7 @@ struct SmemView {
     double* sums;   // [PPB][row stride]
     double *x, *y, *u, *v, *rho, *pre, *vol, *tem;
     int *idx, *own_k, *own_hc;
-    int* nbr;   // in-radius lists, entry e of thread t at nbr[e * blockDim.x + t]
+    unsigned short* nbr;   // in-radius lists (staged indices), entry e of thread t at nbr[e * blockDim.x + t]
 };
 
 // Per-thread in-radius list length: a lane tests at most ceil(9 cap / G) candidates.
@@ -529,9 +532,11 @@ constexpr int SUMS_MAX = sums_stride(15 + 5 * 5 + 1);
 // Dynamic shared memory of one tile CTA; temperature is staged only when `tem` is set.
 __host__ __device__ inline size_t tile_smem_bytes(int cap, int G, bool tem) {
     const size_t maxp = (size_t)HC * cap, maxo = (size_t)OC * cap;
-    const size_t lists = (size_t)PPB * G * nbr_list_len(cap, G);
+    // 16-bit hit lists; the same area is the staging scratch of maxp ints
+    const size_t lists = (size_t)PPB * G * nbr_list_len(cap, G) * sizeof(unsigned short);
+    const size_t area = lists > maxp * sizeof(int) ? lists : maxp * sizeof(int);
     return (size_t)PPB * SUMS_MAX * sizeof(double) + maxp * ((tem ? 8 : 7) * sizeof(double) + sizeof(int)) +
-           2 * maxo * sizeof(int) + lists * sizeof(int);
+           2 * maxo * sizeof(int) + ((area + 7) & ~(size_t)7);
 }
 
 template <bool TEM>
@@ -545,7 +550,7 @@ __device__ __forceinline__ SmemView smem_view(void* raw, int cap) {
     S.pre = d + 5 * maxp; S.vol = d + 6 * maxp; S.tem = TEM ? d + 7 * maxp : nullptr;
     int* q = reinterpret_cast<int*>(d + (TEM ? 8 : 7) * maxp);
     S.idx = q; S.own_k = q + maxp; S.own_hc = q + maxp + maxo;
-    S.nbr = q + maxp + 2 * maxo;
+    S.nbr = reinterpret_cast<unsigned short*>(q + maxp + 2 * maxo);
     return S;
 }
 
@@ -813,12 +818,12 @@ __device__ __forceinline__ int tile_pairs(const TileHdr& T, const SmemView& S, b
                                           int skip, double mx, double my, double h_eff_sq, Fn&& f) {
     int nl = 0;
     const int stride = blockDim.x;
-    int* list = S.nbr + threadIdx.x;
+    unsigned short* list = S.nbr + threadIdx.x;
     if (active) {
         for_tile_candidates<G>(T, hc, lane, [&](int k) {
             const double xji = S.x[k] - mx;
             const double yji = S.y[k] - my;
-            if (k != skip && !(xji * xji + yji * yji > h_eff_sq)) { list[nl * stride] = k; ++nl; }
+            if (k != skip && !(xji * xji + yji * yji > h_eff_sq)) { list[nl * stride] = (unsigned short)k; ++nl; }
         });
     }
     if constexpr (G == 1) {
@@ -1428,7 +1433,7 @@ __device__ __forceinline__ void stage_body_classical(const Phys& P, const Fld& c
     }
 }
 
-template <int NB, int G, bool TIGHT = false>
+template <int NB, int G, int TIGHT = 0>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_stage_classical(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln,
                       const int* __restrict__ gstart, const int* __restrict__ glist, const Work W, const StageCfg S,
@@ -1445,7 +1450,7 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
     else stage_body_fp64<NB, G, false>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
 }
 
-template <int NB, int G, bool TIGHT = false, bool MIXED = false>
+template <int NB, int G, int TIGHT = 0, bool MIXED = false>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
             const int* __restrict__ glist, const Work W, const StageCfg S, Scalars* sc, int ntx,
@@ -1946,7 +1951,7 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
     else pst_body_fp64<NB, G, false, K>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
 }
 
-template <int NB, int G, bool TIGHT = false, bool MIXED = false, int K = 2>
+template <int NB, int G, int TIGHT = 0, bool MIXED = false, int K = 2>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
           const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
@@ -1998,7 +2003,7 @@ __device__ __forceinline__ const SolveDesc& load_desc(const SolveDesc* D, int s,
     return sd;
 }
 
-template <int NB, int G, bool TIGHT = false, bool MIXED = false>
+template <int NB, int G, int TIGHT = 0, bool MIXED = false>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_stage(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
                                                     int ps, int pl) {
     __shared__ SolveDesc sd;
@@ -2024,7 +2029,7 @@ __global__ void __launch_bounds__(PPB * G) kb_ghost(const SolveDesc* __restrict_
                           zero_other ? d.L[prev_list(lb)].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
 }
 
-template <int NB, int G, bool TIGHT = false, bool MIXED = false>
+template <int NB, int G, int TIGHT = 0, bool MIXED = false>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(const SolveDesc* __restrict__ D, const BatchMap M, int ps, int pl) {
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];

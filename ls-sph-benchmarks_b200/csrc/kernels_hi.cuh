@@ -116,7 +116,7 @@ __device__ __forceinline__ SmemView hi_smem_view(void* raw, int cap, double*& wa
     V.pre = d + 5 * maxp; V.vol = d + 6 * maxp; V.tem = TEM ? d + 7 * maxp : nullptr;
     int* q = reinterpret_cast<int*>(d + (TEM ? 8 : 7) * maxp);
     V.idx = q; V.own_k = q + maxp; V.own_hc = q + maxp + maxo;
-    V.nbr = q + maxp + 2 * maxo;
+    V.nbr = reinterpret_cast<unsigned short*>(q + maxp + 2 * maxo);
     return V;
 }
 
@@ -323,7 +323,7 @@ __device__ __forceinline__ void stage_body_hi(const Phys& P, const Fld& cur, con
     const int n_own = T.own_off[OC];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double* wa = warp_area + warp * S::WARP_DOUBLES;
-    int* hits = SM.nbr + warp * 9 * P.cap;
+    int* hits = reinterpret_cast<int*>(SM.nbr) + warp * 9 * P.cap;
     int eu[S::PER], ev[S::PER];
     hi_entries<S>(eu, ev);
     double ih[5];
@@ -412,7 +412,7 @@ __device__ __forceinline__ void pst_body_hi(const Phys& P, const Fld& cur, const
     const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double* wa = warp_area + warp * S::WARP_DOUBLES;
-    int* hits = SM.nbr + warp * 9 * P.cap;
+    int* hits = reinterpret_cast<int*>(SM.nbr) + warp * 9 * P.cap;
     int eu[S::PER], ev[S::PER];
     hi_entries<S>(eu, ev);
     double ih[5];
@@ -548,7 +548,7 @@ __device__ __forceinline__ SmemView tpp_smem_view(void* raw, int cap, double*& s
     V.pre = d + 5 * maxp; V.vol = d + 6 * maxp; V.tem = TEM ? d + 7 * maxp : nullptr;
     int* q = reinterpret_cast<int*>(d + (TEM ? 8 : 7) * maxp);
     V.idx = q; V.own_k = q + maxp; V.own_hc = q + maxp + maxo;
-    V.nbr = q + maxp + 2 * maxo;   // staging scratch, then the per-thread hit chunks
+    V.nbr = reinterpret_cast<unsigned short*>(q + maxp + 2 * maxo);   // staging scratch, then the per-thread hit chunks
     return V;
 }
 

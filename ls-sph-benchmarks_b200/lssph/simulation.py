@@ -252,7 +252,7 @@ class Simulation:
         self._chk(self._lib.lssph_get_tuning(self._h, C.byref(lanes), C.byref(tight), C.byref(lo), C.byref(ti)))
         nt, ni, ov = C.c_int32(), C.c_int32(), C.c_int32()
         self._chk(self._lib.lssph_get_schedule(self._h, C.byref(nt), C.byref(ni), C.byref(ov)))
-        return {"lanes": lanes.value, "register_budget": "tight" if tight.value else "loose",
+        return {"lanes": lanes.value, "register_budget": ("loose", "tight", "five")[tight.value],
                 "rhs_us_loose": lo.value, "rhs_us_tight": ti.value, "tiles": nt.value,
                 "interior_tiles": ni.value, "ghost_overlap": bool(ov.value)}
 
