@@ -225,7 +225,7 @@ SolveDesc make_desc(const lssph_handle* h) {
     d.ntx = h->ntx;
     d.sb = h->sb;
     d.lb = h->lb;
-    d.nchunk = h->nvt;
+    d.nchunk = std::max(h->nvt, 1);   // a periodic solve (no ghosts) keeps one bookkeeping CTA
     const double dt = h->p.dt;   // the step sizes enq_stage (engine.cu) hands each stage
     if (h->p.rk == 2) {
         d.dt2[0] = dt / 2.0;
@@ -310,7 +310,7 @@ int rebuild(lssph_batch* b) {
             const lssph_handle* h = b->members[g.members[s]];
             desc.push_back(make_desc(h));
             for (int t = 0; t < h->ntiles; ++t) tiles.push_back(make_int2((int)s, t));
-            for (int c = 0; c < h->nvt; ++c) chunks.push_back(make_int2((int)s, c));
+            for (int c = 0; c < std::max(h->nvt, 1); ++c) chunks.push_back(make_int2((int)s, c));
             g.smem = std::max(g.smem, h->smem_bytes);
             g.smem_ghost = std::max(g.smem_ghost, h->smem_ghost);
             g.tight = g.tight || h->tight;
@@ -434,7 +434,6 @@ int lssph_batch_add(lssph_batch* b, lssph_handle* h) {
     if (b->in_flight) return bfail(b, LSSPH_E_BAD_PARAM, "a batch step call is in flight");
     if (h->p.sph_model != 3)
         return bfail(b, LSSPH_E_UNSUPPORTED, "batched solves run the 2nd-order LS-SPH model (SPH_MODEL 3) only");
-    if (h->p.periodic) return bfail(b, LSSPH_E_UNSUPPORTED, "batched solves run the closed box only");
     b->members.push_back(h);
     h->batch = b;
     b->dirty = true;

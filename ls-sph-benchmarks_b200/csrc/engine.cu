@@ -576,8 +576,6 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         return fail(nullptr, LSSPH_E_BAD_PARAM, "bad particle counts");
     if (pin->periodic && num_total != num_int)
         return fail(nullptr, LSSPH_E_BAD_PARAM, "a periodic domain has no ghost particles (num_total == num_int)");
-    if (pin->periodic && pin->precision == LSSPH_PRECISION_MIXED)
-        return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs the closed box only");
     for (int i = 0; i < num_total; ++i) {
         if ((i < num_int) != (ptype[i] == 0))
             return fail(nullptr, LSSPH_E_BAD_PARAM, "ptype must be 0 for the first num_int particles and 1..8 after");

@@ -719,12 +719,18 @@ __device__ __forceinline__ TileRef stage_fields_mx(const Phys& P, const Fld& F, 
         R.u = __ldg(F.u + j0); R.v = __ldg(F.v + j0); R.rho = __ldg(F.rho + j0); R.pre = __ldg(F.pre + j0);
         if (WITH_TEM) R.tem = __ldg(F.tem + j0);
     }
-    const double cw = sqrt(P.h_eff_sq);
+    const double cw = P.periodic ? 1.0 / P.inv_h_eff : sqrt(P.h_eff_sq);   // cell width
     const double x0 = (double)cx0 * cw, y0 = (double)cy0 * cw;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int j = S.idx[k];
-        S.ox[k] = (float)(__ldg(F.x + j) - x0);
-        S.oy[k] = (float)(__ldg(F.y + j) - y0);
+        double xj = __ldg(F.x + j), yj = __ldg(F.y + j);
+        if (P.periodic) {   // wrapped halo cells: positions shifted by -+Lx
+            const int h = halo_cell_of(T, k);
+            xj = xj + T.sx[h];
+            yj = yj + T.sy[h];
+        }
+        S.ox[k] = (float)(xj - x0);
+        S.oy[k] = (float)(yj - y0);
         S.u[k] = (float)(__ldg(F.u + j) - R.u);
         S.v[k] = (float)(__ldg(F.v + j) - R.v);
         S.rho[k] = (float)(__ldg(F.rho + j) - R.rho);
@@ -1484,6 +1490,10 @@ __device__ __forceinline__ void ghost_work(const Phys& P, const Fld& F, const Ls
         for (int c = chunk * blockDim.x + threadIdx.x; c < P.ncell; c += nchunk * blockDim.x) zero_cnt[c] = 0;
     }
     if (reset_umax && chunk == 0 && threadIdx.x == 0) sc->umax2 = 0ull;
+    if (P.num_ext == 0) {   // periodic domain: no ghosts, only the bookkeeping above (one chunk)
+        pdl_release();
+        return;
+    }
     constexpr int Q = (WQ == 1) ? 1 : WQ;
     constexpr int NU = Q * (Q + 1) / 2;
     __shared__ TileHdr T;
@@ -1926,7 +1936,8 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
                 for (int k = 0; k < Q; ++k) sacc = fma(a[k], sm[15 + 5 * c + k], sacc);
                 acc[c] = sacc;
             }
-            const double xn = my_x + dx, yn = my_y + dy;
+            double xn = my_x + dx, yn = my_y + dy;
+            if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
             const double un = my_u + acc[0], vn = my_v + acc[1], rn = my_rho + acc[2];
             nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
             nxt.pre[i] = P.c_sq * (rn - P.rho_ref);

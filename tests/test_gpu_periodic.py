@@ -99,13 +99,53 @@ def test_periodic_diffusion_matches_the_analytic_decay():
     sim.close()
 
 
-def test_periodic_is_rejected_where_unsupported():
-    p = lssph.taylor_green_params(num=32, PERIODIC=1)
-    with pytest.raises(lssph.LssphError):
-        lssph.Simulation.new(lssph.make_params(p, precision=lssph.PRECISION_MIXED), ghost=False)
-    sim = lssph.Simulation.new(p, ghost=False)
+def test_mixed_precision_periodic_within_bound():
+    # FP32 pair phase with the periodic shift in the FP32 offsets; bound as for the box
+    p = lssph.taylor_green_params(num=64, PERIODIC=1)
+    out = {}
+    for prec in (lssph.PRECISION_FP64, lssph.PRECISION_MIXED):
+        q = lssph.make_params(p, precision=prec)
+        st, ni = lssph.setup_particles(q)
+        st.u[:] += 2.0                       # particles cross the boundary
+        sim = lssph.Simulation(q, st, ni)
+        sim.step(100)
+        out[prec] = sim.download()
+        sim.close()
+    a, b = out[lssph.PRECISION_FP64], out[lssph.PRECISION_MIXED]
+    for k in ("u", "v", "rho"):
+        assert _rel_l2(getattr(b, k), getattr(a, k)) <= 1e-5, k
+    assert (b.x > 0).all() and (b.x <= p.len_x).all()
+
+
+def test_periodic_members_in_a_batch_equal_solo():
+    # periodic members (no ghosts: one bookkeeping CTA in the batched ghost launch) beside
+    # closed-box ones; each ends bit for bit as it does alone
+    mk = [lambda: lssph.taylor_green_params(num=48, PERIODIC=1),
+          lambda: lssph.diffusion_params(num=40, seed=2, PERIODIC=1),
+          lambda: lssph.cavity_params(num=40),
+          lambda: lssph.make_params(lssph.taylor_green_params(num=32, PERIODIC=1), precision=lssph.PRECISION_MIXED)]
+
+    def make(f, i):
+        p = f()
+        st, ni = lssph.setup_particles(p)
+        if p.target_problem == 2:
+            st.u[:ni] += 1.0
+        sim = lssph.Simulation(p, st, ni)
+        sim.ghost()
+        return sim
+
+    solo = [make(f, i) for i, f in enumerate(mk)]
+    mem = [make(f, i) for i, f in enumerate(mk)]
     b = lssph.Batch()
-    with pytest.raises(lssph.LssphError):
-        b.add(sim)
+    for m in mem:
+        b.add(m)
+    b.step(25)
+    for s in solo:
+        s.step(25)
+    for i, (s, m) in enumerate(zip(solo, mem)):
+        gs, gm = s.download(), m.download()
+        for k in FIELDS:
+            assert np.array_equal(getattr(gs, k), getattr(gm, k)), (i, k)
     b.close()
-    sim.close()
+    for x in solo + mem:
+        x.close()
