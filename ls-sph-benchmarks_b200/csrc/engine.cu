@@ -497,8 +497,14 @@ namespace {
 
 int check_scalars(lssph_handle* h, Scalars* out) {
     Scalars s{};
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    CUDA_TRY(h, cudaMemcpy(&s, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+    if (h->sc_host) {   // one copy into pinned memory behind the queued work, one sync
+        CUDA_TRY(h, cudaMemcpyAsync(h->sc_host, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        s = *h->sc_host;
+    } else {
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        CUDA_TRY(h, cudaMemcpy(&s, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+    }
     if (out) *out = s;
     // a NaN position also leaves the grid: report the root cause first
     if (s.err & ERR_NONFINITE) return fail(h, LSSPH_E_NONFINITE, "a non-finite value appeared in the particle state");
@@ -520,18 +526,26 @@ int rebuild_cells(lssph_handle* h) {
     return LSSPH_OK;
 }
 
+// The current buffer gets every particle.  On a later upload (both = false) the other buffer
+// needs the ghost particles only: the next stage (or PST) writes every interior field of it
+// before anything reads it -- except in problem 1, whose stages write u alone, so there it
+// gets every particle too.
 int upload_fields(lssph_handle* h, const double* x, const double* y, const double* u, const double* v,
-                  const double* rho, const double* pre, const double* tem) {
-    const size_t bytes = sizeof(double) * (size_t)h->num_total;
+                  const double* rho, const double* pre, const double* tem, bool both = true) {
     for (int b = 0; b < 2; ++b) {
         const Fld& F = h->F[b];
-        if (x) CUDA_TRY(h, cudaMemcpyAsync(F.x, x, bytes, cudaMemcpyHostToDevice, h->stream));
-        if (y) CUDA_TRY(h, cudaMemcpyAsync(F.y, y, bytes, cudaMemcpyHostToDevice, h->stream));
-        if (u) CUDA_TRY(h, cudaMemcpyAsync(F.u, u, bytes, cudaMemcpyHostToDevice, h->stream));
-        if (v) CUDA_TRY(h, cudaMemcpyAsync(F.v, v, bytes, cudaMemcpyHostToDevice, h->stream));
-        if (rho) CUDA_TRY(h, cudaMemcpyAsync(F.rho, rho, bytes, cudaMemcpyHostToDevice, h->stream));
-        if (pre) CUDA_TRY(h, cudaMemcpyAsync(F.pre, pre, bytes, cudaMemcpyHostToDevice, h->stream));
-        if (tem && h->has_tem) CUDA_TRY(h, cudaMemcpyAsync(F.tem, tem, bytes, cudaMemcpyHostToDevice, h->stream));
+        const size_t first = (both || b == h->sb || h->p1) ? 0 : (size_t)h->num_int;
+        const size_t n = (size_t)h->num_total - first;
+        if (n == 0) continue;
+        const size_t bytes = sizeof(double) * n;
+        if (x) CUDA_TRY(h, cudaMemcpyAsync(F.x + first, x + first, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (y) CUDA_TRY(h, cudaMemcpyAsync(F.y + first, y + first, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (u) CUDA_TRY(h, cudaMemcpyAsync(F.u + first, u + first, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (v) CUDA_TRY(h, cudaMemcpyAsync(F.v + first, v + first, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (rho) CUDA_TRY(h, cudaMemcpyAsync(F.rho + first, rho + first, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (pre) CUDA_TRY(h, cudaMemcpyAsync(F.pre + first, pre + first, bytes, cudaMemcpyHostToDevice, h->stream));
+        if (tem && h->has_tem)
+            CUDA_TRY(h, cudaMemcpyAsync(F.tem + first, tem + first, bytes, cudaMemcpyHostToDevice, h->stream));
         k_volume<<<blocks_for(h->num_total, 128), 128, 0, h->stream>>>(h->P, F);
     }
     return LSSPH_OK;
@@ -546,6 +560,7 @@ void free_handle(lssph_handle* h) {
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);
     if (h->block) cudaFree(h->block);
+    if (h->sc_host) cudaFreeHost(h->sc_host);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -707,6 +722,11 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     // one device block for every array of the solve (one cudaMalloc, one cudaFree)
     const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles);
     {
+        // pinned scalar copy target (optional: without it the checks copy through pageable memory)
+        if (cudaMallocHost((void**)&h->sc_host, sizeof(Scalars)) != cudaSuccess) {
+            h->sc_host = nullptr;
+            cudaGetLastError();
+        }
         const cudaError_t e = cudaMalloc(&h->block, block);
         if (e != cudaSuccess) {
             free_handle(h);
@@ -1022,7 +1042,7 @@ int lssph_get_progress(lssph_handle* h, int32_t* steps_done, int32_t* stopped) {
 int lssph_upload(lssph_handle* h, const double* x, const double* y, const double* u, const double* v,
                  const double* rho, const double* pre, const double* tem) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
-    int rc = upload_fields(h, x, y, u, v, rho, pre, tem);
+    int rc = upload_fields(h, x, y, u, v, rho, pre, tem, false);
     if (rc != LSSPH_OK) return rc;
     if (!h->p1 && (x || y)) {
         if ((rc = rebuild_cells(h)) != LSSPH_OK) return rc;

@@ -61,6 +61,7 @@ struct lssph_handle {
     size_t smem_ghost = 0;              // ... of ghost CTAs
     bool preparing = false;             // launch helpers only set kernel attributes
     lssph::Scalars* sc = nullptr;
+    lssph::Scalars* sc_host = nullptr;  // pinned copy target for the scalar checks
     int sb = 0, lb = 0;
     cudaGraphExec_t graph[2][lssph::kLists] = {};   // per (state parity, list index)
     int graph_launches = 0;   // kernels per captured step

@@ -94,3 +94,27 @@ def test_restart_from_async_snapshot_is_bit_identical(case, tmp_path):
         assert np.array_equal(getattr(g, k), getattr(r, k)), k
     run.close()
     resumed.close()
+
+
+@pytest.mark.parametrize("case", ["diffusion", "taylor_green", "cavity", "boussinesq", "tg_periodic", "tg_mixed",
+                                  "cavity_classical"])
+def test_upload_mid_run_continues_bit_identically(case):
+    # lssph_upload into a solve at another point of its run (other buffer parity, other
+    # list rotation): the state it continues from is the uploaded one, nothing else
+    mk = dict(CASES)
+    mk["tg_periodic"] = lambda: lssph.taylor_green_params(num=48, PERIODIC=1)
+    mk["tg_mixed"] = lambda: lssph.make_params(lssph.taylor_green_params(num=48), precision=lssph.PRECISION_MIXED)
+    mk["cavity_classical"] = lambda: lssph.cavity_params(num=40, SPH_MODEL=1)
+    p = mk[case]()
+    a, b = _sim(p), _sim(p)
+    a.step(10)
+    mid = a.download()
+    a.step(10)
+    b.step(3)                 # b is elsewhere in its run
+    b.upload(mid)
+    b.step(10)
+    ga, gb = a.download(), b.download()
+    for k in ("x", "y", "u", "v", "rho", "pre") + (("tem",) if p.target_problem == 4 else ()):
+        assert np.array_equal(getattr(ga, k), getattr(gb, k)), k
+    a.close()
+    b.close()
