@@ -216,3 +216,38 @@ def test_classical_rejects_mixed_precision():
     st, ni = lssph.setup_particles(p)
     with pytest.raises(lssph.LssphError):
         lssph.Simulation(p, st, ni)
+
+
+# Known answers independent of the oracle: order-k LS differentiates degree-k polynomials
+# exactly (up to round-off), and LS type B reproduces linear fields at the virtual markers.
+from test_oracle import POLY_CASES, _poly_case  # noqa: E402
+
+
+@pytest.mark.parametrize("sm,deg,kw", POLY_CASES)
+@pytest.mark.parametrize("shape", ["thread", "warp"])
+def test_gpu_reproduces_polynomials_of_its_order(sm, deg, kw, shape, monkeypatch):
+    monkeypatch.setenv("LSSPH_HI_KERNEL", shape)
+    p, st, ni, lap, src = _poly_case(sm, deg, kw)
+    sim = lssph.Simulation(p, st, ni)
+    sim.calculate_rhs()
+    err = np.abs((sim.rhs()["u"] - src) - lap).max() / np.abs(lap).max()
+    assert err < 1e-10, err
+    sim.close()
+
+
+def test_gpu_ls_type_b_interpolates_linear_fields_exactly():
+    p = lssph.cavity_params(num=32)
+    st, ni = lssph.setup_particles(p)
+    rng = np.random.default_rng(3)
+    st.x[:ni] += 0.15 * p.dx * (2 * rng.random(ni) - 1)
+    st.y[:ni] += 0.15 * p.dx * (2 * rng.random(ni) - 1)
+    st.u[:] = 0.3 + 1.7 * st.x - 0.4 * st.y
+    st.v[:] = -0.2 + 0.5 * st.x + 2.1 * st.y
+    st.pre[:] = 1.0 - 3.0 * st.x + 0.25 * st.y
+    sim = lssph.Simulation(p, st, ni)
+    sim.ghost()
+    vm = sim.virtual_markers()
+    np.testing.assert_allclose(vm["u"], 0.3 + 1.7 * vm["x"] - 0.4 * vm["y"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(vm["v"], -0.2 + 0.5 * vm["x"] + 2.1 * vm["y"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(vm["pre"], 1.0 - 3.0 * vm["x"] + 0.25 * vm["y"], rtol=0, atol=1e-11)
+    sim.close()

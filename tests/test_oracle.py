@@ -213,3 +213,50 @@ def test_periodic_taylor_green_decays_at_the_analytic_rate():
 def test_periodic_rejects_wall_problems():
     with pytest.raises(lssph.LssphError):
         lssph.cavity_params(num=32, PERIODIC=1)
+
+
+def _poly_case(sm, deg, kw):
+    # a random polynomial of degree `deg` on a jittered problem-1 lattice, and its Laplacian
+    p = lssph.diffusion_params(num=30, pos_pert=0.2, seed=7, SPH_MODEL=sm, **kw)
+    st, ni = lssph.setup_particles(p)
+    X, Y = st.x - p.WL_thick, st.y - p.WL_thick
+    rng = np.random.default_rng(sm)
+    coef = {(i, j): rng.normal() for i in range(deg + 1) for j in range(deg + 1 - i)}
+    st.u[:] = sum(c * X ** i * Y ** j for (i, j), c in coef.items())
+    lap = sum(c * (i * (i - 1) * X ** max(i - 2, 0) * Y ** j + j * (j - 1) * X ** i * Y ** max(j - 2, 0))
+              for (i, j), c in coef.items())
+    x, y = st.x[:ni], st.y[:ni]
+    src = 2 * np.pi ** 2 * np.sin(np.pi * (x - p.WL_thick)) * np.cos(np.pi * (y - p.WL_thick))
+    return p, st, ni, lap[:ni], src
+
+
+POLY_CASES = [(3, 2, {}), (4, 3, {}), (5, 4, {}), (6, 5, {"KERNEL_TYPE": 2})]
+
+
+@pytest.mark.parametrize("sm,deg,kw", POLY_CASES)
+def test_ls_type_a_reproduces_polynomials_of_its_order(sm, deg, kw):
+    # order-k LS (SPH_MODEL 3..6) differentiates degree-k polynomials exactly on any cloud
+    # with enough neighbours: problem 1's RHS minus its source is the exact Laplacian
+    p, st, ni, lap, src = _poly_case(sm, deg, kw)
+    o = O.Oracle(p, st, ni, ghost=False)
+    o.calculate_rhs()
+    err = np.abs((o.rhs()["u"] - src) - lap).max() / np.abs(lap).max()
+    assert err < 1e-10, err
+
+
+def test_ls_type_b_interpolates_linear_fields_exactly():
+    # LS type B (q = 3, interpolate_LSSPH_B_mod.f90) reproduces a linear field exactly at
+    # every virtual marker (fluid-only neighbours)
+    p = lssph.cavity_params(num=32)
+    st, ni = lssph.setup_particles(p)
+    rng = np.random.default_rng(3)
+    st.x[:ni] += 0.15 * p.dx * (2 * rng.random(ni) - 1)
+    st.y[:ni] += 0.15 * p.dx * (2 * rng.random(ni) - 1)
+    st.u[:] = 0.3 + 1.7 * st.x - 0.4 * st.y
+    st.v[:] = -0.2 + 0.5 * st.x + 2.1 * st.y
+    st.pre[:] = 1.0 - 3.0 * st.x + 0.25 * st.y
+    o = O.Oracle(p, st, ni, ghost=True)
+    vm = o.vm()
+    np.testing.assert_allclose(vm["u"], 0.3 + 1.7 * vm["x"] - 0.4 * vm["y"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(vm["v"], -0.2 + 0.5 * vm["x"] + 2.1 * vm["y"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(vm["pre"], 1.0 - 3.0 * vm["x"] + 0.25 * vm["y"], rtol=0, atol=1e-11)
