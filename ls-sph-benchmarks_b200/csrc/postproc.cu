@@ -239,11 +239,207 @@ __global__ void __launch_bounds__(128) k_pp_points(PConst pc, PGrid g, double sh
     o[2] = b[2] / pc.h;
 }
 
+// ---- q >= 10: one warp per point ----------------------------------------------------------
+// A q = 21 system (231 packed moments) does not fit one thread.  The warp compacts the hits
+// with a ballot (same order as the thread kernel: cells row by row, ascending index within a
+// cell), evaluates up to 32 hits at a time into a shared-memory table (w a_i, a_i, f), and
+// each lane adds the table rows to its own accumulator entries in hit order -- the thread
+// kernel's fma chain for each entry.  The pivoted elimination then runs with one matrix row
+// per lane.
+constexpr int PP_WARPS = 4;
+
+template <int Q>
+struct PPWarp {
+    static constexpr int QU = Q * (Q + 1) / 2;
+    static constexpr int E = QU + Q;              // moment entries, then b entries
+    static constexpr int PER = (E + 31) / 32;
+    static constexpr int RS = (2 * Q + 1) | 1;    // table row: w a_0..w a_{Q-1}, a_0..a_{Q-1}, f
+    static constexpr int TABLE = 32 * RS;
+    static constexpr int MS = (Q + 1) | 1;        // matrix row: M(i, 0..Q-1), b_i
+    static constexpr int MAT = Q * MS;
+    static constexpr int DOUBLES = TABLE > MAT ? TABLE : MAT;
+    static constexpr size_t BYTES = (size_t)PP_WARPS * (DOUBLES * sizeof(double) + 64 * sizeof(int));
+};
+
+template <int Q>
+__global__ void __launch_bounds__(32 * PP_WARPS) k_pp_points_warp(PConst pc, PGrid g, double shift,
+                                                                 const double* __restrict__ x, const double* __restrict__ y,
+                                                                 const double* __restrict__ val,
+                                                                 const double* __restrict__ rho,
+                                                                 const int* __restrict__ start,
+                                                                 const int* __restrict__ list, int nt,
+                                                                 const double* __restrict__ tx,
+                                                                 const double* __restrict__ ty, double* __restrict__ out) {
+    using S = PPWarp<Q>;
+    extern __shared__ double pp_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * PP_WARPS + warp;
+    if (t >= nt) return;   // whole warp
+    double* tab = pp_smem + warp * S::DOUBLES;
+    int* hits = reinterpret_cast<int*>(pp_smem + PP_WARPS * S::DOUBLES) + warp * 64;
+    // this lane's entries: e < QU -> moment (row j, col i), j <= i; else b_i
+    int eu[S::PER], ev[S::PER];
+#pragma unroll
+    for (int k = 0; k < S::PER; ++k) {
+        const int e = lane + 32 * k;
+        if (e < S::QU) {
+            int i = 0;
+            while ((i + 1) * (i + 2) / 2 <= e) ++i;
+            eu[k] = i;
+            ev[k] = Q + (e - i * (i + 1) / 2);   // a_j in the table's second block
+        } else if (e < S::E) {
+            eu[k] = e - S::QU;
+            ev[k] = 2 * Q;                        // f
+        } else {
+            eu[k] = -1;
+            ev[k] = 0;
+        }
+    }
+    double acc[S::PER];
+#pragma unroll
+    for (int k = 0; k < S::PER; ++k) acc[k] = 0.0;
+    const double px = tx[t], py = ty[t];
+    int n = 0, pending = 0;
+    // evaluate hits[0..m) into the table, add them to the entries
+    auto flush = [&](int m) {
+        if (lane < m) {
+            const int j = hits[lane];
+            const double dx = (x[j] - shift) - px, dy = (y[j] - shift) - py;
+            const double w = dev_W<double>(pc.kt, sqrt(dx * dx + dy * dy), pc.ih1, pc.wnorm) * (pc.mass / rho[j]);
+            double a[Q];
+            pp_basis<Q>(dx / pc.h, dy / pc.h, a);
+            double* row = tab + lane * S::RS;
+#pragma unroll
+            for (int i = 0; i < Q; ++i) { row[i] = w * a[i]; row[Q + i] = a[i]; }
+            row[2 * Q] = val[j];
+        }
+        __syncwarp();
+#pragma unroll 1
+        for (int h = 0; h < m; ++h) {
+            const double* row = tab + h * S::RS;
+#pragma unroll
+            for (int k = 0; k < S::PER; ++k)
+                if (eu[k] >= 0) acc[k] = fma(row[eu[k]], row[ev[k]], acc[k]);
+        }
+        __syncwarp();
+    };
+    const double fx = floor((px - g.x0) / g.he), fy = floor((py - g.y0) / g.he);
+    if (fx >= -1.0 && fx <= (double)g.ncx && fy >= -1.0 && fy <= (double)g.ncy) {
+        const int cx = (int)fx, cy = (int)fy;
+        for (int yy = max(cy - 1, 0); yy <= min(cy + 1, g.ncy - 1); ++yy)
+            for (int xx = max(cx - 1, 0); xx <= min(cx + 1, g.ncx - 1); ++xx) {
+                const int c = xx + yy * g.ncx, s0 = start[c], s1 = start[c + 1];
+                for (int b = s0; b < s1; b += 32) {
+                    const int s = b + lane;
+                    bool hit = false;
+                    int j = 0;
+                    if (s < s1) {
+                        j = list[s];
+                        const double dx = (x[j] - shift) - px, dy = (y[j] - shift) - py;
+                        hit = !(dx * dx + dy * dy > pc.he2);
+                    }
+                    const unsigned mk = __ballot_sync(0xffffffffu, hit);
+                    if (hit) hits[pending + __popc(mk & ((1u << lane) - 1u))] = j;
+                    pending += __popc(mk);
+                    n += __popc(mk);
+                    __syncwarp();
+                    if (pending >= 32) {   // evaluate 32, keep the rest (< 32) at the front
+                        flush(32);
+                        if (lane < pending - 32) hits[lane] = hits[32 + lane];
+                        pending -= 32;
+                        __syncwarp();
+                    }
+                }
+            }
+    }
+    if (pending > 0) flush(pending);
+    double* o = out + 3 * (size_t)t;
+    if (n < Q) {
+        if (lane == 0) o[0] = o[1] = o[2] = CUDART_NAN;
+        return;
+    }
+    // symmetric matrix rows; lane r < Q loads row r (M(r, 0..Q-1), b_r)
+    double* Mx = tab;
+#pragma unroll
+    for (int k = 0; k < S::PER; ++k) {
+        if (eu[k] < 0) continue;
+        if (ev[k] < 2 * Q) {
+            const int i = eu[k], j = ev[k] - Q;
+            Mx[i * S::MS + j] = acc[k];
+            Mx[j * S::MS + i] = acc[k];
+        } else {
+            Mx[eu[k] * S::MS + Q] = acc[k];
+        }
+    }
+    __syncwarp();
+    const bool live = lane < Q;
+    const int r = live ? lane : 0;
+    double A[Q];
+#pragma unroll
+    for (int j = 0; j < Q; ++j) A[j] = Mx[r * S::MS + j];
+    double bv = Mx[r * S::MS + Q];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        // pivot: the first row >= k with the largest |A(i,k)|; NaN never wins
+        const double mine = fabs(A[k]);
+        const double akk = __shfl_sync(0xffffffffu, mine, k);
+        double av = (live && lane >= k && !isnan(mine)) ? mine : -1.0;
+        int ai = lane;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, av, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, ai, off);
+            if (ov > av || (ov == av && oi < ai)) { av = ov; ai = oi; }
+        }
+        const int p = (isnan(akk) || !(av > akk)) ? k : ai;
+        const double apk = __shfl_sync(0xffffffffu, A[k], p);
+        if (apk == 0.0) { ok = false; break; }
+        if (p != k) {
+            const int src = lane == k ? p : (lane == p ? k : lane);
+#pragma unroll
+            for (int j = 0; j < Q; ++j) A[j] = __shfl_sync(0xffffffffu, A[j], src);
+            bv = __shfl_sync(0xffffffffu, bv, src);
+        }
+        const double l = A[k] * (1.0 / apk);
+#pragma unroll
+        for (int j = k + 1; j < Q; ++j) {
+            const double akj = __shfl_sync(0xffffffffu, A[j], k);
+            if (lane > k) A[j] = fma(-l, akj, A[j]);
+        }
+        const double bk = __shfl_sync(0xffffffffu, bv, k);
+        if (lane > k) bv = fma(-l, bk, bv);
+    }
+    if (!ok) {
+        if (lane == 0) o[0] = o[1] = o[2] = CUDART_NAN;
+        return;
+    }
+    // back substitution, column by column
+#pragma unroll
+    for (int k = Q - 1; k >= 0; --k) {
+        if (lane == k) bv = bv / A[k];
+        const double bk = __shfl_sync(0xffffffffu, bv, k);
+        if (lane < k) bv = fma(-A[k], bk, bv);
+    }
+    const double d0 = __shfl_sync(0xffffffffu, bv, 0), d1 = __shfl_sync(0xffffffffu, bv, 1),
+                 d2 = __shfl_sync(0xffffffffu, bv, 2);
+    if (lane == 0) {
+        o[0] = d0;
+        o[1] = d1 / pc.h;
+        o[2] = d2 / pc.h;
+    }
+}
+
 template <int Q>
 void launch_points(const PConst& pc, const PGrid& g, double shift, const double* x, const double* y,
                    const double* val, const double* rho, const int* start, const int* list, int nt, const double* tx,
                    const double* ty, double* out, cudaStream_t st) {
-    k_pp_points<Q><<<(nt + 127) / 128, 128, 0, st>>>(pc, g, shift, x, y, val, rho, start, list, nt, tx, ty, out);
+    if constexpr (Q >= 10) {
+        k_pp_points_warp<Q><<<(nt + PP_WARPS - 1) / PP_WARPS, 32 * PP_WARPS, PPWarp<Q>::BYTES, st>>>(
+            pc, g, shift, x, y, val, rho, start, list, nt, tx, ty, out);
+    } else {
+        k_pp_points<Q><<<(nt + 127) / 128, 128, 0, st>>>(pc, g, shift, x, y, val, rho, start, list, nt, tx, ty, out);
+    }
 }
 
 // Scratch of one call, carved from one stream-ordered allocation.
