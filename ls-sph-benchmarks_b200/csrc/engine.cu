@@ -360,6 +360,12 @@ void enq_pst(lssph_handle* h) {
 void prepare_kernels(lssph_handle* h) {
     h->preparing = true;
     StageCfg S{};
+    if (h->lanes_auto) {   // the other lane count the measurement may pick
+        h->G = 2;
+        launch_stage_any(h, S);
+        launch_pst_any(h, all_tiles(h));
+        h->G = 4;
+    }
     launch_stage_any(h, S);
     launch_ghost(h);
     launch_pst_any(h, all_tiles(h));
@@ -457,27 +463,39 @@ int autotune(lssph_handle* h) {
         h->tight = h->budget >= 1;
         return LSSPH_OK;
     }
-    for (int t = 0; t < levels; ++t) {
-        h->tight = t >= 1;
-        h->budget = t;
-        launch_stage_any(h, S);   // warm-up (instruction cache, L2)
-        CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
-        for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
-        CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
-        CUDA_TRY(h, cudaEventSynchronize(h->ev1));
-        float ms = 0.f;
-        CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-        h->tune_us[t] = 1e3 * ms / 3.0;
+    // lanes = 0 on an FP64 q = 5 solve: 4 lanes per particle unless 2 lanes run the RHS
+    // pass at least 5 % faster (the margin keeps the pick, and with it the summation order,
+    // the same from run to run when the two are close)
+    const int nlanes = h->lanes_auto ? 2 : 1;
+    const int lane_opts[2] = {h->G, 2};
+    double us[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    int best_t[2] = {0, 0};
+    for (int g = 0; g < nlanes; ++g) {
+        h->G = lane_opts[g];
+        for (int t = 0; t < levels; ++t) {
+            h->tight = t >= 1;
+            h->budget = t;
+            launch_stage_any(h, S);   // warm-up (instruction cache, L2)
+            CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+            for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
+            CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+            CUDA_TRY(h, cudaEventSynchronize(h->ev1));
+            float ms = 0.f;
+            CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+            us[g][t] = 1e3 * ms / 3.0;
+        }
+        // In the overlapped step the interior tiles share the SMs with the ghost launch: four
+        // CTAs per SM (the tight budget) leave room for it where three do not, which an RHS
+        // pass alone does not show, so the overlapped step always takes the tight budget.
+        for (int t = 1; t < levels; ++t)
+            if (us[g][t] < us[g][best_t[g]]) best_t[g] = t;
+        if (h->overlap) best_t[g] = 1;
     }
-    // In the overlapped step the interior tiles share the SMs with the ghost launch: four
-    // CTAs per SM (the tight budget) leave room for it where three do not, which an RHS
-    // pass alone does not show, so the overlapped step always takes the tight budget.
-    int best = 0;
-    for (int t = 1; t < levels; ++t)
-        if (h->tune_us[t] < h->tune_us[best]) best = t;
-    if (h->overlap) best = 1;
-    h->budget = best;
-    h->tight = best >= 1;
+    const int pick = (nlanes == 2 && us[1][best_t[1]] < 0.95 * us[0][best_t[0]]) ? 1 : 0;
+    h->G = lane_opts[pick];
+    for (int t = 0; t < 3; ++t) h->tune_us[t] = us[pick][t];
+    h->budget = best_t[pick];
+    h->tight = h->budget >= 1;
     h->launch_counter = c0;
     return sync_check(h);
 }
@@ -719,6 +737,10 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->n_int = (int)t_int.size();
     h->n_wall = (int)t_wall.size();
     h->overlap = h->overlap_allowed && h->n_int > 0 && h->n_wall > 0 && !p.periodic;
+    // lanes = 0: the first solo launch measures 2 and 4 lanes (FP64 q = 5 LS, no overlapped
+    // ghost schedule) and keeps the faster; the shared memory covers both
+    h->lanes_auto = h->p.lanes == 0 && !h->mixed && !h->classical && h->order == 2 && !h->overlap;
+    if (h->lanes_auto) h->smem_bytes = std::max(h->smem_bytes, tile_smem_bytes(h->grid.cap, 2, h->has_tem));
     // one device block for every array of the solve (one cudaMalloc, one cudaFree)
     const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles);
     {

@@ -29,6 +29,7 @@ struct lssph_handle {
     bool hi_thread = false;             // order >= 3: thread per particle (else warp per particle)
     bool pdl = true;                    // programmatic dependent launches in the time step
     bool tuned = false;                 // register budget measured (first solo launch)
+    bool lanes_auto = false;            // lanes = 0 on an FP64 q = 5 LS solve: 2 or 4 by measurement
     bool tight = false;                 // register budget of stage/PST kernels (autotuned): 4 CTAs/SM or more
     int budget = 0;                     // 0 loose, 1 tight (4 CTAs/SM), 2 five CTAs/SM (FP64 q = 5 solo)
     double tune_us[3] = {0.0, 0.0, 0.0};   // RHS pass time per budget level

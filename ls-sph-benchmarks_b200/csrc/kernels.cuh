@@ -956,99 +956,156 @@ __device__ __forceinline__ void rhs_ls(const Phys& P, const Work& W, int i, doub
     }
 }
 
-// Tail of a stage: keep the RHS, RK stage update, EOS, scatter into the next cell list.
-// Returns this particle's value for the U_max / steady-state max reductions.
+// Tail of a stage, in pieces (RK2_mod.f90:87-108 / RK4_mod.f90:109-159): keep the RHS;
+// the start-of-step and RK4 accumulator values; the new position and its cell key (which
+// need the current velocity only, not the RHS); the new fields and the EOS; the scatter
+// into the next cell list.  stage_advance runs them in that order for one particle.  The
+// LS tile kernel moves its particles on the warps that have no solve to do, so that the
+// position loads and the scatter's atomics overlap the solve.
 template <int NB>
-__device__ __forceinline__ double stage_advance(const Phys& P, const Fld& nxt, const Lst& Ln,
-                                                const int* __restrict__ gstart, const Work& W, const StageCfg& S,
-                                                Scalars* sc, int i, double my_x, double my_y, double my_u,
-                                                double my_v, double my_rho, double my_tem, double Ru, double Rv,
-                                                double Rr, double Rt) {
+__device__ __forceinline__ void keep_rhs(const Work& W, const StageCfg& S, int i, double Ru, double Rv, double Rr,
+                                         double Rt) {
     if (S.write_rhs) {
         W.rhs_u[i] = Ru;
         if constexpr (NB >= 4) { W.rhs_v[i] = Rv; W.rhs_rho[i] = Rr; }
         if constexpr (NB == 5) W.rhs_tem[i] = Rt;
     }
-    if (S.mode == MODE_RHS_ONLY) return 0.0;
+}
 
-    // ---- stage update (RK2_mod.f90:87-108 / RK4_mod.f90:109-159) ----
-    constexpr bool p1 = (NB == 1);   // problem 1 updates u only and keeps positions
-    double xo = 0, yo = 0, uo, vo = 0, ro = 0, to = 0;
-    if (S.stage == 1) {
-        xo = my_x; yo = my_y; uo = my_u; vo = my_v; ro = my_rho; to = my_tem;
-        W.u_old[i] = uo;
-        if constexpr (!p1) { W.x_old[i] = xo; W.y_old[i] = yo; W.v_old[i] = vo; W.rho_old[i] = ro; }
-        if constexpr (NB == 5) W.tem_old[i] = to;
-    } else {
-        uo = W.u_old[i];
-        if constexpr (!p1) { xo = W.x_old[i]; yo = W.y_old[i]; vo = W.v_old[i]; ro = W.rho_old[i]; }
-        if constexpr (NB == 5) to = W.tem_old[i];
+// Start-of-step values (old) and RK4 accumulators (acc) of the fields; stage 1 takes the
+// current values for both.
+struct OldFields {
+    double uo, vo, ro, to, ua, va, ra, ta;
+};
+
+template <int NB>
+__device__ __forceinline__ OldFields load_old_fields(const Phys& P, const Work& W, const StageCfg& S, int i,
+                                                     double my_u, double my_v, double my_rho, double my_tem) {
+    constexpr bool p1 = (NB == 1);   // problem 1 updates u only
+    OldFields o{my_u, my_v, my_rho, my_tem, my_u, my_v, my_rho, my_tem};
+    if (S.stage != 1) {
+        o.uo = W.u_old[i];
+        if constexpr (!p1) { o.vo = W.v_old[i]; o.ro = W.rho_old[i]; }
+        if constexpr (NB == 5) o.to = W.tem_old[i];
+        if (P.rk != 2) {
+            o.ua = W.u_acc[i];
+            if constexpr (!p1) { o.va = W.v_acc[i]; o.ra = W.rho_acc[i]; }
+            if constexpr (NB == 5) o.ta = W.tem_acc[i];
+        }
     }
-    double xn = my_x, yn = my_y, un, vn = my_v, rn = my_rho, tn = my_tem;
+    return o;
+}
+
+// New position (problems 2-4), wrapped into the periodic box; returns its cell key when
+// the stage rebuilds the cell list, else -1.
+template <int NB>
+__device__ __forceinline__ int stage_position(const Phys& P, const Fld& nxt, const Work& W, const StageCfg& S,
+                                              Scalars* sc, int i, double my_x, double my_y, double my_u,
+                                              double my_v) {
+    double xo, yo, xn, yn;
+    if (S.stage == 1) {
+        xo = my_x; yo = my_y;
+        W.x_old[i] = xo; W.y_old[i] = yo;
+    } else {
+        xo = W.x_old[i]; yo = W.y_old[i];
+    }
+    if (P.rk == 2) {
+        const double dt = S.dt2;
+        xn = xo + my_u * dt;
+        yn = yo + my_v * dt;
+    } else {
+        double xa = my_x, ya = my_y;
+        if (S.stage != 1) { xa = W.x_acc[i]; ya = W.y_acc[i]; }
+        xa = xa + my_u * S.dt1;
+        ya = ya + my_v * S.dt1;
+        if (!S.last) {
+            W.x_acc[i] = xa; W.y_acc[i] = ya;
+            xn = xo + my_u * S.dt2;
+            yn = yo + my_v * S.dt2;
+        } else {
+            xn = xa; yn = ya;
+        }
+    }
+    if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
+    nxt.x[i] = xn;
+    nxt.y[i] = yn;
+    if (!(isfinite(xn) && isfinite(yn))) atomicOr(&sc->err, ERR_NONFINITE);
+    int nk = -1;
+    if (S.do_scatter) {
+        nk = cell_key_mul(P, xn, yn, sc);
+        if (nk >= 0) W.key[i] = nk;
+    }
+    return nk;
+}
+
+// Cell key of a stage: the new position's (problems 2-4), or the fixed one (problem 1).
+template <int NB>
+__device__ __forceinline__ int stage_key(const Phys& P, const Fld& nxt, const Work& W, const StageCfg& S,
+                                         Scalars* sc, int i, double my_x, double my_y, double my_u, double my_v) {
+    if constexpr (NB != 1) return stage_position<NB>(P, nxt, W, S, sc, i, my_x, my_y, my_u, my_v);
+    int nk = -1;
+    if (S.do_scatter) {
+        nk = cell_key_mul(P, my_x, my_y, sc);
+        if (nk >= 0) W.key[i] = nk;
+    }
+    return nk;
+}
+
+// New fields, EOS and volume; returns this particle's value for the U_max / steady-state
+// max reductions.
+template <int NB>
+__device__ __forceinline__ double stage_fields(const Phys& P, const Fld& nxt, const Work& W, const StageCfg& S,
+                                               Scalars* sc, int i, double my_v, double my_rho, double my_tem,
+                                               double Ru, double Rv, double Rr, double Rt, const OldFields& o) {
+    constexpr bool p1 = (NB == 1);
+    if (S.stage == 1) {
+        W.u_old[i] = o.uo;
+        if constexpr (!p1) { W.v_old[i] = o.vo; W.rho_old[i] = o.ro; }
+        if constexpr (NB == 5) W.tem_old[i] = o.to;
+    }
+    double un, vn = my_v, rn = my_rho, tn = my_tem;
     if (P.rk == 2) {
         const double dt = S.dt2;
         if constexpr (!p1) {
-            xn = xo + my_u * dt;
-            yn = yo + my_v * dt;
-            vn = vo + Rv * dt;
-            rn = ro + Rr * dt;
+            vn = o.vo + Rv * dt;
+            rn = o.ro + Rr * dt;
         }
-        un = uo + Ru * dt;
-        if constexpr (NB == 5) tn = to + Rt * dt;
+        un = o.uo + Ru * dt;
+        if constexpr (NB == 5) tn = o.to + Rt * dt;
     } else {
-        double ua, va = 0, xa = 0, ya = 0, ra = 0, ta = 0;
-        if (S.stage == 1) {
-            ua = my_u; va = my_v; xa = my_x; ya = my_y; ra = my_rho; ta = my_tem;
-        } else {
-            ua = W.u_acc[i];
-            if constexpr (!p1) { va = W.v_acc[i]; xa = W.x_acc[i]; ya = W.y_acc[i]; ra = W.rho_acc[i]; }
-            if constexpr (NB == 5) ta = W.tem_acc[i];
-        }
-        ua = ua + Ru * S.dt1;
+        const double ua = o.ua + Ru * S.dt1;
+        double va = 0, ra = 0, ta = 0;
         if constexpr (!p1) {
-            va = va + Rv * S.dt1;
-            xa = xa + my_u * S.dt1;
-            ya = ya + my_v * S.dt1;
-            ra = ra + Rr * S.dt1;
+            va = o.va + Rv * S.dt1;
+            ra = o.ra + Rr * S.dt1;
         }
-        if constexpr (NB == 5) ta = ta + Rt * S.dt1;
+        if constexpr (NB == 5) ta = o.ta + Rt * S.dt1;
         if (!S.last) {
             W.u_acc[i] = ua;
-            if constexpr (!p1) { W.v_acc[i] = va; W.x_acc[i] = xa; W.y_acc[i] = ya; W.rho_acc[i] = ra; }
+            if constexpr (!p1) { W.v_acc[i] = va; W.rho_acc[i] = ra; }
             if constexpr (NB == 5) W.tem_acc[i] = ta;
             if constexpr (!p1) {
-                xn = xo + my_u * S.dt2;
-                yn = yo + my_v * S.dt2;
-                vn = vo + Rv * S.dt2;
-                rn = ro + Rr * S.dt2;
+                vn = o.vo + Rv * S.dt2;
+                rn = o.ro + Rr * S.dt2;
             }
-            un = uo + Ru * S.dt2;
-            if constexpr (NB == 5) tn = to + Rt * S.dt2;
+            un = o.uo + Ru * S.dt2;
+            if constexpr (NB == 5) tn = o.to + Rt * S.dt2;
         } else {
             un = ua;
-            if constexpr (!p1) { vn = va; xn = xa; yn = ya; rn = ra; }
+            if constexpr (!p1) { vn = va; rn = ra; }
             if constexpr (NB == 5) tn = ta;
         }
-    }
-    if constexpr (!p1) {
-        if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
     }
     nxt.u[i] = un;
     bool finite = isfinite(un);
     if constexpr (!p1) {
-        nxt.x[i] = xn; nxt.y[i] = yn; nxt.v[i] = vn; nxt.rho[i] = rn;
+        nxt.v[i] = vn; nxt.rho[i] = rn;
         nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
         nxt.vol[i] = P.SP_mass / rn;
-        finite = finite && isfinite(xn) && isfinite(yn) && isfinite(vn) && isfinite(rn);
+        finite = finite && isfinite(vn) && isfinite(rn);
     }
     if constexpr (NB == 5) { nxt.tem[i] = tn; finite = finite && isfinite(tn); }
     if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
-
-    if (S.do_scatter) {
-        const int nk = cell_key_mul(P, xn, yn, sc);
-        if (nk >= 0) W.key[i] = nk;
-        scatter_to_cell(P, Ln, gstart, nk, i, sc);
-    }
     double red = 0.0;
     if (S.last && S.do_umax) red = un * un + vn * vn;
     if (S.last && S.do_steady) {
@@ -1056,6 +1113,37 @@ __device__ __forceinline__ double stage_advance(const Phys& P, const Fld& nxt, c
         W.f_prev[i] = un;
     }
     return red;
+}
+
+// The whole tail for one particle.
+template <int NB>
+__device__ __forceinline__ double stage_advance(const Phys& P, const Fld& nxt, const Lst& Ln,
+                                                const int* __restrict__ gstart, const Work& W, const StageCfg& S,
+                                                Scalars* sc, int i, double my_x, double my_y, double my_u,
+                                                double my_v, double my_rho, double my_tem, double Ru, double Rv,
+                                                double Rr, double Rt) {
+    keep_rhs<NB>(W, S, i, Ru, Rv, Rr, Rt);
+    if (S.mode == MODE_RHS_ONLY) return 0.0;
+    const OldFields o = load_old_fields<NB>(P, W, S, i, my_u, my_v, my_rho, my_tem);
+    const int nk = stage_key<NB>(P, nxt, W, S, sc, i, my_x, my_y, my_u, my_v);
+    const double red = stage_fields<NB>(P, nxt, W, S, sc, i, my_v, my_rho, my_tem, Ru, Rv, Rr, Rt, o);
+    if (S.do_scatter) scatter_to_cell(P, Ln, gstart, nk, i, sc);
+    return red;
+}
+
+// New position, cell key and scatter of own particles first, first + step, ... (threads
+// of a tile CTA that have no solve to do).
+template <int NB>
+__device__ __forceinline__ void stage_move_own(const Phys& P, const Fld& nxt, const Lst& Ln,
+                                               const int* __restrict__ gstart, const Work& W, const StageCfg& S,
+                                               Scalars* sc, const SmemView& SM, int n_own, int first, int step) {
+    for (int o = first; o < n_own; o += step) {
+        const int ki = SM.own_k[o];
+        const int i = SM.idx[ki];
+        const double vv = NB >= 4 ? SM.v[ki] : 0.0;
+        const int nk = stage_key<NB>(P, nxt, W, S, sc, i, SM.x[ki], SM.y[ki], SM.u[ki], vv);
+        if (S.do_scatter) scatter_to_cell(P, Ln, gstart, nk, i, sc);
+    }
 }
 
 // LS tail of k_stage: RHS from the derivatives, then the stage update.
@@ -1089,6 +1177,7 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
     if (stop) return;
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
+    const bool early = S.mode == MODE_STAGE;
     for (int ob = 0; ob < n_own; ob += PPB) {
         // ---- pair phase: G lanes per particle ----
         {
@@ -1152,7 +1241,11 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
         if ((int)threadIdx.x < PPB && o < n_own) {
             double* sm = SM.sums + threadIdx.x * SR;
             const int ki = SM.own_k[o];
+            const int i = SM.idx[ki];
             const int cnt = (int)sm[SR - 1];
+            double my_v = 0, my_rho = 0, my_tem = 0;
+            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
+            if constexpr (NB == 5) my_tem = SM.tem[ki];
             double d[NB][Q];
             {
                 double A[Q][Q];
@@ -1178,16 +1271,24 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
                         for (int k = 0; k < Q; ++k) d[c][k] = 0.0;
                 }
             }
-            double my_v = 0, my_rho = 0, my_tem = 0;
-            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
-            if constexpr (NB == 5) my_tem = SM.tem[ki];
-            red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, SM.idx[ki], SM.x[ki], SM.y[ki], SM.u[ki], my_v,
-                                   my_rho, my_tem, d);
+            double Ru, Rv, Rr, Rt;
+            rhs_ls<NB>(P, W, i, my_rho, my_tem, d, Ru, Rv, Rr, Rt);
+            keep_rhs<NB>(W, S, i, Ru, Rv, Rr, Rt);
+            if (early) {
+                const OldFields of = load_old_fields<NB>(P, W, S, i, SM.u[ki], my_v, my_rho, my_tem);
+                red = stage_fields<NB>(P, nxt, W, S, sc, i, my_v, my_rho, my_tem, Ru, Rv, Rr, Rt, of);
+            }
+        } else if (G > 1 && early && ob == 0 && (int)threadIdx.x >= PPB) {
+            // the warps idle in the solve phase move every own particle (the new position
+            // needs no RHS), key it and append it to the next cell list
+            stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, SM, n_own, (int)threadIdx.x - PPB, blockDim.x - PPB);
         }
         if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
             warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
         __syncthreads();
     }
+    if constexpr (G == 1)
+        if (early) stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, SM, n_own, threadIdx.x, blockDim.x);
 }
 
 

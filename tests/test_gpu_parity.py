@@ -3,8 +3,9 @@
 Tolerances:
   * lanes = 1 (one thread per particle, reference summation order): results must be
     bit-identical to the oracle (same operation sequence, explicit FMAs only);
-  * lanes = 4 (default, warp-shuffle reductions): single-stage results within a relative
-    1e-12 of the field scale; whole runs within relative L2 1e-10 (the stated bound).
+  * lanes = 2 / 4 / 8 (warp-shuffle reductions; 0 lets the engine pick 2 or 4): single-stage
+    results within a relative 1e-12 of the field scale; whole runs within relative L2
+    1e-10 (the stated bound).
 Neighbour sets are compared exactly as sorted index sets.
 """
 import numpy as np
@@ -153,6 +154,52 @@ def test_wall_problems_rel_l2(case):
     g, o = sim.download(), orc.get()
     for k in ("u", "v", "pre") + (("tem",) if p.target_problem == 4 else ()):
         assert _rel_l2(getattr(g, k), o[k]) <= 1e-10, k
+
+
+LANE_CASES = {
+    "taylor_green": lambda **kw: lssph.taylor_green_params(num=48, **kw),
+    "taylor_green_periodic": lambda **kw: lssph.taylor_green_params(num=48, PERIODIC=1, **kw),
+    "cavity": lambda **kw: lssph.cavity_params(num=40, **kw),
+    "boussinesq": lambda **kw: lssph.boussinesq_params(num=40, ra=1e5, **kw),
+}
+
+
+@pytest.mark.parametrize("lanes", [2, 8])
+@pytest.mark.parametrize("case", list(LANE_CASES))
+def test_other_lane_counts_rel_l2(case, lanes):
+    # 2 and 8 lanes per particle: the same sums split over another number of lanes, so the
+    # same bound as 4 lanes (relative L2 1e-10 over a run)
+    p = LANE_CASES[case]()
+    sim, orc = _pair(p, lanes=lanes, amp=0.1, seed=7)
+    sim.step(60)
+    orc.run(60)
+    g, o = sim.download(), orc.get()
+    assert sim.tuning()["lanes"] == lanes
+    for k in ("u", "v", "pre") + (("tem",) if p.target_problem == 4 else ()):
+        assert _rel_l2(getattr(g, k), o[k]) <= 1e-10, k
+
+
+@pytest.mark.parametrize("case", ["taylor_green_periodic_128", "taylor_green_periodic_96", "cavity_64"])
+def test_automatic_lanes_equal_the_picked_count(case):
+    # lanes = 0: the engine measures 2 and 4 lanes (FP64 q = 5 LS) and keeps the faster; the
+    # run is then bit for bit the run with that count given explicitly.  The closed box
+    # (ghost launches beside the interior tiles) keeps 4.
+    mk = {"taylor_green_periodic_128": lambda **kw: lssph.taylor_green_params(num=128, PERIODIC=1, **kw),
+          "taylor_green_periodic_96": lambda **kw: lssph.taylor_green_params(num=96, PERIODIC=1, **kw),
+          "cavity_64": lambda **kw: lssph.cavity_params(num=64, **kw)}[case]
+    auto = lssph.Simulation.new(mk(lanes=0))
+    picked = auto.tuning()["lanes"]
+    assert picked in (2, 4)
+    if auto.tuning()["ghost_overlap"]:
+        assert picked == 4
+    fixed = lssph.Simulation.new(mk(lanes=picked))
+    auto.step(20)
+    fixed.step(20)
+    ga, gf = auto.download(), fixed.download()
+    for k in FIELDS:
+        assert np.array_equal(getattr(ga, k), getattr(gf, k)), k
+    auto.close()
+    fixed.close()
 
 
 def test_steady_state_detection_matches_oracle():
