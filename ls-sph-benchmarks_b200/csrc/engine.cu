@@ -539,17 +539,57 @@ int sync_check(lssph_handle* h) {
 
 // Build the cell list of the current positions into list buffer lb (fresh).
 int rebuild_cells(lssph_handle* h) {
-    for (int b = 0; b < kLists; ++b) CUDA_TRY(h, cudaMemsetAsync(h->L[b].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
+    static_assert(kLists == 3, "k_clear_counts zeroes three lists");
+    k_clear_counts<<<blocks_for(h->grid.ncell, 256), 256, 0, h->stream>>>(h->L[0].cnt, h->L[1].cnt, h->L[2].cnt,
+                                                                          h->grid.ncell);
     k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->gstart, h->W.key, h->sc);
     return LSSPH_OK;
+}
+
+// Device address of a caller's host buffer of `bytes` that the GPU can read and write
+// directly (page-locked and mapped, e.g. from cudaHostAlloc or cudaHostRegister: both its
+// first and its last byte), else nullptr (ordinary pageable memory goes through copies).
+void* mapped_host(const void* p, size_t bytes) {
+    if (!p || bytes == 0) return nullptr;
+    cudaPointerAttributes a{}, b{};
+    const char* last = static_cast<const char*>(p) + (bytes - 1);
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaPointerGetAttributes(&b, last) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost || !a.devicePointer || !b.devicePointer)
+        return nullptr;
+    if (static_cast<char*>(b.devicePointer) != static_cast<char*>(a.devicePointer) + (bytes - 1)) return nullptr;
+    return a.devicePointer;
+}
+
+// Every non-null field mapped: device addresses into out[0..6], true.
+bool all_mapped(const double* const (&f)[7], size_t bytes, double* (&out)[7]) {
+    for (int k = 0; k < 7; ++k) {
+        out[k] = nullptr;
+        if (!f[k]) continue;
+        out[k] = static_cast<double*>(mapped_host(f[k], bytes));
+        if (!out[k]) return false;
+    }
+    return true;
 }
 
 // The current buffer gets every particle.  On a later upload (both = false) the other buffer
 // needs the ghost particles only: the next stage (or PST) writes every interior field of it
 // before anything reads it -- except in problem 1, whose stages write u alone, so there it
-// gets every particle too.
+// gets every particle too.  Page-locked, mapped host buffers are read by one kernel.
 int upload_fields(lssph_handle* h, const double* x, const double* y, const double* u, const double* v,
                   const double* rho, const double* pre, const double* tem, bool both = true) {
+    {
+        const double* const f[7] = {x, y, u, v, rho, pre, h->has_tem ? tem : nullptr};
+        double* d[7];
+        if (all_mapped(f, sizeof(double) * (size_t)h->num_total, d)) {
+            const int first_b = (both || h->p1) ? 0 : h->num_int;
+            k_upload_mapped<<<blocks_for(h->num_total, 256), 256, 0, h->stream>>>(
+                h->P, h->F[h->sb], h->F[h->sb ^ 1], HostFld{d[0], d[1], d[2], d[3], d[4], d[5], d[6]}, first_b);
+            return LSSPH_OK;
+        }
+    }
     for (int b = 0; b < 2; ++b) {
         const Fld& F = h->F[b];
         const size_t first = (both || b == h->sb || h->p1) ? 0 : (size_t)h->num_int;
@@ -1077,6 +1117,19 @@ int lssph_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
     const size_t bytes = sizeof(double) * (size_t)h->num_total;
     const Fld& F = h->F[h->sb];
+    {   // page-locked, mapped host buffers: one kernel writes them
+        const double* const f[7] = {x, y, u, v, rho, pre, h->has_tem ? tem : nullptr};
+        double* d[7];
+        if (all_mapped(f, bytes, d)) {
+            k_download_mapped<<<blocks_for(h->num_total, 256), 256, 0, h->stream>>>(
+                h->P, F, HostOut{d[0], d[1], d[2], d[3], d[4], d[5], d[6]});
+            if (tem && !h->has_tem) std::memset(tem, 0, bytes);
+            if (ptype) std::memcpy(ptype, h->ptype.data(), sizeof(int32_t) * h->num_total);
+            CUDA_TRY(h, cudaGetLastError());
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            return LSSPH_OK;
+        }
+    }
     if (x) CUDA_TRY(h, cudaMemcpyAsync(x, F.x, bytes, cudaMemcpyDeviceToHost, h->stream));
     if (y) CUDA_TRY(h, cudaMemcpyAsync(y, F.y, bytes, cudaMemcpyDeviceToHost, h->stream));
     if (u) CUDA_TRY(h, cudaMemcpyAsync(u, F.u, bytes, cudaMemcpyDeviceToHost, h->stream));

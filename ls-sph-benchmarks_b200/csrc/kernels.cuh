@@ -2236,6 +2236,58 @@ static __global__ void k_volume(const Phys P, const Fld F) {
     if (i < P.num_total) F.vol[i] = P.SP_mass / F.rho[i];
 }
 
+// Host state in page-locked, mapped memory (device addresses of the caller's buffers; a
+// null field is left as it is on the device).
+struct HostFld {
+    const double *x, *y, *u, *v, *rho, *pre, *tem;
+};
+struct HostOut {
+    double *x, *y, *u, *v, *rho, *pre, *tem;
+};
+
+// Upload read straight from mapped host memory (one pass over PCIe instead of one copy per
+// field): every particle into the current buffer A, particles from `first_b` on into the
+// other buffer B, and the volumes of both.
+static __global__ void k_upload_mapped(const Phys P, const Fld A, const Fld B, const HostFld H, int first_b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.num_total) return;
+    const bool toB = i >= first_b;
+    auto put = [&](const double* src, double* a, double* b) {
+        if (!src) return;
+        const double v = src[i];
+        a[i] = v;
+        if (toB) b[i] = v;
+    };
+    put(H.x, A.x, B.x);
+    put(H.y, A.y, B.y);
+    put(H.u, A.u, B.u);
+    put(H.v, A.v, B.v);
+    put(H.rho, A.rho, B.rho);
+    put(H.pre, A.pre, B.pre);
+    put(H.tem, A.tem, B.tem);
+    A.vol[i] = P.SP_mass / A.rho[i];
+    if (toB) B.vol[i] = P.SP_mass / B.rho[i];
+}
+
+// Download written straight into mapped host memory.
+static __global__ void k_download_mapped(const Phys P, const Fld F, const HostOut H) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.num_total) return;
+    if (H.x) H.x[i] = F.x[i];
+    if (H.y) H.y[i] = F.y[i];
+    if (H.u) H.u[i] = F.u[i];
+    if (H.v) H.v[i] = F.v[i];
+    if (H.rho) H.rho[i] = F.rho[i];
+    if (H.pre) H.pre[i] = F.pre[i];
+    if (H.tem) H.tem[i] = F.tem[i];
+}
+
+// Counters of the rotating cell lists to zero (one launch for all of them).
+static __global__ void k_clear_counts(int* a, int* b, int* c, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { a[i] = 0; b[i] = 0; c[i] = 0; }
+}
+
 // In-radius neighbour lists for parity checks (unsorted, fixed stride per particle).
 static __global__ void k_neighbors(const Phys P, const Fld F, const Lst L, const int* __restrict__ gstart,
                             const int* __restrict__ glist, const int* key, const VMd V, int which, int stride,

@@ -1,0 +1,97 @@
+"""Host transfers through page-locked buffers (needs a B200).
+
+lssph_upload and lssph_download read and write page-locked, mapped host buffers (from
+cudaHostAlloc, or torch's pin_memory) directly from one kernel, and go through copies for
+ordinary pageable memory.  Both paths must move the same bytes: a download fills the
+same values, and a solve continues bit for bit from either upload.
+"""
+import numpy as np
+import pytest
+import torch
+
+import lssph
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("x", "y", "u", "v", "rho", "pre")
+
+CASES = {
+    "diffusion": lambda: lssph.diffusion_params(num=40, seed=3),
+    "taylor_green": lambda: lssph.taylor_green_params(num=48),
+    "taylor_green_periodic": lambda: lssph.taylor_green_params(num=48, PERIODIC=1),
+    "cavity": lambda: lssph.cavity_params(num=40),
+    "boussinesq": lambda: lssph.boussinesq_params(num=40),
+}
+
+
+def _pinned(a):
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+    t[:] = a
+    return t
+
+
+def _pinned_state(st, with_tem):
+    tem = _pinned(st.tem) if with_tem else None
+    return lssph.State(st.ptype.copy(), *(_pinned(getattr(st, k)) for k in FIELDS), tem)
+
+
+def _sim(p):
+    s = lssph.Simulation.new(p)
+    return s
+
+
+def _keys(p):
+    return FIELDS + (("tem",) if p.target_problem == 4 else ())
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_pinned_download_equals_pageable(case):
+    p = CASES[case]()
+    sim = _sim(p)
+    sim.step(7)
+    ref = sim.download()
+    pin = _pinned_state(ref, p.target_problem == 4)
+    for k in _keys(p):
+        getattr(pin, k)[:] = -1.0
+    sim.download_into(pin)
+    for k in _keys(p):
+        assert np.array_equal(getattr(pin, k), getattr(ref, k)), k
+    sim.close()
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_pinned_upload_mid_run_equals_pageable(case):
+    p = CASES[case]()
+    a, b, c = _sim(p), _sim(p), _sim(p)
+    a.step(10)
+    mid = a.download()
+    a.step(10)
+    b.step(3)                     # b and c are elsewhere in their runs
+    b.upload(mid)
+    b.step(10)
+    c.step(3)
+    c.upload(_pinned_state(mid, p.target_problem == 4))
+    c.step(10)
+    ga, gb, gc = a.download(), b.download(), c.download()
+    for k in _keys(p):
+        assert np.array_equal(getattr(gb, k), getattr(ga, k)), k
+        assert np.array_equal(getattr(gc, k), getattr(ga, k)), k
+    for s in (a, b, c):
+        s.close()
+
+
+def test_pinned_round_trip_every_step_equals_resident_run():
+    # the end-to-end pattern: upload, one step, download, each step, from pinned buffers
+    p = lssph.taylor_green_params(num=64, PERIODIC=1)
+    res, e2e = _sim(p), _sim(p)
+    host = _pinned_state(e2e.download(), False)
+    for _ in range(12):
+        e2e.upload(host)
+        e2e.step(1)
+        e2e.download_into(host)
+    res.step(12)
+    g = res.download()
+    for k in FIELDS:
+        assert np.array_equal(getattr(host, k), getattr(g, k)), k
+    res.close()
+    e2e.close()
