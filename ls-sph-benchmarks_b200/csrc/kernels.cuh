@@ -1132,29 +1132,19 @@ __device__ __forceinline__ double stage_advance(const Phys& P, const Fld& nxt, c
 }
 
 // New position, cell key and scatter of own particles first, first + step, ... (threads
-// of a tile CTA that have no solve to do).
-template <int NB>
+// of a tile CTA that have no solve to do); get(o, i, x, y, u, v) reads own particle o's
+// index and FP64 position and velocity.
+template <int NB, class Get>
 __device__ __forceinline__ void stage_move_own(const Phys& P, const Fld& nxt, const Lst& Ln,
                                                const int* __restrict__ gstart, const Work& W, const StageCfg& S,
-                                               Scalars* sc, const SmemView& SM, int n_own, int first, int step) {
+                                               Scalars* sc, int n_own, int first, int step, Get&& get) {
     for (int o = first; o < n_own; o += step) {
-        const int ki = SM.own_k[o];
-        const int i = SM.idx[ki];
-        const double vv = NB >= 4 ? SM.v[ki] : 0.0;
-        const int nk = stage_key<NB>(P, nxt, W, S, sc, i, SM.x[ki], SM.y[ki], SM.u[ki], vv);
+        int i;
+        double x, y, u, v;
+        get(o, i, x, y, u, v);
+        const int nk = stage_key<NB>(P, nxt, W, S, sc, i, x, y, u, v);
         if (S.do_scatter) scatter_to_cell(P, Ln, gstart, nk, i, sc);
     }
-}
-
-// LS tail of k_stage: RHS from the derivatives, then the stage update.
-template <int NB>
-__device__ __forceinline__ double stage_finish(const Phys& P, const Fld& nxt, const Lst& Ln,
-                                               const int* __restrict__ gstart, const Work& W, const StageCfg& S,
-                                               Scalars* sc, int i, double my_x, double my_y, double my_u,
-                                               double my_v, double my_rho, double my_tem, const double (&d)[NB][5]) {
-    double Ru, Rv, Rr, Rt;
-    rhs_ls<NB>(P, W, i, my_rho, my_tem, d, Ru, Rv, Rr, Rt);
-    return stage_advance<NB>(P, nxt, Ln, gstart, W, S, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem, Ru, Rv, Rr, Rt);
 }
 
 // One tile of one solve (the CTA's work in both the single-solve and the batched kernel).
@@ -1178,6 +1168,14 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
     const bool early = S.mode == MODE_STAGE;
+    auto own = [&](int o, int& i, double& x, double& y, double& u, double& v) {
+        const int ki = SM.own_k[o];
+        i = SM.idx[ki];
+        x = SM.x[ki];
+        y = SM.y[ki];
+        u = SM.u[ki];
+        v = NB >= 4 ? SM.v[ki] : 0.0;
+    };
     for (int ob = 0; ob < n_own; ob += PPB) {
         // ---- pair phase: G lanes per particle ----
         {
@@ -1281,14 +1279,14 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
         } else if (G > 1 && early && ob == 0 && (int)threadIdx.x >= PPB) {
             // the warps idle in the solve phase move every own particle (the new position
             // needs no RHS), key it and append it to the next cell list
-            stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, SM, n_own, (int)threadIdx.x - PPB, blockDim.x - PPB);
+            stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, n_own, (int)threadIdx.x - PPB, blockDim.x - PPB, own);
         }
         if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
             warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
         __syncthreads();
     }
     if constexpr (G == 1)
-        if (early) stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, SM, n_own, threadIdx.x, blockDim.x);
+        if (early) stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, n_own, threadIdx.x, blockDim.x, own);
 }
 
 
@@ -1350,6 +1348,14 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
     const int lane = threadIdx.x & (G - 1);
     const float heff2 = (float)P.h_eff_sq;
     const PairConst<float> C(P);
+    const bool early = S.mode == MODE_STAGE;
+    auto own = [&](int o, int& i, double& x, double& y, double& u, double& v) {
+        i = SM.idx[SM.own_k[o]];
+        x = cur.x[i];
+        y = cur.y[i];
+        u = cur.u[i];
+        v = NB >= 4 ? cur.v[i] : 0.0;
+    };
     for (int ob = 0; ob < n_own; ob += PPB) {
         {
             const int slot = (int)threadIdx.x / G;
@@ -1409,7 +1415,7 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
             double* sm = SM.sums + threadIdx.x * SR;
             const int i = SM.idx[SM.own_k[o]];
             // the particle's own FP64 state (loads issued before the solve they do not need)
-            const double my_x = cur.x[i], my_y = cur.y[i], my_u = cur.u[i];
+            const double my_u = cur.u[i];
             double my_v = 0, my_rho = 0, my_tem = 0;
             if constexpr (NB >= 4) { my_v = cur.v[i]; my_rho = cur.rho[i]; }
             if constexpr (NB == 5) my_tem = cur.tem[i];
@@ -1419,12 +1425,23 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
             for (int c = 0; c < NB; ++c)
 #pragma unroll
                 for (int k = 0; k < Q; ++k) d[c][k] = sm[15 + 5 * c + k];
-            red = stage_finish<NB>(P, nxt, Ln, gstart, W, S, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem, d);
+            double Ru, Rv, Rr, Rt;
+            rhs_ls<NB>(P, W, i, my_rho, my_tem, d, Ru, Rv, Rr, Rt);
+            keep_rhs<NB>(W, S, i, Ru, Rv, Rr, Rt);
+            if (early) {
+                const OldFields of = load_old_fields<NB>(P, W, S, i, my_u, my_v, my_rho, my_tem);
+                red = stage_fields<NB>(P, nxt, W, S, sc, i, my_v, my_rho, my_tem, Ru, Rv, Rr, Rt, of);
+            }
+        } else if (G > 1 && early && ob == 0 && (int)threadIdx.x >= PPB) {
+            // the warps idle in the solve phase move the own particles (FP64 state from HBM)
+            stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, n_own, (int)threadIdx.x - PPB, blockDim.x - PPB, own);
         }
         if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
             warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
         __syncthreads();
     }
+    if constexpr (G == 1)
+        if (early) stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, n_own, threadIdx.x, blockDim.x, own);
 }
 
 // =======================================================================================
@@ -1476,6 +1493,15 @@ __device__ __forceinline__ void stage_body_classical(const Phys& P, const Fld& c
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
     const bool sum_model = P.sph_model == 1;
+    const bool early = S.mode == MODE_STAGE;
+    auto own = [&](int o, int& i, double& x, double& y, double& u, double& v) {
+        const int ki = SM.own_k[o];
+        i = SM.idx[ki];
+        x = SM.x[ki];
+        y = SM.y[ki];
+        u = SM.u[ki];
+        v = NB >= 4 ? SM.v[ki] : 0.0;
+    };
     for (int ob = 0; ob < n_own; ob += PPB) {
         {
             const int slot = (int)threadIdx.x / G;
@@ -1531,13 +1557,21 @@ __device__ __forceinline__ void stage_body_classical(const Phys& P, const Fld& c
             const int i = SM.idx[ki];
             double Ru, Rv, Rr, Rt;
             rhs_classical<NB>(P, W, i, my_rho, my_tem, sm, Ru, Rv, Rr, Rt);
-            red = stage_advance<NB>(P, nxt, Ln, gstart, W, S, sc, i, SM.x[ki], SM.y[ki], SM.u[ki], my_v, my_rho,
-                                    my_tem, Ru, Rv, Rr, Rt);
+            keep_rhs<NB>(W, S, i, Ru, Rv, Rr, Rt);
+            if (early) {
+                const OldFields of = load_old_fields<NB>(P, W, S, i, SM.u[ki], my_v, my_rho, my_tem);
+                red = stage_fields<NB>(P, nxt, W, S, sc, i, my_v, my_rho, my_tem, Ru, Rv, Rr, Rt, of);
+            }
+        } else if (G > 1 && early && ob == 0 && (int)threadIdx.x >= PPB) {
+            // the warps idle while the RHS is formed move the own particles
+            stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, n_own, (int)threadIdx.x - PPB, blockDim.x - PPB, own);
         }
         if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
             warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
         __syncthreads();
     }
+    if constexpr (G == 1)
+        if (early) stage_move_own<NB>(P, nxt, Ln, gstart, W, S, sc, n_own, threadIdx.x, blockDim.x, own);
 }
 
 template <int NB, int G, int TIGHT = 0>
