@@ -173,7 +173,10 @@ int lssph_set_step_budget(lssph_handle* h, int32_t nsteps);
    used up. */
 int lssph_get_progress(lssph_handle* h, int32_t* steps_done, int32_t* stopped);
 
-/* Host <-> device state (caller buffers of length num_total; tem may be NULL). */
+/* Host <-> device state (caller buffers of length num_total; tem may be NULL).  Both return
+   after the transfer is complete, so the buffers may be reused at once.  Page-locked,
+   mapped buffers (cudaHostAlloc, cudaMallocHost, cudaHostRegister) are read and written by
+   one kernel over the bus; other host memory goes through one copy per field. */
 int lssph_upload(lssph_handle* h, const double* x, const double* y, const double* u,
                  const double* v, const double* rho, const double* pre, const double* tem);
 int lssph_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u,
