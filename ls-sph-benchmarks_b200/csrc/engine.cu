@@ -614,6 +614,7 @@ void free_handle(lssph_handle* h) {
     if (h->batch) batch_forget(h->batch, h);
     if (h->stream) cudaStreamSynchronize(h->stream);
     snapshot_release(h);
+    postproc_release(h);
     for (auto& row : h->graph)
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);

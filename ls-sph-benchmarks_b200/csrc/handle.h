@@ -13,6 +13,7 @@
 
 namespace lssph {
 struct SnapState;   // asynchronous snapshots (snapshot.cu)
+struct PPScratch;   // post-processing stream and scratch (postproc.cu)
 }
 
 struct lssph_handle {
@@ -78,6 +79,7 @@ struct lssph_handle {
     size_t prof_next = 0;
     lssph_batch* batch = nullptr;   // the batch this solve is a member of, if any
     lssph::SnapState* snap = nullptr;   // snapshot slots and side stream, set up on first use
+    lssph::PPScratch* pp = nullptr;     // lssph_interpolate stream and scratch, set up on first use
     std::string err;
 };
 
@@ -124,6 +126,7 @@ void batch_forget(lssph_batch* b, lssph_handle* h);
 
 // Finish and free a handle's asynchronous snapshots (snapshot.cu).
 void snapshot_release(lssph_handle* h);
+void postproc_release(lssph_handle* h);
 
 // Higher-order LS stage and PST launches, SPH_MODEL 4 / 5 / 6 (highorder.cu).  tiles:
 // tile of each CTA (NULL: CTA i runs tile i); while h->preparing they only set the

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 
 #include "handle.h"
@@ -517,6 +518,59 @@ int pp_fail(lssph_handle* h, int code, const std::string& msg) {
 }  // namespace
 }  // namespace lssph
 
+namespace lssph {
+
+// A call's private stream, its event and a grow-only device scratch, kept between calls:
+// creating a stream and drawing a few MB from the stream-ordered pool (which hands the
+// memory back at every synchronisation) cost about 0.55 ms per call, several times the
+// interpolation itself.
+struct PPScratch {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    char* buf = nullptr;
+    size_t bytes = 0;
+};
+
+// Stream and event on first use; a scratch of at least `bytes` (a larger one replaces it).
+cudaError_t pp_ready(PPScratch* s, size_t bytes, const char** stage) {
+    cudaError_t e = cudaSuccess;
+    *stage = "stream set-up";
+    if (!s->st) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !s->ev) e = cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming);
+    if (e == cudaSuccess && s->bytes < bytes) {
+        *stage = "cudaMalloc of the scratch";
+        if (s->buf) cudaFree(s->buf);
+        s->buf = nullptr;
+        s->bytes = 0;
+        e = cudaMalloc((void**)&s->buf, bytes);
+        if (e == cudaSuccess) s->bytes = bytes;
+    }
+    return e;
+}
+
+void pp_free(PPScratch* s) {
+    if (!s) return;
+    if (s->st) cudaStreamSynchronize(s->st);
+    if (s->buf) cudaFree(s->buf);
+    if (s->ev) cudaEventDestroy(s->ev);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+}
+
+void postproc_release(lssph_handle* h) {
+    pp_free(h->pp);
+    h->pp = nullptr;
+}
+
+namespace {
+// lssph_lsb_interpolate has no handle: one scratch per device, one call at a time per
+// device, kept until the process exits.
+std::mutex g_pp_mu[64];
+PPScratch g_pp[64];
+}  // namespace
+
+}  // namespace lssph
+
 using namespace lssph;
 
 extern "C" {
@@ -544,12 +598,15 @@ int lssph_lsb_interpolate(const lssph_params* p, int32_t n, const double* x, con
     const size_t N = (size_t)std::max(n, 1), T = (size_t)n_targets, C = (size_t)g.ncx * g.ncy;
     const size_t bytes = 4 * align256(8 * N) + 2 * align256(8 * T) + align256(8 * 3 * T) + 3 * align256(4 * N) +
                          3 * align256(4 * (C + 1));
-    cudaStream_t st = nullptr;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
-        return pp_fail(nullptr, LSSPH_E_CUDA, "lssph_lsb_interpolate: cudaStreamCreate failed");
-    char* blk = nullptr;
-    const char* stage = "cudaMallocAsync";
-    cudaError_t e = cudaMallocAsync((void**)&blk, bytes, st);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return pp_fail(nullptr, LSSPH_E_CUDA, "lssph_lsb_interpolate: no usable CUDA device");
+    std::lock_guard<std::mutex> lock(g_pp_mu[dev]);
+    PPScratch& S = g_pp[dev];
+    const char* stage = "";
+    cudaError_t e = pp_ready(&S, bytes, &stage);
+    cudaStream_t st = S.st;
+    char* blk = S.buf;
     if (e == cudaSuccess) {
         size_t off = 0;
         auto carve = [&](size_t b) { char* q = blk + off; off += align256(b); return q; };
@@ -566,12 +623,8 @@ int lssph_lsb_interpolate(const lssph_params* p, int32_t n, const double* x, con
         int* cnt = (int*)carve(4 * (C + 1));
         int* start = (int*)carve(4 * (C + 1));
         int* cursor = (int*)carve(4 * (C + 1));
-        if (off > bytes) {   // the carve must stay inside the allocation
-            cudaFreeAsync(blk, st);
-            cudaStreamSynchronize(st);
-            cudaStreamDestroy(st);
+        if (off > bytes)   // the carve must stay inside the allocation
             return pp_fail(nullptr, LSSPH_E_CUDA, "lssph_lsb_interpolate: scratch layout exceeds its allocation");
-        }
         if (n > 0) {
             cudaMemcpyAsync(dx, x, 8 * (size_t)n, cudaMemcpyHostToDevice, st);
             cudaMemcpyAsync(dy, y, 8 * (size_t)n, cudaMemcpyHostToDevice, st);
@@ -586,14 +639,12 @@ int lssph_lsb_interpolate(const lssph_params* p, int32_t n, const double* x, con
             stage = "copy of the results";
             e = cudaMemcpyAsync(out, dout, 8 * 3 * T, cudaMemcpyDeviceToHost, st);
         }
-        cudaFreeAsync(blk, st);
         const cudaError_t e2 = cudaStreamSynchronize(st);
         if (e == cudaSuccess && e2 != cudaSuccess) {
             stage = "stream synchronize";
             e = e2;
         }
     }
-    cudaStreamDestroy(st);
     if (e != cudaSuccess)
         return pp_fail(nullptr, LSSPH_E_CUDA,
                        std::string("lssph_lsb_interpolate: ") + stage + ": " + cudaGetErrorString(e));
@@ -617,19 +668,14 @@ int lssph_interpolate(lssph_handle* h, int32_t field, int32_t n_targets, const d
     PGrid g{-wl, -wl, h->p.h_eff, h->grid.nx, h->grid.ny};
     const size_t N = (size_t)h->num_total, T = (size_t)n_targets, C = (size_t)g.ncx * g.ncy;
     const size_t bytes = 2 * align256(8 * T) + align256(8 * 3 * T) + 3 * align256(4 * N) + 3 * align256(4 * (C + 1));
-    char* blk = nullptr;
-    // a private stream that starts after the handle's queued work
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev = nullptr;
-    const char* stage = "stream set-up";
-    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventRecord(ev, h->stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev, 0);
-    if (e == cudaSuccess) {
-        stage = "cudaMallocAsync";
-        e = cudaMallocAsync((void**)&blk, bytes, st);
-    }
+    // the handle's private stream, started after the handle's queued work
+    if (!h->pp) h->pp = new PPScratch();
+    const char* stage = "";
+    cudaError_t e = pp_ready(h->pp, bytes, &stage);
+    cudaStream_t st = h->pp->st;
+    char* blk = h->pp->buf;
+    if (e == cudaSuccess) e = cudaEventRecord(h->pp->ev, h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->pp->ev, 0);
     if (e == cudaSuccess) {
         size_t off = 0;
         auto carve = [&](size_t b) { char* q = blk + off; off += align256(b); return q; };
@@ -657,15 +703,12 @@ int lssph_interpolate(lssph_handle* h, int32_t field, int32_t n_targets, const d
             stage = "copy of the results";
             e = cudaMemcpyAsync(out, dout, 8 * 3 * T, cudaMemcpyDeviceToHost, st);
         }
-        cudaFreeAsync(blk, st);
         const cudaError_t e2 = cudaStreamSynchronize(st);
         if (e == cudaSuccess && e2 != cudaSuccess) {
             stage = "stream synchronize";
             e = e2;
         }
     }
-    if (ev) cudaEventDestroy(ev);
-    if (st) cudaStreamDestroy(st);
     if (e != cudaSuccess)
         return pp_fail(h, LSSPH_E_CUDA, std::string("lssph_interpolate: ") + stage + ": " + cudaGetErrorString(e));
     return LSSPH_OK;
