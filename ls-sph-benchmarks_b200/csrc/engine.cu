@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -33,6 +34,36 @@ using namespace lssph;
 
 
 namespace {
+
+// Page-locked slots for the handles' scalar read-back, shared by the process: page-locking
+// a buffer per handle (and unlocking it at destroy) cost about 2 ms per handle, half of a
+// handle's create + destroy.  Chunks of slots are locked on demand and kept; a handle takes
+// a slot at create and returns it at destroy, after its stream has drained.  Portable, so
+// that handles on any device of the process can use a slot.
+std::mutex g_pin_mu;
+std::vector<Scalars*> g_pin_free;
+constexpr int kPinChunk = 256;
+
+Scalars* pinned_slot() {
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    if (g_pin_free.empty()) {
+        Scalars* chunk = nullptr;
+        if (cudaHostAlloc((void**)&chunk, sizeof(Scalars) * kPinChunk, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;   // the checks then copy through pageable memory
+        }
+        for (int k = kPinChunk - 1; k >= 0; --k) g_pin_free.push_back(chunk + k);
+    }
+    Scalars* s = g_pin_free.back();
+    g_pin_free.pop_back();
+    return s;
+}
+
+void return_pinned_slot(Scalars* s) {
+    if (!s) return;
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    g_pin_free.push_back(s);
+}
 
 int fail(lssph_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
@@ -619,7 +650,7 @@ void free_handle(lssph_handle* h) {
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);
     if (h->block) cudaFree(h->block);
-    if (h->sc_host) cudaFreeHost(h->sc_host);
+    return_pinned_slot(h->sc_host);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -786,10 +817,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles);
     {
         // pinned scalar copy target (optional: without it the checks copy through pageable memory)
-        if (cudaMallocHost((void**)&h->sc_host, sizeof(Scalars)) != cudaSuccess) {
-            h->sc_host = nullptr;
-            cudaGetLastError();
-        }
+        h->sc_host = pinned_slot();
         const cudaError_t e = cudaMalloc(&h->block, block);
         if (e != cudaSuccess) {
             free_handle(h);
