@@ -702,11 +702,12 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->classical = h->p.sph_model <= 2;
     h->order = h->p.sph_model >= 4 ? h->p.sph_model - 1 : 2;   // LSSPH_A_mod.f90:46-56
     {
-        // Higher-order kernel shape: thread per particle is faster for q = 9 (its 1 KB
-        // shared-memory slot per particle still leaves a few warps per SM), warp per
-        // particle for q = 14 / 20.  LSSPH_HI_KERNEL=thread|warp overrides.
+        // Higher-order kernel shape, measured on B200 (Taylor-Green 128^2 / 256^2, closed
+        // box and periodic): thread per particle is faster for q = 9 (1.5-1.6x) and q = 14
+        // (1.04-1.6x), warp per particle for q = 20 (1.7-1.8x), where the thread's shared-
+        // memory slot leaves too few warps per SM.  LSSPH_HI_KERNEL=thread|warp overrides.
         const char* v = std::getenv("LSSPH_HI_KERNEL");
-        h->hi_thread = h->order == 3;
+        h->hi_thread = h->order <= 4;
         if (v && std::strcmp(v, "warp") == 0) h->hi_thread = false;
         if (v && std::strcmp(v, "thread") == 0) h->hi_thread = true;
     }
