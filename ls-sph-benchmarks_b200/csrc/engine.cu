@@ -1008,13 +1008,16 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
     if (steady_step_out) *steady_step_out = 0;
     if (nsteps <= 0) return LSSPH_OK;
-    Scalars s0{};
-    int rc = check_scalars(h, &s0);
+    int rc = ensure_tuned(h);
     if (rc != LSSPH_OK) return rc;
-    if (s0.steady || s0.done) return LSSPH_OK;   // the reference leaves the time loop at a steady state
-    if ((rc = ensure_tuned(h)) != LSSPH_OK) return rc;
     const int64_t launches0 = h->launch_counter;
     const int sb_start = h->sb, lb_start = h->lb;
+    // The step count at entry, recorded on the device behind the queued work, in place of a
+    // read-back before the launches: every kernel of a halted solve (steady state -- where
+    // the reference leaves its time loop --, step budget, error) does nothing, so the one
+    // read-back after the launches tells how many steps ran and why they stopped.
+    CUDA_TRY(h, cudaMemcpyAsync(&h->sc->step_mark, &h->sc->step_count, sizeof(int), cudaMemcpyDeviceToDevice,
+                                h->stream));
     CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
     for (int st = 0; st < nsteps; ++st) {
         cudaGraphExec_t& ge = h->graph[h->sb][h->lb];
@@ -1051,13 +1054,13 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
     h->last_launches = h->launch_counter - launches0;
     // steps after a stop (steady state, step budget, error) ran as no-ops: the buffers
     // sit where the last executed step left them
-    const int executed = s1.step_count - s0.step_count;
+    const int executed = s1.step_count - s1.step_mark;
     if (executed != nsteps) {
         h->sb = sb_start ^ (h->step_sbf & executed & 1);
         h->lb = (lb_start + h->step_lba * executed) % kLists;
     }
     if (rc != LSSPH_OK) return rc;
-    if (s1.steady && steady_step_out) *steady_step_out = s1.steady_step - s0.step_count;
+    if (s1.steady && steady_step_out && s1.steady_step > s1.step_mark) *steady_step_out = s1.steady_step - s1.step_mark;
     return LSSPH_OK;
 }
 

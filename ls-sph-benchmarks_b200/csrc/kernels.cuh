@@ -53,6 +53,7 @@ struct Scalars {
     int step_limit;             // stop once step_count reaches it (0 = no budget)
     int done;                   // 1 once the step budget is used up
     int ctas_done;              // CTAs of the current end-of-step launch that have finished
+    int step_mark;              // step_count at the start of the current lssph_step call
 };
 static_assert(offsetof(Scalars, done) == offsetof(Scalars, step_limit) + sizeof(int),
               "step_limit and done are written together");
