@@ -1809,6 +1809,22 @@ __global__ void __launch_bounds__(PPB * G) k_ghost(const Phys P, const Fld F, co
 // k_pst: particle shifting (q = 5) + copy-back + EOS + cell scatter.
 // NB = 3 (u,v,rho) or 4 (+T).  umax2 holds max(u^2+v^2) of the state being shifted.
 // =======================================================================================
+// Shifted position of the own particle at staged position ki, its cell key, and its entry
+// in the next cell list (PST_mod.f90:85-113 with update_cell).
+__device__ __forceinline__ void pst_move(const Phys& P, const Fld& nxt, const Lst& Ln, const int* __restrict__ gstart,
+                                         const Work& W, Scalars* sc, const SmemView& SM, int ki, double dx,
+                                         double dy) {
+    const int i = SM.idx[ki];
+    double xn = SM.x[ki] + dx, yn = SM.y[ki] + dy;
+    if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
+    nxt.x[i] = xn;
+    nxt.y[i] = yn;
+    if (!(isfinite(xn) && isfinite(yn))) atomicOr(&sc->err, ERR_NONFINITE);
+    const int nk = cell_key_mul(P, xn, yn, sc);
+    if (nk >= 0) W.key[i] = nk;
+    scatter_to_cell(P, Ln, gstart, nk, i, sc);
+}
+
 // K: order of the Taylor basis (2: q = 5 for SPH_MODEL 3; 1: q = 2 for the classical models).
 template <int NB, int G, bool MIXED, int K = 2>
 __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
@@ -1896,17 +1912,26 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
         }
         __syncthreads();
         const int o = ob + (int)threadIdx.x;
-        if ((int)threadIdx.x < PPB && o < n_own) {
-            const double* sm = SM.sums + threadIdx.x * SR;
-            const int ki = SM.own_k[o];
-            const int cnt = (int)sm[SR - 1];
-            // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
-            double dx = -coe * sm[SR - 3], dy = -coe * sm[SR - 2];
+        // shift vector of pass slot t, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
+        auto shift = [&](int t, double& dx, double& dy) {
+            const double* sm = SM.sums + t * SR;
+            dx = -coe * sm[SR - 3];
+            dy = -coe * sm[SR - 2];
             const double rr = sqrt(dx * dx + dy * dy);
             if (rr > 0.2 * P.h) {
                 dx = ((0.2 * P.h) * dx) / rr;
                 dy = ((0.2 * P.h) * dy) / rr;
             }
+        };
+        // with more than one warp, the warps idle in the solve move this pass's particles,
+        // key them and append them to the next cell list (the shift needs no solve)
+        constexpr bool split = G > 1;
+        if ((int)threadIdx.x < PPB && o < n_own) {
+            const double* sm = SM.sums + threadIdx.x * SR;
+            const int ki = SM.own_k[o];
+            const int cnt = (int)sm[SR - 1];
+            double dx, dy;
+            shift(threadIdx.x, dx, dy);
             double B[NB][Q];
             {
                 double A[Q][Q];
@@ -1939,19 +1964,20 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
                 acc[c] = sacc;
             }
             const int i = SM.idx[ki];
-            const double my_x = SM.x[ki], my_y = SM.y[ki];
-            double xn = my_x + dx, yn = my_y + dy;
-            if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
             const double un = SM.u[ki] + acc[0], vn = SM.v[ki] + acc[1], rn = SM.rho[ki] + acc[2];
-            nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
+            nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
             nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
             nxt.vol[i] = P.SP_mass / rn;
-            bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
+            bool finite = isfinite(un) && isfinite(vn) && isfinite(rn);
             if constexpr (NB == 4) { const double tn = SM.tem[ki] + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
             if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
-            const int nk = cell_key_mul(P, xn, yn, sc);
-            if (nk >= 0) W.key[i] = nk;
-            scatter_to_cell(P, Ln, gstart, nk, i, sc);
+            if (!split) pst_move(P, nxt, Ln, gstart, W, sc, SM, ki, dx, dy);
+        } else if (split && (int)threadIdx.x >= PPB) {
+            for (int t = (int)threadIdx.x - PPB; t < PPB && ob + t < n_own; t += blockDim.x - PPB) {
+                double dx, dy;
+                shift(t, dx, dy);
+                pst_move(P, nxt, Ln, gstart, W, sc, SM, SM.own_k[ob + t], dx, dy);
+            }
         }
         __syncthreads();
     }
