@@ -961,8 +961,9 @@ __device__ __forceinline__ void rhs_ls(const Phys& P, const Work& W, int i, doub
 // the start-of-step and RK4 accumulator values; the new position and its cell key (which
 // need the current velocity only, not the RHS); the new fields and the EOS; the scatter
 // into the next cell list.  stage_advance runs them in that order for one particle.  The
-// LS tile kernel moves its particles on the warps that have no solve to do, so that the
-// position loads and the scatter's atomics overlap the solve.
+// tile stage kernels (LS in FP64 and mixed precision, classical) with more than one warp
+// move their particles on the warps that have no solve to do, so that the position loads
+// and the scatter's atomics overlap the solve.
 template <int NB>
 __device__ __forceinline__ void keep_rhs(const Work& W, const StageCfg& S, int i, double Ru, double Rv, double Rr,
                                          double Rt) {
