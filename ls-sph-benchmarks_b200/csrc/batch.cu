@@ -115,10 +115,13 @@ void optin(K kernel) {
 }
 
 // Launch (or, with prep, only opt in the shared memory of) one batched phase kernel.
-// Precision x lanes: the mixed-precision kernels exist for 4 lanes only.
+// Precision x lanes: the mixed-precision kernels exist for 2 and 4 lanes.
 template <class F>
 void dispatch_kind(const BatchGroup& g, F&& f) {
-    if (g.mixed) f(std::integral_constant<int, 4>{}, std::true_type{});
+    if (g.mixed) {
+        if (g.G == 2) f(std::integral_constant<int, 2>{}, std::true_type{});
+        else f(std::integral_constant<int, 4>{}, std::true_type{});
+    }
     else dispatch_lanes(g.G, [&](auto GG) { f(GG, std::false_type{}); });
 }
 

@@ -188,7 +188,7 @@ struct Where {
 Where all_tiles(const lssph_handle* h) { return Where{nullptr, h->ntiles, h->stream, h->pdl, 0}; }
 
 // ---- kernel dispatch on lanes, register budget and precision ------------------------------
-// The mixed-precision kernels exist for 4 lanes per particle only.
+// The mixed-precision kernels exist for 2 and 4 lanes per particle.
 template <int NB, int GG, bool MX>
 void run_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     if (h->classical) {   // SPH_MODEL 1 / 2 (FP64 only)
@@ -226,7 +226,11 @@ template <int NB>
 void launch_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_STAGE);
     if (h->order >= 3) { launch_stage_hi(h, S, w.tiles, w.count, w.stream, w.pdl, w.priority); return; }
-    if (h->mixed) { run_stage<NB, 4, true>(h, S, w); return; }
+    if (h->mixed) {
+        if (h->G == 2) run_stage<NB, 2, true>(h, S, w);
+        else run_stage<NB, 4, true>(h, S, w);
+        return;
+    }
     switch (h->G) {
         case 1: run_stage<NB, 1, false>(h, S, w); break;
         case 2: run_stage<NB, 2, false>(h, S, w); break;
@@ -331,7 +335,11 @@ template <int NB>
 void launch_pst_t(lssph_handle* h, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_PST);
     if (h->order >= 3) { launch_pst_hi(h, w.tiles, w.count, w.stream, w.pdl, w.priority); return; }
-    if (h->mixed) { run_pst<NB, 4, true>(h, w); return; }
+    if (h->mixed) {
+        if (h->G == 2) run_pst<NB, 2, true>(h, w);
+        else run_pst<NB, 4, true>(h, w);
+        return;
+    }
     switch (h->G) {
         case 1: run_pst<NB, 1, false>(h, w); break;
         case 2: run_pst<NB, 2, false>(h, w); break;
@@ -494,7 +502,7 @@ int autotune(lssph_handle* h) {
         h->tight = h->budget >= 1;
         return LSSPH_OK;
     }
-    // lanes = 0 on an FP64 q = 5 solve: 4 lanes per particle unless 2 lanes run the RHS
+    // lanes = 0 on a q = 5 LS solve: 4 lanes per particle unless 2 lanes run the RHS
     // pass at least 5 % faster (the margin keeps the pick, and with it the summation order,
     // the same from run to run when the two are close)
     const int nlanes = h->lanes_auto ? 2 : 1;
@@ -674,8 +682,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs the LS-SPH model (SPH_MODEL 3) only");
     if (pin->precision != LSSPH_PRECISION_FP64 && pin->precision != LSSPH_PRECISION_MIXED)
         return fail(nullptr, LSSPH_E_BAD_PARAM, "precision must be LSSPH_PRECISION_FP64 or LSSPH_PRECISION_MIXED");
-    if (pin->precision == LSSPH_PRECISION_MIXED && pin->lanes != 0 && pin->lanes != 4)
-        return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs with 4 lanes per particle (lanes = 0 or 4)");
+    if (pin->precision == LSSPH_PRECISION_MIXED && pin->lanes != 0 && pin->lanes != 2 && pin->lanes != 4)
+        return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs with 2 or 4 lanes per particle (lanes = 0, 2 or 4)");
     if (pin->target_problem == 4 && !tem) return fail(nullptr, LSSPH_E_BAD_PARAM, "tem required for problem 4");
     if (num_int <= 0 || num_total < num_int || (num_total == num_int && !pin->periodic))
         return fail(nullptr, LSSPH_E_BAD_PARAM, "bad particle counts");
@@ -810,10 +818,13 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->n_int = (int)t_int.size();
     h->n_wall = (int)t_wall.size();
     h->overlap = h->overlap_allowed && h->n_int > 0 && h->n_wall > 0 && !p.periodic;
-    // lanes = 0: the first solo launch measures 2 and 4 lanes (FP64 q = 5 LS, no overlapped
-    // ghost schedule) and keeps the faster; the shared memory covers both
-    h->lanes_auto = h->p.lanes == 0 && !h->mixed && !h->classical && h->order == 2 && !h->overlap;
-    if (h->lanes_auto) h->smem_bytes = std::max(h->smem_bytes, tile_smem_bytes(h->grid.cap, 2, h->has_tem));
+    // lanes = 0: the first solo launch measures 2 and 4 lanes (q = 5 LS in FP64 or mixed
+    // precision, no overlapped ghost schedule) and keeps the faster; the shared memory
+    // covers both
+    h->lanes_auto = h->p.lanes == 0 && !h->classical && h->order == 2 && !h->overlap;
+    if (h->lanes_auto)
+        h->smem_bytes = std::max(h->smem_bytes, h->mixed ? tile_smem_bytes_mx(h->grid.cap, 2, h->has_tem)
+                                                         : tile_smem_bytes(h->grid.cap, 2, h->has_tem));
     // one device block for every array of the solve (one cudaMalloc, one cudaFree)
     const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles);
     {

@@ -91,6 +91,40 @@ def test_mixed_taylor_green_decay_error_unchanged():
     assert abs(errs[lssph.PRECISION_MIXED] - errs[lssph.PRECISION_FP64]) <= 1e-2 * errs[lssph.PRECISION_FP64], errs
 
 
+@pytest.mark.parametrize("case", ["taylor_green", "cavity", "boussinesq"])
+def test_mixed_two_lanes_within_bound_of_fp64(case):
+    # the mixed kernels at 2 lanes per particle: the same sums split over 2 lanes, the same
+    # bound against FP64
+    mk, steps = CASES[case]
+    p = mk()
+    s64 = _sim(p, lssph.PRECISION_FP64)
+    smx = _sim(lssph.make_params(p, lanes=2), lssph.PRECISION_MIXED)
+    assert smx.tuning()["lanes"] == 2
+    assert s64.step(steps) == smx.step(steps) == 0
+    g64, gmx = s64.download(), smx.download()
+    ni = s64.num_int
+    for k in _fields(p):
+        err = _rel(getattr(gmx, k)[:ni], getattr(g64, k)[:ni])
+        assert err <= TOL, (k, err)
+
+
+def test_mixed_two_lane_members_identical_alone_and_batched():
+    mk = [lambda: lssph.make_params(lssph.taylor_green_params(num=48, PERIODIC=1), lanes=2),
+          lambda: lssph.make_params(lssph.cavity_params(num=40), lanes=2)]
+    solo = [_sim(f(), lssph.PRECISION_MIXED, seed=i) for i, f in enumerate(mk)]
+    mem = [_sim(f(), lssph.PRECISION_MIXED, seed=i) for i, f in enumerate(mk)]
+    with lssph.Batch() as b:
+        for m in mem:
+            b.add(m)
+        b.step(5)
+    for s in solo:
+        s.step(5)
+    for s, m in zip(solo, mem):
+        gs, gm = s.download(), m.download()
+        for k in _fields(s.params):
+            assert np.array_equal(getattr(gs, k), getattr(gm, k)), k
+
+
 def test_mixed_members_identical_alone_and_batched():
     mk = [lambda: lssph.taylor_green_params(num=48), lambda: lssph.boussinesq_params(num=40),
           lambda: lssph.diffusion_params(num=30)]

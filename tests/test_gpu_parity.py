@@ -179,14 +179,17 @@ def test_other_lane_counts_rel_l2(case, lanes):
         assert _rel_l2(getattr(g, k), o[k]) <= 1e-10, k
 
 
-@pytest.mark.parametrize("case", ["taylor_green_periodic_128", "taylor_green_periodic_96", "cavity_64"])
+@pytest.mark.parametrize("case", ["taylor_green_periodic_128", "taylor_green_periodic_96", "cavity_64",
+                                  "taylor_green_periodic_128_mixed"])
 def test_automatic_lanes_equal_the_picked_count(case):
     # lanes = 0: the engine measures 2 and 4 lanes (FP64 q = 5 LS) and keeps the faster; the
     # run is then bit for bit the run with that count given explicitly.  The closed box
     # (ghost launches beside the interior tiles) keeps 4.
     mk = {"taylor_green_periodic_128": lambda **kw: lssph.taylor_green_params(num=128, PERIODIC=1, **kw),
           "taylor_green_periodic_96": lambda **kw: lssph.taylor_green_params(num=96, PERIODIC=1, **kw),
-          "cavity_64": lambda **kw: lssph.cavity_params(num=64, **kw)}[case]
+          "cavity_64": lambda **kw: lssph.cavity_params(num=64, **kw),
+          "taylor_green_periodic_128_mixed": lambda **kw: lssph.make_params(
+              lssph.taylor_green_params(num=128, PERIODIC=1, **kw), precision=lssph.PRECISION_MIXED)}[case]
     auto = lssph.Simulation.new(mk(lanes=0))
     picked = auto.tuning()["lanes"]
     assert picked in (2, 4)

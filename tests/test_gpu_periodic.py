@@ -126,7 +126,9 @@ def test_periodic_members_in_a_batch_equal_solo():
           lambda: lssph.make_params(lssph.taylor_green_params(num=32, PERIODIC=1), precision=lssph.PRECISION_MIXED)]
 
     def make(f, i):
-        p = f()
+        # lanes fixed: with lanes = 0 a solo run picks 2 or 4 by timing at its first launch,
+        # while a batch member that never ran alone keeps 4
+        p = lssph.make_params(f(), lanes=4)
         st, ni = lssph.setup_particles(p)
         if p.target_problem == 2:
             st.u[:ni] += 1.0

@@ -185,9 +185,11 @@ def test_status_strings():
         assert lib.lssph_status_string(code)
 
 
-def test_mixed_precision_requires_four_lanes():
+def test_mixed_precision_runs_two_or_four_lanes():
+    # the mixed-precision kernels exist for 2 and 4 lanes per particle; 8 is refused before
+    # any device work
     import lssph
-    p = lssph.make_params(lssph.taylor_green_params(num=16), precision=lssph.PRECISION_MIXED, lanes=2)
+    p = lssph.make_params(lssph.taylor_green_params(num=16), precision=lssph.PRECISION_MIXED, lanes=8)
     st, ni = lssph.setup_particles(p)
     with pytest.raises(lssph.LssphError) as e:
         lssph.Simulation(p, st, ni)
