@@ -304,13 +304,25 @@ def bench_mixed(steps: int = 100, acc_steps: int = 500) -> dict:
     out = {"workload": "cavity_re1000_256x256_rk4_pst", "steps": steps,
            "l2": "inputs larger than L2 not required: per-step working set ~45 MB, warm"}
     states = {}
+    # each precision at the lane count (2 or 4 per particle) that runs it faster here
     for name, prec in (("fp64", lssph.PRECISION_FP64), ("mixed", lssph.PRECISION_MIXED)):
-        p = lssph.make_params(lssph.cavity_params(num=256, re=1000.0), precision=prec)
-        sim = lssph.Simulation.new(p)
-        sim.step(5)
-        sim.step(steps)
-        ms, _ = sim.last_step_stats()
-        out[f"{name}_value"] = sim.num_int * steps / (ms * 1e-3)
+        best = None
+        for lanes in (4, 2):
+            p = lssph.make_params(lssph.cavity_params(num=256, re=1000.0), precision=prec, lanes=lanes)
+            sim = lssph.Simulation.new(p)
+            sim.step(5)
+            sim.step(steps)
+            ms, _ = sim.last_step_stats()
+            v = sim.num_int * steps / (ms * 1e-3)
+            if best is None or v > best[0]:
+                if best is not None:
+                    best[2].close()
+                best = (v, lanes, sim)
+            else:
+                sim.close()
+        v, lanes, sim = best
+        out[f"{name}_value"] = v
+        out[f"{name}_lanes"] = lanes
         out[f"{name}_register_budget"] = sim.tuning()["register_budget"]
         sim.step(acc_steps - 5 - steps)
         states[name] = (sim.download(), sim.num_int)
