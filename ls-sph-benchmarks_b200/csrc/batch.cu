@@ -437,6 +437,8 @@ int lssph_batch_add(lssph_batch* b, lssph_handle* h) {
     if (b->in_flight) return bfail(b, LSSPH_E_BAD_PARAM, "a batch step call is in flight");
     if (h->p.sph_model != 3)
         return bfail(b, LSSPH_E_UNSUPPORTED, "batched solves run the 2nd-order LS-SPH model (SPH_MODEL 3) only");
+    // a member with lanes = 0 picks its lane count now, as its first solo launch would
+    if (const int rc = resolve_lanes(h)) return bfail(b, rc, "measuring a member's lane count failed");
     b->members.push_back(h);
     h->batch = b;
     b->dirty = true;

@@ -545,6 +545,8 @@ int ensure_tuned(lssph_handle* h) { return h->tuned ? LSSPH_OK : autotune(h); }
 
 }  // namespace
 
+int lssph::resolve_lanes(lssph_handle* h) { return (h->lanes_auto && !h->tuned) ? autotune(h) : LSSPH_OK; }
+
 bool lssph::pdl_enabled() {
     const char* v = std::getenv("LSSPH_PDL");
     return !(v && std::strcmp(v, "0") == 0);

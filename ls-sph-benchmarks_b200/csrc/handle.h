@@ -127,6 +127,9 @@ void batch_forget(lssph_batch* b, lssph_handle* h);
 // Finish and free a handle's asynchronous snapshots (snapshot.cu).
 void snapshot_release(lssph_handle* h);
 void postproc_release(lssph_handle* h);
+// lanes = 0 on a handle not yet measured: measure 2 and 4 lanes now (engine.cu), so that a
+// batch member runs the lane count its solo run would.
+int resolve_lanes(lssph_handle* h);
 
 // Higher-order LS stage and PST launches, SPH_MODEL 4 / 5 / 6 (highorder.cu).  tiles:
 // tile of each CTA (NULL: CTA i runs tile i); while h->preparing they only set the
