@@ -84,8 +84,12 @@ typedef struct lssph_params {
     double  dt, dt_CFL, dt_vis, dt_th, dt_CFL_relax, dt_vis_relax;
     /* ---- engine options (no reference counterpart) ---- */
     int32_t  precision;   /* LSSPH_PRECISION_* */
-    int32_t  lanes;       /* lanes per particle in neighbour loops: 0 = auto,
-                             1 = reference summation order (bit-exact vs the oracle) */
+    int32_t  lanes;       /* lanes per particle in neighbour loops: 1 = reference
+                             summation order (bit-exact vs the oracle); 2, 4, 8 (mixed
+                             precision 2, 4); 0 = auto: a q = 5 LS solve without the
+                             overlapped ghost schedule (periodic) times 2 and 4 at its
+                             first solo launch or batch join and keeps the faster unless
+                             4 is within 5 %, any other solve runs 4 */
     uint64_t seed;        /* POS_PERT jitter seed (the reference seeds from the clock,
                              impose_initial_conditions_mod.f90:43-51) */
     int32_t  periodic;    /* 1: periodic square [0, LEN_X)^2 without walls (problems 1, 2);
