@@ -166,6 +166,17 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, dist, device: str = "cuda") -> float:
+    """The largest x of all ranks (each rank passes its own device time); x itself when
+    there is no process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _profile_traffic():
     """DRAM bytes per k_stage launch from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "k_stage_taylor_green_128_periodic.txt")
@@ -649,9 +660,7 @@ def run_engine(args) -> int:
             launches += nl
     torch.cuda.synchronize()
     if dist:
-        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
+        dev_ms = max_over_ranks(dev_ms, dist)
         dist.barrier()
     value = ws * ni * args.steps / (dev_ms * 1e-3)
 
@@ -705,10 +714,7 @@ def run_engine(args) -> int:
         sim.step(1)
         sim.download_into(hst)
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
     nbytes = 6 * n_total * 8
     e2e = {"value": ws * ni * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nbytes,
            "d2h_bytes_per_step": nbytes, "steps": e2e_steps,
