@@ -102,7 +102,8 @@ def test_upload_mid_run_continues_bit_identically(case):
     # lssph_upload into a solve at another point of its run (other buffer parity, other
     # list rotation): the state it continues from is the uploaded one, nothing else
     mk = dict(CASES)
-    mk["tg_periodic"] = lambda: lssph.taylor_green_params(num=48, PERIODIC=1)
+    # lanes fixed: with lanes = 0 each handle of a periodic solve picks 2 or 4 by timing
+    mk["tg_periodic"] = lambda: lssph.taylor_green_params(num=48, PERIODIC=1, lanes=4)
     mk["tg_mixed"] = lambda: lssph.make_params(lssph.taylor_green_params(num=48), precision=lssph.PRECISION_MIXED)
     mk["cavity_classical"] = lambda: lssph.cavity_params(num=40, SPH_MODEL=1)
     p = mk[case]()

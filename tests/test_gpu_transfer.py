@@ -18,7 +18,8 @@ FIELDS = ("x", "y", "u", "v", "rho", "pre")
 CASES = {
     "diffusion": lambda: lssph.diffusion_params(num=40, seed=3),
     "taylor_green": lambda: lssph.taylor_green_params(num=48),
-    "taylor_green_periodic": lambda: lssph.taylor_green_params(num=48, PERIODIC=1),
+    # lanes fixed: with lanes = 0 each handle of a periodic solve picks 2 or 4 by timing
+    "taylor_green_periodic": lambda: lssph.taylor_green_params(num=48, PERIODIC=1, lanes=4),
     "cavity": lambda: lssph.cavity_params(num=40),
     "boussinesq": lambda: lssph.boussinesq_params(num=40),
 }
@@ -82,7 +83,7 @@ def test_pinned_upload_mid_run_equals_pageable(case):
 
 def test_pinned_round_trip_every_step_equals_resident_run():
     # the end-to-end pattern: upload, one step, download, each step, from pinned buffers
-    p = lssph.taylor_green_params(num=64, PERIODIC=1)
+    p = lssph.taylor_green_params(num=64, PERIODIC=1, lanes=4)
     res, e2e = _sim(p), _sim(p)
     host = _pinned_state(e2e.download(), False)
     for _ in range(12):
