@@ -34,23 +34,37 @@ UNIT = "particle-updates/s"
 WORKLOAD = "taylor_green_re100_128x128_periodic_rk4_pst_fp64"
 
 
+# The headline workload's parameters: Taylor-Green, Re = 100, 128^2, RK4 + PST, CFL 0.1,
+# TG_A = TG_B = 2.  periodic: the benchmark's periodic unit square (its u = -cos 2pi x
+# sin 2pi y is the reference's sin 2pi x cos 2pi y moved by a quarter period, the same
+# flow); else the reference's free-slip closed box.
+HEADLINE = dict(num=128, re=100.0, coe_cfl=0.1, tg=2)
+
+
 def _params(lanes: int = 0, periodic: bool = True):
-    """Taylor-Green, Re = 100, 128^2, RK4 + PST, CFL 0.1.  periodic: the benchmark's periodic
-    unit square (its u = -cos 2pi x sin 2pi y is the reference's sin 2pi x cos 2pi y moved by
-    a quarter period, the same flow); else the reference's free-slip closed box."""
+    """The engine arm's parameters, built by the engine's host code."""
     import lssph
-    return lssph.taylor_green_params(num=128, re=100.0, coe_cfl=0.1, tg=2, lanes=lanes,
-                                     PERIODIC=1 if periodic else 0)
+    return lssph.taylor_green_params(**HEADLINE, lanes=lanes, PERIODIC=1 if periodic else 0)
 
 
-def _config(p, extra=None):
-    cfg = {"workload": WORKLOAD, "problem": "taylor_green", "num_x": p.num_x, "num_y": p.num_y,
-           "num_int": None, "num_total": None, "rk": p.rk, "pst": True, "re": 1.0 / p.vis_ref,
-           "dt": p.dt, "precision": "fp64", "domain": "periodic unit square" if p.periodic else "closed box",
-           "l2": "flushed between timed steps (256 MB write)"}
-    if extra:
-        cfg.update(extra)
-    return cfg
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O
+
+
+def _oracle_params(periodic: bool = True):
+    """The CPU arms' parameters, built by the oracle alone (its config.h defaults and
+    init_param restatement), so that the reference arm never loads the engine library."""
+    return _oracle().taylor_green_params(**HEADLINE, PERIODIC=1 if periodic else 0)
+
+
+def _config(p, num_int, num_total):
+    """The workload, identical in both arms' lines (arm-specific settings go elsewhere)."""
+    return {"workload": WORKLOAD, "problem": "taylor_green", "num_x": p.num_x, "num_y": p.num_y,
+            "num_int": num_int, "num_total": num_total, "rk": p.rk, "pst": True, "re": 1.0 / p.vis_ref,
+            "dt": p.dt, "precision": "fp64", "domain": "periodic unit square" if p.periodic else "closed box",
+            "l2": "device arm: a 256 MB write flushes L2 between timed steps; host arm: not applicable"}
 
 
 # ---------------------------------------------------------------------------------------
@@ -245,11 +259,9 @@ def _fp64_peak():
 
 def cpu_baseline(min_seconds: float = 10.0, max_steps: int = 2000) -> dict:
     """The oracle on all host cores for a bounded sample of the same workload."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    O = _oracle()
     cores = O.set_threads(os.cpu_count() or 1)
-    p = _params()
-    orc = O.Oracle(p)
+    orc = O.Oracle(_oracle_params())
     orc.run(2)                       # warm-up
     steps, t0 = 0, time.perf_counter()
     while steps < max_steps:
@@ -267,21 +279,21 @@ def run_reference(args) -> int:
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    O = _oracle()
     cores = O.set_threads(os.cpu_count() or 1)
-    p = _params()
+    p = _oracle_params()
     orc = O.Oracle(p)
     orc.run(args.warmup)
     t0 = time.perf_counter()
     orc.run(args.steps)
     dt = time.perf_counter() - t0
     value = orc.num_int * args.steps / dt
-    cfg = _config(p, {"num_int": orc.num_int, "num_total": orc.num_total, "parallelism": "cpu",
-                      "l2": "n/a (host CPU)"})
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config(p, orc.num_int, orc.num_total),
+            "arm": {"parallelism": f"host CPU, OpenMP over {cores} threads (rank 0 only)",
+                    "library": "oracle/_build/liblssph_oracle.so"},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{args.steps} time steps after {args.warmup} warm-up steps"},
@@ -531,6 +543,7 @@ def bench_batched(steps: int = 20) -> dict:
         seq_units += ni * steps
         sim.close()
     out["sequential_fp64_value"] = seq_units / (seq_ms * 1e-3)
+    finals = {}
     for name, prec in (("batched_fp64", lssph.PRECISION_FP64), ("batched_mixed", lssph.PRECISION_MIXED)):
         sims = []
         units = 0
@@ -547,8 +560,20 @@ def bench_batched(steps: int = 20) -> dict:
             ms, launches = b.last_step_stats()
         out[f"{name}_value"] = units * steps / (ms * 1e-3)
         out[f"{name}_launches_per_step"] = launches // steps
+        finals[name] = [(sim.download(), sim.num_int) for sim in sims]
         for sim in sims:
             sim.close()
+    # every field of every member, mixed against FP64 after the same 3 + steps steps
+    import numpy as np
+    worst = {}
+    for (g64, ni), (gmx, _) in zip(finals["batched_fp64"], finals["batched_mixed"]):
+        for k in ("x", "y", "u", "v", "rho", "pre"):
+            ref = getattr(g64, k)[:ni]
+            den = np.linalg.norm(ref)
+            if den > 0:
+                worst[k] = max(worst.get(k, 0.0), float(np.linalg.norm(getattr(gmx, k)[:ni] - ref) / den))
+    out["rel_l2_mixed_vs_fp64_worst_member"] = worst
+    out["max_rel_l2_mixed_vs_fp64"] = max(worst.values()) if worst else None
     out["total_particles"] = units
     out["value"] = out["batched_mixed_value"]
     out["unit"] = UNIT
@@ -607,6 +632,10 @@ def bench_serving() -> dict:
     srv = Server(max_active=64, chunk_steps=20, keep_results=False)
     st = srv.run(reqs)
     srv.close()
+    return {"scaled": _serving_record(st, reqs, scale)}
+
+
+def _serving_record(st, reqs, scale) -> dict:
     return {"workload": "Poisson 20/s for 8 s; 50% Boussinesq Ra [1e4,1e6], 50% cavity Re [100,3200]; "
                         "sides 64..384 step 32; mixed precision",
             "t_end_scale": scale, "t_end": 20.0 * scale, "requests": len(reqs), "completed": st.completed,
@@ -687,15 +716,20 @@ def run_engine(args) -> int:
     tune = sim.tuning()
     fp64_peak = _fp64_peak()
     fp64_achieved = flops_per_launch / stage_avg_s / 1e12
-    roofline = {"bound": "hbm", "kernel": f"k_stage<NB=4,G={tune['lanes']},{tune['register_budget']} registers>", "achieved": achieved_gbs, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": bytes_per_launch,
-                "fp64": {"achieved_tflops": fp64_achieved, "peak_tflops": fp64_peak,
-                         "frac": fp64_achieved / fp64_peak,
-                         "peak_source": "measured here: cuBLAS DGEMM 8192^3, best of 5",
-                         "flops_per_launch": flops_per_launch, "mean_neighbours": mean_p},
-                "frac_max_of_fp64_and_hbm": max(fp64_achieved / fp64_peak, achieved_gbs / hbm_peak),
+    f_frac, b_frac = fp64_achieved / fp64_peak, achieved_gbs / hbm_peak
+    # roofline of the dominant kernel: max(F / F_peak, B / B_peak), reported in the unit of
+    # the term that wins; the other term rides along
+    fp64_term = {"achieved": fp64_achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": f_frac,
+                 "peak_source": "measured here: cuBLAS DGEMM 8192^3, best of 5 (the measured-peaks "
+                                "file has no FP64 figure)",
+                 "flops_per_launch": flops_per_launch, "mean_neighbours": mean_p}
+    hbm_term = {"achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": b_frac,
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": bytes_per_launch}
+    win = fp64_term if f_frac >= b_frac else hbm_term
+    roofline = {"bound": "fp64" if win is fp64_term else "hbm",
+                "kernel": f"k_stage<NB=4,G={tune['lanes']},{tune['register_budget']} registers>",
+                "achieved": win["achieved"], "peak": win["peak"], "unit": win["unit"], "frac": win["frac"],
+                "traffic": traffic, "fp64": fp64_term, "hbm": hbm_term,
                 "launch_avg_us": stage_avg_s * 1e6,
                 "kernel_share": {k: v[0] for k, v in prof.items()}}
 
@@ -723,34 +757,64 @@ def run_engine(args) -> int:
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
-    extras = {}
+    extras, configs = {}, {}
     if rank == 0 and ws == 1 and not args.no_extras:
+        # detail sections first; the configurations the metric names (mixed precision,
+        # batched, serving) last, so that the end of the line carries their figures
         extras["closed_box"] = bench_closed_box()
-        extras["mixed"] = bench_mixed()
-        extras["batched"] = bench_batched()
-        extras["serving"] = bench_serving()
         extras["variants"] = bench_variants()
         extras["postproc"] = bench_postproc()
         extras["snapshots"] = bench_snapshots()
+        configs["mixed"] = bench_mixed()
+        configs["batched"] = bench_batched()
+        configs["serving"] = bench_serving()
 
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    cfg = _config(p, {"num_int": ni, "num_total": n_total, "parallelism": f"replicas{ws}",
-                      "lanes": tune["lanes"], "register_budget": tune["register_budget"],
-                      "global_batch": ni * ws})
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config(p, ni, n_total),
+            "engine": {"parallelism": f"replicas{ws}", "lanes": tune["lanes"],
+                       "register_budget": tune["register_budget"], "global_batch": ni * ws},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "particle_stages_per_s": value * p.rk,
             "velocity_rel_l2_vs_analytic": {"value": l2_analytic, "t": t_now,
                                             "steps": args.warmup + args.steps},
-            "clocks": clocks.summary(), **extras}
+            "clocks": clocks.summary(), **extras, **configs}
+    if configs:
+        line["summary_configs"] = summarize_configs(configs)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def summarize_configs(c: dict) -> dict:
+    """Compact figures of the mixed-precision, batched and serving configurations (the last
+    key of the line)."""
+    m, b, s = c.get("mixed", {}), c.get("batched", {}), c.get("serving", {})
+    r3 = lambda x: None if x is None else float(f"{x:.3g}")   # noqa: E731
+    out = {"unit": UNIT}
+    if m:
+        out["mixed_cavity256"] = {"fp64": r3(m["fp64_value"]), "mixed": r3(m["mixed_value"]),
+                                  "speedup": r3(m["speedup_vs_fp64"]),
+                                  "max_rel_l2_vs_fp64": r3(max(m["rel_l2_vs_fp64"].values())),
+                                  "after_steps": m["rel_l2_after_steps"]}
+    if b:
+        out["batched_64"] = {"sequential_fp64": r3(b["sequential_fp64_value"]),
+                             "batched_fp64": r3(b["batched_fp64_value"]),
+                             "batched_mixed": r3(b["batched_mixed_value"]),
+                             "speedup_mixed_vs_sequential_fp64": r3(b["speedup_vs_sequential_fp64"]),
+                             "max_rel_l2_mixed_vs_fp64": r3(b.get("max_rel_l2_mixed_vs_fp64"))}
+    for key, name in (("scaled", "serving_scaled"), ("capacity", "serving_real_physics")):
+        if key in s:
+            d = s[key]
+            out[name] = {k: r3(d[k]) if isinstance(d[k], float) else d[k]
+                         for k in ("t_end", "requests", "completed", "p50_s", "p99_s", "solves_per_s",
+                                   "max_queue", "mean_queue") if k in d}
+    return out
 
 
 def main() -> int:

@@ -308,21 +308,24 @@ int lssph_interpolate(lssph_handle* h, int32_t field, int32_t n_targets, const d
                       const double* ty, double* out);
 
 /* ---- allocation-free RHS (no counterpart in the reference) ---------------------------- */
-/* One calculate_RHS pass (LS-SPH type A, problems 2-4, FP64) over a particle state that
-   already lives in caller-owned device memory, writing the RHS arrays to caller-owned
-   device memory, for callers that cannot allocate GPU memory at the point of the call
-   (their memory is already committed to their own pool, or the call sits in a loop where
-   a driver allocation is not acceptable).  It calls no cudaMalloc/cudaFree: its working
-   set is one statically sized device array that every GPU loading this library reserves
-   until the process exits.  Limits: num_total <= LSSPH_NOALLOC_MAX_PARTICLES, cell grid
-   <= LSSPH_NOALLOC_MAX_CELLS cells, at most LSSPH_NOALLOC_CELL_CAP particles per cell;
-   larger inputs return LSSPH_E_CAPACITY before any GPU work.  The first call on a device
-   sets that device up (looks up the array's device address), so make that first call
-   before any stream capture.  The call runs on `stream` (NULL = default stream) and
-   returns when that work is done.  All calls share the one array: calls that overlap on
-   the GPU (other threads or streams) race and give wrong results.  Inputs x..pre (and tem
-   for problem 4) have num_total entries in the reference particle order; rhs_* have
-   num_int entries (rhs_tem only for problem 4). */
+/* One calculate_RHS pass (LS-SPH type A, problems 2-4, FP64, closed box) over a particle
+   state that already lives in caller-owned device memory, writing the RHS arrays to
+   caller-owned device memory, for callers that cannot allocate GPU memory at the point of
+   the call (their memory is already committed to their own pool, or the call sits in a
+   loop where a driver allocation is not acceptable).  It calls no cudaMalloc/cudaFree: its
+   working set is one statically sized device array that every GPU loading this library
+   reserves until the process exits.  Limits: num_total <= LSSPH_NOALLOC_MAX_PARTICLES,
+   cell grid <= LSSPH_NOALLOC_MAX_CELLS cells, at most LSSPH_NOALLOC_CELL_CAP particles per
+   cell; larger inputs return LSSPH_E_CAPACITY before any GPU work.  p->lanes picks the
+   lanes per particle of the neighbour sums as for a handle: 1 (the reference summation
+   order), 2 or 4 (0 means 4); other values, a periodic domain, problem 1 and mixed
+   precision return LSSPH_E_UNSUPPORTED.  Every call looks up the array's device address on
+   the current device.  The call runs on `stream` (NULL = default stream), waits for that
+   stream, and returns the cell-overflow / out-of-domain errors its kernels recorded.  All
+   calls share the one array and it keeps the last call's contents (each call clears what
+   must start at zero): calls that overlap on the GPU (other threads or streams) race and
+   give wrong results.  Inputs x..pre (and tem for problem 4) have num_total entries in the
+   reference particle order; rhs_* have num_int entries (rhs_tem only for problem 4). */
 #define LSSPH_NOALLOC_MAX_PARTICLES 262144
 #define LSSPH_NOALLOC_MAX_CELLS     32768
 #define LSSPH_NOALLOC_CELL_CAP      32

@@ -17,7 +17,7 @@ LIB = os.path.join(LIB_DIR, "liblssph.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 
 SOURCES = ["host.cpp", "engine.cu", "batch.cu", "noalloc.cu", "highorder.cu", "postproc.cu", "snapshot.cu"]
-HEADERS = ["engine.h", "handle.h", "kernels.cuh", "kernels_hi.cuh"]
+HEADERS = ["engine.h", "handle.h", "hostmem.h", "kernels.cuh", "kernels_hi.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -16,6 +16,8 @@
 // (2 x {stage, ghost} + epilogue).  Each step is captured once in a CUDA graph and
 // replayed.
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,6 +31,7 @@
 
 #include "engine.h"
 #include "handle.h"
+#include "hostmem.h"
 
 using namespace lssph;
 
@@ -507,22 +510,30 @@ int autotune(lssph_handle* h) {
     // the same from run to run when the two are close)
     const int nlanes = h->lanes_auto ? 2 : 1;
     const int lane_opts[2] = {h->G, 2};
-    double us[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    double us[2][3] = {{1e30, 1e30, 1e30}, {1e30, 1e30, 1e30}};
     int best_t[2] = {0, 0};
-    for (int g = 0; g < nlanes; ++g) {
-        h->G = lane_opts[g];
-        for (int t = 0; t < levels; ++t) {
-            h->tight = t >= 1;
-            h->budget = t;
-            launch_stage_any(h, S);   // warm-up (instruction cache, L2)
-            CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
-            for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
-            CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
-            CUDA_TRY(h, cudaEventSynchronize(h->ev1));
-            float ms = 0.f;
-            CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-            us[g][t] = 1e3 * ms / 3.0;
+    // Every option is timed in each of several interleaved rounds and keeps its fastest
+    // round, so that a clock ramp or a neighbour's burst during one round does not decide
+    // the pick (a single round swung the choice by about 10 % between machines).
+    constexpr int kRounds = 5;
+    for (int round = 0; round < kRounds; ++round) {
+        for (int g = 0; g < nlanes; ++g) {
+            h->G = lane_opts[g];
+            for (int t = 0; t < levels; ++t) {
+                h->tight = t >= 1;
+                h->budget = t;
+                launch_stage_any(h, S);   // warm-up (instruction cache, L2)
+                CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+                for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
+                CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+                CUDA_TRY(h, cudaEventSynchronize(h->ev1));
+                float ms = 0.f;
+                CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+                us[g][t] = std::min(us[g][t], 1e3 * ms / 3.0);
+            }
         }
+    }
+    for (int g = 0; g < nlanes; ++g) {
         // In the overlapped step the interior tiles share the SMs with the ghost launch: four
         // CTAs per SM (the tight budget) leave room for it where three do not, which an RHS
         // pass alone does not show, so the overlapped step always takes the tight budget.
@@ -532,7 +543,7 @@ int autotune(lssph_handle* h) {
     }
     const int pick = (nlanes == 2 && us[1][best_t[1]] < 0.95 * us[0][best_t[0]]) ? 1 : 0;
     h->G = lane_opts[pick];
-    for (int t = 0; t < 3; ++t) h->tune_us[t] = us[pick][t];
+    for (int t = 0; t < 3; ++t) h->tune_us[t] = us[pick][t] < 1e29 ? us[pick][t] : 0.0;
     h->budget = best_t[pick];
     h->tight = h->budget >= 1;
     h->launch_counter = c0;
@@ -604,13 +615,37 @@ void* mapped_host(const void* p, size_t bytes) {
     return a.devicePointer;
 }
 
-// Every non-null field mapped: device addresses into out[0..6], true.
-bool all_mapped(const double* const (&f)[7], size_t bytes, double* (&out)[7]) {
+// Access flags of the current device on host memory p (cuPointerGetAttribute with
+// CU_POINTER_ATTRIBUTE_ACCESS_FLAGS, reached through the runtime's driver entry point so
+// that the library does not link libcuda), or -1 when the driver cannot be asked.
+long long host_access_flags(const void* p) {
+    static_assert(CU_POINTER_ATTRIBUTE_ACCESS_FLAG_READ == kAccessRead &&
+                  CU_POINTER_ATTRIBUTE_ACCESS_FLAG_READWRITE == kAccessReadWrite, "access flag values");
+    static const PFN_cuPointerGetAttribute_v4000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<PFN_cuPointerGetAttribute_v4000>(f);
+    }();
+    if (!fn) return -1;
+    unsigned long long flags = 0;   // the driver writes a 32-bit enum into the low bytes
+    if (fn(&flags, CU_POINTER_ATTRIBUTE_ACCESS_FLAGS, (CUdeviceptr)(uintptr_t)p) != CUDA_SUCCESS) return -1;
+    return (long long)(flags & 0xffffffffull);
+}
+
+// Every non-null field mapped (and, for a kernel that stores into them, writable from the
+// device at both ends): device addresses into out[0..6], true.
+bool all_mapped(const double* const (&f)[7], size_t bytes, double* (&out)[7], bool store = false) {
     for (int k = 0; k < 7; ++k) {
         out[k] = nullptr;
         if (!f[k]) continue;
         out[k] = static_cast<double*>(mapped_host(f[k], bytes));
         if (!out[k]) return false;
+        if (store && !(mapped_store_allowed(host_access_flags(f[k])) &&
+                       mapped_store_allowed(host_access_flags(reinterpret_cast<const char*>(f[k]) + bytes - 1))))
+            return false;
     }
     return true;
 }
@@ -1166,7 +1201,7 @@ int lssph_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double
     {   // page-locked, mapped host buffers: one kernel writes them
         const double* const f[7] = {x, y, u, v, rho, pre, h->has_tem ? tem : nullptr};
         double* d[7];
-        if (all_mapped(f, bytes, d)) {
+        if (all_mapped(f, bytes, d, true)) {
             k_download_mapped<<<blocks_for(h->num_total, 256), 256, 0, h->stream>>>(
                 h->P, F, HostOut{d[0], d[1], d[2], d[3], d[4], d[5], d[6]});
             if (tem && !h->has_tem) std::memset(tem, 0, bytes);

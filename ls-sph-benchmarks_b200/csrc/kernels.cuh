@@ -590,8 +590,10 @@ __device__ __forceinline__ void stage_lists(const Phys& P, const Lst& L, const i
         if (cx >= 0 && cx < P.nx && cy >= 0 && cy < P.ny) {
             c = cx + cy * P.nx;
             g0 = __ldg(gstart + c);
-            const int gc = __ldg(gstart + c + 1) - g0;
-            nf = min(__ldg(L.cnt + c), P.cap - gc);
+            // a cell never stages more than cap particles, whatever its counters say (a
+            // counter past cap has already raised the cell-overflow error)
+            const int gc = min(__ldg(gstart + c + 1) - g0, P.cap);
+            nf = max(0, min(__ldg(L.cnt + c), P.cap - gc));
             ng = FLUID_ONLY ? 0 : gc;
         }
         T.nf[tid] = nf;

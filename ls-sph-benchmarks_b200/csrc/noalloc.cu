@@ -19,7 +19,6 @@
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "engine.h"
@@ -27,6 +26,9 @@
 
 namespace lssph {
 namespace {
+
+using KernelPtr = void (*)(const Phys, const Fld, const Fld, const Lst, const Lst, const int*, const int*, const Work,
+                           const StageCfg, Scalars*, int, const int*);
 
 // Byte layout of the scratch array (offsets aligned to 256 bytes).
 constexpr size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
@@ -49,7 +51,7 @@ static __device__ __align__(256) unsigned char g_rhs_scratch[kScratchBytes];
 
 // ---- set-up kernels -------------------------------------------------------------------
 // Volumes of all particles, cell keys (ghosts: division form of init_cell_mod.f90:76-78;
-// interior: multiplication form of update_cell_mod.f90:238-240), per-cell ghost counts and
+// interior: multiplication form of update_cell_mod.f90:53-55), per-cell ghost counts and
 // the scatter of interior particles into their cells.
 __global__ void k_na_keys(const Phys P, double h_eff, const Fld F, Lst L, int* gkey, int* gcnt, Scalars* sc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,29 +124,29 @@ __global__ void k_na_sort_ghosts(const Phys P, const int* cnt, const int* gstart
 }
 
 // ---- host side ----------------------------------------------------------------------------
-std::mutex g_mu;
-unsigned char* g_base[64] = {nullptr};   // device address of g_rhs_scratch per device
-bool g_ready[64] = {false};
-
-// Once per device, with that device current: look up the device address of the scratch
-// array and opt the RHS kernels in to the shared memory they need.
-int scratch_base(int dev, unsigned char** out, std::string* msg) {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (dev < 0 || dev >= 64) { *msg = "device ordinal out of range"; return LSSPH_E_CUDA; }
-    if (!g_ready[dev]) {
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_rhs_scratch);
-        if (e != cudaSuccess) { *msg = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return LSSPH_E_CUDA; }
-        // the same opt-in value the simulation handles use for these kernels
-        const int bytes = (int)tile_smem_bytes(64, 8, true);
-        for (cudaError_t a : {cudaFuncSetAttribute(k_stage<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-                              cudaFuncSetAttribute(k_stage<5, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)}) {
-            if (a != cudaSuccess) { *msg = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(a); return LSSPH_E_CUDA; }
-        }
-        g_base[dev] = static_cast<unsigned char*>(ptr);
-        g_ready[dev] = true;
+// The tile kernels this entry point launches, by lanes per particle.
+template <int NB>
+KernelPtr stage_kernel(int lanes) {
+    switch (lanes) {
+        case 1: return k_stage<NB, 1>;
+        case 2: return k_stage<NB, 2>;
+        default: return k_stage<NB, 4>;
     }
-    *out = g_base[dev];
+}
+
+// With the caller's device current: the device address of the scratch array, and the
+// shared-memory opt-in of the kernel about to run.  Both are looked up on every call (they
+// allocate nothing), so nothing goes stale when the caller resets the device or switches
+// contexts between calls.
+template <int NB>
+int scratch_base(int lanes, unsigned char** out, std::string* msg) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_rhs_scratch);
+    if (e != cudaSuccess) { *msg = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return LSSPH_E_CUDA; }
+    const int bytes = (int)tile_smem_bytes(kCap, lanes, NB == 5);
+    const cudaError_t a = cudaFuncSetAttribute(stage_kernel<NB>(lanes), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (a != cudaSuccess) { *msg = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(a); return LSSPH_E_CUDA; }
+    *out = static_cast<unsigned char*>(ptr);
     return LSSPH_OK;
 }
 
@@ -166,6 +168,11 @@ extern "C" int lssph_rhs_noalloc(const lssph_params* pin, int32_t num_total, int
     init_param(&p);
     if (p.target_problem == 1 || p.sph_model != 3 || p.precision != LSSPH_PRECISION_FP64)
         return fail(LSSPH_E_UNSUPPORTED, "lssph_rhs_noalloc: FP64 SPH_MODEL 3 for problems 2-4 only");
+    if (p.periodic)
+        return fail(LSSPH_E_UNSUPPORTED, "lssph_rhs_noalloc: the closed box only (its cell grid has no periodic wrap)");
+    if (!(p.lanes == 0 || p.lanes == 1 || p.lanes == 2 || p.lanes == 4))
+        return fail(LSSPH_E_UNSUPPORTED, "lssph_rhs_noalloc: lanes must be 1, 2 or 4 (0 means 4)");
+    const int lanes = p.lanes == 0 ? 4 : p.lanes;
     if (p.target_problem == 4 && (!tem || !rhs_tem)) return fail(LSSPH_E_BAD_PARAM, "lssph_rhs_noalloc: tem required");
     const int nx = (int)std::ceil((p.len_x + 2.0 * p.WL_thick) / p.h_eff);
     const int ny = (int)std::ceil((p.len_y + 2.0 * p.WL_thick) / p.h_eff);
@@ -174,11 +181,9 @@ extern "C" int lssph_rhs_noalloc(const lssph_params* pin, int32_t num_total, int
         return fail(LSSPH_E_CAPACITY, "lssph_rhs_noalloc: at most " + std::to_string(kMaxN) + " particles and " +
                                           std::to_string(kMaxCells) + " cells (got " + std::to_string(num_total) +
                                           " particles, " + std::to_string((long)nx * ny) + " cells)");
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return fail(LSSPH_E_CUDA, "lssph_rhs_noalloc: no CUDA device");
     unsigned char* base = nullptr;
-    int rc = scratch_base(dev, &base, &msg);
-    if (rc != LSSPH_OK) return fail(rc, msg);
+    const int rc = p.target_problem == 4 ? scratch_base<5>(lanes, &base, &msg) : scratch_base<4>(lanes, &base, &msg);
+    if (rc != LSSPH_OK) return fail(rc, "lssph_rhs_noalloc: " + msg);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
     Phys P{};
@@ -227,11 +232,11 @@ extern "C" int lssph_rhs_noalloc(const lssph_params* pin, int32_t num_total, int
     S.stage = 1;
     S.write_rhs = 1;
     const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY;
-    const size_t sm = tile_smem_bytes(kCap, 4, p.target_problem == 4);
+    const size_t sm = tile_smem_bytes(kCap, lanes, p.target_problem == 4);
     if (p.target_problem == 4)
-        k_stage<5, 4><<<ntx * nty, PPB * 4, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx, nullptr);
+        stage_kernel<5>(lanes)<<<ntx * nty, PPB * lanes, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx, nullptr);
     else
-        k_stage<4, 4><<<ntx * nty, PPB * 4, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx, nullptr);
+        stage_kernel<4>(lanes)<<<ntx * nty, PPB * lanes, sm, s>>>(P, F, F, L, L, gstart, glist, W, S, sc, ntx, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(LSSPH_E_CUDA, std::string("lssph_rhs_noalloc: launch: ") + cudaGetErrorString(e));
     Scalars hs{};

@@ -1206,6 +1206,38 @@ int orc_set_threads(int n) {
 
 int orc_init_param(lssph_params* p) { init_param(p); return 0; }
 
+size_t orc_params_sizeof(void) { return sizeof(lssph_params); }
+
+// The reference's shipped config.h (config.h:24-200: TARGET_PROBLEM 2 ... WALL_MODEL 2),
+// then init_param, so that the oracle builds its parameters without the engine library.
+// precision / lanes / seed / periodic are engine-side extensions and start at zero.
+int orc_params_default(lssph_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->target_problem = 2;                                            // config.h:24
+    p->u_bc_top = 1; p->u_bc_bottom = 1; p->u_bc_left = 1; p->u_bc_right = 1;   // :35-38
+    p->u_top = 1.0;                                                   // :42
+    p->tem_bc_top = 1; p->tem_bc_bottom = 1; p->tem_bc_left = 2; p->tem_bc_right = 2;  // :52-55
+    p->tem_top = 0.0; p->tem_bottom = 1.0e-2; p->tem_left = 0.0; p->tem_right = 0.0;  // :59-62
+    std::snprintf(p->save_name, sizeof(p->save_name), "%s", "tg_compare_100_write");  // :69
+    std::snprintf(p->read_name, sizeof(p->read_name), "%s", "new");                   // :72
+    p->omp_threads = 8;                                               // :79
+    p->len_x = 1.0; p->len_y = 1.0;                                   // :86-87
+    p->num_x = 100; p->num_y = 100;                                   // :91-92
+    p->rk = 4;                                                        // :99
+    p->start_step = 1; p->end_step = 10000; p->write_step = 100;      // :103-109
+    p->threshold = 1.0e-10;                                           // :112
+    p->coe_CFL = 0.5; p->coe_dif = 0.2;                               // :117-118
+    p->zeta_RSST = 1.0; p->xi_VIM = 1.0;                              // :123-124
+    p->rho_ref = 1.0; p->vis_ref = 1.0e-2; p->K_ref = 1.0e2;          // :131-137
+    p->k_th_ref = 1.0e-2; p->cp_ref = 1.0e3; p->alpha_ref = 7.1e-3;   // :140-146
+    p->gravity = 10.0; p->pos_pert = 0.0;                             // :152-155
+    p->tg_a = 1; p->tg_b = 1;                                         // :158-159
+    p->coe_h = 1.2; p->PST_c = 1.5; p->coe_delta_sph = 0.0;           // :166-175
+    p->kernel_type = 3; p->sph_model = 3; p->wall_model = 2;          // :188-213
+    init_param(p);
+    return 0;
+}
+
 double orc_kernel_W(int kt, double r, double h) { return cal_W(kt, r, h); }
 double orc_kernel_dW(int kt, double r, double h) { return cal_dW(kt, r, h); }
 

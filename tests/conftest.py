@@ -39,8 +39,9 @@ def golden_dir():
 
 @pytest.fixture(scope="session")
 def reference_root():
-    """The reference checkout, only present where the fixtures are generated."""
-    path = os.environ.get("LSSPH_REFERENCE_ROOT", "/root/reference")
-    if not os.path.isdir(os.path.join(path, "analysis")):
+    """The reference checkout named by $LSSPH_REFERENCE_ROOT, only present where the
+    fixtures are generated; tests that need it are skipped elsewhere."""
+    path = os.environ.get("LSSPH_REFERENCE_ROOT", "")
+    if not path or not os.path.isdir(os.path.join(path, "analysis")):
         pytest.skip("reference checkout not available on this machine")
     return path

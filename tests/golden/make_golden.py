@@ -1,8 +1,9 @@
 """Generate the golden vectors of tests/golden/ from the reference's own Python code.
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
+    LSSPH_REFERENCE_ROOT=... python tests/golden/make_golden.py
 
-Needs the LS-SPH-Benchmarks checkout (default /root/reference) for
+Needs the LS-SPH-Benchmarks checkout (the argument, else $LSSPH_REFERENCE_ROOT) for
 analysis/common/kernel_functions.py and analysis/common/lssph_b.py, plus numpy/scipy.
 The fixtures it writes are committed; the tests read only the .npz files.
 
@@ -87,4 +88,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LSSPH_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set LSSPH_REFERENCE_ROOT)")
+    main(root)

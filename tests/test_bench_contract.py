@@ -44,6 +44,37 @@ def test_reference_arm_prints_one_contract_line():
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
+def test_reference_arm_never_loads_the_engine_library():
+    # the reference arm builds its parameters with the oracle alone: no lssph module and no
+    # liblssph.so mapping in its process
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '3']\n"
+            "try:\n    runpy.run_path('bench.py', run_name='__main__')\nexcept SystemExit:\n    pass\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('ENGINE_SO', 'liblssph.so' in maps, 'ORACLE_SO', 'liblssph_oracle.so' in maps,"
+            " 'LSSPH_MODULE', any(m == 'lssph' or m.startswith('lssph.') for m in sys.modules))\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "ENGINE_SO False ORACLE_SO True LSSPH_MODULE False" in r.stdout, r.stdout[-2000:]
+
+
+def test_both_arms_report_the_same_config():
+    # the oracle's parameter builder gives the engine's bytes, and both lines carry one dict
+    sys.path.insert(0, ROOT)
+    import bench
+    import lssph
+    import oracle as O
+    pe, po = bench._params(), bench._oracle_params()
+    assert bytes(pe) == bytes(O.as_params(pe)) and bytes(po) == bytes(O.as_params(pe))
+    for kw in ({}, {"PERIODIC": 0}, {"num": 64, "re": 400.0}):
+        a = lssph.taylor_green_params(**{**bench.HEADLINE, **{k: v for k, v in kw.items() if k != "PERIODIC"}},
+                                      PERIODIC=kw.get("PERIODIC", 1))
+        b = O.taylor_green_params(**{**bench.HEADLINE, **{k: v for k, v in kw.items() if k != "PERIODIC"}},
+                                  PERIODIC=kw.get("PERIODIC", 1))
+        assert bytes(a) == bytes(b), kw
+    assert bytes(lssph.default_params()) == bytes(O.params_default())
+    assert bench._config(pe, 16384, 16384) == bench._config(po, 16384, 16384)
+
+
 def test_reference_arm_under_torchrun_prints_once():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),

@@ -204,3 +204,38 @@ def test_device_footprint_estimate_is_host_only_and_grows_with_size():
     p = lssph.taylor_green_params(num=128)
     nt, ni = lssph.setup_particles(p)[0].num_total, 128 * 128
     assert 200 * nt < sizes[2] < 2000 * nt
+
+
+def test_noalloc_rejects_unsupported_options_before_any_gpu_work():
+    # lssph_rhs_noalloc checks its options on the host: a periodic domain (its cell grid
+    # has no wrap) and lane counts other than 0, 1, 2, 4 return LSSPH_E_UNSUPPORTED with
+    # their own messages, before any CUDA call (so this runs without a GPU)
+    import ctypes as C
+
+    from lssph import _abi
+    lib = lssph.load()
+    fake = C.c_void_p(256)   # never dereferenced
+    args = lambda n: (n, 1024, *([fake] * 6), None, *([fake] * 3), None, None)   # noqa: E731
+    p = lssph.taylor_green_params(num=32, PERIODIC=1)
+    assert lib.lssph_rhs_noalloc(C.byref(p), *args(1024)) == _abi.E_UNSUPPORTED
+    assert b"closed box only" in lib.lssph_last_error()
+    p = lssph.taylor_green_params(num=32, lanes=8)
+    assert lib.lssph_rhs_noalloc(C.byref(p), *args(1444)) == _abi.E_UNSUPPORTED
+    assert b"lanes must be" in lib.lssph_last_error()
+    p = lssph.taylor_green_params(num=32)
+    assert lib.lssph_rhs_noalloc(C.byref(p), *args(262145)) == _abi.E_CAPACITY
+
+
+def test_mapped_downloads_need_device_write_access(tmp_path):
+    # the predicate that keeps k_download_mapped away from page-locked buffers the device may
+    # only read (cudaHostRegisterReadOnly): only read-write access flags allow the in-place
+    # kernel; read-only, none and "driver could not say" (-1) go through copies
+    import subprocess
+    hdr = os.path.join(os.path.dirname(lssph.__file__), "..", "csrc", "hostmem.h")
+    src = tmp_path / "t.cpp"
+    src.write_text('#include "%s"\n#include <cstdio>\nint main() { const long long fl[] = {-1, 0, 1, 2, 3}; for (long long f : fl)'
+                   ' std::printf("%%lld:%%d ", f, (int)lssph::mapped_store_allowed(f)); }\n' % hdr)
+    exe = tmp_path / "t"
+    subprocess.run(["g++", "-std=c++17", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["-1:0", "0:0", "1:0", "2:0", "3:1"]
