@@ -260,3 +260,26 @@ def test_ls_type_b_interpolates_linear_fields_exactly():
     np.testing.assert_allclose(vm["u"], 0.3 + 1.7 * vm["x"] - 0.4 * vm["y"], rtol=0, atol=1e-11)
     np.testing.assert_allclose(vm["v"], -0.2 + 0.5 * vm["x"] + 2.1 * vm["y"], rtol=0, atol=1e-11)
     np.testing.assert_allclose(vm["pre"], 1.0 - 3.0 * vm["x"] + 0.25 * vm["y"], rtol=0, atol=1e-11)
+
+
+def test_oracle_amplifies_one_ulp_in_the_positions():
+    # the sensitivity horizon of the reference algorithm itself: periodic Taylor-Green
+    # Re = 100, 64^2, RK4 + PST; one ulp added to every position stays at the rounding level
+    # for 200 steps and has grown to the percent level of the velocity by 1000.  So two
+    # correct FP64 runs that differ only in rounding (summation order, compiler, FMA
+    # placement) agree field by field only before that horizon.
+    p = lssph.taylor_green_params(num=64, re=100.0, coe_cfl=0.1, tg=2, lanes=1, PERIODIC=1)
+    st, ni = lssph.setup_particles(p)
+    st2 = st.copy()
+    st2.x[:] = np.nextafter(st2.x, 2.0)
+    a, b = O.Oracle(p, st, ni, ghost=False), O.Oracle(p, st2, ni, ghost=False)
+    rel = {}
+    done = 0
+    for n in (200, 1000):
+        a.run(n - done)
+        b.run(n - done)
+        done = n
+        ua, ub = a.get()["u"], b.get()["u"]
+        rel[n] = np.linalg.norm(ub - ua) / np.linalg.norm(ua)
+    assert 0 < rel[200] < 1e-12, rel
+    assert rel[1000] > 1e-4, rel
