@@ -626,13 +626,98 @@ def serving_requests(seed: int = 5, rate: float = 20.0, window_s: float = 8.0, m
     return reqs, scale
 
 
-def bench_serving() -> dict:
+def _serving_request(rng, rid, t, sides, t_end):
+    """One request of the configuration-5 mix: 50% bottom-heated Boussinesq (Ra
+    log-uniform [1e4, 1e6], Pr 0.71, seeded T perturbation 1e-3), 50% lid-driven cavity (Re
+    log-uniform [100, 3200]); side drawn from `sides`; mixed precision; run to t_end."""
+    import numpy as np
+
+    import lssph
+    from lssph import Request
+    side = int(rng.choice(sides))
+    if rng.random() < 0.5:
+        ra = float(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
+        p = lssph.make_params(lssph.boussinesq_params(num=side, ra=ra, pr=0.71), precision=lssph.PRECISION_MIXED)
+        init, tag = _perturbed_temperature(p, int(rng.integers(1 << 30))), "boussinesq"
+    else:
+        re = float(np.exp(rng.uniform(np.log(100.0), np.log(3200.0))))
+        p = lssph.make_params(lssph.cavity_params(num=side, re=re), precision=lssph.PRECISION_MIXED)
+        init, tag = None, "cavity"
+    return Request(rid=rid, params=p, nsteps=max(1, int(round(t_end / p.dt))), arrival=t, tag=tag, init=init)
+
+
+CAPACITY_SIDES = (32, 48, 64)
+
+
+def serving_capacity(sides=CAPACITY_SIDES, steps: int = 300, seed: int = 6) -> dict:
+    """Measured capacity of the batched engine on the unscaled request mix (t_end = 20)
+    restricted to `sides`: 24 requests of the mix stepped together for `steps` steps give
+    the sustained particle-steps/s; divided by the mean work of a request (interior
+    particles x steps to t = 20, averaged over the mix) it gives requests/s."""
+    import numpy as np
+
+    import lssph
+    rng = np.random.default_rng(seed)
+    reqs = [_serving_request(rng, k, 0.0, sides, 20.0) for k in range(24)]
+    sims = []
+    with lssph.Batch() as b:
+        for r in reqs:
+            if r.init is not None:
+                sim = lssph.Simulation(r.params, r.init(), lssph.setup_particles(r.params)[1])
+                sim.ghost()
+            else:
+                sim = lssph.Simulation.new(r.params)
+            sims.append(sim)
+            b.add(sim)
+        b.step(20)
+        b.step(steps)
+        ms, _ = b.last_step_stats()
+    ps = sum(s.num_int for s in sims) * steps / (ms * 1e-3)
+    for s in sims:
+        s.close()
+    work = []
+    for k in range(400):
+        r = _serving_request(rng, k, 0.0, sides, 20.0)
+        work.append(lssph.setup_particles(r.params)[1] * r.nsteps)
+    return {"particle_steps_per_s": ps, "mean_request_particle_steps": float(np.mean(work)),
+            "requests_per_s": ps / float(np.mean(work))}
+
+
+def bench_serving(capacity_window_s: float = 120.0) -> dict:
+    """The configuration-5 stream twice: (1) scaled -- arrivals at 20/s for 8 s over sides
+    64..384 with t_end scaled so the median request runs 60 steps; (2) real physics --
+    unscaled t_end = 20 over sides 32..64, arrivals at 90 % of the measured capacity for
+    `capacity_window_s` seconds, run until every request has finished."""
+    import numpy as np
+
     from lssph import Server
     reqs, scale = serving_requests()
     srv = Server(max_active=64, chunk_steps=20, keep_results=False)
     st = srv.run(reqs)
     srv.close()
-    return {"scaled": _serving_record(st, reqs, scale)}
+    out = {"scaled": _serving_record(st, reqs, scale)}
+    if capacity_window_s > 0:
+        cap = serving_capacity()
+        rate = 0.9 * cap["requests_per_s"]
+        rng = np.random.default_rng(7)
+        t, creqs = 0.0, []
+        while True:
+            t += float(rng.exponential(1.0 / rate))
+            if t > capacity_window_s:
+                break
+            creqs.append(_serving_request(rng, len(creqs), t, CAPACITY_SIDES, 20.0))
+        srv = Server(max_active=64, chunk_steps=100, keep_results=False)
+        st = srv.run(creqs)
+        srv.close()
+        rec = _serving_record(st, creqs, 1.0)
+        rec["workload"] = (f"Poisson {rate:.2f}/s (90 % of the measured capacity) for {capacity_window_s:.0f} s; "
+                           "50% Boussinesq Ra [1e4,1e6], 50% cavity Re [100,3200]; sides 32, 48, 64; "
+                           "unscaled t_end = 20; mixed precision")
+        rec["capacity"] = cap
+        rec["arrival_rate_per_s"] = rate
+        rec["steps_per_request_median"] = float(np.median([r.nsteps for r in creqs]))
+        out["capacity"] = rec
+    return out
 
 
 def _serving_record(st, reqs, scale) -> dict:
@@ -767,7 +852,7 @@ def run_engine(args) -> int:
         extras["snapshots"] = bench_snapshots()
         configs["mixed"] = bench_mixed()
         configs["batched"] = bench_batched()
-        configs["serving"] = bench_serving()
+        configs["serving"] = bench_serving(args.serving_seconds)
 
     if dist:
         dist.barrier()
@@ -827,8 +912,16 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-precision, batched and serving configurations")
+    ap.add_argument("--serving-seconds", type=float, default=120.0,
+                    help="arrival window of the real-physics serving stream (0 skips it)")
+    ap.add_argument("--validate", action="store_true",
+                    help="only the validation runs of lssph.validation (minutes), as one JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.validate:
+        from lssph import validation
+        print(json.dumps({"validation": validation.run()}), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_engine(args)

@@ -931,6 +931,42 @@ __device__ __forceinline__ void group_reduce_to(const R (&v)[N], double (&out)[N
     group_reduce<G>(out);
 }
 
+// ---- compensated FP32 sums of the mixed-precision pair phase ------------------------------
+// Kahan summation (Kahan 1965; Higham, Accuracy and Stability of Numerical Algorithms,
+// section 4.3): each FP32 sum s carries c, minus the low-order part the last additions
+// dropped, so s - c is the sum to about FP32 eps^2 relative to the summands instead of
+// n eps.  The file is compiled with -fmad=false and nvcc does not reassociate, so the
+// correction terms are evaluated as written.
+__device__ __forceinline__ void kahan_add(float& s, float& c, float t) {
+    const float y = t - c;
+    const float u = s + y;
+    c = (u - s) - y;
+    s = u;
+}
+
+// accumulate_A with compensated sums (moment matrix and b vectors).
+template <int NB, int Q>
+__device__ __forceinline__ void accumulate_A_kahan(float (&Mu)[Q * (Q + 1) / 2], float (&Mc)[Q * (Q + 1) / 2],
+                                                   float (&B)[NB][Q], float (&Bc)[NB][Q], float VW,
+                                                   const float (&a)[Q], const float (&df)[NB]) {
+#pragma unroll
+    for (int ii = 0; ii < Q; ++ii) {
+        const float VWa = VW * a[ii];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) kahan_add(B[c][ii], Bc[c][ii], VWa * df[c]);
+#pragma unroll
+        for (int jj = 0; jj <= ii; ++jj) kahan_add(Mu[UT(jj, ii)], Mc[UT(jj, ii)], VWa * a[jj]);
+    }
+}
+
+// Widen compensated lane sums (s - c, formed in FP64) and combine the G lanes in FP64.
+template <int G, int N>
+__device__ __forceinline__ void group_reduce_kahan(const float (&v)[N], const float (&c)[N], double (&out)[N]) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) out[k] = (double)v[k] - (double)c[k];
+    group_reduce<G>(out);
+}
+
 // =======================================================================================
 // k_stage: LS-SPH type-A RHS (q = 5, SPH_MODEL 3) + RK stage update + cell scatter.
 // NB = number of b-vector columns: 1 (problem 1: u only), 4 (u,v,rho,p), 5 (+T).
@@ -1372,14 +1408,14 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
             float my_v = 0.f, my_rho = 0.f, my_pre = 0.f, my_tem = 0.f;
             if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
             if constexpr (NB == 5) my_tem = SM.tem[ki];
-            float Mu[15];
-            float B[NB][Q];
+            float Mu[15], Mc[15];
+            float B[NB][Q], Bc[NB][Q];
 #pragma unroll
-            for (int k = 0; k < 15; ++k) Mu[k] = 0.f;
+            for (int k = 0; k < 15; ++k) { Mu[k] = 0.f; Mc[k] = 0.f; }
 #pragma unroll
             for (int c = 0; c < NB; ++c)
 #pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = 0.f;
+                for (int k = 0; k < Q; ++k) { B[c][k] = 0.f; Bc[c][k] = 0.f; }
             const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2,
                                              [&](int k, float xji, float yji) {
                 const float r = sqrtf(xji * xji + yji * yji);
@@ -1395,12 +1431,12 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
                     df[3] = SM.pre[k] - my_pre;
                 }
                 if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
-                accumulate_A<NB, float>(Mu, B, VW, a, df);
+                accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
             });
             double Md[15], Bd[NB][Q];
-            group_reduce_to<G>(Mu, Md);
+            group_reduce_kahan<G>(Mu, Mc, Md);
 #pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+            for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
@@ -2024,15 +2060,15 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
             const float my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
             float my_tem = 0.f;
             if constexpr (NB == 4) my_tem = SM.tem[ki];
-            float Mu[15];
-            float B[NB][Q];
+            float Mu[15], Mc[15];
+            float B[NB][Q], Bc[NB][Q];
 #pragma unroll
-            for (int k = 0; k < 15; ++k) Mu[k] = 0.f;
+            for (int k = 0; k < 15; ++k) { Mu[k] = 0.f; Mc[k] = 0.f; }
 #pragma unroll
             for (int c = 0; c < NB; ++c)
 #pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = 0.f;
-            float sxy[2] = {0.f, 0.f};
+                for (int k = 0; k < Q; ++k) { B[c][k] = 0.f; Bc[c][k] = 0.f; }
+            float sxy[2] = {0.f, 0.f}, sxc[2] = {0.f, 0.f};
             const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2,
                                              [&](int k, float xji, float yji) {
                 const float r = sqrtf(xji * xji + yji * yji);
@@ -2045,8 +2081,8 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
                 const float gy = ((dWdr * (-yji)) * rinv) * Vj;
                 const float t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
                 const float fac = 1.f + 0.2f * t4;
-                sxy[0] = fmaf(fac, gx, sxy[0]);
-                sxy[1] = fmaf(fac, gy, sxy[1]);
+                kahan_add(sxy[0], sxc[0], fac * gx);
+                kahan_add(sxy[1], sxc[1], fac * gy);
                 float a[Q];
                 basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
                 float df[NB];
@@ -2054,13 +2090,13 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
                 df[1] = SM.v[k] - my_v;
                 df[2] = SM.rho[k] - my_rho;
                 if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
-                accumulate_A<NB, float>(Mu, B, VW, a, df);
+                accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
             });
             double Md[15], Bd[NB][Q], sd[2];
-            group_reduce_to<G>(Mu, Md);
+            group_reduce_kahan<G>(Mu, Mc, Md);
 #pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
-            group_reduce_to<G>(sxy, sd);
+            for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
+            group_reduce_kahan<G>(sxy, sxc, sd);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
