@@ -89,6 +89,7 @@ void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t 
     for (int b = 0; b < 2; ++b) {
         Fld& F = h->F[b];
         A(&F.x, N); A(&F.y, N); A(&F.u, N); A(&F.v, N); A(&F.rho, N); A(&F.pre, N); A(&F.tem, N); A(&F.vol, N);
+        A(&F.ox, N); A(&F.oy, N);
     }
     for (int b = 0; b < kLists; ++b) {
         Lst& L = h->L[b];
@@ -589,12 +590,20 @@ int sync_check(lssph_handle* h) {
     return check_scalars(h, nullptr);
 }
 
+// Mixed precision: the split-precision positions of the current state, both buffers.
+void write_split_pos(lssph_handle* h) {
+    if (!h->P.split_pos) return;
+    k_split_pos<<<blocks_for(std::max(h->num_int, h->grid.ncell), 128), 128, 0, h->stream>>>(
+        h->P, h->F[h->sb], h->F[h->sb ^ 1], h->W.key, h->gstart, h->glist);
+}
+
 // Build the cell list of the current positions into list buffer lb (fresh).
 int rebuild_cells(lssph_handle* h) {
     static_assert(kLists == 3, "k_clear_counts zeroes three lists");
     k_clear_counts<<<blocks_for(h->grid.ncell, 256), 256, 0, h->stream>>>(h->L[0].cnt, h->L[1].cnt, h->L[2].cnt,
                                                                           h->grid.ncell);
     k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[h->lb], h->gstart, h->W.key, h->sc);
+    write_split_pos(h);
     return LSSPH_OK;
 }
 
@@ -793,6 +802,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     P.ih2B = P.ih1 * P.ih1;        // inv_h2 = inv_h*inv_h  (interpolate_LSSPH_B_mod.f90:151-152)
     P.h_eff_sq = p.h_eff * p.h_eff;
     P.inv_h_eff = p.periodic ? h->grid.inv_cw : 1.0 / p.h_eff;   // cell keys
+    P.cw = p.periodic ? p.len_x / (double)h->grid.nx : p.h_eff;    // cell origins
+    P.split_pos = h->mixed ? 1 : 0;
     P.SP_mass = p.SP_mass;
     P.W_ave = p.W_ave;
     P.wnorm = kernel_norm(p.kernel_type, p.h);
@@ -1001,6 +1012,7 @@ int lssph_update_cell(lssph_handle* h) {
     CUDA_TRY(h, cudaMemsetAsync(h->L[next_list(h->lb)].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
     k_scatter<<<blocks_for(h->num_int, 128), 128, 0, h->stream>>>(h->P, h->F[h->sb], h->L[next_list(h->lb)], h->gstart,
                                                                      h->W.key, h->sc);
+    write_split_pos(h);
     h->lb = next_list(h->lb);
     CUDA_TRY(h, cudaMemsetAsync(h->L[prev_list(h->lb)].cnt, 0, sizeof(int) * h->grid.ncell, h->stream));
     return sync_check(h);

@@ -65,7 +65,8 @@ struct Phys {
     int tem_bc_top, tem_bc_bottom, tem_bc_left, tem_bc_right;
     int nx, ny, ncell, cap;
     int num_total, num_int, num_ext, sph_model;
-    int periodic, pad_;   // periodic: square domain (0, Lx]^2, cells wrap, no ghosts
+    int periodic;         // periodic: square domain (0, Lx]^2, cells wrap, no ghosts
+    int split_pos;        // mixed precision: every position write also writes Fld::ox, oy
     double u_top, tem_top, tem_bottom, tem_left, tem_right;
     double h, ih1, ih2A, ih2B, h_eff_sq, inv_h_eff, SP_mass, W_ave, wnorm, dt;
     double c_sq, rho_ref, vis_ref, delta, zeta_sq, xi_sq, alpha_ref, gravity, tem_ave;
@@ -73,6 +74,7 @@ struct Phys {
     // reciprocals of loop-invariant divisors (1/W_ave, 1/zeta^2, 1/xi^2, -3/h, -5/h)
     double iWave, izeta2, ixi2, m3h, m5h;
     double Lx;   // periodic domain side
+    double cw;   // cell width: the origin of cell (cx, cy) is (cx * cw, cy * cw)
 };
 
 // Periodic position wrap into (0, L] (the oracle's wrap_pos).
@@ -80,7 +82,17 @@ __device__ __forceinline__ double wrap_pos(double x, double L) { return x <= 0.0
 
 struct Fld {   // SoA particle state over num_total
     double *x, *y, *u, *v, *rho, *pre, *tem, *vol;
+    // Split-precision positions (mixed precision): the FP32 offset of each particle from the
+    // FP64 origin of the cell that holds it, kept beside the FP64 positions of the RK update.
+    float *ox, *oy;
 };
+
+// Split-precision position of particle i, held by cell `key`.
+__device__ __forceinline__ void put_split_pos(const Phys& P, const Fld& F, int i, double x, double y, int key) {
+    const int cx = key % P.nx, cy = key / P.nx;
+    F.ox[i] = (float)(x - (double)cx * P.cw);
+    F.oy[i] = (float)(y - (double)cy * P.cw);
+}
 // Cell lists rotate through three buffers: a stage reads list l and scatters into list
 // l + 1 while the ghost launch after it clears list l - 1, so a list is cleared well
 // before the next scatter into it and no clearing sits between two launches that read
@@ -722,18 +734,15 @@ __device__ __forceinline__ TileRef stage_fields_mx(const Phys& P, const Fld& F, 
         R.u = __ldg(F.u + j0); R.v = __ldg(F.v + j0); R.rho = __ldg(F.rho + j0); R.pre = __ldg(F.pre + j0);
         if (WITH_TEM) R.tem = __ldg(F.tem + j0);
     }
-    const double cw = P.periodic ? 1.0 / P.inv_h_eff : sqrt(P.h_eff_sq);   // cell width
-    const double x0 = (double)cx0 * cw, y0 = (double)cy0 * cw;
+    // positions from the split-precision copy in HBM: a particle of halo cell (hx, hy) sits at
+    // (hx, hy) * cw + (ox, oy) from the tile's halo corner, which also holds for a wrapped
+    // periodic neighbour (its cell origin moved by -+Lx = -+nx cw)
+    const float cwf = (float)P.cw;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int j = S.idx[k];
-        double xj = __ldg(F.x + j), yj = __ldg(F.y + j);
-        if (P.periodic) {   // wrapped halo cells: positions shifted by -+Lx
-            const int h = halo_cell_of(T, k);
-            xj = xj + T.sx[h];
-            yj = yj + T.sy[h];
-        }
-        S.ox[k] = (float)(xj - x0);
-        S.oy[k] = (float)(yj - y0);
+        const int h = halo_cell_of(T, k);
+        S.ox[k] = __ldg(F.ox + j) + (float)(h % HX) * cwf;
+        S.oy[k] = __ldg(F.oy + j) + (float)(h / HX) * cwf;
         S.u[k] = (float)(__ldg(F.u + j) - R.u);
         S.v[k] = (float)(__ldg(F.v + j) - R.v);
         S.rho[k] = (float)(__ldg(F.rho + j) - R.rho);
@@ -1073,7 +1082,10 @@ __device__ __forceinline__ int stage_position(const Phys& P, const Fld& nxt, con
     int nk = -1;
     if (S.do_scatter) {
         nk = cell_key_mul(P, xn, yn, sc);
-        if (nk >= 0) W.key[i] = nk;
+        if (nk >= 0) {
+            W.key[i] = nk;
+            if (P.split_pos) put_split_pos(P, nxt, i, xn, yn, nk);
+        }
     }
     return nk;
 }
@@ -1860,7 +1872,10 @@ __device__ __forceinline__ void pst_move(const Phys& P, const Fld& nxt, const Ls
     nxt.y[i] = yn;
     if (!(isfinite(xn) && isfinite(yn))) atomicOr(&sc->err, ERR_NONFINITE);
     const int nk = cell_key_mul(P, xn, yn, sc);
-    if (nk >= 0) W.key[i] = nk;
+    if (nk >= 0) {
+        W.key[i] = nk;
+        if (P.split_pos) put_split_pos(P, nxt, i, xn, yn, nk);
+    }
     scatter_to_cell(P, Ln, gstart, nk, i, sc);
 }
 
@@ -2147,7 +2162,10 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
             if constexpr (NB == 4) { const double tn = my_tem + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
             if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
             const int nk = cell_key_mul(P, xn, yn, sc);
-            if (nk >= 0) W.key[i] = nk;
+            if (nk >= 0) {
+                W.key[i] = nk;
+                if (P.split_pos) put_split_pos(P, nxt, i, xn, yn, nk);
+            }
             scatter_to_cell(P, Ln, gstart, nk, i, sc);
         }
         __syncthreads();
@@ -2329,6 +2347,26 @@ static __global__ void kb_epilogue(const SolveDesc* __restrict__ D, int nsolve) 
 static __global__ void kb_gather_scalars(const SolveDesc* __restrict__ D, int nsolve, Scalars* out) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < nsolve) out[s] = *D[s].sc;
+}
+
+// Split-precision positions of every particle in both state buffers from the positions of
+// A: interior particles by their cell keys, ghosts by the static cell that lists them.
+static __global__ void k_split_pos(const Phys P, const Fld A, const Fld B, const int* __restrict__ key,
+                                   const int* __restrict__ gstart, const int* __restrict__ glist) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < P.num_int) {
+        const int k = key[t];
+        if (k >= 0 && k < P.ncell) {
+            put_split_pos(P, A, t, A.x[t], A.y[t], k);
+            put_split_pos(P, B, t, A.x[t], A.y[t], k);
+        }
+    }
+    if (t < P.ncell)
+        for (int g = gstart[t]; g < gstart[t + 1]; ++g) {
+            const int j = glist[g];
+            put_split_pos(P, A, j, A.x[j], A.y[j], t);
+            put_split_pos(P, B, j, A.x[j], A.y[j], t);
+        }
 }
 
 static __global__ void k_volume(const Phys P, const Fld F) {
