@@ -46,6 +46,7 @@ extern "C" {
 /* ---- engine options (no counterpart in the reference) ----------------------------- */
 #define LSSPH_PRECISION_FP64   0     /* plain FP64 path (reference arithmetic) */
 #define LSSPH_PRECISION_MIXED  1     /* FP32 pair sums, FP64 solve + refinement */
+#define LSSPH_PRECISION_MIXED_COMPENSATED 2  /* as MIXED, with Kahan-compensated FP32 pair sums */
 
 /*
  * lssph_params -- mirrors Param_type (source/core/global_types.f90:22-73) plus the

@@ -37,7 +37,7 @@ constexpr int kPeriod = 2 * kLists;   // step period of (state parity, list inde
 
 struct BatchGroup {
     int nb = 4, nbg = 3, wq = 3, rk = 4, G = 4;
-    bool p1 = false, pst_on = true, mixed = false;
+    bool p1 = false, pst_on = true, mixed = false, comp = false;
     bool pdl = true;               // programmatic dependent launches between the group's kernels
     const int* tstep = nullptr;    // the batch's device step counter
     int sbf = 1;                   // state-buffer flip per step (0/1)
@@ -118,17 +118,20 @@ void optin(K kernel) {
 // Precision x lanes: the mixed-precision kernels exist for 2 and 4 lanes.
 template <class F>
 void dispatch_kind(const BatchGroup& g, F&& f) {
-    if (g.mixed) {
-        if (g.G == 2) f(std::integral_constant<int, 2>{}, std::true_type{});
-        else f(std::integral_constant<int, 4>{}, std::true_type{});
+    if (g.mixed && g.comp) {
+        if (g.G == 2) f(std::integral_constant<int, 2>{}, std::integral_constant<int, 2>{});
+        else f(std::integral_constant<int, 4>{}, std::integral_constant<int, 2>{});
+    } else if (g.mixed) {
+        if (g.G == 2) f(std::integral_constant<int, 2>{}, std::integral_constant<int, 1>{});
+        else f(std::integral_constant<int, 4>{}, std::integral_constant<int, 1>{});
     }
-    else dispatch_lanes(g.G, [&](auto GG) { f(GG, std::false_type{}); });
+    else dispatch_lanes(g.G, [&](auto GG) { f(GG, std::integral_constant<int, 0>{}); });
 }
 
 void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
     dispatch_kind(g, [&](auto GG, auto MXc) {
         constexpr int G = decltype(GG)::value;
-        constexpr bool MX = decltype(MXc)::value;
+        constexpr int MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
             launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles, g.tstep, g.sbf, g.lba}, S,
@@ -165,7 +168,7 @@ void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset
 void launch_pst(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
     dispatch_kind(g, [&](auto GG, auto MXc) {
         constexpr int G = decltype(GG)::value;
-        constexpr bool MX = decltype(MXc)::value;
+        constexpr int MX = decltype(MXc)::value;
         auto run = [&](auto loose, auto tight) {
             if (prep) { optin(loose); optin(tight); return; }
             launch_kernel(g.pdl, g.tight ? tight : loose, g.ntiles, PPB * G, g.smem, g.stream, g.D, BatchMap{g.tiles, g.tstep, g.sbf, g.lba}, ps,
@@ -279,7 +282,7 @@ int rebuild(lssph_batch* b) {
     std::map<std::tuple<int, int, int, int, int>, int> index;
     for (size_t i = 0; i < n; ++i) {
         const lssph_handle* h = b->members[i];
-        const auto key = std::make_tuple(h->nb_rhs, h->wq, h->p.rk, h->G, h->mixed ? 1 : 0);
+        const auto key = std::make_tuple(h->nb_rhs, h->wq, h->p.rk, h->G, h->mixed ? (h->comp ? 2 : 1) : 0);
         auto it = index.find(key);
         if (it == index.end()) {
             BatchGroup g;
@@ -289,6 +292,7 @@ int rebuild(lssph_batch* b) {
             g.rk = h->p.rk;
             g.G = h->G;
             g.mixed = h->mixed;
+            g.comp = h->comp;
             g.pdl = pdl_enabled();
             g.p1 = h->p1;
             g.pst_on = h->pst_on;

@@ -193,7 +193,8 @@ Where all_tiles(const lssph_handle* h) { return Where{nullptr, h->ntiles, h->str
 
 // ---- kernel dispatch on lanes, register budget and precision ------------------------------
 // The mixed-precision kernels exist for 2 and 4 lanes per particle.
-template <int NB, int GG, bool MX>
+// MX: 0 FP64, 1 mixed precision, 2 mixed precision with compensated pair sums.
+template <int NB, int GG, int MX>
 void run_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     if (h->classical) {   // SPH_MODEL 1 / 2 (FP64 only)
         if constexpr (!MX) {
@@ -213,13 +214,11 @@ void run_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     if (h->preparing) {
         smem_optin(k_stage<NB, GG, 0, MX>);
         smem_optin(k_stage<NB, GG, 1, MX>);
-        if constexpr (!MX) smem_optin(k_stage<NB, GG, 2, MX>);
+        smem_optin(k_stage<NB, GG, 2, MX>);
         return;
     }
     auto kern = h->tight ? k_stage<NB, GG, 1, MX> : k_stage<NB, GG, 0, MX>;
-    if constexpr (!MX) {
-        if (h->budget == 2) kern = k_stage<NB, GG, 2, MX>;
-    }
+    if (h->budget == 2) kern = k_stage<NB, GG, 2, MX>;
     launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P, h->F[h->sb],
                     h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, S, h->sc, h->ntx,
                     w.tiles);
@@ -231,15 +230,20 @@ void launch_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_STAGE);
     if (h->order >= 3) { launch_stage_hi(h, S, w.tiles, w.count, w.stream, w.pdl, w.priority); return; }
     if (h->mixed) {
-        if (h->G == 2) run_stage<NB, 2, true>(h, S, w);
-        else run_stage<NB, 4, true>(h, S, w);
+        if (h->comp) {
+            if (h->G == 2) run_stage<NB, 2, 2>(h, S, w);
+            else run_stage<NB, 4, 2>(h, S, w);
+        } else {
+            if (h->G == 2) run_stage<NB, 2, 1>(h, S, w);
+            else run_stage<NB, 4, 1>(h, S, w);
+        }
         return;
     }
     switch (h->G) {
-        case 1: run_stage<NB, 1, false>(h, S, w); break;
-        case 2: run_stage<NB, 2, false>(h, S, w); break;
-        case 8: run_stage<NB, 8, false>(h, S, w); break;
-        default: run_stage<NB, 4, false>(h, S, w); break;
+        case 1: run_stage<NB, 1, 0>(h, S, w); break;
+        case 2: run_stage<NB, 2, 0>(h, S, w); break;
+        case 8: run_stage<NB, 8, 0>(h, S, w); break;
+        default: run_stage<NB, 4, 0>(h, S, w); break;
     }
 }
 
@@ -302,7 +306,7 @@ void launch_ghost(lssph_handle* h, int zero_list = -1, int reset_umax = 0) {
     launch_ghost_on(h, zero_list, reset_umax, h->stream, h->pdl);
 }
 
-template <int NB, int GG, bool MX>
+template <int NB, int GG, int MX>
 void run_pst(lssph_handle* h, const Where& w) {
     if (h->classical) {   // first-order basis, q = 2 (shift_interpolate_mod.f90:43-44)
         if constexpr (!MX) {
@@ -322,13 +326,11 @@ void run_pst(lssph_handle* h, const Where& w) {
     if (h->preparing) {
         smem_optin(k_pst<NB, GG, 0, MX>);
         smem_optin(k_pst<NB, GG, 1, MX>);
-        if constexpr (!MX) smem_optin(k_pst<NB, GG, 2, MX>);
+        smem_optin(k_pst<NB, GG, 2, MX>);
         return;
     }
     auto kern = h->tight ? k_pst<NB, GG, 1, MX> : k_pst<NB, GG, 0, MX>;
-    if constexpr (!MX) {
-        if (h->budget == 2) kern = k_pst<NB, GG, 2, MX>;
-    }
+    if (h->budget == 2) kern = k_pst<NB, GG, 2, MX>;
     launch_kernel_p(w.pdl, w.priority, kern, w.count, PPB * GG, h->smem_bytes, w.stream, h->P, h->F[h->sb],
                     h->F[h->sb ^ 1], h->L[h->lb], h->L[next_list(h->lb)], h->gstart, h->glist, h->W, h->sc, h->ntx,
                     w.tiles);
@@ -340,15 +342,20 @@ void launch_pst_t(lssph_handle* h, const Where& w) {
     ProfScope prof(h, LSSPH_KIND_PST);
     if (h->order >= 3) { launch_pst_hi(h, w.tiles, w.count, w.stream, w.pdl, w.priority); return; }
     if (h->mixed) {
-        if (h->G == 2) run_pst<NB, 2, true>(h, w);
-        else run_pst<NB, 4, true>(h, w);
+        if (h->comp) {
+            if (h->G == 2) run_pst<NB, 2, 2>(h, w);
+            else run_pst<NB, 4, 2>(h, w);
+        } else {
+            if (h->G == 2) run_pst<NB, 2, 1>(h, w);
+            else run_pst<NB, 4, 1>(h, w);
+        }
         return;
     }
     switch (h->G) {
-        case 1: run_pst<NB, 1, false>(h, w); break;
-        case 2: run_pst<NB, 2, false>(h, w); break;
-        case 8: run_pst<NB, 8, false>(h, w); break;
-        default: run_pst<NB, 4, false>(h, w); break;
+        case 1: run_pst<NB, 1, 0>(h, w); break;
+        case 2: run_pst<NB, 2, 0>(h, w); break;
+        case 8: run_pst<NB, 8, 0>(h, w); break;
+        default: run_pst<NB, 4, 0>(h, w); break;
     }
 }
 
@@ -496,8 +503,8 @@ int autotune(lssph_handle* h) {
     S.stage = 1;
     S.write_rhs = 1;
     const int64_t c0 = h->launch_counter;
-    // level 2 (five CTAs per SM) exists for the FP64 q = 5 stage and PST kernels
-    const int levels = (!h->mixed && !h->classical && h->order == 2) ? 3 : 2;
+    // level 2 (five CTAs per SM) exists for the q = 5 LS stage and PST kernels
+    const int levels = (!h->classical && h->order == 2) ? 3 : 2;
     // LSSPH_REGISTER_BUDGET = loose / tight / five: skip the timing
     const char* force = std::getenv("LSSPH_REGISTER_BUDGET");
     if (force && (std::strcmp(force, "loose") == 0 || std::strcmp(force, "tight") == 0 ||
@@ -724,11 +731,13 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (check_param(pin, &msg) != LSSPH_OK) return fail(nullptr, LSSPH_E_BAD_PARAM, msg);
     if (pin->sph_model < 1 || pin->sph_model > 6)
         return fail(nullptr, LSSPH_E_UNSUPPORTED, "SPH_MODEL must be between 1 and 6");
-    if (pin->sph_model != 3 && pin->precision == LSSPH_PRECISION_MIXED)
+    const bool mixed = pin->precision == LSSPH_PRECISION_MIXED || pin->precision == LSSPH_PRECISION_MIXED_COMPENSATED;
+    if (pin->sph_model != 3 && mixed)
         return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs the LS-SPH model (SPH_MODEL 3) only");
-    if (pin->precision != LSSPH_PRECISION_FP64 && pin->precision != LSSPH_PRECISION_MIXED)
-        return fail(nullptr, LSSPH_E_BAD_PARAM, "precision must be LSSPH_PRECISION_FP64 or LSSPH_PRECISION_MIXED");
-    if (pin->precision == LSSPH_PRECISION_MIXED && pin->lanes != 0 && pin->lanes != 2 && pin->lanes != 4)
+    if (pin->precision != LSSPH_PRECISION_FP64 && !mixed)
+        return fail(nullptr, LSSPH_E_BAD_PARAM,
+                    "precision must be LSSPH_PRECISION_FP64, LSSPH_PRECISION_MIXED or LSSPH_PRECISION_MIXED_COMPENSATED");
+    if (mixed && pin->lanes != 0 && pin->lanes != 2 && pin->lanes != 4)
         return fail(nullptr, LSSPH_E_UNSUPPORTED, "mixed precision runs with 2 or 4 lanes per particle (lanes = 0, 2 or 4)");
     if (pin->target_problem == 4 && !tem) return fail(nullptr, LSSPH_E_BAD_PARAM, "tem required for problem 4");
     if (num_int <= 0 || num_total < num_int || (num_total == num_int && !pin->periodic))
@@ -752,7 +761,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->nb_rhs = h->p1 ? 1 : (h->has_tem ? 5 : 4);
     h->nb_ghost = h->p1 ? 1 : (h->has_tem ? 4 : 3);
     h->wq = h->p.wall_model == 1 ? 1 : (h->p.wall_model == 3 ? 6 : 3);
-    h->mixed = h->p.precision == LSSPH_PRECISION_MIXED;
+    h->mixed = h->p.precision != LSSPH_PRECISION_FP64;
+    h->comp = h->p.precision == LSSPH_PRECISION_MIXED_COMPENSATED;
     h->classical = h->p.sph_model <= 2;
     h->order = h->p.sph_model >= 4 ? h->p.sph_model - 1 : 2;   // LSSPH_A_mod.f90:46-56
     {

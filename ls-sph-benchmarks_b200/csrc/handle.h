@@ -25,6 +25,7 @@ struct lssph_handle {
     int nb_rhs = 4, nb_ghost = 3, nb_pst = 3, wq = 3;
     int G = 4, Gg = 4;
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
+    bool comp = false;                  // mixed precision with compensated (Kahan) FP32 pair sums
     bool classical = false;             // SPH_MODEL 1 / 2: kernel-gradient sums, q = 2 PST basis
     int order = 2;                      // Taylor order k of the LS basis (SPH_MODEL 3: 2; 4 / 5 / 6: 3 / 4 / 5)
     bool hi_thread = false;             // order >= 3: thread per particle (else warp per particle)

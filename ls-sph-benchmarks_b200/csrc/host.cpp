@@ -195,8 +195,10 @@ int check_param(const lssph_params* p, std::string* msg) {
     if (p->PST_c < 0.0 || p->coe_delta_sph < 0.0) return fail("PST_C and COE_DELTA_SPH must be non-negative.");
     const double dx = p->len_x / (double)p->num_x, dy = p->len_y / (double)p->num_y;
     if (std::fabs(dx - dy) > 1.0e-8) return fail("Particle spacing must be isotropic (dx == dy).");
-    if (p->precision != LSSPH_PRECISION_FP64 && p->precision != LSSPH_PRECISION_MIXED)
-        return fail("precision must be LSSPH_PRECISION_FP64 or LSSPH_PRECISION_MIXED.");
+    if (p->precision != LSSPH_PRECISION_FP64 && p->precision != LSSPH_PRECISION_MIXED &&
+        p->precision != LSSPH_PRECISION_MIXED_COMPENSATED)
+        return fail("precision must be LSSPH_PRECISION_FP64, LSSPH_PRECISION_MIXED or "
+                    "LSSPH_PRECISION_MIXED_COMPENSATED.");
     if (!(p->lanes == 0 || p->lanes == 1 || p->lanes == 2 || p->lanes == 4 || p->lanes == 8))
         return fail("lanes must be 0 (auto), 1, 2, 4 or 8.");
     if (p->periodic != 0 && p->periodic != 1) return fail("periodic must be 0 or 1.");

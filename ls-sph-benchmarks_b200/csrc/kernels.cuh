@@ -1377,7 +1377,7 @@ __device__ __forceinline__ void solve_row_refined(const Phys& P, double* row, in
 
 // Mixed-precision stage: FP32 staging and pair phase (offsets from FP64 cell origins and
 // field references), lanes combined in FP64, FP64 solve with refinement, FP64 update.
-template <int NB, int G>
+template <int NB, int G, bool COMP>
 __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
                                               const Lst& Ln, const int* __restrict__ gstart,
                                               const int* __restrict__ glist, const Work& W, const StageCfg& S,
@@ -1443,12 +1443,19 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
                     df[3] = SM.pre[k] - my_pre;
                 }
                 if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
-                accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
+                if constexpr (COMP) accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
+                else accumulate_A<NB, float>(Mu, B, VW, a, df);
             });
             double Md[15], Bd[NB][Q];
-            group_reduce_kahan<G>(Mu, Mc, Md);
+            if constexpr (COMP) {
+                group_reduce_kahan<G>(Mu, Mc, Md);
 #pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
+                for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
+            } else {
+                group_reduce_to<G>(Mu, Md);
+#pragma unroll
+                for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+            }
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
@@ -1635,15 +1642,16 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
                                 tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
-template <int NB, int G, bool MIXED>
+// MIXED: 0 FP64, 1 mixed precision, 2 mixed precision with compensated pair sums.
+template <int NB, int G, int MIXED>
 __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                            const int* __restrict__ gstart, const int* __restrict__ glist,
                                            const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
-    if constexpr (MIXED) stage_body_mx<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
+    if constexpr (MIXED != 0) stage_body_mx<NB, G, MIXED == 2>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
     else stage_body_fp64<NB, G, false>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
 }
 
-template <int NB, int G, int TIGHT = 0, bool MIXED = false>
+template <int NB, int G, int TIGHT = 0, int MIXED = 0>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_stage(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
             const int* __restrict__ glist, const Work W, const StageCfg S, Scalars* sc, int ntx,
@@ -2039,7 +2047,7 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
 
 
 // Mixed-precision PST: FP32 staging and pair phase, FP64 solve with refinement and update.
-template <int NB, int G>
+template <int NB, int G, bool COMP>
 __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
                                             const Lst& Ln, const int* __restrict__ gstart,
                                             const int* __restrict__ glist, const Work& W, Scalars* sc, int ntx,
@@ -2096,8 +2104,13 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
                 const float gy = ((dWdr * (-yji)) * rinv) * Vj;
                 const float t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
                 const float fac = 1.f + 0.2f * t4;
-                kahan_add(sxy[0], sxc[0], fac * gx);
-                kahan_add(sxy[1], sxc[1], fac * gy);
+                if constexpr (COMP) {
+                    kahan_add(sxy[0], sxc[0], fac * gx);
+                    kahan_add(sxy[1], sxc[1], fac * gy);
+                } else {
+                    sxy[0] = fmaf(fac, gx, sxy[0]);
+                    sxy[1] = fmaf(fac, gy, sxy[1]);
+                }
                 float a[Q];
                 basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
                 float df[NB];
@@ -2105,13 +2118,21 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
                 df[1] = SM.v[k] - my_v;
                 df[2] = SM.rho[k] - my_rho;
                 if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
-                accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
+                if constexpr (COMP) accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
+                else accumulate_A<NB, float>(Mu, B, VW, a, df);
             });
             double Md[15], Bd[NB][Q], sd[2];
-            group_reduce_kahan<G>(Mu, Mc, Md);
+            if constexpr (COMP) {
+                group_reduce_kahan<G>(Mu, Mc, Md);
 #pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
-            group_reduce_kahan<G>(sxy, sxc, sd);
+                for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
+                group_reduce_kahan<G>(sxy, sxc, sd);
+            } else {
+                group_reduce_to<G>(Mu, Md);
+#pragma unroll
+                for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+                group_reduce_to<G>(sxy, sd);
+            }
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
@@ -2172,16 +2193,16 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
     }
 }
 
-template <int NB, int G, bool MIXED, int K = 2>
+template <int NB, int G, int MIXED, int K = 2>
 __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                          const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
                                          Scalars* sc, int ntx, int tile) {
-    static_assert(!(MIXED && K != 2), "mixed precision runs the q = 5 basis only");
-    if constexpr (MIXED) pst_body_mx<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
+    static_assert(!(MIXED != 0 && K != 2), "mixed precision runs the q = 5 basis only");
+    if constexpr (MIXED != 0) pst_body_mx<NB, G, MIXED == 2>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
     else pst_body_fp64<NB, G, false, K>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
 }
 
-template <int NB, int G, int TIGHT = 0, bool MIXED = false, int K = 2>
+template <int NB, int G, int TIGHT = 0, int MIXED = 0, int K = 2>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     k_pst(const Phys P, const Fld cur, const Fld nxt, const Lst Lc, const Lst Ln, const int* __restrict__ gstart,
           const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
@@ -2233,7 +2254,7 @@ __device__ __forceinline__ const SolveDesc& load_desc(const SolveDesc* D, int s,
     return sd;
 }
 
-template <int NB, int G, int TIGHT = 0, bool MIXED = false>
+template <int NB, int G, int TIGHT = 0, int MIXED = 0>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_stage(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
                                                     int ps, int pl) {
     __shared__ SolveDesc sd;
@@ -2259,7 +2280,7 @@ __global__ void __launch_bounds__(PPB * G) kb_ghost(const SolveDesc* __restrict_
                           zero_other ? d.L[prev_list(lb)].cnt : nullptr, reset_umax, d.sc, m.y, d.nchunk);
 }
 
-template <int NB, int G, int TIGHT = 0, bool MIXED = false>
+template <int NB, int G, int TIGHT = 0, int MIXED = 0>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(const SolveDesc* __restrict__ D, const BatchMap M, int ps, int pl) {
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];

@@ -14,6 +14,7 @@ module lssph_cuda_mod
 
     integer(c_int), parameter :: LSSPH_OK = 0
     integer(c_int), parameter :: LSSPH_PRECISION_FP64 = 0, LSSPH_PRECISION_MIXED = 1
+    integer(c_int), parameter :: LSSPH_PRECISION_MIXED_COMPENSATED = 2
 
     ! Mirror of lssph_params (same field order and padding as include/lssph.h)
     type, bind(c) :: lssph_params

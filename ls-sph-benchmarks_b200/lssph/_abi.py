@@ -29,6 +29,7 @@ KIND_NAMES = ("stage", "cellsort", "ghost", "pst", "other")
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_MIXED_COMPENSATED = 2
 
 
 class LssphError(RuntimeError):

@@ -29,10 +29,10 @@ import time
 
 import numpy as np
 
-from . import PRECISION_FP64, PRECISION_MIXED, Simulation, boussinesq_params, cavity_params, make_params, \
-    taylor_green_params
+from . import (PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_COMPENSATED, Simulation, boussinesq_params,
+               cavity_params, make_params, taylor_green_params)
 
-PRECISIONS = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}
+PRECISIONS = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED, "mixed_compensated": PRECISION_MIXED_COMPENSATED}
 PROFILE_POINTS = 1025
 
 

@@ -43,12 +43,14 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / n if n > 0 else np.linalg.norm(a - b)
 
 
+@pytest.mark.parametrize("prec", [lssph.PRECISION_MIXED, lssph.PRECISION_MIXED_COMPENSATED])
 @pytest.mark.parametrize("case", list(CASES))
-def test_mixed_within_bound_of_fp64(case):
+def test_mixed_within_bound_of_fp64(case, prec):
+    # both mixed modes: plain FP32 lane sums and Kahan-compensated ones
     mk, steps = CASES[case]
     p = mk()
     s64 = _sim(p, lssph.PRECISION_FP64)
-    smx = _sim(p, lssph.PRECISION_MIXED)
+    smx = _sim(p, prec)
     assert s64.step(steps) == smx.step(steps) == 0
     g64, gmx = s64.download(), smx.download()
     ni = s64.num_int
@@ -142,3 +144,41 @@ def test_mixed_members_identical_alone_and_batched():
         gs, gm = s.download(), m.download()
         for k in _fields(s.params):
             assert np.array_equal(getattr(gs, k), getattr(gm, k)), k
+
+
+def test_compensated_and_plain_mixed_members_identical_alone_and_batched():
+    # a batch holding both mixed modes keeps them in separate groups; each member ends
+    # bit for bit as it does alone
+    mk = [(lambda: lssph.taylor_green_params(num=48), lssph.PRECISION_MIXED_COMPENSATED),
+          (lambda: lssph.taylor_green_params(num=48), lssph.PRECISION_MIXED),
+          (lambda: lssph.cavity_params(num=40), lssph.PRECISION_MIXED_COMPENSATED)]
+    solo = [_sim(f(), prec, seed=i) for i, (f, prec) in enumerate(mk)]
+    mem = [_sim(f(), prec, seed=i) for i, (f, prec) in enumerate(mk)]
+    with lssph.Batch() as b:
+        for m in mem:
+            b.add(m)
+        b.step(5)
+    for s in solo:
+        s.step(5)
+    for s, m in zip(solo, mem):
+        gs, gm = s.download(), m.download()
+        for k in _fields(s.params):
+            assert np.array_equal(getattr(gs, k), getattr(gm, k)), k
+    # the two modes are different arithmetic on the same inputs
+    assert not np.array_equal(solo[0].download().u, solo[1].download().u)
+
+
+def test_split_precision_positions_follow_the_fp64_positions():
+    # the FP32 offsets from the cell origins that the mixed staging reads: a mixed solve that
+    # is downloaded, re-created from its state (which recomputes the offsets from the FP64
+    # positions) and stepped on ends bit for bit as the uninterrupted solve
+    p = lssph.make_params(lssph.cavity_params(num=40), lanes=4)
+    a = _sim(p, lssph.PRECISION_MIXED, seed=5)
+    b = _sim(p, lssph.PRECISION_MIXED, seed=5)
+    a.step(7)
+    b.step(4)
+    c = lssph.Simulation(b.params, b.download(), b.num_int)
+    c.step(3)
+    ga, gc = a.download(), c.download()
+    for k in _fields(p):
+        assert np.array_equal(getattr(ga, k), getattr(gc, k)), k
