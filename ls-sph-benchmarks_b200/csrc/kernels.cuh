@@ -736,13 +736,14 @@ __device__ __forceinline__ TileRef stage_fields_mx(const Phys& P, const Fld& F, 
     }
     // positions from the split-precision copy in HBM: a particle of halo cell (hx, hy) sits at
     // (hx, hy) * cw + (ox, oy) from the tile's halo corner, which also holds for a wrapped
-    // periodic neighbour (its cell origin moved by -+Lx = -+nx cw)
-    const float cwf = (float)P.cw;
+    // periodic neighbour (its cell origin moved by -+Lx = -+nx cw).  The cell offset is added
+    // in FP64 and the sum rounded once: an FP32 cell width would shift every particle of a
+    // halo column by the same rounding error, a bias between the columns' pair offsets.
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int j = S.idx[k];
         const int h = halo_cell_of(T, k);
-        S.ox[k] = __ldg(F.ox + j) + (float)(h % HX) * cwf;
-        S.oy[k] = __ldg(F.oy + j) + (float)(h / HX) * cwf;
+        S.ox[k] = (float)((double)__ldg(F.ox + j) + (double)(h % HX) * P.cw);
+        S.oy[k] = (float)((double)__ldg(F.oy + j) + (double)(h / HX) * P.cw);
         S.u[k] = (float)(__ldg(F.u + j) - R.u);
         S.v[k] = (float)(__ldg(F.v + j) - R.v);
         S.rho[k] = (float)(__ldg(F.rho + j) - R.rho);
