@@ -186,6 +186,15 @@ int lssph_upload(lssph_handle* h, const double* x, const double* y, const double
                  const double* v, const double* rho, const double* pre, const double* tem);
 int lssph_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u,
                    double* v, double* rho, double* pre, double* tem);
+/* Upload the state from host arrays (as lssph_upload, positions included), run nsteps time
+   steps (as lssph_step) and write the new state back into the same arrays (as
+   lssph_download), queued back to back with one synchronisation: the call of a host that
+   keeps the particle state in its own arrays between steps, as the reference's driver keeps
+   SP%x..SP%tem (main.f90:119-166).  x..pre (and tem for problem 4) have num_total entries;
+   page-locked mapped buffers are read and written in place by one kernel each way.  No
+   reference counterpart as one call (it fuses the loop body with the copies). */
+int lssph_advance_host(lssph_handle* h, int32_t nsteps, double* x, double* y, double* u,
+                       double* v, double* rho, double* pre, double* tem, int32_t* steady_step);
 /* RHS arrays of the last calculate_RHS (length num_int; rhs_tem may be NULL). */
 int lssph_download_rhs(lssph_handle* h, double* rhs_u, double* rhs_v, double* rhs_rho,
                        double* rhs_tem);

@@ -597,6 +597,76 @@ int sync_check(lssph_handle* h) {
     return check_scalars(h, nullptr);
 }
 
+// The launches of nsteps time steps behind whatever is queued on the handle's stream (graph
+// replays, captured on first use per parity), no synchronisation.  finish_steps reads the
+// scalars back (one synchronisation) and puts the buffer parities where the last executed
+// step left them.
+struct StepMark {
+    int64_t launches0;
+    int sb_start, lb_start;
+};
+
+int enqueue_steps(lssph_handle* h, int32_t nsteps, StepMark* mark) {
+    mark->launches0 = h->launch_counter;
+    mark->sb_start = h->sb;
+    mark->lb_start = h->lb;
+    // The step count at entry, recorded on the device behind the queued work, in place of a
+    // read-back before the launches: every kernel of a halted solve (steady state -- where
+    // the reference leaves its time loop --, step budget, error) does nothing, so the one
+    // read-back after the launches tells how many steps ran and why they stopped.
+    CUDA_TRY(h, cudaMemcpyAsync(&h->sc->step_mark, &h->sc->step_count, sizeof(int), cudaMemcpyDeviceToDevice,
+                                h->stream));
+    CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+    for (int st = 0; st < nsteps; ++st) {
+        cudaGraphExec_t& ge = h->graph[h->sb][h->lb];
+        if (!ge) {
+            const int sb0 = h->sb, lb0 = h->lb;
+            const int64_t c0 = h->launch_counter;
+            CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            if (h->overlap) enq_step_overlap(h);
+            else enq_step(h);
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
+            // per-node priorities: the overlapped step's critical path runs first
+            const cudaError_t e = cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+            h->graph_launches = (int)(h->launch_counter - c0);
+            h->launch_counter = c0;
+            h->step_sbf = h->sb ^ sb0;
+            h->step_lba = (h->lb - lb0 + kLists) % kLists;
+            h->sb = sb0;
+            h->lb = lb0;
+        }
+        CUDA_TRY(h, cudaGraphLaunch(ge, h->stream));
+        h->launch_counter += h->graph_launches;
+        h->sb ^= h->step_sbf;
+        h->lb = (h->lb + h->step_lba) % kLists;
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+    return LSSPH_OK;
+}
+
+// executed: the steps that ran (nsteps unless the solve stopped on the way).
+int finish_steps(lssph_handle* h, int32_t nsteps, const StepMark& mark, int32_t* steady_step_out, int* executed) {
+    Scalars s1{};
+    const int rc = check_scalars(h, &s1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_ms = ms;
+    h->last_launches = h->launch_counter - mark.launches0;
+    // steps after a stop (steady state, step budget, error) ran as no-ops: the buffers
+    // sit where the last executed step left them
+    *executed = s1.step_count - s1.step_mark;
+    if (*executed != nsteps) {
+        h->sb = mark.sb_start ^ (h->step_sbf & *executed & 1);
+        h->lb = (mark.lb_start + h->step_lba * *executed) % kLists;
+    }
+    if (rc != LSSPH_OK) return rc;
+    if (s1.steady && steady_step_out && s1.steady_step > s1.step_mark) *steady_step_out = s1.steady_step - s1.step_mark;
+    return LSSPH_OK;
+}
+
 // Mixed precision: the split-precision positions of the current state, both buffers.
 void write_split_pos(lssph_handle* h) {
     if (!h->P.split_pos) return;
@@ -664,6 +734,35 @@ bool all_mapped(const double* const (&f)[7], size_t bytes, double* (&out)[7], bo
             return false;
     }
     return true;
+}
+
+// The copies (or, into page-locked mapped buffers the device may write, one kernel) of the
+// current state into caller-owned host arrays, queued on the handle's stream: the caller
+// synchronises before reading them.  tem of a solve without temperature is zeroed here.
+int enqueue_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u, double* v, double* rho,
+                     double* pre, double* tem) {
+    const size_t bytes = sizeof(double) * (size_t)h->num_total;
+    const Fld& F = h->F[h->sb];
+    if (tem && !h->has_tem) std::memset(tem, 0, bytes);
+    if (ptype) std::memcpy(ptype, h->ptype.data(), sizeof(int32_t) * h->num_total);
+    {   // page-locked, mapped host buffers: one kernel writes them
+        const double* const f[7] = {x, y, u, v, rho, pre, h->has_tem ? tem : nullptr};
+        double* d[7];
+        if (all_mapped(f, bytes, d, true)) {
+            k_download_mapped<<<blocks_for(h->num_total, 256), 256, 0, h->stream>>>(
+                h->P, F, HostOut{d[0], d[1], d[2], d[3], d[4], d[5], d[6]});
+            CUDA_TRY(h, cudaGetLastError());
+            return LSSPH_OK;
+        }
+    }
+    if (x) CUDA_TRY(h, cudaMemcpyAsync(x, F.x, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (y) CUDA_TRY(h, cudaMemcpyAsync(y, F.y, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (u) CUDA_TRY(h, cudaMemcpyAsync(u, F.u, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (v) CUDA_TRY(h, cudaMemcpyAsync(v, F.v, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, F.rho, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (pre) CUDA_TRY(h, cudaMemcpyAsync(pre, F.pre, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (tem && h->has_tem) CUDA_TRY(h, cudaMemcpyAsync(tem, F.tem, bytes, cudaMemcpyDeviceToHost, h->stream));
+    return LSSPH_OK;
 }
 
 // The current buffer gets every particle.  On a later upload (both = false) the other buffer
@@ -1080,58 +1179,10 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
     if (nsteps <= 0) return LSSPH_OK;
     int rc = ensure_tuned(h);
     if (rc != LSSPH_OK) return rc;
-    const int64_t launches0 = h->launch_counter;
-    const int sb_start = h->sb, lb_start = h->lb;
-    // The step count at entry, recorded on the device behind the queued work, in place of a
-    // read-back before the launches: every kernel of a halted solve (steady state -- where
-    // the reference leaves its time loop --, step budget, error) does nothing, so the one
-    // read-back after the launches tells how many steps ran and why they stopped.
-    CUDA_TRY(h, cudaMemcpyAsync(&h->sc->step_mark, &h->sc->step_count, sizeof(int), cudaMemcpyDeviceToDevice,
-                                h->stream));
-    CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
-    for (int st = 0; st < nsteps; ++st) {
-        cudaGraphExec_t& ge = h->graph[h->sb][h->lb];
-        if (!ge) {
-            const int sb0 = h->sb, lb0 = h->lb;
-            const int64_t c0 = h->launch_counter;
-            CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            if (h->overlap) enq_step_overlap(h);
-            else enq_step(h);
-            cudaGraph_t g = nullptr;
-            CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
-            // per-node priorities: the overlapped step's critical path runs first
-            const cudaError_t e = cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
-            cudaGraphDestroy(g);
-            if (e != cudaSuccess) return fail(h, LSSPH_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-            h->graph_launches = (int)(h->launch_counter - c0);
-            h->launch_counter = c0;
-            h->step_sbf = h->sb ^ sb0;
-            h->step_lba = (h->lb - lb0 + kLists) % kLists;
-            h->sb = sb0;
-            h->lb = lb0;
-        }
-        CUDA_TRY(h, cudaGraphLaunch(ge, h->stream));
-        h->launch_counter += h->graph_launches;
-        h->sb ^= h->step_sbf;
-        h->lb = (h->lb + h->step_lba) % kLists;
-    }
-    CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
-    Scalars s1{};
-    rc = check_scalars(h, &s1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-    h->last_ms = ms;
-    h->last_launches = h->launch_counter - launches0;
-    // steps after a stop (steady state, step budget, error) ran as no-ops: the buffers
-    // sit where the last executed step left them
-    const int executed = s1.step_count - s1.step_mark;
-    if (executed != nsteps) {
-        h->sb = sb_start ^ (h->step_sbf & executed & 1);
-        h->lb = (lb_start + h->step_lba * executed) % kLists;
-    }
-    if (rc != LSSPH_OK) return rc;
-    if (s1.steady && steady_step_out && s1.steady_step > s1.step_mark) *steady_step_out = s1.steady_step - s1.step_mark;
-    return LSSPH_OK;
+    StepMark mark{};
+    if ((rc = enqueue_steps(h, nsteps, &mark)) != LSSPH_OK) return rc;
+    int executed = 0;
+    return finish_steps(h, nsteps, mark, steady_step_out, &executed);
 }
 
 int lssph_mem_info(int64_t* free_bytes, int64_t* total_bytes) {
@@ -1218,34 +1269,41 @@ int lssph_upload(lssph_handle* h, const double* x, const double* y, const double
 int lssph_download(lssph_handle* h, int32_t* ptype, double* x, double* y, double* u, double* v, double* rho,
                    double* pre, double* tem) {
     if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
-    const size_t bytes = sizeof(double) * (size_t)h->num_total;
-    const Fld& F = h->F[h->sb];
-    {   // page-locked, mapped host buffers: one kernel writes them
-        const double* const f[7] = {x, y, u, v, rho, pre, h->has_tem ? tem : nullptr};
-        double* d[7];
-        if (all_mapped(f, bytes, d, true)) {
-            k_download_mapped<<<blocks_for(h->num_total, 256), 256, 0, h->stream>>>(
-                h->P, F, HostOut{d[0], d[1], d[2], d[3], d[4], d[5], d[6]});
-            if (tem && !h->has_tem) std::memset(tem, 0, bytes);
-            if (ptype) std::memcpy(ptype, h->ptype.data(), sizeof(int32_t) * h->num_total);
-            CUDA_TRY(h, cudaGetLastError());
-            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-            return LSSPH_OK;
-        }
-    }
-    if (x) CUDA_TRY(h, cudaMemcpyAsync(x, F.x, bytes, cudaMemcpyDeviceToHost, h->stream));
-    if (y) CUDA_TRY(h, cudaMemcpyAsync(y, F.y, bytes, cudaMemcpyDeviceToHost, h->stream));
-    if (u) CUDA_TRY(h, cudaMemcpyAsync(u, F.u, bytes, cudaMemcpyDeviceToHost, h->stream));
-    if (v) CUDA_TRY(h, cudaMemcpyAsync(v, F.v, bytes, cudaMemcpyDeviceToHost, h->stream));
-    if (rho) CUDA_TRY(h, cudaMemcpyAsync(rho, F.rho, bytes, cudaMemcpyDeviceToHost, h->stream));
-    if (pre) CUDA_TRY(h, cudaMemcpyAsync(pre, F.pre, bytes, cudaMemcpyDeviceToHost, h->stream));
-    if (tem) {
-        if (h->has_tem) CUDA_TRY(h, cudaMemcpyAsync(tem, F.tem, bytes, cudaMemcpyDeviceToHost, h->stream));
-        else std::memset(tem, 0, bytes);
-    }
-    if (ptype) std::memcpy(ptype, h->ptype.data(), sizeof(int32_t) * h->num_total);
+    const int rc = enqueue_download(h, ptype, x, y, u, v, rho, pre, tem);
+    if (rc != LSSPH_OK) return rc;
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return LSSPH_OK;
+}
+
+int lssph_advance_host(lssph_handle* h, int32_t nsteps, double* x, double* y, double* u, double* v, double* rho,
+                       double* pre, double* tem, int32_t* steady_step_out) {
+    if (!h) return fail(nullptr, LSSPH_E_BAD_PARAM, "null handle");
+    if (!x || !y || !u || !v || !rho || !pre || (h->has_tem && !tem))
+        return fail(h, LSSPH_E_BAD_PARAM, "lssph_advance_host: null state array");
+    if (steady_step_out) *steady_step_out = 0;
+    if (nsteps < 0) return fail(h, LSSPH_E_BAD_PARAM, "lssph_advance_host: nsteps must be >= 0");
+    int rc = ensure_tuned(h);   // first call only: measures lanes / register budget
+    if (rc != LSSPH_OK) return rc;
+    // upload (as lssph_upload), steps (as lssph_step), download (as lssph_download), queued
+    // back to back on the handle's stream; the scalar read-back is the one synchronisation
+    if ((rc = upload_fields(h, x, y, u, v, rho, pre, tem, false)) != LSSPH_OK) return rc;
+    if (!h->p1 && (rc = rebuild_cells(h)) != LSSPH_OK) return rc;
+    StepMark mark{};
+    if (nsteps > 0 && (rc = enqueue_steps(h, nsteps, &mark)) != LSSPH_OK) return rc;
+    const int sb_queued = h->sb;
+    if ((rc = enqueue_download(h, nullptr, x, y, u, v, rho, pre, h->has_tem ? tem : nullptr)) != LSSPH_OK) return rc;
+    CUDA_TRY(h, cudaGetLastError());
+    if (nsteps == 0) return sync_check(h);
+    int executed = 0;
+    rc = finish_steps(h, nsteps, mark, steady_step_out, &executed);
+    // a solve that stopped on the way (steady state, step budget, error) sits in the other
+    // buffer when it ran an odd number of steps fewer: read that one instead
+    if (h->sb != sb_queued) {
+        const int rc2 = enqueue_download(h, nullptr, x, y, u, v, rho, pre, h->has_tem ? tem : nullptr);
+        if (rc2 != LSSPH_OK) return rc2;
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    }
+    return rc;
 }
 
 int lssph_download_rhs(lssph_handle* h, double* ru, double* rv, double* rr, double* rt) {

@@ -106,6 +106,16 @@ module lssph_cuda_mod
             real(c_double), intent(out) :: x(*), y(*), u(*), v(*), rho(*), pre(*), tem(*)
         end function
 
+        ! upload + nsteps steps + download in one call, the state updated in place
+        integer(c_int) function lssph_advance_host(h, nsteps, x, y, u, v, rho, pre, tem, steady_step) &
+                bind(c, name="lssph_advance_host")
+            import :: c_int, c_int32_t, c_double, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: nsteps
+            real(c_double), intent(inout) :: x(*), y(*), u(*), v(*), rho(*), pre(*), tem(*)
+            integer(c_int32_t), intent(out) :: steady_step
+        end function
+
         integer(c_int) function lssph_write_param(h, results_root, config_h) bind(c, name="lssph_write_param")
             import :: c_int, c_char, c_ptr
             type(c_ptr), value :: h

@@ -154,6 +154,7 @@ _PROTOS = {
     "lssph_step": (C.c_int, [_H, C.c_int32, _i]),
     "lssph_upload": (C.c_int, [_H, _d, _d, _d, _d, _d, _d, _d]),
     "lssph_download": (C.c_int, [_H, _i, _d, _d, _d, _d, _d, _d, _d]),
+    "lssph_advance_host": (C.c_int, [_H, C.c_int32, _d, _d, _d, _d, _d, _d, _d, _i]),
     "lssph_download_rhs": (C.c_int, [_H, _d, _d, _d, _d]),
     "lssph_download_vm": (C.c_int, [_H, _i, _d, _d, _d, _d, _d, _d]),
     "lssph_neighbors_csr": (C.c_int, [_H, C.c_int32, _i, _i, C.c_int64, _P(C.c_int64)]),

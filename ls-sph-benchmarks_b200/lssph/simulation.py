@@ -174,6 +174,21 @@ class Simulation:
         self._chk(self._lib.lssph_download(self._h, None, dptr(st.x), dptr(st.y), dptr(st.u),
                                            dptr(st.v), dptr(st.rho), dptr(st.pre), dptr(st.tem)))
 
+    def advance_host(self, st: State, nsteps: int = 1) -> int:
+        """Upload ``st`` (positions and fields), run ``nsteps`` steps and write the new state
+        back into ``st``'s arrays, with one synchronisation (lssph_advance_host).  The arrays
+        must be C-contiguous float64 (page-locked ones are read and written in place by one
+        kernel each way).  Returns the step at which problem 1 reached its steady state in
+        this call, or 0."""
+        for a in (st.x, st.y, st.u, st.v, st.rho, st.pre) + ((st.tem,) if self.has_tem else ()):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape[0] != self.num_total:
+                raise ValueError("advance_host needs C-contiguous float64 arrays of num_total entries")
+        steady = C.c_int32()
+        self._chk(self._lib.lssph_advance_host(self._h, int(nsteps), dptr(st.x), dptr(st.y), dptr(st.u),
+                                               dptr(st.v), dptr(st.rho), dptr(st.pre),
+                                               dptr(st.tem) if self.has_tem else None, C.byref(steady)))
+        return steady.value
+
     def upload(self, st: State) -> None:
         arrs = [_c64(a) for a in (st.x, st.y, st.u, st.v, st.rho, st.pre)]
         tem = _c64(st.tem) if self.has_tem else None

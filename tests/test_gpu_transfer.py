@@ -96,3 +96,56 @@ def test_pinned_round_trip_every_step_equals_resident_run():
         assert np.array_equal(getattr(host, k), getattr(g, k)), k
     res.close()
     e2e.close()
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("case", list(CASES))
+def test_advance_host_equals_upload_step_download(case, pinned):
+    # lssph_advance_host (one call, one synchronisation) against the three separate calls,
+    # every step from the host arrays, with page-locked and with pageable buffers
+    p = CASES[case]()
+    sep, fused = _sim(p), _sim(p)
+    a = sep.download()
+    b = _pinned_state(a, p.target_problem == 4) if pinned else sep.download()
+    for n in (1, 3, 1):
+        sep.upload(a)
+        sep.step(n)
+        sep.download_into(a)
+        assert fused.advance_host(b, n) == 0
+        for k in _keys(p):
+            assert np.array_equal(getattr(b, k), getattr(a, k)), (n, k)
+    sep.close()
+    fused.close()
+
+
+def test_advance_host_returns_the_state_where_a_stopped_solve_stopped():
+    # a solve that stops part-way through the call (its step budget; problem 1: its steady
+    # state) hands back the state of its last executed step, as step + download give it.
+    # RK4 + PST flips the state buffers an odd number of times per step, so three of four
+    # steps leave the other buffer current than four would.
+    p = lssph.taylor_green_params(num=48)
+    sep, fused = _sim(p), _sim(p)
+    a = sep.download()
+    b = _pinned_state(a, False)
+    for s in (sep, fused):
+        s.set_step_budget(3)
+    sep.upload(a)
+    sep.step(4)
+    sep.download_into(a)
+    fused.advance_host(b, 4)
+    assert sep.progress() == fused.progress() == (3, "budget")
+    for k in FIELDS:
+        assert np.array_equal(getattr(b, k), getattr(a, k)), k
+    q = lssph.diffusion_params(num=24, seed=1, THRESHOLD=1e-3)
+    sep, fused = _sim(q), _sim(q)
+    a = sep.download()
+    b = _pinned_state(a, False)
+    sep.upload(a)
+    s1 = sep.step(800)
+    sep.download_into(a)
+    s2 = fused.advance_host(b, 800)
+    assert 0 < s1 == s2 < 800
+    for k in FIELDS:
+        assert np.array_equal(getattr(b, k), getattr(a, k)), k
+    sep.close()
+    fused.close()
