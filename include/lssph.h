@@ -230,12 +230,18 @@ int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32
                     double* tem);
 
 /* Kernel configuration the handle runs (no counterpart in the reference): lanes per
-   particle, and the register budget of the stage/PST kernels: 0 loose, 1 tight (four CTAs
-   per SM), 2 five CTAs per SM (FP64 q = 5 only), with the RHS-pass time of the loose and
+   particle, and the register budget of the stage/PST kernels: 0 loose, 1 tight (512 threads
+   per SM), 2 (640 threads per SM, q = 5 LS only), and for the pair kernel of the mixed
+   precision split shape also 3 (768) and 4 (1024), with the RHS-pass time of the loose and
    tight budgets measured when the handle was created.  The budget is picked by that
    measurement; it never changes a result. */
 int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
                      double* rhs_us_tight);
+/* Shape of the mixed-precision stage and PST (no counterpart in the reference): 1 split (an
+   FP32 pair kernel, then an FP64 solve-and-update kernel per particle), 0 fused (one
+   kernel), as the handle's first-launch measurement picked it; FP64 solves report 0.  Both
+   shapes compute identical results. */
+int lssph_get_kernel_shape(const lssph_handle* h, int32_t* split);
 
 /* Time-step schedule (no counterpart in the reference): cell tiles, the tiles whose halo
    holds no ghost particle, and whether lssph_step runs each ghost launch beside the next

@@ -100,6 +100,7 @@ void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t 
     A(&W.x_acc, NI); A(&W.y_acc, NI); A(&W.u_acc, NI); A(&W.v_acc, NI); A(&W.rho_acc, NI); A(&W.tem_acc, NI);
     A(&W.rhs_u, NI); A(&W.rhs_v, NI); A(&W.rhs_rho, NI); A(&W.rhs_tem, NI);
     A(&W.f_prev, NI); A(&W.src, NI); A(&W.key, NI);
+    A(&W.sums, h->mixed ? NI * MXS_ENTRIES : 0);   // mixed precision, split shape
     VMd& V = h->V;
     A(&V.x, NE); A(&V.y, NE); A(&V.nx, NE); A(&V.ny, NE); A(&V.u, NE); A(&V.v, NE); A(&V.pre, NE); A(&V.tem, NE);
     A(&V.K, NE); A(&V.ptype, NE); A(&V.key, NE); A(&V.mode, NE);
@@ -141,37 +142,13 @@ void vm_chunks(const CellGrid& g, int ntx, int ntiles, std::vector<int32_t>* til
 
 // Size of the single device block of a solve of these sizes (every array holds at least
 // one element and starts on a 256-byte boundary).
-int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, int ntiles) {
+int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, int ntiles, bool mixed) {
     lssph_handle layout;
+    layout.mixed = mixed;
     size_t total = 0;
     visit_solve_arrays(&layout, N, NI, NE, NC, cap, nvt, ntiles, [&](auto** p, size_t n) { total += array_bytes(p, n); });
     return (int64_t)total;
 }
-
-inline int blocks_for(long n, int per_block) { return (int)((n + per_block - 1) / per_block); }
-
-// Event pair around one launch while profiling; no-op otherwise (and during capture).
-struct ProfScope {
-    lssph_handle* h;
-    size_t slot = (size_t)-1;
-    ProfScope(lssph_handle* hh, int kind) : h(hh) {
-        if (!h->profiling) return;
-        if (h->prof_next + 2 > h->prof_events.size()) {
-            for (int k = 0; k < 64; ++k) {
-                cudaEvent_t e;
-                if (cudaEventCreate(&e) != cudaSuccess) return;
-                h->prof_events.push_back(e);
-            }
-        }
-        slot = h->prof_next;
-        h->prof_next += 2;
-        h->prof_kinds.push_back(kind);
-        cudaEventRecord(h->prof_events[slot], h->stream);
-    }
-    ~ProfScope() {
-        if (slot != (size_t)-1) cudaEventRecord(h->prof_events[slot + 1], h->stream);
-    }
-};
 
 // Dynamic shared memory above 48 KB needs an opt-in per kernel; set once per
 // instantiation while the handle is prepared (never during graph capture).
@@ -180,16 +157,6 @@ void smem_optin(K kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(64, 8, true));
 }
 
-// Where a launch goes: its tile map (NULL: every tile in order), CTA count, stream, and
-// whether it may be a programmatic dependent launch (not right after a fork or join).
-struct Where {
-    const int* tiles;
-    int count;
-    cudaStream_t stream;
-    bool pdl;
-    int priority;   // 0: default
-};
-Where all_tiles(const lssph_handle* h) { return Where{nullptr, h->ntiles, h->stream, h->pdl, 0}; }
 
 // ---- kernel dispatch on lanes, register budget and precision ------------------------------
 // The mixed-precision kernels exist for 2 and 4 lanes per particle.
@@ -247,13 +214,24 @@ void launch_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
     }
 }
 
+// The stage kernel over the tiles of w.  In the split shape this is the pair kernel only:
+// launch_stage_tail then runs the solve kernel once every tile of the stage is done.
 void launch_stage_any(lssph_handle* h, const StageCfg& S, const Where& w) {
+    if (h->mixed && h->split) { launch_stage_mxp(h, S, w); return; }
     if (h->nb_rhs == 1) launch_stage<1>(h, S, w);
     else if (h->nb_rhs == 5) launch_stage<5>(h, S, w);
     else launch_stage<4>(h, S, w);
 }
 
-void launch_stage_any(lssph_handle* h, const StageCfg& S) { launch_stage_any(h, S, all_tiles(h)); }
+void launch_stage_tail(lssph_handle* h, const StageCfg& S, bool pdl) {
+    if (h->mixed && h->split) launch_stage_mxs(h, S, h->stream, pdl);
+}
+
+// A whole stage (every tile, then the split shape's solve kernel).
+void launch_stage_any(lssph_handle* h, const StageCfg& S) {
+    launch_stage_any(h, S, all_tiles(h));
+    launch_stage_tail(h, S, h->pdl);
+}
 
 // zero_list >= 0: clear that list's scatter counters (the list the preceding stage read).
 template <int NB, int WQ>
@@ -360,8 +338,13 @@ void launch_pst_t(lssph_handle* h, const Where& w) {
 }
 
 void launch_pst_any(lssph_handle* h, const Where& w) {
+    if (h->mixed && h->split) { launch_pst_mxp(h, w); return; }
     if (h->has_tem) launch_pst_t<4>(h, w);
     else launch_pst_t<3>(h, w);
+}
+
+void launch_pst_tail(lssph_handle* h, bool pdl) {
+    if (h->mixed && h->split) launch_pst_mxs(h, h->stream, pdl);
 }
 
 // ---- operator sequences (enqueue only) -----------------------------------------------------
@@ -401,6 +384,7 @@ void enq_stage(lssph_handle* h, int stage, bool fused_step) {
 
 void enq_pst(lssph_handle* h) {
     launch_pst_any(h, all_tiles(h));
+    launch_pst_tail(h, h->pdl);
     h->sb ^= 1;
     h->lb = next_list(h->lb);
     launch_ghost(h, prev_list(h->lb), 1);
@@ -419,6 +403,10 @@ void prepare_kernels(lssph_handle* h) {
     launch_stage_any(h, S);
     launch_ghost(h);
     launch_pst_any(h, all_tiles(h));
+    if (h->mixed) {   // the split shape the measurement may pick
+        launch_stage_mxp(h, S, all_tiles(h));
+        launch_pst_mxp(h, all_tiles(h));
+    }
     h->preparing = false;
 }
 
@@ -470,6 +458,7 @@ void enq_step_overlap(lssph_handle* h) {
         launch_stage_any(h, S, interior);
         launch_stage_any(h, S, wall);
         join();
+        launch_stage_tail(h, S, false);
         h->sb ^= 1;
         if (!h->p1) {
             h->lb = next_list(h->lb);
@@ -482,6 +471,7 @@ void enq_step_overlap(lssph_handle* h) {
         launch_pst_any(h, interior);
         launch_pst_any(h, wall);
         join();
+        launch_pst_tail(h, false);
         h->sb ^= 1;
         h->lb = next_list(h->lb);
         launch_ghost_on(h, prev_list(h->lb), 1, h->stream, false);
@@ -505,21 +495,32 @@ int autotune(lssph_handle* h) {
     const int64_t c0 = h->launch_counter;
     // level 2 (five CTAs per SM) exists for the q = 5 LS stage and PST kernels
     const int levels = (!h->classical && h->order == 2) ? 3 : 2;
+    // mixed precision may also run split (pair kernel, then solve kernel): budget levels 0-4
+    // of its pair kernel.  LSSPH_MIXED_SHAPE = fused / split restricts the choice.
+    const char* shape = std::getenv("LSSPH_MIXED_SHAPE");
+    const bool try_fused = !(h->mixed && shape && std::strcmp(shape, "split") == 0);
+    const bool try_split = h->mixed && !(shape && std::strcmp(shape, "fused") == 0);
     // LSSPH_REGISTER_BUDGET = loose / tight / five: skip the timing
     const char* force = std::getenv("LSSPH_REGISTER_BUDGET");
     if (force && (std::strcmp(force, "loose") == 0 || std::strcmp(force, "tight") == 0 ||
                   std::strcmp(force, "five") == 0)) {
         h->budget = std::strcmp(force, "loose") == 0 ? 0 : (std::strcmp(force, "tight") == 0 ? 1 : levels - 1);
         h->tight = h->budget >= 1;
+        h->split = !try_fused;
         return LSSPH_OK;
     }
     // lanes = 0 on a q = 5 LS solve: 4 lanes per particle unless 2 lanes run the RHS
     // pass at least 5 % faster (the margin keeps the pick, and with it the summation order,
-    // the same from run to run when the two are close)
+    // the same from run to run when the two are close).  The shape and the budget change no
+    // result, so they go to the fastest.
     const int nlanes = h->lanes_auto ? 2 : 1;
     const int lane_opts[2] = {h->G, 2};
-    double us[2][3] = {{1e30, 1e30, 1e30}, {1e30, 1e30, 1e30}};
-    int best_t[2] = {0, 0};
+    // option t: fused at budget t (t < levels), split at budget t - levels
+    constexpr int kOpts = 3 + 5;
+    const int nopt = levels + (try_split ? 5 : 0);
+    double us[2][kOpts];
+    for (auto& row : us)
+        for (double& v : row) v = 1e30;
     // Every option is timed in each of several interleaved rounds and keeps its fastest
     // round, so that a clock ramp or a neighbour's burst during one round does not decide
     // the pick (a single round swung the choice by about 10 % between machines).
@@ -527,9 +528,11 @@ int autotune(lssph_handle* h) {
     for (int round = 0; round < kRounds; ++round) {
         for (int g = 0; g < nlanes; ++g) {
             h->G = lane_opts[g];
-            for (int t = 0; t < levels; ++t) {
-                h->tight = t >= 1;
-                h->budget = t;
+            for (int t = 0; t < nopt; ++t) {
+                h->split = t >= levels;
+                if (!h->split && !try_fused) continue;
+                h->budget = h->split ? t - levels : t;
+                h->tight = h->budget >= 1;
                 launch_stage_any(h, S);   // warm-up (instruction cache, L2)
                 CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
                 for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
@@ -541,18 +544,24 @@ int autotune(lssph_handle* h) {
             }
         }
     }
+    int best_t[2] = {0, 0};
     for (int g = 0; g < nlanes; ++g) {
         // In the overlapped step the interior tiles share the SMs with the ghost launch: four
         // CTAs per SM (the tight budget) leave room for it where three do not, which an RHS
-        // pass alone does not show, so the overlapped step always takes the tight budget.
-        for (int t = 1; t < levels; ++t)
+        // pass alone does not show, so the overlapped step takes the tight budget or tighter.
+        best_t[g] = try_fused ? (h->overlap ? 1 : 0) : levels + 1;
+        for (int t = 0; t < nopt; ++t) {
+            const int level = t >= levels ? t - levels : t;
+            if (h->overlap && level < 1) continue;
+            if (h->overlap && t < levels && t != 1) continue;
             if (us[g][t] < us[g][best_t[g]]) best_t[g] = t;
-        if (h->overlap) best_t[g] = 1;
+        }
     }
     const int pick = (nlanes == 2 && us[1][best_t[1]] < 0.95 * us[0][best_t[0]]) ? 1 : 0;
     h->G = lane_opts[pick];
-    for (int t = 0; t < 3; ++t) h->tune_us[t] = us[pick][t] < 1e29 ? us[pick][t] : 0.0;
-    h->budget = best_t[pick];
+    for (int t = 0; t < 3; ++t) h->tune_us[t] = (t < levels && us[pick][t] < 1e29) ? us[pick][t] : 0.0;
+    h->split = best_t[pick] >= levels;
+    h->budget = h->split ? best_t[pick] - levels : best_t[pick];
     h->tight = h->budget >= 1;
     h->launch_counter = c0;
     return sync_check(h);
@@ -983,7 +992,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         h->smem_bytes = std::max(h->smem_bytes, h->mixed ? tile_smem_bytes_mx(h->grid.cap, 2, h->has_tem)
                                                          : tile_smem_bytes(h->grid.cap, 2, h->has_tem));
     // one device block for every array of the solve (one cudaMalloc, one cudaFree)
-    const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles);
+    const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles, h->mixed);
     {
         // pinned scalar copy target (optional: without it the checks copy through pageable memory)
         h->sc_host = pinned_slot();
@@ -1221,7 +1230,8 @@ int lssph_estimate_device_bytes(const lssph_params* pin, int64_t* bytes) {
     const int ntx = (grid.nx + TX - 1) / TX, nty = (grid.ny + TY - 1) / TY;
     std::vector<int32_t> vt_tile, vt_start, vt_vm;
     vm_chunks(grid, ntx, ntx * nty, &vt_tile, &vt_start, &vt_vm);
-    *bytes = solve_bytes(nt, ni, nt - ni, grid.ncell, grid.cap, (int)vt_tile.size(), ntx * nty);
+    *bytes = solve_bytes(nt, ni, nt - ni, grid.ncell, grid.cap, (int)vt_tile.size(), ntx * nty,
+                         p.precision != LSSPH_PRECISION_FP64);
     return LSSPH_OK;
 }
 
@@ -1445,6 +1455,14 @@ int lssph_get_tuning(const lssph_handle* hc, int32_t* lanes, int32_t* tight, dou
     if (tight) *tight = h->budget;
     if (rhs_us_loose) *rhs_us_loose = h->tune_us[0];
     if (rhs_us_tight) *rhs_us_tight = h->tune_us[1];
+    return LSSPH_OK;
+}
+
+int lssph_get_kernel_shape(const lssph_handle* hc, int32_t* split) {
+    if (!hc || !split) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
+    lssph_handle* h = const_cast<lssph_handle*>(hc);   // the measurement is a cache
+    if (const int rc = ensure_tuned(h)) return rc;
+    *split = (h->mixed && h->split) ? 1 : 0;
     return LSSPH_OK;
 }
 

@@ -26,6 +26,7 @@ struct lssph_handle {
     int G = 4, Gg = 4;
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
     bool comp = false;                  // mixed precision with compensated (Kahan) FP32 pair sums
+    bool split = false;                 // mixed precision: pair and solve kernels apart (autotuned)
     bool classical = false;             // SPH_MODEL 1 / 2: kernel-gradient sums, q = 2 PST basis
     int order = 2;                      // Taylor order k of the LS basis (SPH_MODEL 3: 2; 4 / 5 / 6: 3 / 4 / 5)
     bool hi_thread = false;             // order >= 3: thread per particle (else warp per particle)
@@ -33,7 +34,8 @@ struct lssph_handle {
     bool tuned = false;                 // register budget measured (first solo launch)
     bool lanes_auto = false;            // lanes = 0 on an FP64 q = 5 LS solve: 2 or 4 by measurement
     bool tight = false;                 // register budget of stage/PST kernels (autotuned): 4 CTAs/SM or more
-    int budget = 0;                     // 0 loose, 1 tight (4 CTAs/SM), 2 five CTAs/SM (FP64 q = 5 solo)
+    int budget = 0;                     // 0 loose, 1 tight (4 CTAs/SM), 2 five CTAs/SM; the split
+                                        // shape's pair kernel also 3 (768 threads/SM), 4 (1024)
     double tune_us[3] = {0.0, 0.0, 0.0};   // RHS pass time per budget level
     lssph::CellGrid grid;
     lssph::VirtualMarkers vm;
@@ -131,6 +133,50 @@ void postproc_release(lssph_handle* h);
 // lanes = 0 on a handle not yet measured: measure 2 and 4 lanes now (engine.cu), so that a
 // batch member runs the lane count its solo run would.
 int resolve_lanes(lssph_handle* h);
+
+// ---- launch plumbing shared by the engine's translation units ----------------------------
+inline int blocks_for(long n, int per_block) { return (int)((n + per_block - 1) / per_block); }
+
+// Event pair around one launch while profiling; no-op otherwise (and during capture).
+struct ProfScope {
+    lssph_handle* h;
+    size_t slot = (size_t)-1;
+    ProfScope(lssph_handle* hh, int kind) : h(hh) {
+        if (!h->profiling) return;
+        if (h->prof_next + 2 > h->prof_events.size()) {
+            for (int k = 0; k < 64; ++k) {
+                cudaEvent_t e;
+                if (cudaEventCreate(&e) != cudaSuccess) return;
+                h->prof_events.push_back(e);
+            }
+        }
+        slot = h->prof_next;
+        h->prof_next += 2;
+        h->prof_kinds.push_back(kind);
+        cudaEventRecord(h->prof_events[slot], h->stream);
+    }
+    ~ProfScope() {
+        if (slot != (size_t)-1) cudaEventRecord(h->prof_events[slot + 1], h->stream);
+    }
+};
+
+// Where a launch goes: its tile map (NULL: every tile in order), CTA count, stream, and
+// whether it may be a programmatic dependent launch (not right after a fork or join).
+struct Where {
+    const int* tiles;
+    int count;
+    cudaStream_t stream;
+    bool pdl;
+    int priority;   // 0: default
+};
+inline Where all_tiles(const lssph_handle* h) { return Where{nullptr, h->ntiles, h->stream, h->pdl, 0}; }
+
+// Mixed precision, split shape (mixed_split.cu): the pair kernel over the tiles of w, then
+// (after every tile of the stage) the solve kernel over all interior particles.
+void launch_stage_mxp(lssph_handle* h, const StageCfg& S, const Where& w);
+void launch_stage_mxs(lssph_handle* h, const StageCfg& S, cudaStream_t stream, bool pdl);
+void launch_pst_mxp(lssph_handle* h, const Where& w);
+void launch_pst_mxs(lssph_handle* h, cudaStream_t stream, bool pdl);
 
 // Higher-order LS stage and PST launches, SPH_MODEL 4 / 5 / 6 (highorder.cu).  tiles:
 // tile of each CTA (NULL: CTA i runs tile i); while h->preparing they only set the

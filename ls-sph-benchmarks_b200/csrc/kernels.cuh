@@ -110,6 +110,9 @@ struct Work {  // per-interior-particle arrays
     double *rhs_u, *rhs_v, *rhs_rho, *rhs_tem;
     double *f_prev, *src;
     int* key;
+    // mixed precision, split shape: the reduced pair sums of every interior particle, entry e
+    // of particle i at sums[e * num_int + i] (MXS_ENTRIES entries)
+    double* sums;
 };
 struct VMd {   // virtual markers over num_ext
     double *x, *y, *nx, *ny, *u, *v, *pre, *tem, *K;
@@ -500,8 +503,12 @@ constexpr int PPB = LSSPH_PPB;              // particles per pass: a CTA has PPB
 // which is faster depends on how many tiles a launch has, and each handle times both.
 // Level 2 (FP64 single solves only): at most 102 registers, 640 threads per SM, so that a
 // launch of up to 5 CTAs per SM fits one wave.
+// Levels 3 and 4 (768 and 1024 threads per SM: at most 85 and 64 registers) serve the
+// mixed-precision pair kernel of the split shape, which holds no FP64 solve.
 __host__ __device__ constexpr int tile_min_blocks(int G, int tight) {
-    return tight == 2 ? (PPB * G <= 640 ? 640 / (PPB * G) : 1)
+    return tight == 4 ? (PPB * G <= 1024 ? 1024 / (PPB * G) : 1)
+         : tight == 3 ? (PPB * G <= 768 ? 768 / (PPB * G) : 1)
+         : tight == 2 ? (PPB * G <= 640 ? 640 / (PPB * G) : 1)
                       : ((tight && PPB * G <= 512) ? 512 / (PPB * G) : 1);
 }
 static_assert(HC <= 32 && OC <= 32, "tile scans run in one warp");
@@ -704,19 +711,29 @@ __host__ __device__ inline size_t tile_smem_bytes_mx(int cap, int G, bool tem) {
            2 * maxo * sizeof(int) + lists * sizeof(unsigned short);
 }
 
+// The staged arrays of a mixed tile from f on; sums: the reduced-sums rows (or NULL).
 template <bool TEM>
-__device__ __forceinline__ SmemMx smem_view_mx(void* raw, int cap) {
+__device__ __forceinline__ SmemMx smem_view_mx_at(double* sums, float* f, int cap) {
     SmemMx S;
     const int maxp = HC * cap, maxo = OC * cap;
-    double* d = static_cast<double*>(raw);
-    S.sums = d;
-    float* f = reinterpret_cast<float*>(d + PPB * SUMS_MAX);
+    S.sums = sums;
     S.ox = f; S.oy = f + maxp; S.u = f + 2 * maxp; S.v = f + 3 * maxp; S.rho = f + 4 * maxp;
     S.pre = f + 5 * maxp; S.vol = f + 6 * maxp; S.tem = TEM ? f + 7 * maxp : nullptr;
     int* q = reinterpret_cast<int*>(f + (TEM ? 8 : 7) * maxp);
     S.idx = q; S.own_k = q + maxp; S.own_hc = q + maxp + maxo;
     S.nbr = reinterpret_cast<unsigned short*>(q + maxp + 2 * maxo);
     return S;
+}
+
+template <bool TEM>
+__device__ __forceinline__ SmemMx smem_view_mx(void* raw, int cap) {
+    double* d = static_cast<double*>(raw);
+    return smem_view_mx_at<TEM>(d, reinterpret_cast<float*>(d + PPB * SUMS_MAX), cap);
+}
+
+// Shared memory of a pair CTA of the split shape: the mixed tile without the sums rows.
+__host__ __device__ inline size_t tile_smem_bytes_mxp(int cap, int G, bool tem) {
+    return tile_smem_bytes_mx(cap, G, tem) - (size_t)PPB * SUMS_MAX * sizeof(double);
 }
 
 // Field reference values of a staged tile (FP64); offsets are taken against them.
@@ -2216,6 +2233,246 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
 // buffer parities are the solve's base parity xor the launch's parity, so solves that
 // joined the batch at different times keep their own ping-pong state.
 // =======================================================================================
+// =======================================================================================
+// Mixed precision, split shape.  The fused mixed kernels run the FP64 LS solve in the same
+// CTA as the FP32 pair phase, so the solve's registers and the shared-memory rows that hand
+// the sums to it set the occupancy of the whole kernel, and three of a CTA's four warps wait
+// at a barrier while one solves.  The split shape runs
+//   k_stage_mxp / k_pst_mxp   tile staging + FP32 pair phase; each particle's reduced sums
+//                             go to Work::sums (no solve, no barrier after the staging)
+//   k_stage_mxs / k_pst_mxs   one thread per interior particle: FP64 factorisation with
+//                             refinement, RHS, RK update, cell key and scatter (PST: shift,
+//                             interpolation, move)
+// with the same arithmetic per particle as the fused kernels, so both shapes give identical
+// bits and the autotuner may pick either.
+// =======================================================================================
+constexpr int MXS_ENTRIES = 15 + 5 * 5 + 1;   // the widest row: stage with temperature (41)
+static_assert(15 + 5 * 4 + 3 <= MXS_ENTRIES, "PST rows fit");
+
+// Pair phase of one tile (stage, or PST with its shift sums), sums to Work::sums.
+template <int NB, int G, bool COMP, bool PST>
+__device__ __forceinline__ void pairs_mx(const Phys& P, const Fld& cur, const Lst& Lc, const int* __restrict__ gstart,
+                                         const int* __restrict__ glist, const Work& W, Scalars* sc, int ntx, int tile) {
+    constexpr bool TEM = PST ? (NB == 4) : (NB == 5);
+    constexpr int Q = 5;
+    constexpr int NR = 15 + 5 * NB + (PST ? 2 : 0);   // then the neighbour count
+    pdl_wait();
+    bool stop = halted(sc);
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemMx SM = smem_view_mx_at<TEM>(nullptr, reinterpret_cast<float*>(smem_raw), P.cap);
+    const int tx = tile % ntx, ty = tile / ntx;
+    const int cx0 = tx * TX - 1, cy0 = ty * TY - 1;
+    stage_lists<false>(P, Lc, gstart, glist, cx0, cy0, T, SM);
+    stage_fields_mx<TEM>(P, cur, cx0, cy0, T, SM);
+    pdl_release();
+    // one decision per warp: the shuffles below need every lane of it
+    if (__any_sync(0xffffffffu, stop)) return;
+    const int n_own = T.own_off[OC];
+    const int lane = threadIdx.x & (G - 1);
+    const float heff2 = (float)P.h_eff_sq;
+    const PairConst<float> C(P);
+    const size_t N = (size_t)P.num_int;
+    for (int ob = 0; ob < n_own; ob += PPB) {
+        const int slot = (int)threadIdx.x / G;
+        const int o = ob + slot;
+        const bool active = o < n_own;
+        int ki = 0, hc = 0;
+        if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+        const float oxi = SM.ox[ki], oyi = SM.oy[ki];
+        const float my_u = SM.u[ki];
+        float my_v = 0.f, my_rho = 0.f, my_pre = 0.f, my_tem = 0.f;
+        if constexpr (PST || NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
+        if constexpr (!PST && NB >= 4) my_pre = SM.pre[ki];
+        if constexpr (TEM) my_tem = SM.tem[ki];
+        float Mu[15], Mc[15];
+        float B[NB][Q], Bc[NB][Q];
+        float sxy[2] = {0.f, 0.f}, sxc[2] = {0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < 15; ++k) { Mu[k] = 0.f; Mc[k] = 0.f; }
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) { B[c][k] = 0.f; Bc[c][k] = 0.f; }
+        const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2, [&](int k, float xji, float yji) {
+            const float r = sqrtf(xji * xji + yji * yji);
+            const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
+            const float Vj = SM.vol[k];
+            const float VW = Vj * Wv;
+            if constexpr (PST) {   // shift_interpolate_mod.f90:142-146, as pst_body_mx
+                const float dWdr = dev_dW<float>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
+                const float rinv = 1.f / r;
+                const float gx = ((dWdr * (-xji)) * rinv) * Vj;
+                const float gy = ((dWdr * (-yji)) * rinv) * Vj;
+                const float t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
+                const float fac = 1.f + 0.2f * t4;
+                if constexpr (COMP) {
+                    kahan_add(sxy[0], sxc[0], fac * gx);
+                    kahan_add(sxy[1], sxc[1], fac * gy);
+                } else {
+                    sxy[0] = fmaf(fac, gx, sxy[0]);
+                    sxy[1] = fmaf(fac, gy, sxy[1]);
+                }
+            }
+            float a[Q];
+            basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
+            float df[NB];
+            df[0] = SM.u[k] - my_u;
+            if constexpr (PST) {
+                df[1] = SM.v[k] - my_v;
+                df[2] = SM.rho[k] - my_rho;
+                if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
+            } else {
+                if constexpr (NB >= 4) {
+                    df[1] = SM.v[k] - my_v;
+                    df[2] = SM.rho[k] - my_rho;
+                    df[3] = SM.pre[k] - my_pre;
+                }
+                if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
+            }
+            if constexpr (COMP) accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
+            else accumulate_A<NB, float>(Mu, B, VW, a, df);
+        });
+        double Md[15], Bd[NB][Q], sd[2];
+        if constexpr (COMP) {
+            group_reduce_kahan<G>(Mu, Mc, Md);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
+            group_reduce_kahan<G>(sxy, sxc, sd);
+        } else {
+            group_reduce_to<G>(Mu, Md);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+            group_reduce_to<G>(sxy, sd);
+        }
+        if (active) {   // lane l of the particle's G stores entries l, l + G, ...
+            const int i = SM.idx[ki];
+            double* dst = W.sums + i;
+#pragma unroll
+            for (int e = 0; e <= NR; ++e) {
+                if ((e & (G - 1)) != lane) continue;
+                double val;
+                if (e < 15) val = Md[e];
+                else if (e < 15 + 5 * NB) val = Bd[(e - 15) / 5][(e - 15) % 5];
+                else if (e < NR) val = sd[e - 15 - 5 * NB];
+                else val = (double)cnt;
+                dst[(size_t)e * N] = val;
+            }
+        }
+    }
+}
+
+template <int NB, int G, int TIGHT, bool COMP>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
+    k_stage_mxp(const Phys P, const Fld cur, const Lst Lc, const int* __restrict__ gstart,
+                const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
+    pairs_mx<NB, G, COMP, false>(P, cur, Lc, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
+}
+
+template <int NB, int G, int TIGHT, bool COMP>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
+    k_pst_mxp(const Phys P, const Fld cur, const Lst Lc, const int* __restrict__ gstart,
+              const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
+    pairs_mx<NB, G, COMP, true>(P, cur, Lc, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
+}
+
+// Solve and update of the split shape, one thread per interior particle (the tail of
+// stage_body_mx: FP64 factorisation + refinement, RHS, RK update, key, scatter).
+template <int NB>
+__global__ void __launch_bounds__(128) k_stage_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
+                                                   const int* __restrict__ gstart, const Work W, const StageCfg S,
+                                                   Scalars* sc) {
+    pdl_wait();
+    pdl_release();
+    if (__any_sync(0xffffffffu, halted(sc))) return;   // one decision per warp (warp_max_atomic)
+    constexpr int Q = 5;
+    constexpr int NR = 15 + 5 * NB;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double red = 0.0;
+    if (i < P.num_int) {
+        const size_t N = (size_t)P.num_int;
+        double row[NR];
+#pragma unroll
+        for (int e = 0; e < NR; ++e) row[e] = W.sums[(size_t)e * N + i];
+        const int cnt = (int)W.sums[(size_t)NR * N + i];
+        const double my_x = cur.x[i], my_y = cur.y[i], my_u = cur.u[i];
+        double my_v = 0.0, my_rho = 0.0, my_tem = 0.0;
+        if constexpr (NB >= 4) { my_v = cur.v[i]; my_rho = cur.rho[i]; }
+        if constexpr (NB == 5) my_tem = cur.tem[i];
+        solve_row_refined<Q, NB, true>(P, row, cnt, sc);
+        double d[NB][Q];
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) d[c][k] = row[15 + 5 * c + k];
+        double Ru, Rv, Rr, Rt;
+        rhs_ls<NB>(P, W, i, my_rho, my_tem, d, Ru, Rv, Rr, Rt);
+        red = stage_advance<NB>(P, nxt, Ln, gstart, W, S, sc, i, my_x, my_y, my_u, my_v, my_rho, my_tem, Ru, Rv,
+                                Rr, Rt);
+    }
+    if (S.mode == MODE_STAGE && S.last && (S.do_umax || S.do_steady))
+        warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
+}
+
+// Shift, solve, interpolation and move of the split shape's PST, one thread per interior
+// particle (the tail of pst_body_mx).  NB = 3 (u, v, rho) or 4 (+ T).
+template <int NB>
+__global__ void __launch_bounds__(128) k_pst_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
+                                                 const int* __restrict__ gstart, const Work W, Scalars* sc) {
+    pdl_wait();
+    pdl_release();
+    if (halted(sc)) return;
+    constexpr int Q = 5;
+    constexpr int NR = 15 + 5 * NB;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.num_int) return;
+    const size_t N = (size_t)P.num_int;
+    double row[NR];
+#pragma unroll
+    for (int e = 0; e < NR; ++e) row[e] = W.sums[(size_t)e * N + i];
+    const double sx = W.sums[(size_t)NR * N + i], sy = W.sums[(size_t)(NR + 1) * N + i];
+    const int cnt = (int)W.sums[(size_t)(NR + 2) * N + i];
+    const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
+    const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
+    const double my_x = cur.x[i], my_y = cur.y[i], my_u = cur.u[i], my_v = cur.v[i], my_rho = cur.rho[i];
+    double my_tem = 0.0;
+    if constexpr (NB == 4) my_tem = cur.tem[i];
+    // shift vector, clamped to 0.2 h (shift_interpolate_mod.f90:216-225)
+    double dx = -coe * sx, dy = -coe * sy;
+    const double rr = sqrt(dx * dx + dy * dy);
+    if (rr > 0.2 * P.h) {
+        dx = ((0.2 * P.h) * dx) / rr;
+        dy = ((0.2 * P.h) * dy) / rr;
+    }
+    solve_row_refined<Q, NB, false>(P, row, cnt, sc);
+    // interpolation a(dr) . d (shift_interpolate_mod.f90:255-298)
+    double a[Q];
+    basis_A(P, dx, dy, a);
+    double acc[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        double sacc = 0.0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) sacc = fma(a[k], row[15 + 5 * c + k], sacc);
+        acc[c] = sacc;
+    }
+    double xn = my_x + dx, yn = my_y + dy;
+    if (P.periodic) { xn = wrap_pos(xn, P.Lx); yn = wrap_pos(yn, P.Lx); }
+    const double un = my_u + acc[0], vn = my_v + acc[1], rn = my_rho + acc[2];
+    nxt.x[i] = xn; nxt.y[i] = yn; nxt.u[i] = un; nxt.v[i] = vn; nxt.rho[i] = rn;
+    nxt.pre[i] = P.c_sq * (rn - P.rho_ref);
+    nxt.vol[i] = P.SP_mass / rn;
+    bool finite = isfinite(xn) && isfinite(yn) && isfinite(un) && isfinite(vn) && isfinite(rn);
+    if constexpr (NB == 4) { const double tn = my_tem + acc[3]; nxt.tem[i] = tn; finite = finite && isfinite(tn); }
+    if (!finite) atomicOr(&sc->err, ERR_NONFINITE);
+    const int nk = cell_key_mul(P, xn, yn, sc);
+    if (nk >= 0) {
+        W.key[i] = nk;
+        if (P.split_pos) put_split_pos(P, nxt, i, xn, yn, nk);
+    }
+    scatter_to_cell(P, Ln, gstart, nk, i, sc);
+}
+
 struct SolveDesc {
     Phys P;
     Fld F[2];

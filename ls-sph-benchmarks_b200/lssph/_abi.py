@@ -170,6 +170,7 @@ _PROTOS = {
     "lssph_get_progress": (C.c_int, [_H, _i, _i]),
     "lssph_get_schedule": (C.c_int, [_H, _i, _i, _i]),
     "lssph_get_tuning": (C.c_int, [_H, _i, _i, _P(C.c_double), _P(C.c_double)]),
+    "lssph_get_kernel_shape": (C.c_int, [_H, _i]),
     "lssph_step_profiled": (C.c_int, [_H, C.c_int32, _d, _P(C.c_int64)]),
     "lssph_batch_create": (C.c_int, [_P(C.c_void_p)]),
     "lssph_batch_destroy": (None, [_H]),

@@ -267,7 +267,10 @@ class Simulation:
         self._chk(self._lib.lssph_get_tuning(self._h, C.byref(lanes), C.byref(tight), C.byref(lo), C.byref(ti)))
         nt, ni, ov = C.c_int32(), C.c_int32(), C.c_int32()
         self._chk(self._lib.lssph_get_schedule(self._h, C.byref(nt), C.byref(ni), C.byref(ov)))
-        return {"lanes": lanes.value, "register_budget": ("loose", "tight", "five")[tight.value],
+        shape = C.c_int32()
+        self._chk(self._lib.lssph_get_kernel_shape(self._h, C.byref(shape)))
+        return {"lanes": lanes.value, "register_budget": ("loose", "tight", "five", "six", "eight")[tight.value],
+                "shape": "split" if shape.value else "fused",
                 "rhs_us_loose": lo.value, "rhs_us_tight": ti.value, "tiles": nt.value,
                 "interior_tiles": ni.value, "ghost_overlap": bool(ov.value)}
 

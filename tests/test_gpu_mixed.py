@@ -182,3 +182,21 @@ def test_split_precision_positions_follow_the_fp64_positions():
     ga, gc = a.download(), c.download()
     for k in _fields(p):
         assert np.array_equal(getattr(ga, k), getattr(gc, k)), k
+
+
+@pytest.mark.parametrize("prec", [lssph.PRECISION_MIXED, lssph.PRECISION_MIXED_COMPENSATED])
+@pytest.mark.parametrize("case", list(CASES))
+def test_split_and_fused_shapes_give_identical_bits(case, prec, monkeypatch):
+    # the split shape (pair kernel, then one solve-and-update thread per particle) runs the
+    # fused kernels' arithmetic per particle: same bits, every field, stages and PST
+    mk, _ = CASES[case]
+    out = {}
+    for shape in ("fused", "split"):
+        monkeypatch.setenv("LSSPH_MIXED_SHAPE", shape)
+        sim = _sim(lssph.make_params(mk(), lanes=4), prec, seed=4)
+        sim.step(6)
+        assert sim.tuning()["shape"] == shape
+        out[shape] = sim.download()
+        sim.close()
+    for k in _fields(mk()):
+        assert np.array_equal(getattr(out["fused"], k), getattr(out["split"], k)), k
