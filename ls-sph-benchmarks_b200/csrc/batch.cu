@@ -48,6 +48,11 @@ struct BatchGroup {
     int2* chunks = nullptr;        // (solve, chunk) per CTA of ghost launches
     int ntiles = 0, nchunks = 0;
     bool tight = false;            // register budget of the stage / PST kernels
+    bool split = false;            // mixed precision: pair kernel, then solve kernel (split shape)
+    int split_budget = 1;          // budget level of the split shape's pair kernel (1-4)
+    int2* blocks = nullptr;        // (solve, block of 128 interior particles) per solve-kernel CTA
+    int nblocks = 0;
+    int cap_max = 0;               // largest cell slot capacity of the members (pair-kernel smem)
     size_t smem = 0, smem_ghost = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t join = nullptr;
@@ -128,7 +133,49 @@ void dispatch_kind(const BatchGroup& g, F&& f) {
     else dispatch_lanes(g.G, [&](auto GG) { f(GG, std::integral_constant<int, 0>{}); });
 }
 
+// Split shape: the pair kernel at the group's budget level (prep: every level), then the
+// solve kernel over the group's particle blocks.
+template <int NB, bool PST>
+void launch_split(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
+    constexpr bool TEM = PST ? (NB == 4) : (NB == 5);
+    auto run = [&](auto GG, auto Cc) {
+        constexpr int G = decltype(GG)::value;
+        constexpr bool COMP = decltype(Cc)::value;
+        auto kern_at = [](int t) {
+            switch (t) {
+                case 1: return kb_pairs_mx<NB, G, 1, COMP, PST>;
+                case 2: return kb_pairs_mx<NB, G, 2, COMP, PST>;
+                case 3: return kb_pairs_mx<NB, G, 3, COMP, PST>;
+                default: return kb_pairs_mx<NB, G, 4, COMP, PST>;
+            }
+        };
+        if (prep) {
+            for (int t = 1; t <= 4; ++t) optin(kern_at(t));
+            return;
+        }
+        const size_t smem = tile_smem_bytes_mxp(g.cap_max, G, TEM);
+        launch_kernel(g.pdl, kern_at(g.split_budget), g.ntiles, PPB * G, smem, g.stream, g.D,
+                      BatchMap{g.tiles, g.tstep, g.sbf, g.lba}, ps, pl);
+        launch_kernel(g.pdl, kb_solve_mx<NB, PST>, g.nblocks, 128, 0, g.stream, g.D,
+                      BatchMap{g.blocks, g.tstep, g.sbf, g.lba}, S, ps, pl);
+        *count += 2;
+    };
+    if (g.comp) {
+        if (g.G == 2) run(std::integral_constant<int, 2>{}, std::true_type{});
+        else run(std::integral_constant<int, 4>{}, std::true_type{});
+    } else {
+        if (g.G == 2) run(std::integral_constant<int, 2>{}, std::false_type{});
+        else run(std::integral_constant<int, 4>{}, std::false_type{});
+    }
+}
+
 void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
+    if (g.split) {
+        if (g.nb == 1) launch_split<1, false>(g, S, ps, pl, prep, count);
+        else if (g.nb == 5) launch_split<5, false>(g, S, ps, pl, prep, count);
+        else launch_split<4, false>(g, S, ps, pl, prep, count);
+        return;
+    }
     dispatch_kind(g, [&](auto GG, auto MXc) {
         constexpr int G = decltype(GG)::value;
         constexpr int MX = decltype(MXc)::value;
@@ -166,6 +213,12 @@ void launch_ghost(const BatchGroup& g, int ps, int pl, int zero_other, int reset
 }
 
 void launch_pst(const BatchGroup& g, int ps, int pl, bool prep, int* count) {
+    if (g.split) {
+        const StageCfg S{};
+        if (g.nb == 5) launch_split<4, true>(g, S, ps, pl, prep, count);
+        else launch_split<3, true>(g, S, ps, pl, prep, count);
+        return;
+    }
     dispatch_kind(g, [&](auto GG, auto MXc) {
         constexpr int G = decltype(GG)::value;
         constexpr int MX = decltype(MXc)::value;
@@ -254,6 +307,7 @@ void release_groups(lssph_batch* b) {
         cudaFree(g.D);
         cudaFree(g.tiles);
         cudaFree(g.chunks);
+        cudaFree(g.blocks);
         if (g.join) cudaEventDestroy(g.join);
         if (g.stream) cudaStreamDestroy(g.stream);
     }
@@ -312,12 +366,19 @@ int rebuild(lssph_batch* b) {
     std::vector<SolveDesc> all;
     for (auto& g : b->groups) {
         std::vector<SolveDesc> desc;
-        std::vector<int2> tiles, chunks;
+        std::vector<int2> tiles, chunks, blocks;
         for (size_t s = 0; s < g.members.size(); ++s) {
             const lssph_handle* h = b->members[g.members[s]];
             desc.push_back(make_desc(h));
             for (int t = 0; t < h->ntiles; ++t) tiles.push_back(make_int2((int)s, t));
             for (int c = 0; c < std::max(h->nvt, 1); ++c) chunks.push_back(make_int2((int)s, c));
+            for (int k = 0; k < (h->num_int + 127) / 128; ++k) blocks.push_back(make_int2((int)s, k));
+            g.cap_max = std::max(g.cap_max, h->grid.cap);
+            // the split shape (identical results) once any member measured it faster alone
+            if (h->mixed && h->split) {
+                g.split = true;
+                g.split_budget = std::max(g.split_budget, std::max(h->budget, 1));
+            }
             g.smem = std::max(g.smem, h->smem_bytes);
             g.smem_ghost = std::max(g.smem_ghost, h->smem_ghost);
             g.tight = g.tight || h->tight;
@@ -325,11 +386,18 @@ int rebuild(lssph_batch* b) {
         // the tight budget wins once a launch has more tiles than fit at the loose one
         // (3 CTAs per SM); a member that chose it alone keeps it in the group
         g.tight = g.tight || tiles.size() > kTightTiles;
+        // mixed precision: a launch past two loose waves is in the throughput regime, where
+        // the split shape's occupancy pays (cavity 256^2: 282 vs 317 us per step)
+        if (g.mixed && tiles.size() > kTightTiles) {
+            g.split = true;
+            g.split_budget = std::max(g.split_budget, 2);
+        }
         g.ntiles = (int)tiles.size();
         g.nchunks = (int)chunks.size();
         int rc;
+        g.nblocks = (int)blocks.size();
         if ((rc = upload(b, &g.D, desc)) != LSSPH_OK || (rc = upload(b, &g.tiles, tiles)) != LSSPH_OK ||
-            (rc = upload(b, &g.chunks, chunks)) != LSSPH_OK)
+            (rc = upload(b, &g.chunks, chunks)) != LSSPH_OK || (rc = upload(b, &g.blocks, blocks)) != LSSPH_OK)
             return rc;
         BATCH_TRY(b, cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
         BATCH_TRY(b, cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));

@@ -2379,15 +2379,14 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
 // Solve and update of the split shape, one thread per interior particle (the tail of
 // stage_body_mx: FP64 factorisation + refinement, RHS, RK update, key, scatter).
 template <int NB>
-__global__ void __launch_bounds__(128) k_stage_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
-                                                   const int* __restrict__ gstart, const Work W, const StageCfg S,
-                                                   Scalars* sc) {
+__device__ __forceinline__ void stage_solve_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
+                                               const int* __restrict__ gstart, const Work& W, const StageCfg& S,
+                                               Scalars* sc, int i) {
     pdl_wait();
     pdl_release();
     if (__any_sync(0xffffffffu, halted(sc))) return;   // one decision per warp (warp_max_atomic)
     constexpr int Q = 5;
     constexpr int NR = 15 + 5 * NB;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double red = 0.0;
     if (i < P.num_int) {
         const size_t N = (size_t)P.num_int;
@@ -2414,17 +2413,23 @@ __global__ void __launch_bounds__(128) k_stage_mxs(const Phys P, const Fld cur, 
         warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
 }
 
+template <int NB>
+__global__ void __launch_bounds__(128) k_stage_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
+                                                   const int* __restrict__ gstart, const Work W, const StageCfg S,
+                                                   Scalars* sc) {
+    stage_solve_mx<NB>(P, cur, nxt, Ln, gstart, W, S, sc, (int)(blockIdx.x * blockDim.x + threadIdx.x));
+}
+
 // Shift, solve, interpolation and move of the split shape's PST, one thread per interior
 // particle (the tail of pst_body_mx).  NB = 3 (u, v, rho) or 4 (+ T).
 template <int NB>
-__global__ void __launch_bounds__(128) k_pst_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
-                                                 const int* __restrict__ gstart, const Work W, Scalars* sc) {
+__device__ __forceinline__ void pst_solve_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
+                                             const int* __restrict__ gstart, const Work& W, Scalars* sc, int i) {
     pdl_wait();
     pdl_release();
     if (halted(sc)) return;
     constexpr int Q = 5;
     constexpr int NR = 15 + 5 * NB;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.num_int) return;
     const size_t N = (size_t)P.num_int;
     double row[NR];
@@ -2471,6 +2476,12 @@ __global__ void __launch_bounds__(128) k_pst_mxs(const Phys P, const Fld cur, co
         if (P.split_pos) put_split_pos(P, nxt, i, xn, yn, nk);
     }
     scatter_to_cell(P, Ln, gstart, nk, i, sc);
+}
+
+template <int NB>
+__global__ void __launch_bounds__(128) k_pst_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
+                                                 const int* __restrict__ gstart, const Work W, Scalars* sc) {
+    pst_solve_mx<NB>(P, cur, nxt, Ln, gstart, W, sc, (int)(blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 struct SolveDesc {
@@ -2547,6 +2558,37 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(con
     batch_parity(M, d, ps, pl, sb, lb);
     pst_body<NB, G, MIXED>(d.P, d.F[sb], d.F[sb ^ 1], d.L[lb], d.L[next_list(lb)], d.gstart, d.glist, d.W, d.sc,
                            d.ntx, m.y);
+}
+
+// Mixed precision, split shape, batched: the pair kernel over a group's (solve, tile) map and
+// the solve kernel over its (solve, block of 128 interior particles) map.
+template <int NB, int G, int TIGHT, bool COMP, bool PST>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pairs_mx(const SolveDesc* __restrict__ D,
+                                                                                  const BatchMap M, int ps, int pl) {
+    __shared__ SolveDesc sd;
+    const int2 m = M.cta[blockIdx.x];
+    const SolveDesc& d = load_desc(D, m.x, sd);
+    int sb, lb;
+    batch_parity(M, d, ps, pl, sb, lb);
+    pairs_mx<NB, G, COMP, PST>(d.P, d.F[sb], d.L[lb], d.gstart, d.glist, d.W, d.sc, d.ntx, m.y);
+}
+
+template <int NB, bool PST>
+__global__ void __launch_bounds__(128) kb_solve_mx(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
+                                                   int ps, int pl) {
+    __shared__ SolveDesc sd;
+    const int2 m = M.cta[blockIdx.x];
+    const SolveDesc& d = load_desc(D, m.x, sd);
+    int sb, lb;
+    batch_parity(M, d, ps, pl, sb, lb);
+    const int i = m.y * 128 + (int)threadIdx.x;
+    if constexpr (PST) {
+        pst_solve_mx<NB>(d.P, d.F[sb], d.F[sb ^ 1], d.L[next_list(lb)], d.gstart, d.W, d.sc, i);
+    } else {
+        S.dt1 = d.dt1[S.stage - 1];
+        S.dt2 = d.dt2[S.stage - 1];
+        stage_solve_mx<NB>(d.P, d.F[sb], d.F[sb ^ 1], d.L[next_list(lb)], d.gstart, d.W, S, d.sc, i);
+    }
 }
 
 // =======================================================================================

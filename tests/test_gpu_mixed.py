@@ -200,3 +200,24 @@ def test_split_and_fused_shapes_give_identical_bits(case, prec, monkeypatch):
         sim.close()
     for k in _fields(mk()):
         assert np.array_equal(getattr(out["fused"], k), getattr(out["split"], k)), k
+
+
+def test_split_batch_members_identical_alone():
+    # a mixed batch group past two loose waves of tiles runs the split shape (batched pair
+    # kernel over (solve, tile), solve kernel over (solve, particle block)); each member still
+    # ends bit for bit as it does alone
+    mk = [lambda: lssph.make_params(lssph.cavity_params(num=128), lanes=4),
+          lambda: lssph.make_params(lssph.taylor_green_params(num=128), lanes=4),
+          lambda: lssph.make_params(lssph.boussinesq_params(num=96), lanes=4)]
+    solo = [_sim(f(), lssph.PRECISION_MIXED, seed=i) for i, f in enumerate(mk)]
+    mem = [_sim(f(), lssph.PRECISION_MIXED, seed=i) for i, f in enumerate(mk)]
+    with lssph.Batch() as b:
+        for m in mem:
+            b.add(m)
+        b.step(4)
+    for s in solo:
+        s.step(4)
+    for s, m in zip(solo, mem):
+        gs, gm = s.download(), m.download()
+        for k in _fields(s.params):
+            assert np.array_equal(getattr(gs, k), getattr(gm, k)), k
