@@ -237,10 +237,12 @@ int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32
    measurement; it never changes a result. */
 int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
                      double* rhs_us_tight);
-/* Shape of the mixed-precision stage and PST (no counterpart in the reference): 1 split (an
-   FP32 pair kernel, then an FP64 solve-and-update kernel per particle), 0 fused (one
-   kernel), as the handle's first-launch measurement picked it; FP64 solves report 0.  Both
-   shapes compute identical results. */
+/* Shape of the q = 5 LS stage and PST kernels, FP64 or mixed precision (no counterpart in
+   the reference): 1 split (a pair kernel over the cell tiles, FP64 or FP32, then an FP64
+   solve-and-update kernel with one thread per particle), 0 fused (one kernel), as the
+   handle's first-launch measurement picked it (LSSPH_KERNEL_SHAPE=fused|split fixes it).
+   Solves at 1 or 8 lanes and the other SPH models run fused.  Both shapes compute
+   identical results. */
 int lssph_get_kernel_shape(const lssph_handle* h, int32_t* split);
 
 /* Time-step schedule (no counterpart in the reference): cell tiles, the tiles whose halo

@@ -16,7 +16,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "liblssph.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 
-SOURCES = ["host.cpp", "engine.cu", "mixed_split.cu", "batch.cu", "noalloc.cu", "highorder.cu", "postproc.cu",
+SOURCES = ["host.cpp", "engine.cu", "split_shape.cu", "batch.cu", "noalloc.cu", "highorder.cu", "postproc.cu",
            "snapshot.cu"]
 HEADERS = ["engine.h", "handle.h", "hostmem.h", "kernels.cuh", "kernels_hi.cuh"]
 

@@ -134,39 +134,49 @@ void dispatch_kind(const BatchGroup& g, F&& f) {
 }
 
 // Split shape: the pair kernel at the group's budget level (prep: every level), then the
-// solve kernel over the group's particle blocks.
+// solve kernel over the group's particle blocks.  MX: 0 FP64, 1 mixed, 2 mixed with
+// compensated sums.
 template <int NB, bool PST>
 void launch_split(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
     constexpr bool TEM = PST ? (NB == 4) : (NB == 5);
-    auto run = [&](auto GG, auto Cc) {
+    auto run = [&](auto GG, auto MXc) {
         constexpr int G = decltype(GG)::value;
-        constexpr bool COMP = decltype(Cc)::value;
+        constexpr int MX = decltype(MXc)::value;
         auto kern_at = [](int t) {
-            switch (t) {
-                case 1: return kb_pairs_mx<NB, G, 1, COMP, PST>;
-                case 2: return kb_pairs_mx<NB, G, 2, COMP, PST>;
-                case 3: return kb_pairs_mx<NB, G, 3, COMP, PST>;
-                default: return kb_pairs_mx<NB, G, 4, COMP, PST>;
+            if constexpr (MX == 0) {
+                switch (t) {
+                    case 1: return kb_pairs_fp<NB, G, 1, PST>;
+                    case 2: return kb_pairs_fp<NB, G, 2, PST>;
+                    case 3: return kb_pairs_fp<NB, G, 3, PST>;
+                    default: return kb_pairs_fp<NB, G, 4, PST>;
+                }
+            } else {
+                switch (t) {
+                    case 1: return kb_pairs_mx<NB, G, 1, MX == 2, PST>;
+                    case 2: return kb_pairs_mx<NB, G, 2, MX == 2, PST>;
+                    case 3: return kb_pairs_mx<NB, G, 3, MX == 2, PST>;
+                    default: return kb_pairs_mx<NB, G, 4, MX == 2, PST>;
+                }
             }
         };
         if (prep) {
             for (int t = 1; t <= 4; ++t) optin(kern_at(t));
             return;
         }
-        const size_t smem = tile_smem_bytes_mxp(g.cap_max, G, TEM);
+        const size_t smem = MX == 0 ? tile_smem_bytes_fpp(g.cap_max, G, TEM) : tile_smem_bytes_mxp(g.cap_max, G, TEM);
         launch_kernel(g.pdl, kern_at(g.split_budget), g.ntiles, PPB * G, smem, g.stream, g.D,
                       BatchMap{g.tiles, g.tstep, g.sbf, g.lba}, ps, pl);
-        launch_kernel(g.pdl, kb_solve_mx<NB, PST>, g.nblocks, 128, 0, g.stream, g.D,
+        launch_kernel(g.pdl, kb_solve<NB, PST, (MX != 0)>, g.nblocks, 128, 0, g.stream, g.D,
                       BatchMap{g.blocks, g.tstep, g.sbf, g.lba}, S, ps, pl);
         *count += 2;
     };
-    if (g.comp) {
-        if (g.G == 2) run(std::integral_constant<int, 2>{}, std::true_type{});
-        else run(std::integral_constant<int, 4>{}, std::true_type{});
-    } else {
-        if (g.G == 2) run(std::integral_constant<int, 2>{}, std::false_type{});
-        else run(std::integral_constant<int, 4>{}, std::false_type{});
-    }
+    auto lanes = [&](auto MXc) {
+        if (g.G == 2) run(std::integral_constant<int, 2>{}, MXc);
+        else run(std::integral_constant<int, 4>{}, MXc);
+    };
+    if (!g.mixed) lanes(std::integral_constant<int, 0>{});
+    else if (g.comp) lanes(std::integral_constant<int, 2>{});
+    else lanes(std::integral_constant<int, 1>{});
 }
 
 void launch_stage(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool prep, int* count) {
@@ -367,6 +377,9 @@ int rebuild(lssph_batch* b) {
     for (auto& g : b->groups) {
         std::vector<SolveDesc> desc;
         std::vector<int2> tiles, chunks, blocks;
+        // the split shape needs every member's Work::sums and exists at 2 and 4 lanes
+        bool can_split = g.G == 2 || g.G == 4;
+        for (size_t s = 0; s < g.members.size(); ++s) can_split = can_split && b->members[g.members[s]]->has_sums;
         for (size_t s = 0; s < g.members.size(); ++s) {
             const lssph_handle* h = b->members[g.members[s]];
             desc.push_back(make_desc(h));
@@ -375,7 +388,7 @@ int rebuild(lssph_batch* b) {
             for (int k = 0; k < (h->num_int + 127) / 128; ++k) blocks.push_back(make_int2((int)s, k));
             g.cap_max = std::max(g.cap_max, h->grid.cap);
             // the split shape (identical results) once any member measured it faster alone
-            if (h->mixed && h->split) {
+            if (can_split && h->split) {
                 g.split = true;
                 g.split_budget = std::max(g.split_budget, std::max(h->budget, 1));
             }
@@ -388,7 +401,7 @@ int rebuild(lssph_batch* b) {
         g.tight = g.tight || tiles.size() > kTightTiles;
         // mixed precision: a launch past two loose waves is in the throughput regime, where
         // the split shape's occupancy pays (cavity 256^2: 282 vs 317 us per step)
-        if (g.mixed && tiles.size() > kTightTiles) {
+        if (can_split && g.mixed && tiles.size() > kTightTiles) {
             g.split = true;
             g.split_budget = std::max(g.split_budget, 2);
         }

@@ -100,7 +100,7 @@ void visit_solve_arrays(lssph_handle* h, size_t N, size_t NI, size_t NE, size_t 
     A(&W.x_acc, NI); A(&W.y_acc, NI); A(&W.u_acc, NI); A(&W.v_acc, NI); A(&W.rho_acc, NI); A(&W.tem_acc, NI);
     A(&W.rhs_u, NI); A(&W.rhs_v, NI); A(&W.rhs_rho, NI); A(&W.rhs_tem, NI);
     A(&W.f_prev, NI); A(&W.src, NI); A(&W.key, NI);
-    A(&W.sums, h->mixed ? NI * MXS_ENTRIES : 0);   // mixed precision, split shape
+    A(&W.sums, h->has_sums ? NI * MXS_ENTRIES : 0);   // the split shape's pair sums
     VMd& V = h->V;
     A(&V.x, NE); A(&V.y, NE); A(&V.nx, NE); A(&V.ny, NE); A(&V.u, NE); A(&V.v, NE); A(&V.pre, NE); A(&V.tem, NE);
     A(&V.K, NE); A(&V.ptype, NE); A(&V.key, NE); A(&V.mode, NE);
@@ -142,9 +142,9 @@ void vm_chunks(const CellGrid& g, int ntx, int ntiles, std::vector<int32_t>* til
 
 // Size of the single device block of a solve of these sizes (every array holds at least
 // one element and starts on a 256-byte boundary).
-int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, int ntiles, bool mixed) {
+int64_t solve_bytes(size_t N, size_t NI, size_t NE, size_t NC, int cap, int nvt, int ntiles, bool sums) {
     lssph_handle layout;
-    layout.mixed = mixed;
+    layout.has_sums = sums;
     size_t total = 0;
     visit_solve_arrays(&layout, N, NI, NE, NC, cap, nvt, ntiles, [&](auto** p, size_t n) { total += array_bytes(p, n); });
     return (int64_t)total;
@@ -217,14 +217,14 @@ void launch_stage(lssph_handle* h, const StageCfg& S, const Where& w) {
 // The stage kernel over the tiles of w.  In the split shape this is the pair kernel only:
 // launch_stage_tail then runs the solve kernel once every tile of the stage is done.
 void launch_stage_any(lssph_handle* h, const StageCfg& S, const Where& w) {
-    if (h->mixed && h->split) { launch_stage_mxp(h, S, w); return; }
+    if (h->split) { launch_stage_pairs(h, S, w); return; }
     if (h->nb_rhs == 1) launch_stage<1>(h, S, w);
     else if (h->nb_rhs == 5) launch_stage<5>(h, S, w);
     else launch_stage<4>(h, S, w);
 }
 
 void launch_stage_tail(lssph_handle* h, const StageCfg& S, bool pdl) {
-    if (h->mixed && h->split) launch_stage_mxs(h, S, h->stream, pdl);
+    if (h->split) launch_stage_solve(h, S, h->stream, pdl);
 }
 
 // A whole stage (every tile, then the split shape's solve kernel).
@@ -338,13 +338,13 @@ void launch_pst_t(lssph_handle* h, const Where& w) {
 }
 
 void launch_pst_any(lssph_handle* h, const Where& w) {
-    if (h->mixed && h->split) { launch_pst_mxp(h, w); return; }
+    if (h->split) { launch_pst_pairs(h, w); return; }
     if (h->has_tem) launch_pst_t<4>(h, w);
     else launch_pst_t<3>(h, w);
 }
 
 void launch_pst_tail(lssph_handle* h, bool pdl) {
-    if (h->mixed && h->split) launch_pst_mxs(h, h->stream, pdl);
+    if (h->split) launch_pst_solve(h, h->stream, pdl);
 }
 
 // ---- operator sequences (enqueue only) -----------------------------------------------------
@@ -403,9 +403,9 @@ void prepare_kernels(lssph_handle* h) {
     launch_stage_any(h, S);
     launch_ghost(h);
     launch_pst_any(h, all_tiles(h));
-    if (h->mixed) {   // the split shape the measurement may pick
-        launch_stage_mxp(h, S, all_tiles(h));
-        launch_pst_mxp(h, all_tiles(h));
+    if (split_capable(h)) {   // the split shape the measurement may pick
+        launch_stage_pairs(h, S, all_tiles(h));
+        launch_pst_pairs(h, all_tiles(h));
     }
     h->preparing = false;
 }
@@ -495,19 +495,27 @@ int autotune(lssph_handle* h) {
     const int64_t c0 = h->launch_counter;
     // level 2 (five CTAs per SM) exists for the q = 5 LS stage and PST kernels
     const int levels = (!h->classical && h->order == 2) ? 3 : 2;
-    // mixed precision may also run split (pair kernel, then solve kernel): budget levels 0-4
-    // of its pair kernel.  LSSPH_MIXED_SHAPE = fused / split restricts the choice.
-    const char* shape = std::getenv("LSSPH_MIXED_SHAPE");
-    const bool try_fused = !(h->mixed && shape && std::strcmp(shape, "split") == 0);
-    const bool try_split = h->mixed && !(shape && std::strcmp(shape, "fused") == 0);
-    // LSSPH_REGISTER_BUDGET = loose / tight / five: skip the timing
+    // the q = 5 LS kernels at 2 or 4 lanes may also run split (pair kernel, then solve
+    // kernel): budget levels 0-4 of the pair kernel.  LSSPH_KERNEL_SHAPE = fused / split
+    // restricts the choice.
+    const char* shape = std::getenv("LSSPH_KERNEL_SHAPE");
+    const bool can_split = split_capable(h);
+    const bool try_fused = !(can_split && shape && std::strcmp(shape, "split") == 0);
+    const bool try_split = can_split && !(shape && std::strcmp(shape, "fused") == 0);
+    // LSSPH_REGISTER_BUDGET = loose / tight / five (/ six / eight: the split shape's 768 and
+    // 1024 threads per SM): skip the timing
     const char* force = std::getenv("LSSPH_REGISTER_BUDGET");
-    if (force && (std::strcmp(force, "loose") == 0 || std::strcmp(force, "tight") == 0 ||
-                  std::strcmp(force, "five") == 0)) {
-        h->budget = std::strcmp(force, "loose") == 0 ? 0 : (std::strcmp(force, "tight") == 0 ? 1 : levels - 1);
-        h->tight = h->budget >= 1;
-        h->split = !try_fused;
-        return LSSPH_OK;
+    if (force) {
+        static const char* const names[5] = {"loose", "tight", "five", "six", "eight"};
+        int level = -1;
+        for (int t = 0; t < 5; ++t)
+            if (std::strcmp(force, names[t]) == 0) level = t;
+        if (level >= 0) {
+            h->split = !try_fused;
+            h->budget = std::min(level, h->split ? 4 : levels - 1);
+            h->tight = h->budget >= 1;
+            return LSSPH_OK;
+        }
     }
     // lanes = 0 on a q = 5 LS solve: 4 lanes per particle unless 2 lanes run the RHS
     // pass at least 5 % faster (the margin keeps the pick, and with it the summation order,
@@ -873,6 +881,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->comp = h->p.precision == LSSPH_PRECISION_MIXED_COMPENSATED;
     h->classical = h->p.sph_model <= 2;
     h->order = h->p.sph_model >= 4 ? h->p.sph_model - 1 : 2;   // LSSPH_A_mod.f90:46-56
+    h->has_sums = split_sums(h->p);
     {
         // Higher-order kernel shape, measured on B200 (Taylor-Green 128^2 / 256^2, closed
         // box and periodic): thread per particle is faster for q = 9 (1.5-1.6x) and q = 14
@@ -992,7 +1001,7 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         h->smem_bytes = std::max(h->smem_bytes, h->mixed ? tile_smem_bytes_mx(h->grid.cap, 2, h->has_tem)
                                                          : tile_smem_bytes(h->grid.cap, 2, h->has_tem));
     // one device block for every array of the solve (one cudaMalloc, one cudaFree)
-    const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles, h->mixed);
+    const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles, h->has_sums);
     {
         // pinned scalar copy target (optional: without it the checks copy through pageable memory)
         h->sc_host = pinned_slot();
@@ -1230,8 +1239,7 @@ int lssph_estimate_device_bytes(const lssph_params* pin, int64_t* bytes) {
     const int ntx = (grid.nx + TX - 1) / TX, nty = (grid.ny + TY - 1) / TY;
     std::vector<int32_t> vt_tile, vt_start, vt_vm;
     vm_chunks(grid, ntx, ntx * nty, &vt_tile, &vt_start, &vt_vm);
-    *bytes = solve_bytes(nt, ni, nt - ni, grid.ncell, grid.cap, (int)vt_tile.size(), ntx * nty,
-                         p.precision != LSSPH_PRECISION_FP64);
+    *bytes = solve_bytes(nt, ni, nt - ni, grid.ncell, grid.cap, (int)vt_tile.size(), ntx * nty, split_sums(p));
     return LSSPH_OK;
 }
 
@@ -1462,7 +1470,7 @@ int lssph_get_kernel_shape(const lssph_handle* hc, int32_t* split) {
     if (!hc || !split) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
     lssph_handle* h = const_cast<lssph_handle*>(hc);   // the measurement is a cache
     if (const int rc = ensure_tuned(h)) return rc;
-    *split = (h->mixed && h->split) ? 1 : 0;
+    *split = h->split ? 1 : 0;
     return LSSPH_OK;
 }
 

@@ -26,7 +26,8 @@ struct lssph_handle {
     int G = 4, Gg = 4;
     bool mixed = false;                 // FP32 pair phase, FP64 solve + refinement
     bool comp = false;                  // mixed precision with compensated (Kahan) FP32 pair sums
-    bool split = false;                 // mixed precision: pair and solve kernels apart (autotuned)
+    bool split = false;                 // q = 5 LS stage/PST: pair and solve kernels apart (autotuned)
+    bool has_sums = false;              // Work::sums allocated (the split shape may run)
     bool classical = false;             // SPH_MODEL 1 / 2: kernel-gradient sums, q = 2 PST basis
     int order = 2;                      // Taylor order k of the LS basis (SPH_MODEL 3: 2; 4 / 5 / 6: 3 / 4 / 5)
     bool hi_thread = false;             // order >= 3: thread per particle (else warp per particle)
@@ -171,12 +172,19 @@ struct Where {
 };
 inline Where all_tiles(const lssph_handle* h) { return Where{nullptr, h->ntiles, h->stream, h->pdl, 0}; }
 
-// Mixed precision, split shape (mixed_split.cu): the pair kernel over the tiles of w, then
-// (after every tile of the stage) the solve kernel over all interior particles.
-void launch_stage_mxp(lssph_handle* h, const StageCfg& S, const Where& w);
-void launch_stage_mxs(lssph_handle* h, const StageCfg& S, cudaStream_t stream, bool pdl);
-void launch_pst_mxp(lssph_handle* h, const Where& w);
-void launch_pst_mxs(lssph_handle* h, cudaStream_t stream, bool pdl);
+// Split shape of the q = 5 LS stage and PST kernels, FP64 or mixed precision
+// (split_shape.cu): the pair kernel over the tiles of w, then (after every tile of the
+// stage) the solve kernel over all interior particles.
+void launch_stage_pairs(lssph_handle* h, const StageCfg& S, const Where& w);
+void launch_stage_solve(lssph_handle* h, const StageCfg& S, cudaStream_t stream, bool pdl);
+void launch_pst_pairs(lssph_handle* h, const Where& w);
+void launch_pst_solve(lssph_handle* h, cudaStream_t stream, bool pdl);
+// The handle's kernels can run split: q = 5 LS at 2 or 4 lanes (or lanes = 0).
+bool split_capable(const lssph_handle* h);
+// A solve of these parameters carries Work::sums: SPH_MODEL 3 at lanes 0, 2 or 4.
+inline bool split_sums(const lssph_params& p) {
+    return p.sph_model == 3 && (p.lanes == 0 || p.lanes == 2 || p.lanes == 4);
+}
 
 // Higher-order LS stage and PST launches, SPH_MODEL 4 / 5 / 6 (highorder.cu).  tiles:
 // tile of each CTA (NULL: CTA i runs tile i); while h->preparing they only set the

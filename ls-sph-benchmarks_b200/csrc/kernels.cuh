@@ -559,13 +559,19 @@ __host__ __device__ inline size_t tile_smem_bytes(int cap, int G, bool tem) {
            2 * maxo * sizeof(int) + ((area + 7) & ~(size_t)7);
 }
 
+// Dynamic shared memory of the FP64 split shape's pair kernel: no sums rows.
+__host__ __device__ inline size_t tile_smem_bytes_fpp(int cap, int G, bool tem) {
+    return tile_smem_bytes(cap, G, tem) - (size_t)PPB * SUMS_MAX * sizeof(double);
+}
+
+// with_sums = false: the layout without the sums rows (the split shape's pair kernel).
 template <bool TEM>
-__device__ __forceinline__ SmemView smem_view(void* raw, int cap) {
+__device__ __forceinline__ SmemView smem_view(void* raw, int cap, bool with_sums = true) {
     SmemView S;
     const int maxp = HC * cap, maxo = OC * cap;
     double* d = static_cast<double*>(raw);
-    S.sums = d;
-    d += PPB * SUMS_MAX;
+    S.sums = with_sums ? d : nullptr;
+    if (with_sums) d += PPB * SUMS_MAX;
     S.x = d; S.y = d + maxp; S.u = d + 2 * maxp; S.v = d + 3 * maxp; S.rho = d + 4 * maxp;
     S.pre = d + 5 * maxp; S.vol = d + 6 * maxp; S.tem = TEM ? d + 7 * maxp : nullptr;
     int* q = reinterpret_cast<int*>(d + (TEM ? 8 : 7) * maxp);
@@ -1217,9 +1223,56 @@ __device__ __forceinline__ void stage_move_own(const Phys& P, const Fld& nxt, co
     }
 }
 
+// FP64 pair phase of one own particle of a stage (LSSPH_A_mod.f90:102-197): the G lanes of
+// the particle share its candidates (tile_pairs), and their sums are combined into Md (the
+// packed upper triangle of the moment matrix) and Bd (one b vector per field).  Returns the
+// in-radius count.  Every lane of the warp calls it (shuffles); inactive lanes pass
+// active = false.  The fused stage kernel and the split shape's pair kernel share it, so
+// both shapes form the same sums.
+template <int NB, int G>
+__device__ __forceinline__ int stage_pair_sums(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
+                                               int ki, int hc, int lane, double (&Md)[15], double (&Bd)[NB][5]) {
+    constexpr int Q = 5;
+    const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
+    double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
+    if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
+    if constexpr (NB == 5) my_tem = SM.tem[ki];
+    using R = double;
+    const PairConst<R> C(P);
+    R Mu[15];
+    R B[NB][Q];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) Mu[k] = R(0);
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+#pragma unroll
+        for (int k = 0; k < Q; ++k) B[c][k] = R(0);
+    const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+        const R xji = R(SM.x[k] - my_x);
+        const R yji = R(SM.y[k] - my_y);
+        const R r = sqrt(xji * xji + yji * yji);
+        const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
+        const R VW = R(SM.vol[k]) * Wv;
+        R a[Q];
+        basis_A<R>(C.ih1, C.ih2A, xji, yji, a);
+        R df[NB];
+        df[0] = R(SM.u[k] - my_u);
+        if constexpr (NB >= 4) {
+            df[1] = R(SM.v[k] - my_v);
+            df[2] = R(SM.rho[k] - my_rho);
+            df[3] = R(SM.pre[k] - my_pre);
+        }
+        if constexpr (NB == 5) df[4] = R(SM.tem[k] - my_tem);
+        accumulate_A<NB, R>(Mu, B, VW, a, df);
+    });
+    group_reduce_to<G>(Mu, Md);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+    return cnt;
+}
+
 // One tile of one solve (the CTA's work in both the single-solve and the batched kernel).
-// MIXED: FP32 pair phase (weights, basis, neighbour sums), FP64 solve with refinement.
-template <int NB, int G, bool MIXED>
+template <int NB, int G>
 __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                            const int* __restrict__ gstart, const int* __restrict__ glist,
                                            const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
@@ -1254,43 +1307,8 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
             const bool active = o < n_own;
             int ki = 0, hc = 0;
             if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
-            const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
-            double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
-            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
-            if constexpr (NB == 5) my_tem = SM.tem[ki];
-            using R = typename std::conditional<MIXED, float, double>::type;
-            const PairConst<R> C(P);
-            R Mu[15];
-            R B[NB][Q];
-#pragma unroll
-            for (int k = 0; k < 15; ++k) Mu[k] = R(0);
-#pragma unroll
-            for (int c = 0; c < NB; ++c)
-#pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = R(0);
-            // differences are formed in FP64, then rounded to the working precision
-            const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
-                const R xji = R(SM.x[k] - my_x);
-                const R yji = R(SM.y[k] - my_y);
-                const R r = sqrt(xji * xji + yji * yji);
-                const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
-                const R VW = R(SM.vol[k]) * Wv;
-                R a[Q];
-                basis_A<R>(C.ih1, C.ih2A, xji, yji, a);
-                R df[NB];
-                df[0] = R(SM.u[k] - my_u);
-                if constexpr (NB >= 4) {
-                    df[1] = R(SM.v[k] - my_v);
-                    df[2] = R(SM.rho[k] - my_rho);
-                    df[3] = R(SM.pre[k] - my_pre);
-                }
-                if constexpr (NB == 5) df[4] = R(SM.tem[k] - my_tem);
-                accumulate_A<NB, R>(Mu, B, VW, a, df);
-            });
             double Md[15], Bd[NB][Q];
-            group_reduce_to<G>(Mu, Md);
-#pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+            const int cnt = stage_pair_sums<NB, G>(P, T, SM, active, ki, hc, lane, Md, Bd);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
@@ -1666,7 +1684,7 @@ __device__ __forceinline__ void stage_body(const Phys& P, const Fld& cur, const 
                                            const int* __restrict__ gstart, const int* __restrict__ glist,
                                            const Work& W, const StageCfg& S, Scalars* sc, int ntx, int tile) {
     if constexpr (MIXED != 0) stage_body_mx<NB, G, MIXED == 2>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
-    else stage_body_fp64<NB, G, false>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
+    else stage_body_fp64<NB, G>(P, cur, nxt, Lc, Ln, gstart, glist, W, S, sc, ntx, tile);
 }
 
 template <int NB, int G, int TIGHT = 0, int MIXED = 0>
@@ -1905,8 +1923,64 @@ __device__ __forceinline__ void pst_move(const Phys& P, const Fld& nxt, const Ls
     scatter_to_cell(P, Ln, gstart, nk, i, sc);
 }
 
-// K: order of the Taylor basis (2: q = 5 for SPH_MODEL 3; 1: q = 2 for the classical models).
-template <int NB, int G, bool MIXED, int K = 2>
+// FP64 pair phase of one own particle of PST (shift_interpolate_mod.f90:120-190): the LS
+// moment matrix and b vectors of the fields to interpolate (Md, Bd) and the shift sums
+// sum (1 + 0.2 (W/W_ave)^4) V_j grad W (sd), combined over the particle's G lanes.  Returns
+// the in-radius count.  K: order of the Taylor basis (2: q = 5 for SPH_MODEL 3; 1: q = 2
+// for the classical models).  Shared by the fused PST kernel and the split pair kernel.
+template <int NB, int G, int K>
+__device__ __forceinline__ int pst_pair_sums(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
+                                             int ki, int hc, int lane,
+                                             double (&Md)[((K == 1) ? 2 : 5) * (((K == 1) ? 2 : 5) + 1) / 2],
+                                             double (&Bd)[NB][(K == 1) ? 2 : 5], double (&sd)[2]) {
+    constexpr int Q = (K == 1) ? 2 : 5;
+    constexpr int QU = Q * (Q + 1) / 2;
+    const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
+    double my_tem = 0.0;
+    if constexpr (NB == 4) my_tem = SM.tem[ki];
+    using R = double;
+    const PairConst<R> C(P);
+    R Mu[QU];
+    R B[NB][Q];
+#pragma unroll
+    for (int k = 0; k < QU; ++k) Mu[k] = R(0);
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+#pragma unroll
+        for (int k = 0; k < Q; ++k) B[c][k] = R(0);
+    R sxy[2] = {R(0), R(0)};
+    const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
+        const R xji = R(SM.x[k] - my_x);
+        const R yji = R(SM.y[k] - my_y);
+        const R r = sqrt(xji * xji + yji * yji);
+        const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
+        const R dWdr = dev_dW<R>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
+        const R Vj = R(SM.vol[k]);
+        const R VW = Vj * Wv;
+        const R rinv = R(1) / r;
+        const R gx = ((dWdr * (-xji)) * rinv) * Vj;
+        const R gy = ((dWdr * (-yji)) * rinv) * Vj;
+        const R t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
+        const R fac = R(1.0) + R(0.2) * t4;
+        sxy[0] = fma(fac, gx, sxy[0]);
+        sxy[1] = fma(fac, gy, sxy[1]);
+        R a[Q];
+        basis_A<R>(C.ih1, C.ih2A, xji, yji, a);
+        R df[NB];
+        df[0] = R(SM.u[k] - my_u);
+        df[1] = R(SM.v[k] - my_v);
+        df[2] = R(SM.rho[k] - my_rho);
+        if constexpr (NB == 4) df[3] = R(SM.tem[k] - my_tem);
+        accumulate_A<NB, R>(Mu, B, VW, a, df);
+    });
+    group_reduce_to<G>(Mu, Md);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+    group_reduce_to<G>(sxy, sd);
+    return cnt;
+}
+
+template <int NB, int G, int K = 2>
 __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc, const Lst& Ln,
                                          const int* __restrict__ gstart, const int* __restrict__ glist, const Work& W,
                                          Scalars* sc, int ntx, int tile) {
@@ -1934,49 +2008,8 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
             const bool active = o < n_own;
             int ki = 0, hc = 0;
             if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
-            const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
-            double my_tem = 0.0;
-            if constexpr (NB == 4) my_tem = SM.tem[ki];
-            using R = typename std::conditional<MIXED, float, double>::type;
-            const PairConst<R> C(P);
-            R Mu[QU];
-            R B[NB][Q];
-#pragma unroll
-            for (int k = 0; k < QU; ++k) Mu[k] = R(0);
-#pragma unroll
-            for (int c = 0; c < NB; ++c)
-#pragma unroll
-                for (int k = 0; k < Q; ++k) B[c][k] = R(0);
-            R sxy[2] = {R(0), R(0)};
-            const int cnt = tile_pairs<G>(T, SM, active, hc, lane, ki, my_x, my_y, P.h_eff_sq, [&](int k) {
-                const R xji = R(SM.x[k] - my_x);
-                const R yji = R(SM.y[k] - my_y);
-                const R r = sqrt(xji * xji + yji * yji);
-                const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
-                const R dWdr = dev_dW<R>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
-                const R Vj = R(SM.vol[k]);
-                const R VW = Vj * Wv;
-                const R rinv = R(1) / r;
-                const R gx = ((dWdr * (-xji)) * rinv) * Vj;
-                const R gy = ((dWdr * (-yji)) * rinv) * Vj;
-                const R t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
-                const R fac = R(1.0) + R(0.2) * t4;
-                sxy[0] = fma(fac, gx, sxy[0]);
-                sxy[1] = fma(fac, gy, sxy[1]);
-                R a[Q];
-                basis_A<R>(C.ih1, C.ih2A, xji, yji, a);
-                R df[NB];
-                df[0] = R(SM.u[k] - my_u);
-                df[1] = R(SM.v[k] - my_v);
-                df[2] = R(SM.rho[k] - my_rho);
-                if constexpr (NB == 4) df[3] = R(SM.tem[k] - my_tem);
-                accumulate_A<NB, R>(Mu, B, VW, a, df);
-            });
             double Md[QU], Bd[NB][Q], sd[2];
-            group_reduce_to<G>(Mu, Md);
-#pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
-            group_reduce_to<G>(sxy, sd);
+            const int cnt = pst_pair_sums<NB, G, K>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
@@ -2217,7 +2250,7 @@ __device__ __forceinline__ void pst_body(const Phys& P, const Fld& cur, const Fl
                                          Scalars* sc, int ntx, int tile) {
     static_assert(!(MIXED != 0 && K != 2), "mixed precision runs the q = 5 basis only");
     if constexpr (MIXED != 0) pst_body_mx<NB, G, MIXED == 2>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
-    else pst_body_fp64<NB, G, false, K>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
+    else pst_body_fp64<NB, G, K>(P, cur, nxt, Lc, Ln, gstart, glist, W, sc, ntx, tile);
 }
 
 template <int NB, int G, int TIGHT = 0, int MIXED = 0, int K = 2>
@@ -2240,7 +2273,7 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
 // at a barrier while one solves.  The split shape runs
 //   k_stage_mxp / k_pst_mxp   tile staging + FP32 pair phase; each particle's reduced sums
 //                             go to Work::sums (no solve, no barrier after the staging)
-//   k_stage_mxs / k_pst_mxs   one thread per interior particle: FP64 factorisation with
+//   k_stage_solve / k_pst_solve   one thread per interior particle: FP64 factorisation with
 //                             refinement, RHS, RK update, cell key and scatter (PST: shift,
 //                             interpolation, move)
 // with the same arithmetic per particle as the fused kernels, so both shapes give identical
@@ -2376,10 +2409,39 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     pairs_mx<NB, G, COMP, true>(P, cur, Lc, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
-// Solve and update of the split shape, one thread per interior particle (the tail of
-// stage_body_mx: FP64 factorisation + refinement, RHS, RK update, key, scatter).
-template <int NB>
-__device__ __forceinline__ void stage_solve_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
+// FP64 LS solve of one particle's sums row in place, as the fused FP64 kernels solve it
+// (DGESV, LSSPH_A_mod.f90:203-241, no refinement); the solution replaces the b sums, scaled
+// by the basis factors when SCALE; cnt < Q leaves zeros.
+template <int Q, int NB, bool SCALE>
+__device__ __forceinline__ void solve_row_plain(const Phys& P, double* row, int cnt, Scalars* sc) {
+    if (cnt >= Q) {
+        double A[Q][Q];
+        double B[NB][Q];
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+#pragma unroll
+            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? row[UT(r, c)] : row[UT(c, r)];
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) B[c][k] = row[15 + 5 * c + k];
+        if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) row[15 + 5 * c + k] = SCALE ? B[c][k] * (k < 2 ? P.ih1 : P.ih2A) : B[c][k];
+    } else {
+#pragma unroll
+        for (int k = 15; k < 15 + 5 * NB; ++k) row[k] = 0.0;
+    }
+}
+
+// Solve and update of the split shape, one thread per interior particle (the tail of the
+// fused stage kernels: FP64 factorisation, RHS, RK update, key, scatter).  REF: mixed
+// precision (factorisation with one refinement step, as stage_body_mx); else FP64 (as
+// stage_body_fp64).
+template <int NB, bool REF>
+__device__ __forceinline__ void stage_solve_row(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
                                                const int* __restrict__ gstart, const Work& W, const StageCfg& S,
                                                Scalars* sc, int i) {
     pdl_wait();
@@ -2398,7 +2460,8 @@ __device__ __forceinline__ void stage_solve_mx(const Phys& P, const Fld& cur, co
         double my_v = 0.0, my_rho = 0.0, my_tem = 0.0;
         if constexpr (NB >= 4) { my_v = cur.v[i]; my_rho = cur.rho[i]; }
         if constexpr (NB == 5) my_tem = cur.tem[i];
-        solve_row_refined<Q, NB, true>(P, row, cnt, sc);
+        if constexpr (REF) solve_row_refined<Q, NB, true>(P, row, cnt, sc);
+        else solve_row_plain<Q, NB, true>(P, row, cnt, sc);
         double d[NB][Q];
 #pragma unroll
         for (int c = 0; c < NB; ++c)
@@ -2413,17 +2476,17 @@ __device__ __forceinline__ void stage_solve_mx(const Phys& P, const Fld& cur, co
         warp_max_atomic(S.do_umax ? &sc->umax2 : &sc->dfmax, red);
 }
 
-template <int NB>
-__global__ void __launch_bounds__(128) k_stage_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
-                                                   const int* __restrict__ gstart, const Work W, const StageCfg S,
-                                                   Scalars* sc) {
-    stage_solve_mx<NB>(P, cur, nxt, Ln, gstart, W, S, sc, (int)(blockIdx.x * blockDim.x + threadIdx.x));
+template <int NB, bool REF>
+__global__ void __launch_bounds__(128) k_stage_solve(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
+                                                     const int* __restrict__ gstart, const Work W, const StageCfg S,
+                                                     Scalars* sc) {
+    stage_solve_row<NB, REF>(P, cur, nxt, Ln, gstart, W, S, sc, (int)(blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // Shift, solve, interpolation and move of the split shape's PST, one thread per interior
-// particle (the tail of pst_body_mx).  NB = 3 (u, v, rho) or 4 (+ T).
-template <int NB>
-__device__ __forceinline__ void pst_solve_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
+// particle (the tail of pst_body_mx, REF, or of pst_body_fp64).  NB = 3 (u, v, rho) or 4 (+ T).
+template <int NB, bool REF>
+__device__ __forceinline__ void pst_solve_row(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
                                              const int* __restrict__ gstart, const Work& W, Scalars* sc, int i) {
     pdl_wait();
     pdl_release();
@@ -2449,7 +2512,8 @@ __device__ __forceinline__ void pst_solve_mx(const Phys& P, const Fld& cur, cons
         dx = ((0.2 * P.h) * dx) / rr;
         dy = ((0.2 * P.h) * dy) / rr;
     }
-    solve_row_refined<Q, NB, false>(P, row, cnt, sc);
+    if constexpr (REF) solve_row_refined<Q, NB, false>(P, row, cnt, sc);
+    else solve_row_plain<Q, NB, false>(P, row, cnt, sc);
     // interpolation a(dr) . d (shift_interpolate_mod.f90:255-298)
     double a[Q];
     basis_A(P, dx, dy, a);
@@ -2478,10 +2542,78 @@ __device__ __forceinline__ void pst_solve_mx(const Phys& P, const Fld& cur, cons
     scatter_to_cell(P, Ln, gstart, nk, i, sc);
 }
 
-template <int NB>
-__global__ void __launch_bounds__(128) k_pst_mxs(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
-                                                 const int* __restrict__ gstart, const Work W, Scalars* sc) {
-    pst_solve_mx<NB>(P, cur, nxt, Ln, gstart, W, sc, (int)(blockIdx.x * blockDim.x + threadIdx.x));
+template <int NB, bool REF>
+__global__ void __launch_bounds__(128) k_pst_solve(const Phys P, const Fld cur, const Fld nxt, const Lst Ln,
+                                                   const int* __restrict__ gstart, const Work W, Scalars* sc) {
+    pst_solve_row<NB, REF>(P, cur, nxt, Ln, gstart, W, sc, (int)(blockIdx.x * blockDim.x + threadIdx.x));
+}
+
+// =======================================================================================
+// FP64 split shape: the same two kernels in FP64.  The fused FP64 kernels hold the solve's
+// registers and the sums rows in every CTA and idle three of four warps at a barrier during
+// the solve; the pair kernel below stages the tile as they do, forms the same sums
+// (stage_pair_sums / pst_pair_sums) and stores them to Work::sums in the layout pairs_mx
+// uses, and k_stage_solve / k_pst_solve (REF = false) solve and update one particle per
+// thread exactly as the fused FP64 kernels do.  Both shapes give identical bits.
+// =======================================================================================
+template <int NB, int G, bool PST>
+__device__ __forceinline__ void pairs_fp(const Phys& P, const Fld& cur, const Lst& Lc, const int* __restrict__ gstart,
+                                         const int* __restrict__ glist, const Work& W, Scalars* sc, int ntx, int tile) {
+    constexpr bool TEM = PST ? (NB == 4) : (NB == 5);
+    constexpr int Q = 5;
+    constexpr int NR = 15 + 5 * NB + (PST ? 2 : 0);   // then the neighbour count
+    pdl_wait();
+    const bool stop = halted(sc);
+    __shared__ TileHdr T;
+    extern __shared__ double smem_raw[];
+    const SmemView SM = smem_view<TEM>(smem_raw, P.cap, false);
+    const int tx = tile % ntx, ty = tile / ntx;
+    stage_halo<false, TEM>(P, cur, Lc, gstart, glist, tx * TX - 1, ty * TY - 1, T, SM);
+    pdl_release();
+    // one decision per warp: the shuffles below need every lane of it
+    if (__any_sync(0xffffffffu, stop)) return;
+    const int n_own = T.own_off[OC];
+    const int lane = threadIdx.x & (G - 1);
+    const size_t N = (size_t)P.num_int;
+    for (int ob = 0; ob < n_own; ob += PPB) {
+        const int slot = (int)threadIdx.x / G;
+        const int o = ob + slot;
+        const bool active = o < n_own;
+        int ki = 0, hc = 0;
+        if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
+        double Md[15], Bd[NB][Q], sd[2] = {0.0, 0.0};
+        int cnt;
+        if constexpr (PST) cnt = pst_pair_sums<NB, G, 2>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
+        else cnt = stage_pair_sums<NB, G>(P, T, SM, active, ki, hc, lane, Md, Bd);
+        if (active) {   // lane l of the particle's G stores entries l, l + G, ...
+            const int i = SM.idx[ki];
+            double* dst = W.sums + i;
+#pragma unroll
+            for (int e = 0; e <= NR; ++e) {
+                if ((e & (G - 1)) != lane) continue;
+                double val;
+                if (e < 15) val = Md[e];
+                else if (e < 15 + 5 * NB) val = Bd[(e - 15) / 5][(e - 15) % 5];
+                else if (e < NR) val = sd[e - 15 - 5 * NB];
+                else val = (double)cnt;
+                dst[(size_t)e * N] = val;
+            }
+        }
+    }
+}
+
+template <int NB, int G, int TIGHT>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
+    k_stage_fpp(const Phys P, const Fld cur, const Lst Lc, const int* __restrict__ gstart,
+                const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
+    pairs_fp<NB, G, false>(P, cur, Lc, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
+}
+
+template <int NB, int G, int TIGHT>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
+    k_pst_fpp(const Phys P, const Fld cur, const Lst Lc, const int* __restrict__ gstart,
+              const int* __restrict__ glist, const Work W, Scalars* sc, int ntx, const int* __restrict__ tiles) {
+    pairs_fp<NB, G, true>(P, cur, Lc, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
 struct SolveDesc {
@@ -2560,8 +2692,8 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pst(con
                            d.ntx, m.y);
 }
 
-// Mixed precision, split shape, batched: the pair kernel over a group's (solve, tile) map and
-// the solve kernel over its (solve, block of 128 interior particles) map.
+// Mixed precision, split shape, batched: the FP32 pair kernel over a group's (solve, tile) map
+// (the solve kernel, kb_solve, follows the FP64 pair kernel below).
 template <int NB, int G, int TIGHT, bool COMP, bool PST>
 __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pairs_mx(const SolveDesc* __restrict__ D,
                                                                                   const BatchMap M, int ps, int pl) {
@@ -2573,8 +2705,22 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pairs_m
     pairs_mx<NB, G, COMP, PST>(d.P, d.F[sb], d.L[lb], d.gstart, d.glist, d.W, d.sc, d.ntx, m.y);
 }
 
-template <int NB, bool PST>
-__global__ void __launch_bounds__(128) kb_solve_mx(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
+// FP64 split shape, batched: the FP64 pair kernel over a group's (solve, tile) map.
+template <int NB, int G, int TIGHT, bool PST>
+__global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT)) kb_pairs_fp(const SolveDesc* __restrict__ D,
+                                                                                  const BatchMap M, int ps, int pl) {
+    __shared__ SolveDesc sd;
+    const int2 m = M.cta[blockIdx.x];
+    const SolveDesc& d = load_desc(D, m.x, sd);
+    int sb, lb;
+    batch_parity(M, d, ps, pl, sb, lb);
+    pairs_fp<NB, G, PST>(d.P, d.F[sb], d.L[lb], d.gstart, d.glist, d.W, d.sc, d.ntx, m.y);
+}
+
+// The split shape's solve kernel over a group's (solve, block of 128 interior particles) map;
+// REF as k_stage_solve.
+template <int NB, bool PST, bool REF>
+__global__ void __launch_bounds__(128) kb_solve(const SolveDesc* __restrict__ D, const BatchMap M, StageCfg S,
                                                    int ps, int pl) {
     __shared__ SolveDesc sd;
     const int2 m = M.cta[blockIdx.x];
@@ -2583,11 +2729,11 @@ __global__ void __launch_bounds__(128) kb_solve_mx(const SolveDesc* __restrict__
     batch_parity(M, d, ps, pl, sb, lb);
     const int i = m.y * 128 + (int)threadIdx.x;
     if constexpr (PST) {
-        pst_solve_mx<NB>(d.P, d.F[sb], d.F[sb ^ 1], d.L[next_list(lb)], d.gstart, d.W, d.sc, i);
+        pst_solve_row<NB, REF>(d.P, d.F[sb], d.F[sb ^ 1], d.L[next_list(lb)], d.gstart, d.W, d.sc, i);
     } else {
         S.dt1 = d.dt1[S.stage - 1];
         S.dt2 = d.dt2[S.stage - 1];
-        stage_solve_mx<NB>(d.P, d.F[sb], d.F[sb ^ 1], d.L[next_list(lb)], d.gstart, d.W, S, d.sc, i);
+        stage_solve_row<NB, REF>(d.P, d.F[sb], d.F[sb ^ 1], d.L[next_list(lb)], d.gstart, d.W, S, d.sc, i);
     }
 }
 

@@ -1,8 +1,8 @@
 """Parity at the benchmarked configurations, at their own sizes and horizons (needs a B200).
 
   * configuration 2 as the bench times it: periodic Taylor-Green, Re = 100, 128^2, RK4 +
-    PST, CFL 0.1, with the engine's automatic lane count and each register budget, against
-    the oracle after 120 steps (rel L2 <= 1e-10);
+    PST, CFL 0.1, with the engine's automatic lane count, each kernel shape and each register
+    budget, against the oracle after 120 steps (rel L2 <= 1e-10);
   * configuration 1 as written (periodic 50^2 diffusion, jitter +-0.05 dx, dt = 0.1 dx^2,
     RK2, 1000 steps) and configuration 2 to t = 1 (12,800 steps): with one lane per particle
     (the reference's summation order) every field is bit-identical to the oracle's at the
@@ -57,14 +57,20 @@ def _all_cores():
     O.set_threads(os.cpu_count() or 1)
 
 
-@pytest.mark.parametrize("lanes,budget", [(0, None)] + [(g, b) for g in (2, 4) for b in ("loose", "tight", "five")])
-def test_headline_workload_matches_the_oracle(lanes, budget, monkeypatch):
-    # the kernels the bench may time: lanes = 0 lets the engine pick 2 or 4 and the register
-    # budget by measurement (what the bench runs); the explicit cases cover every pick
-    if budget:
-        monkeypatch.setenv("LSSPH_REGISTER_BUDGET", budget)
-    else:
-        monkeypatch.delenv("LSSPH_REGISTER_BUDGET", raising=False)
+HEADLINE_KERNELS = ([(0, None, None)] + [(g, b, "fused") for g in (2, 4) for b in ("loose", "tight", "five")] +
+                    [(g, b, "split") for g in (2, 4) for b in ("loose", "tight", "five", "six")])
+
+
+@pytest.mark.parametrize("lanes,budget,shape", HEADLINE_KERNELS)
+def test_headline_workload_matches_the_oracle(lanes, budget, shape, monkeypatch):
+    # the kernels the bench may time: lanes = 0 lets the engine pick 2 or 4, the kernel shape
+    # and the register budget by measurement (what the bench runs); the explicit cases cover
+    # every pick
+    for var, val in (("LSSPH_REGISTER_BUDGET", budget), ("LSSPH_KERNEL_SHAPE", shape)):
+        if val:
+            monkeypatch.setenv(var, val)
+        else:
+            monkeypatch.delenv(var, raising=False)
     p = tg_params(lanes=lanes)
     st, ni = lssph.setup_particles(p)
     sim = lssph.Simulation(p, st, ni)
@@ -73,7 +79,7 @@ def test_headline_workload_matches_the_oracle(lanes, budget, monkeypatch):
     orc.run(120)
     tune = sim.tuning()
     if budget:
-        assert tune["register_budget"] == budget and tune["lanes"] == lanes
+        assert tune["register_budget"] == budget and tune["lanes"] == lanes and tune["shape"] == shape
     g, o = sim.download(), orc.get()
     for k in ("x", "y", "u", "v", "pre"):
         assert _rel_l2(getattr(g, k), o[k]) <= 1e-10, (k, tune)

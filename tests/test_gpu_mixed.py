@@ -192,7 +192,7 @@ def test_split_and_fused_shapes_give_identical_bits(case, prec, monkeypatch):
     mk, _ = CASES[case]
     out = {}
     for shape in ("fused", "split"):
-        monkeypatch.setenv("LSSPH_MIXED_SHAPE", shape)
+        monkeypatch.setenv("LSSPH_KERNEL_SHAPE", shape)
         sim = _sim(lssph.make_params(mk(), lanes=4), prec, seed=4)
         sim.step(6)
         assert sim.tuning()["shape"] == shape

@@ -292,3 +292,77 @@ def test_overlapped_step_equals_serial_step(monkeypatch):
             out[ov] = sim.download()
         for k in FIELDS + (("tem",) if p.target_problem == 4 else ()):
             assert np.array_equal(getattr(out["0"], k), getattr(out["1"], k)), (case, k)
+
+
+# ---- the FP64 split shape --------------------------------------------------------------
+# The split shape runs the fused kernels' pair phase in a pair kernel (sums to device
+# memory) and their solve and update in a kernel with one thread per particle; per particle
+# the arithmetic is the fused kernels', so both shapes give the same bits.
+@pytest.mark.parametrize("lanes", [2, 4])
+@pytest.mark.parametrize("case", list(CASES))
+def test_fp64_split_and_fused_shapes_give_identical_bits(case, lanes, monkeypatch):
+    p = lssph.make_params(CASES[case](), lanes=lanes)
+    out = {}
+    for shape in ("fused", "split"):
+        monkeypatch.setenv("LSSPH_KERNEL_SHAPE", shape)
+        st, ni = _perturbed(p, 0.1, 5)
+        sim = lssph.Simulation(p, st, ni)
+        sim.ghost()
+        sim.step(6)
+        assert sim.tuning()["shape"] == shape
+        out[shape] = sim.download()
+        sim.close()
+    for k in FIELDS + (("tem",) if p.target_problem == 4 else ()):
+        assert np.array_equal(getattr(out["fused"], k), getattr(out["split"], k)), (case, k)
+
+
+@pytest.mark.parametrize("budget", ["loose", "tight", "five", "six", "eight"])
+def test_fp64_split_budgets_match_the_oracle(budget, monkeypatch):
+    # every register budget of the FP64 pair kernel (six and eight spill), on the periodic
+    # Taylor-Green square, against the oracle
+    monkeypatch.setenv("LSSPH_KERNEL_SHAPE", "split")
+    monkeypatch.setenv("LSSPH_REGISTER_BUDGET", budget)
+    p = lssph.taylor_green_params(num=64, re=100.0, coe_cfl=0.1, tg=2, lanes=2, PERIODIC=1)
+    st, ni = lssph.setup_particles(p)
+    sim = lssph.Simulation(p, st, ni)
+    orc = O.Oracle(p, st, ni, ghost=False)
+    sim.step(40)
+    orc.run(40)
+    t = sim.tuning()
+    assert t["shape"] == "split" and t["register_budget"] == budget
+    g, o = sim.download(), orc.get()
+    for k in ("x", "y", "u", "v", "pre"):
+        assert _rel_l2(getattr(g, k), o[k]) <= 1e-10, k
+    sim.close()
+
+
+def test_fp64_split_batch_members_identical_alone(monkeypatch):
+    # members that picked the split shape alone make their batch group run it (batched FP64
+    # pair kernel over (solve, tile), solve kernel over (solve, particle block)); each member
+    # still ends bit for bit as it does alone
+    monkeypatch.setenv("LSSPH_KERNEL_SHAPE", "split")
+    mk = [lambda: lssph.make_params(lssph.cavity_params(num=64), lanes=4),
+          lambda: lssph.make_params(lssph.taylor_green_params(num=64), lanes=4),
+          lambda: lssph.make_params(lssph.boussinesq_params(num=48), lanes=4)]
+    solo, mem = [], []
+    for i, f in enumerate(mk):
+        for group in (solo, mem):
+            p = f()
+            st, ni = _perturbed(p, 0.1, 10 + i)
+            sim = lssph.Simulation(p, st, ni)
+            sim.ghost()
+            sim.step(1)   # the first solo launch measures (here: fixes) the shape
+            assert sim.tuning()["shape"] == "split"
+            group.append(sim)
+    with lssph.Batch() as b:
+        for m in mem:
+            b.add(m)
+        b.step(4)
+    for s in solo:
+        s.step(4)
+    for s, m in zip(solo, mem):
+        gs, gm = s.download(), m.download()
+        for k in FIELDS + (("tem",) if s.params.target_problem == 4 else ()):
+            assert np.array_equal(getattr(gs, k), getattr(gm, k)), k
+        s.close()
+        m.close()
