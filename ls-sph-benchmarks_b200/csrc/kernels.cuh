@@ -1229,9 +1229,10 @@ __device__ __forceinline__ void stage_move_own(const Phys& P, const Fld& nxt, co
 // in-radius count.  Every lane of the warp calls it (shuffles); inactive lanes pass
 // active = false.  The fused stage kernel and the split shape's pair kernel share it, so
 // both shapes form the same sums.
-template <int NB, int G>
-__device__ __forceinline__ int stage_pair_sums(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
-                                               int ki, int hc, int lane, double (&Md)[15], double (&Bd)[NB][5]) {
+template <int NB, int G, int KT>
+__device__ __forceinline__ int stage_pair_sums_kt(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
+                                                  int ki, int hc, int lane, double (&Md)[15], double (&Bd)[NB][5]) {
+    const int kt = KT ? KT : P.kt;
     constexpr int Q = 5;
     const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki];
     double my_v = 0, my_rho = 0, my_pre = 0, my_tem = 0;
@@ -1251,7 +1252,7 @@ __device__ __forceinline__ int stage_pair_sums(const Phys& P, const TileHdr& T, 
         const R xji = R(SM.x[k] - my_x);
         const R yji = R(SM.y[k] - my_y);
         const R r = sqrt(xji * xji + yji * yji);
-        const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
+        const R Wv = dev_W<R>(kt, r, C.ih1, C.wnorm);
         const R VW = R(SM.vol[k]) * Wv;
         R a[Q];
         basis_A<R>(C.ih1, C.ih2A, xji, yji, a);
@@ -1269,6 +1270,15 @@ __device__ __forceinline__ int stage_pair_sums(const Phys& P, const TileHdr& T, 
 #pragma unroll
     for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
     return cnt;
+}
+
+// The pair loop is compiled twice: for the Wendland C2 kernel (KERNEL_TYPE 3, the default),
+// whose weight then needs no branch on the kernel type inside the loop, and for any type.
+template <int NB, int G>
+__device__ __forceinline__ int stage_pair_sums(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
+                                               int ki, int hc, int lane, double (&Md)[15], double (&Bd)[NB][5]) {
+    if (P.kt == 3) return stage_pair_sums_kt<NB, G, 3>(P, T, SM, active, ki, hc, lane, Md, Bd);
+    return stage_pair_sums_kt<NB, G, 0>(P, T, SM, active, ki, hc, lane, Md, Bd);
 }
 
 // One tile of one solve (the CTA's work in both the single-solve and the batched kernel).
@@ -1411,6 +1421,97 @@ __device__ __forceinline__ void solve_row_refined(const Phys& P, double* row, in
     }
 }
 
+// Mixed-precision pair phase of one own particle (FP32 offsets and field references staged
+// in shared memory): the stage's sums (LSSPH_A_mod.f90:102-197) or, with PST, the shift
+// interpolation's sums and the shift vector sums (shift_interpolate_mod.f90:120-190), each
+// lane's FP32 partial sums (compensated with COMP) combined over the particle's G lanes in
+// FP64.  Returns the in-radius count.  Every lane of the warp calls it (shuffles).  The
+// fused and split mixed kernels share it; KT as stage_pair_sums_kt.
+template <int NB, int G, bool COMP, bool PST, int KT>
+__device__ __forceinline__ int mx_pair_sums_kt(const Phys& P, const TileHdr& T, const SmemMx& SM, bool active,
+                                               int ki, int hc, int lane, double (&Md)[15], double (&Bd)[NB][5],
+                                               double (&sd)[2]) {
+    constexpr bool TEM = PST ? (NB == 4) : (NB == 5);
+    constexpr int Q = 5;
+    const int kt = KT ? KT : P.kt;
+    const float heff2 = (float)P.h_eff_sq;
+    const PairConst<float> C(P);
+    const float oxi = SM.ox[ki], oyi = SM.oy[ki];
+    const float my_u = SM.u[ki];
+    float my_v = 0.f, my_rho = 0.f, my_pre = 0.f, my_tem = 0.f;
+    if constexpr (PST || NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
+    if constexpr (!PST && NB >= 4) my_pre = SM.pre[ki];
+    if constexpr (TEM) my_tem = SM.tem[ki];
+    float Mu[15], Mc[15];
+    float B[NB][Q], Bc[NB][Q];
+    float sxy[2] = {0.f, 0.f}, sxc[2] = {0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < 15; ++k) { Mu[k] = 0.f; Mc[k] = 0.f; }
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+#pragma unroll
+        for (int k = 0; k < Q; ++k) { B[c][k] = 0.f; Bc[c][k] = 0.f; }
+    const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2, [&](int k, float xji, float yji) {
+        const float r = sqrtf(xji * xji + yji * yji);
+        const float Wv = dev_W<float>(kt, r, C.ih1, C.wnorm);
+        const float Vj = SM.vol[k];
+        const float VW = Vj * Wv;
+        if constexpr (PST) {
+            const float dWdr = dev_dW<float>(kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
+            const float rinv = 1.f / r;
+            const float gx = ((dWdr * (-xji)) * rinv) * Vj;
+            const float gy = ((dWdr * (-yji)) * rinv) * Vj;
+            const float t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
+            const float fac = 1.f + 0.2f * t4;
+            if constexpr (COMP) {
+                kahan_add(sxy[0], sxc[0], fac * gx);
+                kahan_add(sxy[1], sxc[1], fac * gy);
+            } else {
+                sxy[0] = fmaf(fac, gx, sxy[0]);
+                sxy[1] = fmaf(fac, gy, sxy[1]);
+            }
+        }
+        float a[Q];
+        basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
+        float df[NB];
+        df[0] = SM.u[k] - my_u;
+        if constexpr (PST) {
+            df[1] = SM.v[k] - my_v;
+            df[2] = SM.rho[k] - my_rho;
+            if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
+        } else {
+            if constexpr (NB >= 4) {
+                df[1] = SM.v[k] - my_v;
+                df[2] = SM.rho[k] - my_rho;
+                df[3] = SM.pre[k] - my_pre;
+            }
+            if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
+        }
+        if constexpr (COMP) accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
+        else accumulate_A<NB, float>(Mu, B, VW, a, df);
+    });
+    if constexpr (COMP) {
+        group_reduce_kahan<G>(Mu, Mc, Md);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
+        if constexpr (PST) group_reduce_kahan<G>(sxy, sxc, sd);
+    } else {
+        group_reduce_to<G>(Mu, Md);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
+        if constexpr (PST) group_reduce_to<G>(sxy, sd);
+    }
+    return cnt;
+}
+
+template <int NB, int G, bool COMP, bool PST>
+__device__ __forceinline__ int mx_pair_sums(const Phys& P, const TileHdr& T, const SmemMx& SM, bool active, int ki,
+                                            int hc, int lane, double (&Md)[15], double (&Bd)[NB][5],
+                                            double (&sd)[2]) {
+    if (P.kt == 3) return mx_pair_sums_kt<NB, G, COMP, PST, 3>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
+    return mx_pair_sums_kt<NB, G, COMP, PST, 0>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
+}
+
 // Mixed-precision stage: FP32 staging and pair phase (offsets from FP64 cell origins and
 // field references), lanes combined in FP64, FP64 solve with refinement, FP64 update.
 template <int NB, int G, bool COMP>
@@ -1434,8 +1535,6 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
     if (stop) return;
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
-    const float heff2 = (float)P.h_eff_sq;
-    const PairConst<float> C(P);
     const bool early = S.mode == MODE_STAGE;
     auto own = [&](int o, int& i, double& x, double& y, double& u, double& v) {
         i = SM.idx[SM.own_k[o]];
@@ -1451,47 +1550,8 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
             const bool active = o < n_own;
             int ki = 0, hc = 0;
             if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
-            const float oxi = SM.ox[ki], oyi = SM.oy[ki];
-            const float my_u = SM.u[ki];
-            float my_v = 0.f, my_rho = 0.f, my_pre = 0.f, my_tem = 0.f;
-            if constexpr (NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; my_pre = SM.pre[ki]; }
-            if constexpr (NB == 5) my_tem = SM.tem[ki];
-            float Mu[15], Mc[15];
-            float B[NB][Q], Bc[NB][Q];
-#pragma unroll
-            for (int k = 0; k < 15; ++k) { Mu[k] = 0.f; Mc[k] = 0.f; }
-#pragma unroll
-            for (int c = 0; c < NB; ++c)
-#pragma unroll
-                for (int k = 0; k < Q; ++k) { B[c][k] = 0.f; Bc[c][k] = 0.f; }
-            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2,
-                                             [&](int k, float xji, float yji) {
-                const float r = sqrtf(xji * xji + yji * yji);
-                const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
-                const float VW = SM.vol[k] * Wv;
-                float a[Q];
-                basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
-                float df[NB];
-                df[0] = SM.u[k] - my_u;
-                if constexpr (NB >= 4) {
-                    df[1] = SM.v[k] - my_v;
-                    df[2] = SM.rho[k] - my_rho;
-                    df[3] = SM.pre[k] - my_pre;
-                }
-                if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
-                if constexpr (COMP) accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
-                else accumulate_A<NB, float>(Mu, B, VW, a, df);
-            });
-            double Md[15], Bd[NB][Q];
-            if constexpr (COMP) {
-                group_reduce_kahan<G>(Mu, Mc, Md);
-#pragma unroll
-                for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
-            } else {
-                group_reduce_to<G>(Mu, Md);
-#pragma unroll
-                for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
-            }
+            double Md[15], Bd[NB][Q], sd[2];
+            const int cnt = mx_pair_sums<NB, G, COMP, false>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
@@ -1928,11 +1988,12 @@ __device__ __forceinline__ void pst_move(const Phys& P, const Fld& nxt, const Ls
 // sum (1 + 0.2 (W/W_ave)^4) V_j grad W (sd), combined over the particle's G lanes.  Returns
 // the in-radius count.  K: order of the Taylor basis (2: q = 5 for SPH_MODEL 3; 1: q = 2
 // for the classical models).  Shared by the fused PST kernel and the split pair kernel.
-template <int NB, int G, int K>
-__device__ __forceinline__ int pst_pair_sums(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
-                                             int ki, int hc, int lane,
-                                             double (&Md)[((K == 1) ? 2 : 5) * (((K == 1) ? 2 : 5) + 1) / 2],
-                                             double (&Bd)[NB][(K == 1) ? 2 : 5], double (&sd)[2]) {
+template <int NB, int G, int K, int KT>
+__device__ __forceinline__ int pst_pair_sums_kt(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
+                                                int ki, int hc, int lane,
+                                                double (&Md)[((K == 1) ? 2 : 5) * (((K == 1) ? 2 : 5) + 1) / 2],
+                                                double (&Bd)[NB][(K == 1) ? 2 : 5], double (&sd)[2]) {
+    const int kt = KT ? KT : P.kt;
     constexpr int Q = (K == 1) ? 2 : 5;
     constexpr int QU = Q * (Q + 1) / 2;
     const double my_x = SM.x[ki], my_y = SM.y[ki], my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
@@ -1953,8 +2014,8 @@ __device__ __forceinline__ int pst_pair_sums(const Phys& P, const TileHdr& T, co
         const R xji = R(SM.x[k] - my_x);
         const R yji = R(SM.y[k] - my_y);
         const R r = sqrt(xji * xji + yji * yji);
-        const R Wv = dev_W<R>(P.kt, r, C.ih1, C.wnorm);
-        const R dWdr = dev_dW<R>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
+        const R Wv = dev_W<R>(kt, r, C.ih1, C.wnorm);
+        const R dWdr = dev_dW<R>(kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
         const R Vj = R(SM.vol[k]);
         const R VW = Vj * Wv;
         const R rinv = R(1) / r;
@@ -1978,6 +2039,16 @@ __device__ __forceinline__ int pst_pair_sums(const Phys& P, const TileHdr& T, co
     for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
     group_reduce_to<G>(sxy, sd);
     return cnt;
+}
+
+// Compiled for the Wendland C2 kernel and for any type, as stage_pair_sums.
+template <int NB, int G, int K>
+__device__ __forceinline__ int pst_pair_sums(const Phys& P, const TileHdr& T, const SmemView& SM, bool active,
+                                             int ki, int hc, int lane,
+                                             double (&Md)[((K == 1) ? 2 : 5) * (((K == 1) ? 2 : 5) + 1) / 2],
+                                             double (&Bd)[NB][(K == 1) ? 2 : 5], double (&sd)[2]) {
+    if (P.kt == 3) return pst_pair_sums_kt<NB, G, K, 3>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
+    return pst_pair_sums_kt<NB, G, K, 0>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
 }
 
 template <int NB, int G, int K = 2>
@@ -2121,8 +2192,6 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
     const double U_max = sqrt(__longlong_as_double((long long)sc->umax2));
     const double coe = ((P.PST_c * U_max) * P.dt) * P.h;
     const int lane = threadIdx.x & (G - 1);
-    const float heff2 = (float)P.h_eff_sq;
-    const PairConst<float> C(P);
     for (int ob = 0; ob < n_own; ob += PPB) {
         {
             const int slot = (int)threadIdx.x / G;
@@ -2130,60 +2199,8 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
             const bool active = o < n_own;
             int ki = 0, hc = 0;
             if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
-            const float oxi = SM.ox[ki], oyi = SM.oy[ki];
-            const float my_u = SM.u[ki], my_v = SM.v[ki], my_rho = SM.rho[ki];
-            float my_tem = 0.f;
-            if constexpr (NB == 4) my_tem = SM.tem[ki];
-            float Mu[15], Mc[15];
-            float B[NB][Q], Bc[NB][Q];
-#pragma unroll
-            for (int k = 0; k < 15; ++k) { Mu[k] = 0.f; Mc[k] = 0.f; }
-#pragma unroll
-            for (int c = 0; c < NB; ++c)
-#pragma unroll
-                for (int k = 0; k < Q; ++k) { B[c][k] = 0.f; Bc[c][k] = 0.f; }
-            float sxy[2] = {0.f, 0.f}, sxc[2] = {0.f, 0.f};
-            const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2,
-                                             [&](int k, float xji, float yji) {
-                const float r = sqrtf(xji * xji + yji * yji);
-                const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
-                const float dWdr = dev_dW<float>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
-                const float Vj = SM.vol[k];
-                const float VW = Vj * Wv;
-                const float rinv = 1.f / r;
-                const float gx = ((dWdr * (-xji)) * rinv) * Vj;
-                const float gy = ((dWdr * (-yji)) * rinv) * Vj;
-                const float t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
-                const float fac = 1.f + 0.2f * t4;
-                if constexpr (COMP) {
-                    kahan_add(sxy[0], sxc[0], fac * gx);
-                    kahan_add(sxy[1], sxc[1], fac * gy);
-                } else {
-                    sxy[0] = fmaf(fac, gx, sxy[0]);
-                    sxy[1] = fmaf(fac, gy, sxy[1]);
-                }
-                float a[Q];
-                basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
-                float df[NB];
-                df[0] = SM.u[k] - my_u;
-                df[1] = SM.v[k] - my_v;
-                df[2] = SM.rho[k] - my_rho;
-                if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
-                if constexpr (COMP) accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
-                else accumulate_A<NB, float>(Mu, B, VW, a, df);
-            });
             double Md[15], Bd[NB][Q], sd[2];
-            if constexpr (COMP) {
-                group_reduce_kahan<G>(Mu, Mc, Md);
-#pragma unroll
-                for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
-                group_reduce_kahan<G>(sxy, sxc, sd);
-            } else {
-                group_reduce_to<G>(Mu, Md);
-#pragma unroll
-                for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
-                group_reduce_to<G>(sxy, sd);
-            }
+            const int cnt = mx_pair_sums<NB, G, COMP, true>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
             if (active && lane == 0) {
                 double* sm = SM.sums + slot * SR;
 #pragma unroll
@@ -2303,8 +2320,6 @@ __device__ __forceinline__ void pairs_mx(const Phys& P, const Fld& cur, const Ls
     if (__any_sync(0xffffffffu, stop)) return;
     const int n_own = T.own_off[OC];
     const int lane = threadIdx.x & (G - 1);
-    const float heff2 = (float)P.h_eff_sq;
-    const PairConst<float> C(P);
     const size_t N = (size_t)P.num_int;
     for (int ob = 0; ob < n_own; ob += PPB) {
         const int slot = (int)threadIdx.x / G;
@@ -2312,72 +2327,8 @@ __device__ __forceinline__ void pairs_mx(const Phys& P, const Fld& cur, const Ls
         const bool active = o < n_own;
         int ki = 0, hc = 0;
         if (active) { ki = SM.own_k[o]; hc = SM.own_hc[o]; }
-        const float oxi = SM.ox[ki], oyi = SM.oy[ki];
-        const float my_u = SM.u[ki];
-        float my_v = 0.f, my_rho = 0.f, my_pre = 0.f, my_tem = 0.f;
-        if constexpr (PST || NB >= 4) { my_v = SM.v[ki]; my_rho = SM.rho[ki]; }
-        if constexpr (!PST && NB >= 4) my_pre = SM.pre[ki];
-        if constexpr (TEM) my_tem = SM.tem[ki];
-        float Mu[15], Mc[15];
-        float B[NB][Q], Bc[NB][Q];
-        float sxy[2] = {0.f, 0.f}, sxc[2] = {0.f, 0.f};
-#pragma unroll
-        for (int k = 0; k < 15; ++k) { Mu[k] = 0.f; Mc[k] = 0.f; }
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-#pragma unroll
-            for (int k = 0; k < Q; ++k) { B[c][k] = 0.f; Bc[c][k] = 0.f; }
-        const int cnt = tile_pairs_mx<G>(T, SM, active, hc, lane, ki, oxi, oyi, heff2, [&](int k, float xji, float yji) {
-            const float r = sqrtf(xji * xji + yji * yji);
-            const float Wv = dev_W<float>(P.kt, r, C.ih1, C.wnorm);
-            const float Vj = SM.vol[k];
-            const float VW = Vj * Wv;
-            if constexpr (PST) {   // shift_interpolate_mod.f90:142-146, as pst_body_mx
-                const float dWdr = dev_dW<float>(P.kt, r, C.ih1, C.m3h, C.m5h, C.wnorm);
-                const float rinv = 1.f / r;
-                const float gx = ((dWdr * (-xji)) * rinv) * Vj;
-                const float gy = ((dWdr * (-yji)) * rinv) * Vj;
-                const float t = Wv * C.iWave, t2 = t * t, t4 = t2 * t2;
-                const float fac = 1.f + 0.2f * t4;
-                if constexpr (COMP) {
-                    kahan_add(sxy[0], sxc[0], fac * gx);
-                    kahan_add(sxy[1], sxc[1], fac * gy);
-                } else {
-                    sxy[0] = fmaf(fac, gx, sxy[0]);
-                    sxy[1] = fmaf(fac, gy, sxy[1]);
-                }
-            }
-            float a[Q];
-            basis_A<float>(C.ih1, C.ih2A, xji, yji, a);
-            float df[NB];
-            df[0] = SM.u[k] - my_u;
-            if constexpr (PST) {
-                df[1] = SM.v[k] - my_v;
-                df[2] = SM.rho[k] - my_rho;
-                if constexpr (NB == 4) df[3] = SM.tem[k] - my_tem;
-            } else {
-                if constexpr (NB >= 4) {
-                    df[1] = SM.v[k] - my_v;
-                    df[2] = SM.rho[k] - my_rho;
-                    df[3] = SM.pre[k] - my_pre;
-                }
-                if constexpr (NB == 5) df[4] = SM.tem[k] - my_tem;
-            }
-            if constexpr (COMP) accumulate_A_kahan<NB, Q>(Mu, Mc, B, Bc, VW, a, df);
-            else accumulate_A<NB, float>(Mu, B, VW, a, df);
-        });
-        double Md[15], Bd[NB][Q], sd[2];
-        if constexpr (COMP) {
-            group_reduce_kahan<G>(Mu, Mc, Md);
-#pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_kahan<G>(B[c], Bc[c], Bd[c]);
-            group_reduce_kahan<G>(sxy, sxc, sd);
-        } else {
-            group_reduce_to<G>(Mu, Md);
-#pragma unroll
-            for (int c = 0; c < NB; ++c) group_reduce_to<G>(B[c], Bd[c]);
-            group_reduce_to<G>(sxy, sd);
-        }
+        double Md[15], Bd[NB][Q], sd[2] = {0.0, 0.0};
+        const int cnt = mx_pair_sums<NB, G, COMP, PST>(P, T, SM, active, ki, hc, lane, Md, Bd, sd);
         if (active) {   // lane l of the particle's G stores entries l, l + G, ...
             const int i = SM.idx[ki];
             double* dst = W.sums + i;
