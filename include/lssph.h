@@ -231,10 +231,12 @@ int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32
 
 /* Kernel configuration the handle runs (no counterpart in the reference): lanes per
    particle, and the register budget of the stage/PST kernels: 0 loose, 1 tight (512 threads
-   per SM), 2 (640 threads per SM, q = 5 LS only), and for the pair kernel of the mixed
-   precision split shape also 3 (768) and 4 (1024), with the RHS-pass time of the loose and
-   tight budgets measured when the handle was created.  The budget is picked by that
-   measurement; it never changes a result. */
+   per SM), 2 (640 threads per SM, q = 5 LS only), and for the pair kernel of the split shape
+   also 3 (768) and 4 (1024), with the measured time of the fused kernels at the loose and
+   tight budgets.  The measurement runs at the handle's first launch: whole time steps on
+   the solve's own state, which is copied aside first and put back after each option (the
+   RHS pass alone when the device has no room for the copy).  The lane count (lanes = 0),
+   the shape and the budget are picked by it; the budget and shape never change a result. */
 int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, double* rhs_us_loose,
                      double* rhs_us_tight);
 /* Shape of the q = 5 LS stage and PST kernels, FP64 or mixed precision (no counterpart in

@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -483,9 +484,37 @@ void enq_step_overlap(lssph_handle* h) {
 
 int sync_check(lssph_handle* h);
 
-// Pick the register budget of the stage and PST kernels: time the RHS pass of the
-// current state (writes only the RHS arrays) with each budget, keep the faster.  Both
-// budgets give bit-identical results, so the choice never changes an answer.
+// The autotuner's picks, once per process for each solve configuration: every handle of
+// the same configuration (problem, sizes, cell grid and tiles, model, kernel type, walls,
+// precision, schedule, lanes asked for, shape restriction) takes the first one's lanes,
+// shape and budget.  So two handles of one solve (a solve alone and as a batch member, a
+// restart, serving requests of one size) sum in the same order, and a stream of requests
+// of one size is measured once.
+struct TuneKey {
+    int64_t v[20];
+    bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 20, o.v, o.v + 20); }
+};
+struct TunePick {
+    int G, budget;
+    bool split;
+    double us[3];
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TunePick> g_tune_picks;
+
+TuneKey tune_key(const lssph_handle* h, bool try_fused, bool try_split) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const lssph_params& p = h->p;
+    return TuneKey{{dev, p.target_problem, h->num_int, h->num_ext, h->grid.nx, h->grid.ny, h->grid.cap, h->ntiles,
+                    h->n_int, p.sph_model, p.kernel_type, p.wall_model, p.precision, p.rk, p.periodic, p.lanes,
+                    h->overlap ? 1 : 0, h->pdl ? 1 : 0, try_fused ? 1 : 0, try_split ? 1 : 0}};
+}
+
+// Pick the lane count (lanes = 0), the kernel shape and the register budget of the stage
+// and PST kernels by timing each option on the current state, keep the fastest.  Every
+// option gives bit-identical results except the lane count, which changes sums at the
+// rounding level.
 int autotune(lssph_handle* h) {
     h->tuned = true;
     StageCfg S{};
@@ -517,10 +546,51 @@ int autotune(lssph_handle* h) {
             return LSSPH_OK;
         }
     }
+    const TuneKey key = tune_key(h, try_fused, try_split);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        const auto it = g_tune_picks.find(key);
+        if (it != g_tune_picks.end()) {
+            const TunePick& k = it->second;
+            h->G = k.G;
+            h->split = k.split;
+            h->budget = k.budget;
+            h->tight = k.budget >= 1;
+            for (int t = 0; t < 3; ++t) h->tune_us[t] = k.us[t];
+            return LSSPH_OK;
+        }
+    }
     // lanes = 0 on a q = 5 LS solve: 4 lanes per particle unless 2 lanes run the RHS
     // pass at least 5 % faster (the margin keeps the pick, and with it the summation order,
     // the same from run to run when the two are close).  The shape and the budget change no
     // result, so they go to the fastest.
+    //
+    // One timed pass is a whole time step (enq_step, or enq_step_overlap in the overlapped
+    // schedule) run on the solve's own state and undone afterwards: the solve's device block
+    // is copied aside first and copied back after every option, with the host-side buffer
+    // parities, so the measurement leaves no trace.  The RHS pass alone misjudged the
+    // overlapped closed box by about 10 % in both directions (the ghost launches beside the
+    // interior tiles, the split shape's solve kernel after the join, the update and scatter
+    // the RHS pass leaves out).  Without device memory for the copy, the pass is the RHS
+    // over every tile (then the split shape's solve kernel), which writes only the RHS.
+    const int sb0 = h->sb, lb0 = h->lb;
+    const size_t block_bytes = (size_t)h->alloc_bytes;
+    void* saved = nullptr;
+    const bool by_steps = cudaMalloc(&saved, block_bytes) == cudaSuccess;
+    if (!by_steps) cudaGetLastError();   // no room: clear the error, time RHS passes
+    if (by_steps)
+        CUDA_TRY(h, cudaMemcpyAsync(saved, h->block, block_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    auto pass = [&]() {
+        if (!by_steps) launch_stage_any(h, S);
+        else if (h->overlap) enq_step_overlap(h);
+        else enq_step(h);
+    };
+    auto restore = [&]() -> cudaError_t {
+        h->sb = sb0;
+        h->lb = lb0;
+        return by_steps ? cudaMemcpyAsync(h->block, saved, block_bytes, cudaMemcpyDeviceToDevice, h->stream)
+                        : cudaSuccess;
+    };
     const int nlanes = h->lanes_auto ? 2 : 1;
     const int lane_opts[2] = {h->G, 2};
     // option t: fused at budget t (t < levels), split at budget t - levels
@@ -532,7 +602,7 @@ int autotune(lssph_handle* h) {
     // Every option is timed in each of several interleaved rounds and keeps its fastest
     // round, so that a clock ramp or a neighbour's burst during one round does not decide
     // the pick (a single round swung the choice by about 10 % between machines).
-    constexpr int kRounds = 5;
+    const int kRounds = by_steps ? 3 : 5;
     for (int round = 0; round < kRounds; ++round) {
         for (int g = 0; g < nlanes; ++g) {
             h->G = lane_opts[g];
@@ -541,29 +611,33 @@ int autotune(lssph_handle* h) {
                 if (!h->split && !try_fused) continue;
                 h->budget = h->split ? t - levels : t;
                 h->tight = h->budget >= 1;
-                launch_stage_any(h, S);   // warm-up (instruction cache, L2)
+                pass();   // warm-up (instruction cache, L2)
                 CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
-                for (int r = 0; r < 3; ++r) launch_stage_any(h, S);
+                for (int r = 0; r < 3; ++r) pass();
                 CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
                 CUDA_TRY(h, cudaEventSynchronize(h->ev1));
                 float ms = 0.f;
                 CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
                 us[g][t] = std::min(us[g][t], 1e3 * ms / 3.0);
+                CUDA_TRY(h, restore());
             }
         }
     }
     int best_t[2] = {0, 0};
     for (int g = 0; g < nlanes; ++g) {
-        // In the overlapped step the interior tiles share the SMs with the ghost launch: four
-        // CTAs per SM (the tight budget) leave room for it where three do not, which an RHS
-        // pass alone does not show, so the overlapped step takes the tight budget or tighter.
+        // In the overlapped step the interior tiles share the SMs with the ghost launch: the
+        // fused kernels at four CTAs per SM (the tight budget) leave room for it where three
+        // do not, so the overlapped step's fused kernels take the tight budget (the split
+        // shape's pair kernels fit more CTAs per SM at any level).
         best_t[g] = try_fused ? (h->overlap ? 1 : 0) : levels + 1;
         for (int t = 0; t < nopt; ++t) {
-            const int level = t >= levels ? t - levels : t;
-            if (h->overlap && level < 1) continue;
             if (h->overlap && t < levels && t != 1) continue;
             if (us[g][t] < us[g][best_t[g]]) best_t[g] = t;
         }
+    }
+    if (by_steps) {
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        CUDA_TRY(h, cudaFree(saved));
     }
     const int pick = (nlanes == 2 && us[1][best_t[1]] < 0.95 * us[0][best_t[0]]) ? 1 : 0;
     h->G = lane_opts[pick];
@@ -572,7 +646,12 @@ int autotune(lssph_handle* h) {
     h->budget = h->split ? best_t[pick] - levels : best_t[pick];
     h->tight = h->budget >= 1;
     h->launch_counter = c0;
-    return sync_check(h);
+    const int rc = sync_check(h);
+    if (rc == LSSPH_OK) {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_picks.emplace(key, TunePick{h->G, h->budget, h->split, {h->tune_us[0], h->tune_us[1], h->tune_us[2]}});
+    }
+    return rc;
 }
 
 // The handle's own launches use the measured register budget; batches choose per group
@@ -994,9 +1073,8 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     h->n_wall = (int)t_wall.size();
     h->overlap = h->overlap_allowed && h->n_int > 0 && h->n_wall > 0 && !p.periodic;
     // lanes = 0: the first solo launch measures 2 and 4 lanes (q = 5 LS in FP64 or mixed
-    // precision, no overlapped ghost schedule) and keeps the faster; the shared memory
-    // covers both
-    h->lanes_auto = h->p.lanes == 0 && !h->classical && h->order == 2 && !h->overlap;
+    // precision) and keeps the faster; the shared memory covers both
+    h->lanes_auto = h->p.lanes == 0 && !h->classical && h->order == 2;
     if (h->lanes_auto)
         h->smem_bytes = std::max(h->smem_bytes, h->mixed ? tile_smem_bytes_mx(h->grid.cap, 2, h->has_tem)
                                                          : tile_smem_bytes(h->grid.cap, 2, h->has_tem));

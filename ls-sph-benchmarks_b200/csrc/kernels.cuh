@@ -1819,10 +1819,14 @@ __device__ __forceinline__ void ghost_work(const Phys& P, const Fld& F, const Ls
 #pragma unroll
         for (int k = 0; k < Q; ++k) B[c][k] = 0.0;
     int cnt = 0;
-    if (WQ != 1) {
+    // the pair loop is compiled for the Wendland C2 kernel and for any type (as
+    // stage_pair_sums), so that the loop holds no branch on the kernel type
+    auto ls_pairs = [&](auto KTc) {
+        constexpr int KT = decltype(KTc)::value;
+        const int kt = KT ? KT : P.kt;
         cnt = tile_pairs<G>(T, SM, active, hc, lane, -1, my_x, my_y, P.h_eff_sq, [&](int k) {
             const double xji = SM.x[k] - my_x, yji = SM.y[k] - my_y;
-            const double Wv = dev_W(P.kt, sqrt(xji * xji + yji * yji), P.ih1, P.wnorm);
+            const double Wv = dev_W(kt, sqrt(xji * xji + yji * yji), P.ih1, P.wnorm);
             const double VW = SM.vol[k] * Wv;
             double a[Q];
             a[0] = 1.0;
@@ -1848,6 +1852,10 @@ __device__ __forceinline__ void ghost_work(const Phys& P, const Fld& F, const Ls
                 for (int jj = 0; jj <= ii; ++jj) Mu[UT(jj, ii)] = fma(VWa, a[jj], Mu[UT(jj, ii)]);
             }
         });
+    };
+    if constexpr (WQ != 1) {
+        if (P.kt == 3) ls_pairs(std::integral_constant<int, 3>{});
+        else ls_pairs(std::integral_constant<int, 0>{});
     }
     if (active && WQ == 1) {
         for_tile_candidates<G>(T, hc, lane, [&](int k) {

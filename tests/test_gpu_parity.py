@@ -273,14 +273,15 @@ def test_register_budgets_are_bit_identical(case, monkeypatch):
     monkeypatch.delenv("LSSPH_REGISTER_BUDGET")
     t = lssph.Simulation(p, *_perturbed(p, 0.1, 4)).tuning()
     assert t["rhs_us_loose"] > 0 and t["rhs_us_tight"] > 0
-    if t["ghost_overlap"]:   # interior tiles share the SMs with the ghost launch
+    if t["ghost_overlap"] and t["shape"] == "fused":   # the interior tiles share the SMs with the ghost launch
         assert t["register_budget"] == "tight"
 
 
 def test_overlapped_step_equals_serial_step(monkeypatch):
     # ghost launches beside the next stage's interior tiles change no result
     for case in ("taylor_green", "boussinesq", "diffusion"):
-        p = lssph.make_params(CASES[case](), NUM_X=96, NUM_Y=96)
+        # lanes fixed: the automatic count is measured on each schedule and may differ
+        p = lssph.make_params(CASES[case](), NUM_X=96, NUM_Y=96, lanes=4)
         out = {}
         for ov in ("0", "1"):
             monkeypatch.setenv("LSSPH_OVERLAP", ov)
