@@ -347,6 +347,7 @@ def bench_mixed(steps: int = 100, acc_steps: int = 500) -> dict:
         out[f"{name}_value"] = v
         out[f"{name}_lanes"] = lanes
         out[f"{name}_register_budget"] = sim.tuning()["register_budget"]
+        out[f"{name}_shape"] = sim.tuning()["shape"]
         sim.step(acc_steps - 5 - steps)
         states[name] = (sim.download(), sim.num_int)
         sim.close()
