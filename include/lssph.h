@@ -233,7 +233,8 @@ int lssph_read_data(const char* path, int32_t num_total, int32_t with_tem, int32
    particle, and the register budget of the stage/PST kernels: 0 loose, 1 tight (512 threads
    per SM), 2 (640 threads per SM, q = 5 LS only), and for the pair kernel of the split shape
    also 3 (768) and 4 (1024), with the measured time of the fused kernels at the loose and
-   tight budgets.  The measurement runs at the handle's first launch: whole time steps on
+   tight budgets (SPH_MODEL 4-6: of the thread- and warp-per-particle mappings, one of which
+   the measurement picks).  The measurement runs at the handle's first launch: whole time steps on
    the solve's own state, which is copied aside first and put back after each option (the
    RHS pass alone when the device has no room for the copy).  The lane count (lanes = 0),
    the shape and the budget are picked by it; the budget and shape never change a result. */
@@ -243,8 +244,10 @@ int lssph_get_tuning(const lssph_handle* h, int32_t* lanes, int32_t* tight, doub
    the reference): 1 split (a pair kernel over the cell tiles, FP64 or FP32, then an FP64
    solve-and-update kernel with one thread per particle), 0 fused (one kernel), as the
    handle's first-launch measurement picked it (LSSPH_KERNEL_SHAPE=fused|split fixes it).
-   Solves at 1 or 8 lanes and the other SPH models run fused.  Both shapes compute
-   identical results. */
+   Solves at 1 or 8 lanes and the classical models run fused.  For the higher-order models
+   (SPH_MODEL 4-6) the value is the mapping the measurement picked: 2 thread per particle
+   over a cell tile, 3 warp per particle (LSSPH_HI_KERNEL=thread|warp fixes it).  Every
+   shape and mapping computes identical results. */
 int lssph_get_kernel_shape(const lssph_handle* h, int32_t* split);
 
 /* Time-step schedule (no counterpart in the reference): cell tiles, the tiles whose halo

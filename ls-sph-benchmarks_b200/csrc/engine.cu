@@ -404,6 +404,12 @@ void prepare_kernels(lssph_handle* h) {
     launch_stage_any(h, S);
     launch_ghost(h);
     launch_pst_any(h, all_tiles(h));
+    if (h->order >= 3 && !h->hi_fixed) {   // the other mapping the measurement may pick
+        h->hi_thread = !h->hi_thread;
+        launch_stage_any(h, S);
+        launch_pst_any(h, all_tiles(h));
+        h->hi_thread = !h->hi_thread;
+    }
     if (split_capable(h)) {   // the split shape the measurement may pick
         launch_stage_pairs(h, S, all_tiles(h));
         launch_pst_pairs(h, all_tiles(h));
@@ -486,17 +492,17 @@ int sync_check(lssph_handle* h);
 
 // The autotuner's picks, once per process for each solve configuration: every handle of
 // the same configuration (problem, sizes, cell grid and tiles, model, kernel type, walls,
-// precision, schedule, lanes asked for, shape restriction) takes the first one's lanes,
+// precision, schedule, lanes asked for, shape or mapping restriction) takes the first one's lanes,
 // shape and budget.  So two handles of one solve (a solve alone and as a batch member, a
 // restart, serving requests of one size) sum in the same order, and a stream of requests
 // of one size is measured once.
 struct TuneKey {
-    int64_t v[20];
-    bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 20, o.v, o.v + 20); }
+    int64_t v[21];
+    bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 21, o.v, o.v + 21); }
 };
 struct TunePick {
     int G, budget;
-    bool split;
+    bool split, hi_thread;
     double us[3];
 };
 std::mutex g_tune_mu;
@@ -508,7 +514,8 @@ TuneKey tune_key(const lssph_handle* h, bool try_fused, bool try_split) {
     const lssph_params& p = h->p;
     return TuneKey{{dev, p.target_problem, h->num_int, h->num_ext, h->grid.nx, h->grid.ny, h->grid.cap, h->ntiles,
                     h->n_int, p.sph_model, p.kernel_type, p.wall_model, p.precision, p.rk, p.periodic, p.lanes,
-                    h->overlap ? 1 : 0, h->pdl ? 1 : 0, try_fused ? 1 : 0, try_split ? 1 : 0}};
+                    h->overlap ? 1 : 0, h->pdl ? 1 : 0, try_fused ? 1 : 0, try_split ? 1 : 0,
+                    h->hi_fixed ? (h->hi_thread ? 1 : 2) : 0}};
 }
 
 // Pick the lane count (lanes = 0), the kernel shape and the register budget of the stage
@@ -554,6 +561,7 @@ int autotune(lssph_handle* h) {
             const TunePick& k = it->second;
             h->G = k.G;
             h->split = k.split;
+            h->hi_thread = k.hi_thread;
             h->budget = k.budget;
             h->tight = k.budget >= 1;
             for (int t = 0; t < 3; ++t) h->tune_us[t] = k.us[t];
@@ -593,9 +601,13 @@ int autotune(lssph_handle* h) {
     };
     const int nlanes = h->lanes_auto ? 2 : 1;
     const int lane_opts[2] = {h->G, 2};
-    // option t: fused at budget t (t < levels), split at budget t - levels
+    // option t: fused at budget t (t < levels), split at budget t - levels.  The higher-
+    // order kernels (SPH_MODEL 4-6) have one register budget and two mappings instead:
+    // t = 0 thread per particle over a cell tile, t = 1 warp per particle.
+    const bool hi = h->order >= 3;
+    const bool hi_free = hi && !h->hi_fixed;
     constexpr int kOpts = 3 + 5;
-    const int nopt = levels + (try_split ? 5 : 0);
+    const int nopt = hi ? (hi_free ? 2 : 1) : levels + (try_split ? 5 : 0);
     double us[2][kOpts];
     for (auto& row : us)
         for (double& v : row) v = 1e30;
@@ -607,9 +619,15 @@ int autotune(lssph_handle* h) {
         for (int g = 0; g < nlanes; ++g) {
             h->G = lane_opts[g];
             for (int t = 0; t < nopt; ++t) {
-                h->split = t >= levels;
-                if (!h->split && !try_fused) continue;
-                h->budget = h->split ? t - levels : t;
+                if (hi) {
+                    if (hi_free) h->hi_thread = t == 0;
+                    h->split = false;
+                    h->budget = 0;
+                } else {
+                    h->split = t >= levels;
+                    if (!h->split && !try_fused) continue;
+                    h->budget = h->split ? t - levels : t;
+                }
                 h->tight = h->budget >= 1;
                 pass();   // warm-up (instruction cache, L2)
                 CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
@@ -629,9 +647,9 @@ int autotune(lssph_handle* h) {
         // fused kernels at four CTAs per SM (the tight budget) leave room for it where three
         // do not, so the overlapped step's fused kernels take the tight budget (the split
         // shape's pair kernels fit more CTAs per SM at any level).
-        best_t[g] = try_fused ? (h->overlap ? 1 : 0) : levels + 1;
+        best_t[g] = hi ? 0 : (try_fused ? (h->overlap ? 1 : 0) : levels + 1);
         for (int t = 0; t < nopt; ++t) {
-            if (h->overlap && t < levels && t != 1) continue;
+            if (!hi && h->overlap && t < levels && t != 1) continue;
             if (us[g][t] < us[g][best_t[g]]) best_t[g] = t;
         }
     }
@@ -642,14 +660,21 @@ int autotune(lssph_handle* h) {
     const int pick = (nlanes == 2 && us[1][best_t[1]] < 0.95 * us[0][best_t[0]]) ? 1 : 0;
     h->G = lane_opts[pick];
     for (int t = 0; t < 3; ++t) h->tune_us[t] = (t < levels && us[pick][t] < 1e29) ? us[pick][t] : 0.0;
-    h->split = best_t[pick] >= levels;
-    h->budget = h->split ? best_t[pick] - levels : best_t[pick];
+    if (hi) {
+        if (hi_free) h->hi_thread = best_t[pick] == 0;
+        h->split = false;
+        h->budget = 0;
+    } else {
+        h->split = best_t[pick] >= levels;
+        h->budget = h->split ? best_t[pick] - levels : best_t[pick];
+    }
     h->tight = h->budget >= 1;
     h->launch_counter = c0;
     const int rc = sync_check(h);
     if (rc == LSSPH_OK) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
-        g_tune_picks.emplace(key, TunePick{h->G, h->budget, h->split, {h->tune_us[0], h->tune_us[1], h->tune_us[2]}});
+        g_tune_picks.emplace(key, TunePick{h->G, h->budget, h->split, h->hi_thread,
+                                           {h->tune_us[0], h->tune_us[1], h->tune_us[2]}});
     }
     return rc;
 }
@@ -966,8 +991,11 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
         // box and periodic): thread per particle is faster for q = 9 (1.5-1.6x) and q = 14
         // (1.04-1.6x), warp per particle for q = 20 (1.7-1.8x), where the thread's shared-
         // memory slot leaves too few warps per SM.  LSSPH_HI_KERNEL=thread|warp overrides.
+        // That is the starting choice; the autotuner times both mappings on the solve itself
+        // at its first launch and keeps the faster (both give identical results).
         const char* v = std::getenv("LSSPH_HI_KERNEL");
         h->hi_thread = h->order <= 4;
+        h->hi_fixed = v && (std::strcmp(v, "warp") == 0 || std::strcmp(v, "thread") == 0);
         if (v && std::strcmp(v, "warp") == 0) h->hi_thread = false;
         if (v && std::strcmp(v, "thread") == 0) h->hi_thread = true;
     }
@@ -1548,7 +1576,7 @@ int lssph_get_kernel_shape(const lssph_handle* hc, int32_t* split) {
     if (!hc || !split) return fail(nullptr, LSSPH_E_BAD_PARAM, "null argument");
     lssph_handle* h = const_cast<lssph_handle*>(hc);   // the measurement is a cache
     if (const int rc = ensure_tuned(h)) return rc;
-    *split = h->split ? 1 : 0;
+    *split = h->order >= 3 ? (h->hi_thread ? 2 : 3) : (h->split ? 1 : 0);
     return LSSPH_OK;
 }
 

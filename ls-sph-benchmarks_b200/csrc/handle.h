@@ -31,6 +31,7 @@ struct lssph_handle {
     bool classical = false;             // SPH_MODEL 1 / 2: kernel-gradient sums, q = 2 PST basis
     int order = 2;                      // Taylor order k of the LS basis (SPH_MODEL 3: 2; 4 / 5 / 6: 3 / 4 / 5)
     bool hi_thread = false;             // order >= 3: thread per particle (else warp per particle)
+    bool hi_fixed = false;              // the mapping is fixed by LSSPH_HI_KERNEL (else autotuned)
     bool pdl = true;                    // programmatic dependent launches in the time step
     bool tuned = false;                 // register budget measured (first solo launch)
     bool lanes_auto = false;            // lanes = 0 on an FP64 q = 5 LS solve: 2 or 4 by measurement

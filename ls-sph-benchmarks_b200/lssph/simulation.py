@@ -270,7 +270,7 @@ class Simulation:
         shape = C.c_int32()
         self._chk(self._lib.lssph_get_kernel_shape(self._h, C.byref(shape)))
         return {"lanes": lanes.value, "register_budget": ("loose", "tight", "five", "six", "eight")[tight.value],
-                "shape": "split" if shape.value else "fused",
+                "shape": ("fused", "split", "thread", "warp")[shape.value],
                 "rhs_us_loose": lo.value, "rhs_us_tight": ti.value, "tiles": nt.value,
                 "interior_tiles": ni.value, "ghost_overlap": bool(ov.value)}
 

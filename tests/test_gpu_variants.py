@@ -182,18 +182,24 @@ def test_high_order_steps_rel_l2(variant):
     sim.close()
 
 
-@pytest.mark.parametrize("shape", ["thread", "warp"])
+@pytest.mark.parametrize("shape", ["thread", "warp", "measured"])
 @pytest.mark.parametrize("variant", [("cavity", {"SPH_MODEL": 4}), ("boussinesq", {"SPH_MODEL": 5}),
                                      ("taylor_green", {"SPH_MODEL": 6, "KERNEL_TYPE": 2})], ids=_ids)
 def test_high_order_kernel_shapes_bit_exact(variant, shape, monkeypatch):
-    # both kernel shapes (thread per particle, warp per particle) run the oracle's
-    # operation sequence; the engine picks one per order, LSSPH_HI_KERNEL forces either
-    monkeypatch.setenv("LSSPH_HI_KERNEL", shape)
+    # both kernel mappings (thread per particle, warp per particle) run the oracle's
+    # operation sequence; the autotuner times both on the solve's first launch and keeps the
+    # faster, LSSPH_HI_KERNEL forces either
+    if shape == "measured":
+        monkeypatch.delenv("LSSPH_HI_KERNEL", raising=False)
+    else:
+        monkeypatch.setenv("LSSPH_HI_KERNEL", shape)
     case, kw = variant
     p = BASE[case](**kw)
     sim, orc = _pair(p, lanes=1, amp=0.1, seed=10)
     sim.step(4)
     orc.run(4)
+    picked = sim.tuning()["shape"]
+    assert picked == shape if shape != "measured" else picked in ("thread", "warp")
     g, o = sim.download(), orc.get()
     for k in FIELDS + (("tem",) if p.target_problem == 4 else ()):
         assert np.array_equal(getattr(g, k), o[k]), k
