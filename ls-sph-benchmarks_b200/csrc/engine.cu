@@ -593,6 +593,14 @@ int autotune(lssph_handle* h) {
         else if (h->overlap) enq_step_overlap(h);
         else enq_step(h);
     };
+    // A solve that a step budget or the steady state has stopped would time no-op steps:
+    // the measured steps run with both lifted (the copy puts them back).
+    auto lift_stops = [&]() -> cudaError_t {
+        if (!by_steps) return cudaSuccess;
+        cudaError_t e = cudaMemsetAsync(&h->sc->steady, 0, sizeof(int), h->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(&h->sc->step_limit, 0, 2 * sizeof(int), h->stream);
+        return e;
+    };
     auto restore = [&]() -> cudaError_t {
         h->sb = sb0;
         h->lb = lb0;
@@ -629,6 +637,7 @@ int autotune(lssph_handle* h) {
                     h->budget = h->split ? t - levels : t;
                 }
                 h->tight = h->budget >= 1;
+                CUDA_TRY(h, lift_stops());
                 pass();   // warm-up (instruction cache, L2)
                 CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
                 for (int r = 0; r < 3; ++r) pass();

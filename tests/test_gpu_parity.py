@@ -367,3 +367,33 @@ def test_fp64_split_batch_members_identical_alone(monkeypatch):
             assert np.array_equal(getattr(gs, k), getattr(gm, k)), k
         s.close()
         m.close()
+
+
+# ---- the autotuner's measurement leaves no trace -------------------------------------------
+@pytest.mark.parametrize("case", ["periodic", "cavity"])
+def test_measurement_leaves_no_trace(case, monkeypatch):
+    # the first launch times whole steps of every option on the solve's own state and puts
+    # the state back (step budget and step count included); a budget of 3 set before that
+    # launch still stops the solve after exactly 3 steps, at the state that a run with the
+    # picked configuration fixed (no measurement) reaches
+    monkeypatch.delenv("LSSPH_KERNEL_SHAPE", raising=False)
+    monkeypatch.delenv("LSSPH_REGISTER_BUDGET", raising=False)
+    base = (lssph.taylor_green_params(num=48, PERIODIC=1, coe_cfl=0.1) if case == "periodic"
+            else lssph.cavity_params(num=48))
+    st, ni = _perturbed(base, 0.1, 21)
+    a = lssph.Simulation(base, st, ni)
+    a.ghost()
+    a.set_step_budget(3)
+    a.step(10)
+    assert a.progress() == (3, "budget")
+    t = a.tuning()
+    monkeypatch.setenv("LSSPH_KERNEL_SHAPE", t["shape"])
+    monkeypatch.setenv("LSSPH_REGISTER_BUDGET", t["register_budget"])
+    b = lssph.Simulation(lssph.make_params(base, lanes=t["lanes"]), st, ni)
+    b.ghost()
+    b.step(3)
+    ga, gb = a.download(), b.download()
+    for k in FIELDS:
+        assert np.array_equal(getattr(ga, k), getattr(gb, k)), (k, t)
+    a.close()
+    b.close()
