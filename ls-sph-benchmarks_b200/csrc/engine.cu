@@ -586,6 +586,12 @@ int autotune(lssph_handle* h) {
     void* saved = nullptr;
     const bool by_steps = cudaMalloc(&saved, block_bytes) == cudaSuccess;
     if (!by_steps) cudaGetLastError();   // no room: clear the error, time RHS passes
+    struct FreeOnExit {   // an error return below still releases the copy
+        void*& p;
+        ~FreeOnExit() {
+            if (p) cudaFree(p);
+        }
+    } free_on_exit{saved};
     if (by_steps)
         CUDA_TRY(h, cudaMemcpyAsync(saved, h->block, block_bytes, cudaMemcpyDeviceToDevice, h->stream));
     auto pass = [&]() {
@@ -664,7 +670,9 @@ int autotune(lssph_handle* h) {
     }
     if (by_steps) {
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-        CUDA_TRY(h, cudaFree(saved));
+        const cudaError_t e = cudaFree(saved);
+        saved = nullptr;
+        CUDA_TRY(h, e);
     }
     const int pick = (nlanes == 2 && us[1][best_t[1]] < 0.95 * us[0][best_t[0]]) ? 1 : 0;
     h->G = lane_opts[pick];
