@@ -45,8 +45,9 @@ extern "C" {
 
 /* ---- engine options (no counterpart in the reference) ----------------------------- */
 #define LSSPH_PRECISION_FP64   0     /* plain FP64 path (reference arithmetic) */
-#define LSSPH_PRECISION_MIXED  1     /* FP32 pair sums, FP64 solve + refinement */
-#define LSSPH_PRECISION_MIXED_COMPENSATED 2  /* as MIXED, with Kahan-compensated FP32 pair sums */
+#define LSSPH_PRECISION_MIXED  1     /* FP32 pair sums, FP64 solve */
+#define LSSPH_PRECISION_MIXED_COMPENSATED 2  /* as MIXED, with Kahan-compensated FP32 pair sums
+                                                and one refinement step of the FP64 solve */
 
 /*
  * lssph_params -- mirrors Param_type (source/core/global_types.f90:22-73) plus the
@@ -87,10 +88,9 @@ typedef struct lssph_params {
     int32_t  precision;   /* LSSPH_PRECISION_* */
     int32_t  lanes;       /* lanes per particle in neighbour loops: 1 = reference
                              summation order (bit-exact vs the oracle); 2, 4, 8 (mixed
-                             precision 2, 4); 0 = auto: a q = 5 LS solve without the
-                             overlapped ghost schedule (periodic) times 2 and 4 at its
-                             first solo launch or batch join and keeps the faster unless
-                             4 is within 5 %, any other solve runs 4 */
+                             precision 2, 4); 0 = auto: a q = 5 LS solve times 2 and 4 at
+                             its first solo launch or batch join and keeps the faster
+                             unless 4 is within 5 %, any other solve runs 4 */
     uint64_t seed;        /* POS_PERT jitter seed (the reference seeds from the clock,
                              impose_initial_conditions_mod.f90:43-51) */
     int32_t  periodic;    /* 1: periodic square [0, LEN_X)^2 without walls (problems 1, 2);

@@ -166,7 +166,7 @@ void launch_split(const BatchGroup& g, const StageCfg& S, int ps, int pl, bool p
         const size_t smem = MX == 0 ? tile_smem_bytes_fpp(g.cap_max, G, TEM) : tile_smem_bytes_mxp(g.cap_max, G, TEM);
         launch_kernel(g.pdl, kern_at(g.split_budget), g.ntiles, PPB * G, smem, g.stream, g.D,
                       BatchMap{g.tiles, g.tstep, g.sbf, g.lba}, ps, pl);
-        launch_kernel(g.pdl, kb_solve<NB, PST, (MX != 0)>, g.nblocks, 128, 0, g.stream, g.D,
+        launch_kernel(g.pdl, kb_solve<NB, PST, (MX == 2)>, g.nblocks, 128, 0, g.stream, g.D,
                       BatchMap{g.blocks, g.tstep, g.sbf, g.lba}, S, ps, pl);
         *count += 2;
     };

@@ -1388,6 +1388,33 @@ __device__ __forceinline__ void stage_body_fp64(const Phys& P, const Fld& cur, c
 }
 
 
+// FP64 LS solve of one particle's sums row in place, as the fused FP64 kernels solve it
+// (DGESV, LSSPH_A_mod.f90:203-241, no refinement); the solution replaces the b sums, scaled
+// by the basis factors when SCALE; cnt < Q leaves zeros.
+template <int Q, int NB, bool SCALE>
+__device__ __forceinline__ void solve_row_plain(const Phys& P, double* row, int cnt, Scalars* sc) {
+    if (cnt >= Q) {
+        double A[Q][Q];
+        double B[NB][Q];
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+#pragma unroll
+            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? row[UT(r, c)] : row[UT(c, r)];
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) B[c][k] = row[15 + 5 * c + k];
+        if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+#pragma unroll
+            for (int k = 0; k < Q; ++k) row[15 + 5 * c + k] = SCALE ? B[c][k] * (k < 2 ? P.ih1 : P.ih2A) : B[c][k];
+    } else {
+#pragma unroll
+        for (int k = 15; k < 15 + 5 * NB; ++k) row[k] = 0.0;
+    }
+}
+
 // ---- mixed precision: LS solve of one particle's sums row in place ----------------------
 // FP64 LU of the moment matrix (packed upper triangle at row[0..14]), then per right-hand
 // side the DGESV substitutions plus one refinement step; the solution replaces the b sums
@@ -1513,7 +1540,8 @@ __device__ __forceinline__ int mx_pair_sums(const Phys& P, const TileHdr& T, con
 }
 
 // Mixed-precision stage: FP32 staging and pair phase (offsets from FP64 cell origins and
-// field references), lanes combined in FP64, FP64 solve with refinement, FP64 update.
+// field references), lanes combined in FP64, FP64 solve (COMP: compensated lane sums and one
+// refinement step of the solve), FP64 update.
 template <int NB, int G, bool COMP>
 __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
                                               const Lst& Ln, const int* __restrict__ gstart,
@@ -1574,7 +1602,8 @@ __device__ __forceinline__ void stage_body_mx(const Phys& P, const Fld& cur, con
             double my_v = 0, my_rho = 0, my_tem = 0;
             if constexpr (NB >= 4) { my_v = cur.v[i]; my_rho = cur.rho[i]; }
             if constexpr (NB == 5) my_tem = cur.tem[i];
-            solve_row_refined<Q, NB, true>(P, sm, (int)sm[SR - 1], sc);
+            if constexpr (COMP) solve_row_refined<Q, NB, true>(P, sm, (int)sm[SR - 1], sc);
+            else solve_row_plain<Q, NB, true>(P, sm, (int)sm[SR - 1], sc);
             double d[NB][Q];
 #pragma unroll
             for (int c = 0; c < NB; ++c)
@@ -2176,7 +2205,8 @@ __device__ __forceinline__ void pst_body_fp64(const Phys& P, const Fld& cur, con
 }
 
 
-// Mixed-precision PST: FP32 staging and pair phase, FP64 solve with refinement and update.
+// Mixed-precision PST: FP32 staging and pair phase, FP64 solve (COMP: compensated sums and
+// one refinement step) and update.
 template <int NB, int G, bool COMP>
 __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Lc,
                                             const Lst& Ln, const int* __restrict__ gstart,
@@ -2237,7 +2267,8 @@ __device__ __forceinline__ void pst_body_mx(const Phys& P, const Fld& cur, const
                 dx = ((0.2 * P.h) * dx) / rr;
                 dy = ((0.2 * P.h) * dy) / rr;
             }
-            solve_row_refined<Q, NB, false>(P, sm, (int)sm[SR - 1], sc);
+            if constexpr (COMP) solve_row_refined<Q, NB, false>(P, sm, (int)sm[SR - 1], sc);
+            else solve_row_plain<Q, NB, false>(P, sm, (int)sm[SR - 1], sc);
             // interpolation a(dr) . d (shift_interpolate_mod.f90:255-298)
             double a[Q];
             basis_A(P, dx, dy, a);
@@ -2298,9 +2329,9 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
 // at a barrier while one solves.  The split shape runs
 //   k_stage_mxp / k_pst_mxp   tile staging + FP32 pair phase; each particle's reduced sums
 //                             go to Work::sums (no solve, no barrier after the staging)
-//   k_stage_solve / k_pst_solve   one thread per interior particle: FP64 factorisation with
-//                             refinement, RHS, RK update, cell key and scatter (PST: shift,
-//                             interpolation, move)
+//   k_stage_solve / k_pst_solve   one thread per interior particle: FP64 factorisation (the
+//                             compensated mode: plus one refinement step), RHS, RK update,
+//                             cell key and scatter (PST: shift, interpolation, move)
 // with the same arithmetic per particle as the fused kernels, so both shapes give identical
 // bits and the autotuner may pick either.
 // =======================================================================================
@@ -2368,37 +2399,10 @@ __global__ void __launch_bounds__(PPB * G, tile_min_blocks(G, TIGHT))
     pairs_mx<NB, G, COMP, true>(P, cur, Lc, gstart, glist, W, sc, ntx, tiles ? tiles[blockIdx.x] : (int)blockIdx.x);
 }
 
-// FP64 LS solve of one particle's sums row in place, as the fused FP64 kernels solve it
-// (DGESV, LSSPH_A_mod.f90:203-241, no refinement); the solution replaces the b sums, scaled
-// by the basis factors when SCALE; cnt < Q leaves zeros.
-template <int Q, int NB, bool SCALE>
-__device__ __forceinline__ void solve_row_plain(const Phys& P, double* row, int cnt, Scalars* sc) {
-    if (cnt >= Q) {
-        double A[Q][Q];
-        double B[NB][Q];
-#pragma unroll
-        for (int r = 0; r < Q; ++r)
-#pragma unroll
-            for (int c = 0; c < Q; ++c) A[r][c] = (r <= c) ? row[UT(r, c)] : row[UT(c, r)];
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-#pragma unroll
-            for (int k = 0; k < Q; ++k) B[c][k] = row[15 + 5 * c + k];
-        if (!lu_solve<Q, NB>(A, B)) atomicOr(&sc->warn, WARN_SINGULAR);
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-#pragma unroll
-            for (int k = 0; k < Q; ++k) row[15 + 5 * c + k] = SCALE ? B[c][k] * (k < 2 ? P.ih1 : P.ih2A) : B[c][k];
-    } else {
-#pragma unroll
-        for (int k = 15; k < 15 + 5 * NB; ++k) row[k] = 0.0;
-    }
-}
-
 // Solve and update of the split shape, one thread per interior particle (the tail of the
-// fused stage kernels: FP64 factorisation, RHS, RK update, key, scatter).  REF: mixed
-// precision (factorisation with one refinement step, as stage_body_mx); else FP64 (as
-// stage_body_fp64).
+// fused stage kernels: FP64 factorisation, RHS, RK update, key, scatter).  REF: one
+// refinement step after the factorisation (the compensated mixed mode, as stage_body_mx with
+// COMP); else the DGESV sequence of stage_body_fp64 and of the plain mixed mode.
 template <int NB, bool REF>
 __device__ __forceinline__ void stage_solve_row(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
                                                const int* __restrict__ gstart, const Work& W, const StageCfg& S,
@@ -2443,7 +2447,8 @@ __global__ void __launch_bounds__(128) k_stage_solve(const Phys P, const Fld cur
 }
 
 // Shift, solve, interpolation and move of the split shape's PST, one thread per interior
-// particle (the tail of pst_body_mx, REF, or of pst_body_fp64).  NB = 3 (u, v, rho) or 4 (+ T).
+// particle (the tail of pst_body_mx or of pst_body_fp64; REF as stage_solve_row).  NB = 3
+// (u, v, rho) or 4 (+ T).
 template <int NB, bool REF>
 __device__ __forceinline__ void pst_solve_row(const Phys& P, const Fld& cur, const Fld& nxt, const Lst& Ln,
                                              const int* __restrict__ gstart, const Work& W, Scalars* sc, int i) {

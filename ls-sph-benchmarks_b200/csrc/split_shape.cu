@@ -120,7 +120,7 @@ void launch_stage_solve(lssph_handle* h, const StageCfg& S, cudaStream_t stream,
     auto go = [&](auto kern) {
         launch_kernel(pdl, kern, blocks, 128, 0, stream, h->P, cur, nxt, Ln, h->gstart, h->W, S, h->sc);
     };
-    if (h->mixed) {
+    if (h->comp) {   // the compensated mode's solve has one refinement step
         if (h->nb_rhs == 1) go(k_stage_solve<1, true>);
         else if (h->nb_rhs == 5) go(k_stage_solve<5, true>);
         else go(k_stage_solve<4, true>);
@@ -140,7 +140,7 @@ void launch_pst_solve(lssph_handle* h, cudaStream_t stream, bool pdl) {
     const Fld& nxt = h->F[h->sb ^ 1];
     const Lst& Ln = h->L[next_list(h->lb)];
     auto go = [&](auto kern) { launch_kernel(pdl, kern, blocks, 128, 0, stream, h->P, cur, nxt, Ln, h->gstart, h->W, h->sc); };
-    if (h->mixed) {
+    if (h->comp) {
         if (h->has_tem) go(k_pst_solve<4, true>);
         else go(k_pst_solve<3, true>);
     } else {

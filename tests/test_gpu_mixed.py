@@ -1,6 +1,7 @@
 """Mixed precision: FP32 kernel weights, basis and neighbour sums (over FP64-formed,
-FP32-rounded offsets and field differences), FP64 moment-matrix factorisation with one
-refinement step, FP64 RK update.
+FP32-rounded offsets and field differences), FP64 moment-matrix factorisation (the
+compensated mode: Kahan-compensated sums and one refinement step of the solve), FP64 RK
+update.
 
 Bound (stated): every field within relative L2 1e-5 of the FP64 path on the same inputs
 after the stated step count, and analytical-solution errors unchanged.  Needs a B200.
