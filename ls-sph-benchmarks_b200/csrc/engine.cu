@@ -554,8 +554,10 @@ int autotune(lssph_handle* h) {
         }
     }
     const TuneKey key = tune_key(h, try_fused, try_split);
+    // held for the whole measurement, so that a second handle of the same configuration
+    // (on another thread) waits and takes this pick instead of measuring its own
+    std::unique_lock<std::mutex> tune_lock(g_tune_mu);
     {
-        std::lock_guard<std::mutex> lock(g_tune_mu);
         const auto it = g_tune_picks.find(key);
         if (it != g_tune_picks.end()) {
             const TunePick& k = it->second;
@@ -688,11 +690,9 @@ int autotune(lssph_handle* h) {
     h->tight = h->budget >= 1;
     h->launch_counter = c0;
     const int rc = sync_check(h);
-    if (rc == LSSPH_OK) {
-        std::lock_guard<std::mutex> lock(g_tune_mu);
+    if (rc == LSSPH_OK)
         g_tune_picks.emplace(key, TunePick{h->G, h->budget, h->split, h->hi_thread,
                                            {h->tune_us[0], h->tune_us[1], h->tune_us[2]}});
-    }
     return rc;
 }
 
