@@ -109,9 +109,6 @@ class Server:
         self.batch = Batch()
         self.waiting: deque[Request] = deque()
         self.active: list[tuple[Request, Simulation]] = []
-        # members that finished in the last batch call: out of the batch, their results are
-        # downloaded and their device memory freed while the next call runs
-        self.retiring: list[tuple[Request, Simulation]] = []
         self.done: list[Request] = []
         self.used = 0
         self.peak_used = 0
@@ -211,25 +208,10 @@ class Server:
         return sim
 
     # ---- one batch call ---------------------------------------------------------------
-    def _finish_retired(self) -> None:
-        """Download the results of the members retired by the last batch call and free their
-        device memory (freeing waits for the device, so this runs after the set-up work)."""
-        t0 = self.clock()
-        for req, sim in self.retiring:
-            if self.keep_results and req.status == _abi.OK:
-                req.result = sim.download()
-            sim.close()
-            self.used -= req.footprint
-            req.finished = self.now()
-            self.done.append(req)
-        self.retiring = []
-        self.host_retire_s += self.clock() - t0
-
     def step_once(self) -> int:
-        """One batch call of up to chunk_steps steps.  While the GPU steps the current
-        members, requests admitted now are set up on the host and copied to the device (they
-        join the batch for the next call), and the members the last call retired are
-        downloaded and freed.  Returns the number of members this call retired."""
+        """One batch call of up to chunk_steps steps.  Requests admitted now are set up on
+        the host and copied to the device while the GPU steps the current members; they
+        join the batch for the next call.  Returns the number of members retired."""
         picked = self._pick()
         launched = bool(self.active)
         t0 = self.clock()
@@ -238,8 +220,6 @@ class Server:
         created = [(req, self._create(req)) for req in picked]     # overlaps the batch call
         t1 = self.clock()
         self.host_create_s += t1 - t0
-        self._finish_retired()                                      # overlaps it too
-        t1 = self.clock()
         retired = []
         if launched:
             status, steady, steps = self.batch.wait(raise_on_error=False)
@@ -261,8 +241,13 @@ class Server:
                     retired.append(i)
             for i in reversed(retired):
                 req, sim = self.active.pop(i)
+                if self.keep_results and req.status == _abi.OK:
+                    req.result = sim.download()
                 self.batch.remove(sim)
-                self.retiring.append((req, sim))
+                sim.close()
+                self.used -= req.footprint
+                req.finished = self.now()
+                self.done.append(req)
             self.host_retire_s += self.clock() - t2
         for req, sim in created:
             self.batch.add(sim)
@@ -284,7 +269,6 @@ class Server:
                     r.arrival = 0.0
                 self.submit(r)
             if not self.active and pending and not any(r.arrival <= self.now() for r in self.waiting):
-                self._finish_retired()      # nothing to overlap with: finish them now
                 time.sleep(max(0.0, min(pending[0].arrival - self.now(), 0.05)))
                 continue
             self.queue_samples.append(len(self.waiting))
@@ -307,7 +291,6 @@ class Server:
                            latencies_s=lat)
 
     def close(self) -> None:
-        self._finish_retired()
         for _, sim in self.active:
             sim.close()
         self.active = []
