@@ -735,6 +735,7 @@ def _serving_record(st, reqs, scale) -> dict:
             "makespan_s": st.makespan_s, "max_active": st.max_active, "batch_calls": st.batch_calls,
             "max_queue": st.max_queue, "mean_queue": st.mean_queue,
             "host_setup_s": st.host_create_s, "host_wait_s": st.wait_s, "host_retire_s": st.host_retire_s,
+            "host_launch_s": st.host_launch_s, "host_join_s": st.host_join_s,
             "admission": "first fit by exact device footprint within 80% of free HBM, 64 slots"}
 
 

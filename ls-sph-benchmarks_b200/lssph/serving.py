@@ -85,6 +85,8 @@ class ServerStats:
     host_create_s: float = 0.0
     wait_s: float = 0.0
     host_retire_s: float = 0.0
+    host_launch_s: float = 0.0
+    host_join_s: float = 0.0
     max_queue: int = 0               # most requests waiting for admission at one scheduling point
     mean_queue: float = 0.0          # waiting requests averaged over scheduling points
     preemptions: int = 0             # active solves suspended for higher-priority requests
@@ -116,7 +118,9 @@ class Server:
         self.device_ms = 0.0
         self.host_create_s = 0.0     # setting up admitted solves (overlaps batch calls)
         self.wait_s = 0.0            # waiting for batch calls after the set-up work
-        self.host_retire_s = 0.0     # downloading results, freeing solves
+        self.host_retire_s = 0.0     # bookkeeping after each call, downloading results, freeing solves
+        self.host_launch_s = 0.0     # starting batch calls (a changed membership re-captures the graph)
+        self.host_join_s = 0.0       # adding set-up solves to the batch (first of a configuration: measured)
         self.batch_calls = 0
         self.queue_samples: list[int] = []
         self.peak_active = 0
@@ -217,9 +221,11 @@ class Server:
         t0 = self.clock()
         if launched:
             self.batch.launch(self.chunk_steps)
+        tl = self.clock()
+        self.host_launch_s += tl - t0
         created = [(req, self._create(req)) for req in picked]     # overlaps the batch call
         t1 = self.clock()
-        self.host_create_s += t1 - t0
+        self.host_create_s += t1 - tl
         retired = []
         if launched:
             status, steady, steps = self.batch.wait(raise_on_error=False)
@@ -249,9 +255,11 @@ class Server:
                 req.finished = self.now()
                 self.done.append(req)
             self.host_retire_s += self.clock() - t2
+        tj = self.clock()
         for req, sim in created:
             self.batch.add(sim)
             self.active.append((req, sim))
+        self.host_join_s += self.clock() - tj
         self.peak_active = max(self.peak_active, len(self.active))
         return len(retired)
 
@@ -285,6 +293,7 @@ class Server:
                            particle_updates_per_s=self.particle_steps / span if span > 0 else math.nan,
                            device_ms=self.device_ms, max_active=self.peak_active, batch_calls=self.batch_calls,
                            host_create_s=self.host_create_s, wait_s=self.wait_s, host_retire_s=self.host_retire_s,
+                           host_launch_s=self.host_launch_s, host_join_s=self.host_join_s,
                            max_queue=max(self.queue_samples, default=0),
                            mean_queue=float(np.mean(self.queue_samples)) if self.queue_samples else 0.0,
                            preemptions=self.preemptions,
