@@ -943,6 +943,28 @@ int upload_fields(lssph_handle* h, const double* x, const double* y, const doubl
     return LSSPH_OK;
 }
 
+// Solve blocks come from the device's default stream-ordered memory pool, which keeps freed
+// blocks for reuse (release threshold at its maximum): a destroy then frees with
+// cudaFreeAsync on the solve's own stream instead of cudaFree, which synchronised the whole
+// device and now and then took a good fraction of a second in a serving loop that creates
+// and destroys solves while batch calls run.  lssph_mem_info trims the pool first, so the
+// free memory it reports still counts freed blocks as free.
+cudaError_t pool_for_blocks(cudaMemPool_t* pool) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceGetDefaultMemPool(pool, dev)) != cudaSuccess) return e;
+    static std::mutex mu;
+    static bool configured[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        uint64_t keep = UINT64_MAX;
+        if ((e = cudaMemPoolSetAttribute(*pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    return cudaSuccess;
+}
+
 void free_handle(lssph_handle* h) {
     if (!h) return;
     if (h->batch) batch_forget(h->batch, h);
@@ -952,7 +974,10 @@ void free_handle(lssph_handle* h) {
     for (auto& row : h->graph)
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);
-    if (h->block) cudaFree(h->block);
+    if (h->block) {
+        cudaFreeAsync(h->block, h->stream);
+        cudaStreamSynchronize(h->stream);
+    }
     return_pinned_slot(h->sc_host);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1128,15 +1153,22 @@ int create_impl(const lssph_params* pin, int num_total, int num_int, const int32
     if (h->lanes_auto)
         h->smem_bytes = std::max(h->smem_bytes, h->mixed ? tile_smem_bytes_mx(h->grid.cap, 2, h->has_tem)
                                                          : tile_smem_bytes(h->grid.cap, 2, h->has_tem));
-    // one device block for every array of the solve (one cudaMalloc, one cudaFree)
+    // one device block for every array of the solve (one allocation from the stream-ordered
+    // pool on the solve's stream, freed the same way)
     const size_t block = (size_t)solve_bytes(N, NI, NE, NC, h->grid.cap, h->nvt, h->ntiles, h->has_sums);
     {
         // pinned scalar copy target (optional: without it the checks copy through pageable memory)
         h->sc_host = pinned_slot();
-        const cudaError_t e = cudaMalloc(&h->block, block);
+        cudaMemPool_t pool;
+        cudaError_t e = pool_for_blocks(&pool);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&h->block, block, pool, h->stream);
+        // a pooled block may hold an earlier solve's data: every array starts at zero (the
+        // arrays a problem never writes, e.g. the v and rho RHS of problem 1, read as zeros)
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->block, 0, block, h->stream);
         if (e != cudaSuccess) {
+            h->block = nullptr;
             free_handle(h);
-            return fail(nullptr, LSSPH_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            return fail(nullptr, LSSPH_E_CUDA, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
         }
         h->alloc_bytes = (int64_t)block;
         size_t off = 0;
@@ -1333,6 +1365,9 @@ int lssph_step(lssph_handle* h, int32_t nsteps, int32_t* steady_step_out) {
 
 int lssph_mem_info(int64_t* free_bytes, int64_t* total_bytes) {
     size_t f = 0, t = 0;
+    cudaMemPool_t pool;
+    if (pool_for_blocks(&pool) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);   // freed blocks count as free
+    cudaGetLastError();
     const cudaError_t err = cudaMemGetInfo(&f, &t);
     if (err != cudaSuccess) return fail(nullptr, LSSPH_E_CUDA, std::string("cudaMemGetInfo: ") + cudaGetErrorString(err));
     if (free_bytes) *free_bytes = (int64_t)f;
